@@ -1,0 +1,273 @@
+/*
+ * vlasov_b200.h -- C ABI of the B200 (sm_100a) library that serves the
+ * per-step pseudo-particle loop of LaurentPlagne/Vlasov.jl.
+ *
+ * The entry points are the calls the reference's host makes on its device
+ * accelerator (src/accelerator.jl, src/devicemesh.jl, src/simulation.jl),
+ * flattened to plain pointers and sizes.  Each declaration names the
+ * reference interface it replaces.
+ *
+ * Conventions
+ *   - Every function returns an int: 0 on success, a negative VLB_ERR_* code
+ *     otherwise; vlb_last_error() gives a message (thread-local).  Nothing
+ *     throws or aborts across this boundary.
+ *   - The library owns every device allocation (the opaque vlb_ctx); the
+ *     caller owns every host pointer it passes, and each call copies.
+ *   - All work of a context runs on one library-owned CUDA stream.  Calls that
+ *     return host values synchronise that stream; the others are ordered on
+ *     it.  A context is not re-entrant; separate contexts are independent.
+ *   - Particles are held as the reference's packed form (PackedParticle,
+ *     src/particles.jl:86-91): per axis the 1-based nearest fine knot `k`
+ *     (int32, unclamped) and the offset `delta` from it (float32), for the
+ *     current and the previous position.  Host arrays are structure-of-arrays
+ *     of length 3*npart: all x, then all y, then all z.
+ *   - Cells are 0-based: cell = (kx-1) + nk*((ky-1) + nk*(kz-1)) with each k
+ *     clamped to [1, nk] (src/kernels.jl:902-908 minus one).
+ *   - Grids are n^3 float32 arrays, i fastest (the reference's column-major
+ *     (i,j,k) layout).
+ */
+#ifndef VLASOV_B200_H
+#define VLASOV_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define VLB_API __attribute__((visibility("default")))
+#else
+#define VLB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VLB_OK 0
+#define VLB_ERR_ARG (-1)      /* bad size, null handle, non-uniform axis ... */
+#define VLB_ERR_CUDA (-2)     /* a CUDA call failed */
+#define VLB_ERR_STATE (-3)    /* call out of order (e.g. forces before a sort) */
+#define VLB_ERR_TIMEOUT (-4)  /* a bounded device wait gave up */
+#define VLB_ERR_NOMEM (-5)
+
+typedef struct vlb_ctx vlb_ctx;
+
+/* One cubic mesh level: the tables of SplineMesh (src/mesh.jl:327-382) that
+ * the step reads, in float64 (converted to float32 on upload, as DeviceMesh
+ * does, src/devicemesh.jl:49-81).  The three axes of a level are identical. */
+typedef struct vlb_level_desc {
+  int32_t nknots;              /* knots per axis; n = 2*nknots points per axis */
+  const double* knots;         /* [nknots] */
+  const double* colloc;        /* [n] collocation points */
+  const double* sinv;          /* [n*n] row-major S^-1 (src/collocation.jl:53) */
+  const double* laplacian;     /* [n*n] row-major D = S'' S^-1 (src/collocation.jl:94) */
+  const double* eigvec;        /* [(n-2)^2] row-major M of D[2:end-1,2:end-1] */
+  const double* eigvec_inv;    /* [(n-2)^2] row-major M^-1 */
+  const double* eigval;        /* [n-2] real eigenvalues */
+  const double* dual_moments;  /* [3*n] S^-T m_k, k = 0,1,2 (src/mesh.jl:367-368) */
+  const double* dual_lengths;  /* [n] (src/deposition.jl:23-33) */
+  double locate_x0;            /* LocateTable (src/splines.jl:362-376) */
+  double locate_invwidth;
+  int32_t locate_ncells;
+  const int32_t* locate_cells; /* [locate_ncells], 1-based cells */
+} vlb_level_desc;
+
+/* GaussianSmoothing tables (src/fields.jl:44-53), column-major: the values of
+ * one table column are contiguous. */
+typedef struct vlb_smoothing_desc {
+  int32_t nbdt;                /* columns - 1 (1000) */
+  double spacing;              /* fine step h */
+  const double* overlap;       /* [(nbdt+1)*10] */
+  const double* gradient;      /* [(nbdt+1)*10] */
+  const double* nodes;         /* [(nbdt+1)*8] */
+} vlb_smoothing_desc;
+
+typedef struct vlb_config {
+  int64_t npart;
+  double weight;               /* electrons carried by one pseudo-particle */
+  vlb_level_desc fine;         /* uniform axis */
+  vlb_level_desc coarse;       /* stretched axis */
+  vlb_smoothing_desc smoothing;
+  int32_t device;              /* CUDA device ordinal */
+  int32_t flags;               /* reserved, 0 */
+} vlb_config;
+
+/* Projectile state (src/projectile.jl:141-150).  `sigma` is the width of
+ * the Gaussian kernel the fused force path uses, scale(softening)
+ * (src/accelerator.jl:632); `ball_radius` the ball softening applied to
+ * out-of-stencil particles (src/accelerator.jl:719-723). */
+typedef struct vlb_projectile {
+  double position[3];
+  double previous[3];
+  double velocity[3];
+  double charge;
+  double mass;
+  double sigma;
+  double ball_radius;
+  int32_t active;              /* 0: isolated cluster, no projectile */
+  int32_t pad_;
+} vlb_projectile;
+
+/* Parameters of one fused step (step!(sim; energy=false), src/simulation.jl:382-416). */
+typedef struct vlb_step_params {
+  double dt;
+  double rcmax;                /* radius beyond which a particle counts as gone */
+  double jellium_nions;        /* Jellium (src/meanfield.jl:332-340) */
+  double jellium_radius;
+  double capture_radius;       /* q(<R) around the projectile after the step; <= 0 skips */
+  int32_t deposit_mode;        /* VLB_DEPOSIT_FLOAT32 or VLB_DEPOSIT_FIXED64 */
+  int32_t advance_projectile;  /* 0 during priming (src/simulation.jl:254) */
+  int32_t push;                /* 0: forces only, no Verlet (priming) */
+  int32_t use_graph;           /* 1: replay the step as one captured CUDA graph */
+} vlb_step_params;
+
+#define VLB_DEPOSIT_FLOAT32 0
+#define VLB_DEPOSIT_FIXED64 1   /* int64 fixed point, charge scaled by 2^40 */
+
+typedef struct vlb_step_result {
+  double kinetic;              /* step!(cloud, dt, acc) diagnostics */
+  double escaped;
+  double angular[3];
+  double projectile_force[3];  /* projectile_forces!(..., acc) */
+  double e_electrons;
+  double e_jellium;
+  double enclosed_charge;      /* q(<capture_radius) after the step */
+  double total_charge;         /* fine charge before renormalisation */
+  int32_t nout;                /* outside the fine deposit window */
+  int32_t outcount;            /* 10^3 stencil leaves the fine grid */
+  int32_t noccupied;           /* occupied fine cells */
+  int32_t status;              /* device-side error flags, 0 when clean */
+} vlb_step_result;
+
+/* Grid selectors for vlb_get_grid / vlb_set_grid. */
+#define VLB_GRID_RHO_FINE 0
+#define VLB_GRID_RHO_COARSE 1
+#define VLB_GRID_PHI_FINE 2
+#define VLB_GRID_PHI_COARSE 3
+#define VLB_GRID_CSOL_FINE 4
+#define VLB_GRID_CSOL_COARSE 5
+
+/* Precision of the Poisson mode products. */
+#define VLB_POISSON_FP32 0
+
+VLB_API const char* vlb_last_error(void);
+VLB_API const char* vlb_version(void);
+
+/* DeviceState(backend, E, meshes, sm, npart; packed=true)
+ * (src/simulation.jl:104-115) + DeviceAccelerator (src/accelerator.jl:281-331):
+ * uploads every table once and allocates the run's buffers. */
+VLB_API int vlb_create(const vlb_config* cfg, vlb_ctx** out);
+VLB_API int vlb_destroy(vlb_ctx* ctx);
+
+/* upload!(acc.particles) / download!(acc.particles, backend)
+ * (src/accelerator.jl:48-68).  SoA host arrays of 3*npart. */
+VLB_API int vlb_upload_particles(vlb_ctx* ctx, const int32_t* knode, const float* delta,
+                         const int32_t* pknode, const float* pdelta);
+VLB_API int vlb_download_particles(vlb_ctx* ctx, int32_t* knode, float* delta,
+                           int32_t* pknode, float* pdelta);
+
+/* _pack!(acc, ::PackedPositions) -> _sort_and_list! (src/accelerator.jl:360-387,
+ * 466-503): stable counting sort of the cloud by cell (the particles are
+ * moved), occupied-cell list, bounds, out-of-stencil list.  Returns the
+ * number of occupied cells and the out-of-stencil count. */
+VLB_API int vlb_sort(vlb_ctx* ctx, int32_t* noccupied, int32_t* outcount);
+
+/* The sort's products, for inspection: perm[s] = index before the sort of
+ * the particle now in slot s; occupied[g] (0-based cells, increasing);
+ * bounds[g] .. bounds[g+1] the slots of occupied cell g (bounds[0] = 0);
+ * outlist[t] increasing slots whose stencil leaves the fine grid.  Any
+ * pointer may be NULL.  Sizes: npart, noccupied, noccupied+1, outcount. */
+VLB_API int vlb_get_sort(vlb_ctx* ctx, int32_t* perm, int32_t* occupied, int32_t* bounds,
+                 int32_t* outlist);
+
+/* deposit_smoothed!(rho, acc, mesh, sm, positions; charge)
+ * (src/accelerator.jl:531-565): table columns, sorted 8^3 deposit, charge
+ * renormalisation.  Needs vlb_sort.  `mode` is VLB_DEPOSIT_*.  Returns nout
+ * and the charge before renormalisation. */
+VLB_API int vlb_deposit_fine(vlb_ctx* ctx, double charge, int32_t mode, int32_t* nout,
+                     double* total_charge);
+
+/* deposit_cic!(rho, dm, acc, npart, charge, x0f, hf) (src/devicemesh.jl:93-106) */
+VLB_API int vlb_deposit_coarse(vlb_ctx* ctx, double charge);
+
+/* poisson!(phis, rhos, dms) (src/devicemesh.jl:160-169): coarse multipole
+ * faces + solve, fine faces from the coarse spline + solve. */
+VLB_API int vlb_poisson(vlb_ctx* ctx, int32_t precision);
+
+/* spline_coefficients!(csol, phi, dm) (src/devicemesh.jl:126-127) into the
+ * level's csol grid.  level: 0 fine, 1 coarse. */
+VLB_API int vlb_coefficients(vlb_ctx* ctx, int32_t level);
+
+/* effective_potential!(csol, rho, dm, jel) (src/devicemesh.jl:171-183):
+ * csol += S^-1 [V_xc(rho) + V_jel(r)]. */
+VLB_API int vlb_mean_field(vlb_ctx* ctx, int32_t level, double nions, double radius);
+
+/* forces!(cloud, acc, fine, csolf, coarse, csolc, sm; projectile, packed=true)
+ * (src/accelerator.jl:607-733), with the out-of-stencil tail on the device.
+ * Uses the csol grids in place.  red[4] receives the projectile sums. */
+VLB_API int vlb_forces(vlb_ctx* ctx, const vlb_projectile* proj, double red[4], int32_t* outcount);
+
+/* projectile_forces!(cloud, acc, proj, jel) (src/accelerator.jl:746-756)
+ * from the sums of the last vlb_forces. */
+VLB_API int vlb_projectile_forces(vlb_ctx* ctx, const vlb_projectile* proj, double nions,
+                          double jellium_radius, double force[3], double* e_electrons,
+                          double* e_jellium);
+
+/* step!(cloud, dt, acc; rcmax) (src/accelerator.jl:580-605): packed Verlet.
+ * diag = kinetic, escaped, angular x, y, z. */
+VLB_API int vlb_push(vlb_ctx* ctx, double dt, double rcmax, double diag[5]);
+
+/* step!(sim; energy=false) on the resident path (src/simulation.jl:382-416,
+ * 472-531) fused into one stream of kernels with no host synchronisation
+ * inside; `proj` is read and updated (the projectile's Verlet step,
+ * src/projectile.jl:298-304). */
+VLB_API int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params,
+             vlb_step_result* result);
+
+/* sync_host! (src/simulation.jl:544-552) for one grid, and its inverse. */
+VLB_API int vlb_get_grid(vlb_ctx* ctx, int32_t which, float* host);
+VLB_API int vlb_set_grid(vlb_ctx* ctx, int32_t which, const float* host);
+
+/* The force buffer acc.force, SoA 3*npart, in slot order. */
+VLB_API int vlb_get_forces(vlb_ctx* ctx, float* host);
+VLB_API int vlb_set_forces(vlb_ctx* ctx, const float* host);
+
+/* enclosed_charge(cloud, proj, radius) (src/projectile.jl:243-247) on the
+ * device-resident cloud. */
+VLB_API int vlb_enclosed_charge(vlb_ctx* ctx, const double position[3], double radius, double* q);
+
+/* Accumulated device time per stage since the last reset (ms), measured
+ * with CUDA events when profiling is on; names via vlb_stage_name. */
+VLB_API int vlb_profile(vlb_ctx* ctx, int32_t enable);
+VLB_API int vlb_stage_count(void);
+VLB_API const char* vlb_stage_name(int32_t i);
+VLB_API int vlb_stage_times(vlb_ctx* ctx, double* ms, int32_t n);
+/* Kernel launches issued by this context so far. */
+VLB_API int vlb_launch_count(vlb_ctx* ctx, int64_t* count);
+/* The context's CUDA stream (cudaStream_t), for event timing by a caller. */
+VLB_API int vlb_stream(vlb_ctx* ctx, void** stream);
+
+/* ---- host-side set-up helpers (no GPU needed) ---- */
+
+/* sample_thomas_fermi(profile::RadialProfile, npart, weight; rng = Ran2(seed))
+ * (src/initial.jl:184-203) with the thesis's ran2 (src/random.jl:31-90;
+ * consistent != 0 restores IQ1 = 53668).  positions, momenta: AoS 3*npart. */
+VLB_API int vlb_sample_thomas_fermi(const double* quantiles, int32_t nq, const double* density,
+                            int32_t nrho, double rmax, int64_t npart, double weight,
+                            int32_t seed, int32_t consistent, double* positions,
+                            double* momenta);
+
+/* next!(Ran2(seed)) n times (src/random.jl:80-90). */
+VLB_API int vlb_ran2(int32_t seed, int32_t consistent, int64_t n, float* out);
+
+/* PackedPositions setindex! split (src/particles.jl:135-149): positions AoS
+ * 3*npart -> knode, delta SoA 3*npart; and the inverse getindex
+ * (src/particles.jl:128-132). */
+VLB_API int vlb_pack_positions(int64_t npart, const double* positions, double x0, double h,
+                       int32_t* knode, float* delta);
+VLB_API int vlb_unpack_positions(int64_t npart, const int32_t* knode, const float* delta,
+                         double x0, double h, double* positions);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VLASOV_B200_H */

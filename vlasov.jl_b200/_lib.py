@@ -1,0 +1,167 @@
+"""ctypes binding of the C ABI (include/vlasov_b200.h).
+
+The shared library lives in-tree at ``vlasov.jl_b200/lib/libvlasov_b200.so``.
+Loading fails loudly when it is missing: there is no CPU fallback for the
+product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libvlasov_b200.so"
+
+VLB_OK = 0
+VLB_ERR_ARG = -1
+VLB_ERR_CUDA = -2
+VLB_ERR_STATE = -3
+VLB_ERR_TIMEOUT = -4
+VLB_ERR_NOMEM = -5
+
+VLB_DEPOSIT_FLOAT32 = 0
+VLB_DEPOSIT_FIXED64 = 1
+
+VLB_GRID_RHO_FINE = 0
+VLB_GRID_RHO_COARSE = 1
+VLB_GRID_PHI_FINE = 2
+VLB_GRID_PHI_COARSE = 3
+VLB_GRID_CSOL_FINE = 4
+VLB_GRID_CSOL_COARSE = 5
+
+VLB_POISSON_FP32 = 0
+
+# every symbol include/vlasov_b200.h declares
+EXPORTS = (
+    "vlb_last_error", "vlb_version", "vlb_create", "vlb_destroy", "vlb_upload_particles",
+    "vlb_download_particles", "vlb_sort", "vlb_get_sort", "vlb_deposit_fine", "vlb_deposit_coarse",
+    "vlb_poisson", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
+    "vlb_push", "vlb_step", "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
+    "vlb_enclosed_charge", "vlb_profile", "vlb_stage_count", "vlb_stage_name", "vlb_stage_times",
+    "vlb_launch_count", "vlb_stream", "vlb_sample_thomas_fermi", "vlb_ran2", "vlb_pack_positions",
+    "vlb_unpack_positions",
+)
+
+P_D = C.POINTER(C.c_double)
+P_F = C.POINTER(C.c_float)
+P_I = C.POINTER(C.c_int32)
+
+
+class LevelDesc(C.Structure):
+    _fields_ = [("nknots", C.c_int32), ("knots", P_D), ("colloc", P_D), ("sinv", P_D),
+                ("laplacian", P_D), ("eigvec", P_D), ("eigvec_inv", P_D), ("eigval", P_D),
+                ("dual_moments", P_D), ("dual_lengths", P_D), ("locate_x0", C.c_double),
+                ("locate_invwidth", C.c_double), ("locate_ncells", C.c_int32), ("locate_cells", P_I)]
+
+
+class SmoothingDesc(C.Structure):
+    _fields_ = [("nbdt", C.c_int32), ("spacing", C.c_double), ("overlap", P_D), ("gradient", P_D),
+                ("nodes", P_D)]
+
+
+class Config(C.Structure):
+    _fields_ = [("npart", C.c_int64), ("weight", C.c_double), ("fine", LevelDesc), ("coarse", LevelDesc),
+                ("smoothing", SmoothingDesc), ("device", C.c_int32), ("flags", C.c_int32)]
+
+
+class ProjectileDesc(C.Structure):
+    _fields_ = [("position", C.c_double * 3), ("previous", C.c_double * 3), ("velocity", C.c_double * 3),
+                ("charge", C.c_double), ("mass", C.c_double), ("sigma", C.c_double),
+                ("ball_radius", C.c_double), ("active", C.c_int32), ("pad_", C.c_int32)]
+
+
+class StepParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("rcmax", C.c_double), ("jellium_nions", C.c_double),
+                ("jellium_radius", C.c_double), ("capture_radius", C.c_double), ("deposit_mode", C.c_int32),
+                ("advance_projectile", C.c_int32), ("push", C.c_int32), ("use_graph", C.c_int32)]
+
+
+class StepResult(C.Structure):
+    _fields_ = [("kinetic", C.c_double), ("escaped", C.c_double), ("angular", C.c_double * 3),
+                ("projectile_force", C.c_double * 3), ("e_electrons", C.c_double), ("e_jellium", C.c_double),
+                ("enclosed_charge", C.c_double), ("total_charge", C.c_double), ("nout", C.c_int32),
+                ("outcount", C.c_int32), ("noccupied", C.c_int32), ("status", C.c_int32)]
+
+
+class VlbError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"vlb error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with vlasov.jl_b200/build.py "
+                               "(the device path has no CPU fallback)")
+        L = C.CDLL(str(LIB_PATH))
+        vp = C.c_void_p
+        sig = {
+            "vlb_last_error": (C.c_char_p, []),
+            "vlb_version": (C.c_char_p, []),
+            "vlb_create": (C.c_int, [C.POINTER(Config), C.POINTER(vp)]),
+            "vlb_destroy": (C.c_int, [vp]),
+            "vlb_upload_particles": (C.c_int, [vp, P_I, P_F, P_I, P_F]),
+            "vlb_download_particles": (C.c_int, [vp, P_I, P_F, P_I, P_F]),
+            "vlb_sort": (C.c_int, [vp, P_I, P_I]),
+            "vlb_get_sort": (C.c_int, [vp, P_I, P_I, P_I, P_I]),
+            "vlb_deposit_fine": (C.c_int, [vp, C.c_double, C.c_int32, P_I, P_D]),
+            "vlb_deposit_coarse": (C.c_int, [vp, C.c_double]),
+            "vlb_poisson": (C.c_int, [vp, C.c_int32]),
+            "vlb_coefficients": (C.c_int, [vp, C.c_int32]),
+            "vlb_mean_field": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double]),
+            "vlb_forces": (C.c_int, [vp, C.POINTER(ProjectileDesc), P_D, P_I]),
+            "vlb_projectile_forces": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.c_double, C.c_double, P_D,
+                                                P_D, P_D]),
+            "vlb_push": (C.c_int, [vp, C.c_double, C.c_double, P_D]),
+            "vlb_step": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams), C.POINTER(StepResult)]),
+            "vlb_get_grid": (C.c_int, [vp, C.c_int32, P_F]),
+            "vlb_set_grid": (C.c_int, [vp, C.c_int32, P_F]),
+            "vlb_get_forces": (C.c_int, [vp, P_F]),
+            "vlb_set_forces": (C.c_int, [vp, P_F]),
+            "vlb_enclosed_charge": (C.c_int, [vp, P_D, C.c_double, P_D]),
+            "vlb_profile": (C.c_int, [vp, C.c_int32]),
+            "vlb_stage_count": (C.c_int, []),
+            "vlb_stage_name": (C.c_char_p, [C.c_int32]),
+            "vlb_stage_times": (C.c_int, [vp, P_D, C.c_int32]),
+            "vlb_launch_count": (C.c_int, [vp, C.POINTER(C.c_int64)]),
+            "vlb_stream": (C.c_int, [vp, C.POINTER(vp)]),
+            "vlb_sample_thomas_fermi": (C.c_int, [P_D, C.c_int32, P_D, C.c_int32, C.c_double, C.c_int64,
+                                                  C.c_double, C.c_int32, C.c_int32, P_D, P_D]),
+            "vlb_ran2": (C.c_int, [C.c_int32, C.c_int32, C.c_int64, P_F]),
+            "vlb_pack_positions": (C.c_int, [C.c_int64, P_D, C.c_double, C.c_double, P_I, P_F]),
+            "vlb_unpack_positions": (C.c_int, [C.c_int64, P_I, P_F, C.c_double, C.c_double, P_D]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int):
+    if rc != VLB_OK:
+        raise VlbError(rc, lib().vlb_last_error().decode())
+
+
+def ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def pd(a):
+    return ptr(a, C.c_double)
+
+
+def pf(a):
+    return ptr(a, C.c_float)
+
+
+def pi(a):
+    return ptr(a, C.c_int32)

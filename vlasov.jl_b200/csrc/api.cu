@@ -1,0 +1,752 @@
+// The C ABI of the library (include/vlasov_b200.h): context set-up, the
+// reference-facing calls, and the fused step with its CUDA-graph replay.
+
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <cmath>
+#include <new>
+
+#include "vlb_internal.cuh"
+
+namespace vlb {
+
+void deposit_setup(Ctx& c);
+int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
+
+namespace {
+
+thread_local std::string g_err;
+
+const char* kStageNames[kNumStages] = {"sort",          "deposit_fine", "deposit_coarse", "poisson",
+                                        "coefficients",  "forces",       "projectile",     "push",
+                                        "capture",       "transfer",     "reserved10",     "reserved11"};
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const CudaError& e) {
+    char buf[512];
+    snprintf(buf, sizeof buf, "CUDA error %d (%s) at %s:%d", (int)e.err, cudaGetErrorString(e.err), e.file, e.line);
+    return fail(VLB_ERR_CUDA, buf);
+  } catch (const ArgError& e) {
+    return fail(VLB_ERR_ARG, e.msg);
+  } catch (const std::bad_alloc&) {
+    return fail(VLB_ERR_NOMEM, "host allocation failed");
+  }
+}
+
+template <class T>
+T* dalloc(size_t count) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) throw CudaError(e, __FILE__, __LINE__);
+  return static_cast<T*>(p);
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+std::vector<float> to_float(const double* src, size_t n) {
+  std::vector<float> v(n);
+  for (size_t i = 0; i < n; ++i) v[i] = (float)src[i];
+  return v;
+}
+
+template <class T>
+T* upload(const T* host, size_t n) {
+  T* d = dalloc<T>(n);
+  VLB_CUDA(cudaMemcpy(d, host, n * sizeof(T), cudaMemcpyHostToDevice));
+  return d;
+}
+
+float* upload_f(const double* src, size_t n) {
+  std::vector<float> v = to_float(src, n);
+  return upload(v.data(), n);
+}
+
+// A^T zero-padded to `pad` columns: out[i][r] = A[r][i]
+float* upload_transposed(const double* A, int n, int pad) {
+  std::vector<float> v((size_t)n * pad, 0.f);
+  for (int r = 0; r < n; ++r)
+    for (int i = 0; i < n; ++i) v[(size_t)i * pad + r] = (float)A[(size_t)r * n + i];
+  return upload(v.data(), v.size());
+}
+
+void check_level(const vlb_level_desc& L, const char* name) {
+  if (L.nknots < 6) throw ArgError(std::string(name) + ": at least 6 knots are required");
+  if (!L.knots || !L.colloc || !L.sinv || !L.laplacian || !L.eigvec || !L.eigvec_inv || !L.eigval ||
+      !L.dual_moments || !L.dual_lengths || !L.locate_cells || L.locate_ncells < 1)
+    throw ArgError(std::string(name) + ": a table pointer is null");
+  for (int i = 1; i < L.nknots; ++i)
+    if (!(L.knots[i] > L.knots[i - 1])) throw ArgError(std::string(name) + ": knots must increase");
+}
+
+void setup_level(Level& D, const vlb_level_desc& L, bool coarse) {
+  D.nk = L.nknots;
+  D.n = 2 * L.nknots;
+  D.ni = D.n - 2;
+  D.npad = (D.n + 7) / 8 * 8;
+  D.nipad = (D.ni + 7) / 8 * 8;
+  if (D.npad > 256) throw ArgError("at most 128 knots per axis are supported");
+  const int n = D.n, ni = D.ni;
+  D.h_knots.assign(L.knots, L.knots + D.nk);
+  D.h_colloc.assign(L.colloc, L.colloc + n);
+  D.colloc = upload_f(L.colloc, n);
+  D.knots = upload_f(L.knots, D.nk);
+  D.knots_d = upload(L.knots, D.nk);
+  D.sinvT = upload_transposed(L.sinv, n, D.npad);
+  D.MT = upload_transposed(L.eigvec, ni, D.nipad);
+  D.MinvT = upload_transposed(L.eigvec_inv, ni, D.nipad);
+  D.lap = upload_f(L.laplacian, (size_t)n * n);
+  {
+    std::vector<float> il((size_t)ni * ni * ni);
+    const double* lam = L.eigval;
+    for (int k = 0; k < ni; ++k)
+      for (int j = 0; j < ni; ++j)
+        for (int i = 0; i < ni; ++i) {
+          const double s = (lam[i] + lam[j]) + lam[k];
+          if (s == 0.0) throw ArgError("eigenvalue sum vanishes: singular operator");
+          il[(size_t)i + (size_t)ni * (j + (size_t)ni * k)] = (float)(1.0 / s);
+        }
+    D.invlsum = upload(il.data(), il.size());
+  }
+  D.dual = upload_f(L.dual_moments, 3 * (size_t)n);
+  D.dual_d = upload(L.dual_moments, 3 * (size_t)n);
+  D.dlen = upload_f(L.dual_lengths, n);
+  D.loc_cells = upload(L.locate_cells, L.locate_ncells);
+  D.loc_ncell = L.locate_ncells;
+  D.loc_x0 = (float)L.locate_x0;
+  D.loc_invw = (float)L.locate_invwidth;
+  const size_t tot = (size_t)n * n * n;
+  D.rho = dalloc<float>(tot);
+  D.phi = dalloc<float>(tot);
+  D.csol = dalloc<float>(tot);
+  VLB_CUDA(cudaMemset(D.rho, 0, tot * sizeof(float)));
+  VLB_CUDA(cudaMemset(D.phi, 0, tot * sizeof(float)));
+  VLB_CUDA(cudaMemset(D.csol, 0, tot * sizeof(float)));
+  if (coarse) {
+    D.csol_hartree = dalloc<float>(tot);
+    VLB_CUDA(cudaMemset(D.csol_hartree, 0, tot * sizeof(float)));
+  }
+}
+
+void free_level(Level& D) {
+  dfree(D.colloc); dfree(D.knots); dfree(D.knots_d); dfree(D.sinvT); dfree(D.MT); dfree(D.MinvT);
+  dfree(D.lap); dfree(D.invlsum); dfree(D.dual); dfree(D.dual_d); dfree(D.dlen); dfree(D.loc_cells);
+  dfree(D.rho); dfree(D.phi); dfree(D.csol); dfree(D.csol_hartree);
+}
+
+void destroy_ctx(Ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int g = 0; g < 2; ++g) {
+    if (c->gexec[g]) cudaGraphExecDestroy(c->gexec[g]);
+    c->gexec[g] = nullptr;
+  }
+  free_level(c->fine);
+  free_level(c->coarse);
+  dfree(c->overlap); dfree(c->gradient); dfree(c->nodes);
+  for (int b = 0; b < 2; ++b) {
+    dfree(c->part[b].k); dfree(c->part[b].d); dfree(c->part[b].pk); dfree(c->part[b].pd);
+  }
+  dfree(c->force);
+  dfree(c->keys); dfree(c->keys_alt); dfree(c->skeys); dfree(c->perm); dfree(c->vals_alt);
+  dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off); dfree(c->occupied); dfree(c->bounds);
+  dfree(c->outlist); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
+  for (auto& w : c->work) dfree(w);
+  dfree(c->dsc);
+  if (c->hsc) cudaFreeHost(c->hsc);
+  if (c->hin) cudaFreeHost(c->hin);
+  if (c->evs_made)
+    for (auto& e : c->ev) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+Level& level_of(Ctx& c, int level) {
+  if (level == 0) return c.fine;
+  if (level == 1) return c.coarse;
+  throw ArgError("level must be 0 (fine) or 1 (coarse)");
+}
+
+float* grid_ptr(Ctx& c, int which) {
+  switch (which) {
+    case VLB_GRID_RHO_FINE: return c.fine.rho;
+    case VLB_GRID_RHO_COARSE: return c.coarse.rho;
+    case VLB_GRID_PHI_FINE: return c.fine.phi;
+    case VLB_GRID_PHI_COARSE: return c.coarse.phi;
+    case VLB_GRID_CSOL_FINE: return c.fine.csol;
+    case VLB_GRID_CSOL_COARSE: return c.coarse.csol;
+    default: throw ArgError("unknown grid selector");
+  }
+}
+
+size_t grid_size(Ctx& c, int which) {
+  const Level& L = (which % 2 == 0) ? c.fine : c.coarse;
+  return (size_t)L.n * L.n * L.n;
+}
+
+// projectile -> device scalars (persistent part)
+void upload_projectile(Ctx& c, const vlb_projectile* p) {
+  DeviceScalars& h = *c.hin;
+  for (int d = 0; d < 3; ++d) {
+    h.proj_pos[d] = p ? p->position[d] : 0.0;
+    h.proj_prev[d] = p ? p->previous[d] : 0.0;
+    h.proj_vel[d] = p ? p->velocity[d] : 0.0;
+    h.proj_force[d] = 0.0;
+  }
+  h.proj_charge = p ? p->charge : 0.0;
+  h.proj_mass = p ? p->mass : 1.0;
+  h.proj_sigma = p ? p->sigma : 1.0;
+  h.proj_ball = p ? p->ball_radius : 1.0;
+  h.proj_active = p ? p->active : 0;
+  const size_t off = offsetof(DeviceScalars, proj_pos);
+  const size_t len = offsetof(DeviceScalars, pad1) - off;
+  VLB_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(c.dsc) + off, reinterpret_cast<char*>(c.hin) + off, len,
+                           cudaMemcpyHostToDevice, c.stream));
+}
+
+void fetch_scalars(Ctx& c) {
+  VLB_CUDA(cudaMemcpyAsync(c.hsc, c.dsc, sizeof(DeviceScalars), cudaMemcpyDeviceToHost, c.stream));
+  VLB_CUDA(cudaStreamSynchronize(c.stream));
+}
+
+int status_code(Ctx& c) {
+  int s = c.hsc->status;
+  if (s & kStatusScanTimeout) return fail(VLB_ERR_TIMEOUT, "a device scan gave up waiting on a predecessor tile");
+  if (s) return fail(VLB_ERR_STATE, "device status flags set: " + std::to_string(s));
+  return VLB_OK;
+}
+
+void stage_mark(Ctx& c, int i) {
+  if (c.profile) VLB_CUDA(cudaEventRecord(c.ev[i], c.stream));
+}
+
+void reset_step_scalars(Ctx& c) {
+  VLB_CUDA(cudaMemsetAsync(c.dsc, 0, offsetof(DeviceScalars, reset_end), c.stream));
+}
+
+// The fused step: everything on the stream, no host synchronisation.
+// Stage events are recorded only when profiling (never inside a capture).
+void enqueue_step(Ctx& c, const vlb_step_params& p) {
+  reset_step_scalars(c);
+  stage_mark(c, 0);
+  launch_sort(c);
+  stage_mark(c, 1);
+  launch_deposit_fine(c, c.weight, p.deposit_mode);
+  stage_mark(c, 2);
+  launch_deposit_coarse(c, c.weight);
+  stage_mark(c, 3);
+  launch_poisson(c);
+  stage_mark(c, 4);
+  launch_mean_field_coefficients(c, c.fine, c.fine.phi, c.fine.csol, p.jellium_nions, p.jellium_radius);
+  launch_mean_field_coefficients(c, c.coarse, c.coarse.phi, c.coarse.csol, p.jellium_nions, p.jellium_radius);
+  stage_mark(c, 5);
+  launch_forces(c);
+  stage_mark(c, 6);
+  launch_projectile_update(c, p.dt, p.jellium_nions, p.jellium_radius, p.advance_projectile);
+  stage_mark(c, 7);
+  if (p.push) launch_push(c, p.dt, p.rcmax);
+  stage_mark(c, 8);
+  if (p.capture_radius > 0) launch_enclosed(c, p.capture_radius);
+  stage_mark(c, 9);
+}
+
+bool same_params(const vlb_step_params& a, const vlb_step_params& b) {
+  return a.dt == b.dt && a.rcmax == b.rcmax && a.jellium_nions == b.jellium_nions &&
+         a.jellium_radius == b.jellium_radius && a.capture_radius == b.capture_radius &&
+         a.deposit_mode == b.deposit_mode && a.advance_projectile == b.advance_projectile && a.push == b.push;
+}
+
+// Two graphs, one per parity of the sort's double buffer: the step moves
+// the cloud from part[cur] to part[cur^1], so graph g starts from cur == g.
+void capture_graphs(Ctx& c, const vlb_step_params& p) {
+  const int saved = c.cur;
+  for (int g = 0; g < 2; ++g) {
+    if (c.gexec[g]) {
+      VLB_CUDA(cudaGraphExecDestroy(c.gexec[g]));
+      c.gexec[g] = nullptr;
+    }
+    c.cur = g;
+    cudaGraph_t graph = nullptr;
+    VLB_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue_step(c, p);
+    } catch (...) {
+      cudaStreamEndCapture(c.stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      c.cur = saved;
+      throw;
+    }
+    VLB_CUDA(cudaStreamEndCapture(c.stream, &graph));
+    VLB_CUDA(cudaGraphInstantiate(&c.gexec[g], graph, 0));
+    VLB_CUDA(cudaGraphDestroy(graph));
+  }
+  c.cur = saved;
+  c.graph_params = p;
+  c.graph_valid = true;
+}
+
+}  // namespace
+
+std::string cuda_msg(cudaError_t e, const char* what) {
+  return std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+}  // namespace vlb
+
+using namespace vlb;
+
+extern "C" {
+
+const char* vlb_last_error(void) { return g_err.c_str(); }
+const char* vlb_version(void) { return "vlasov_b200 0.1 (sm_100a)"; }
+
+int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
+  if (!cfg || !out) return fail(VLB_ERR_ARG, "null config or output handle");
+  *out = nullptr;
+  Ctx* c = nullptr;
+  int rc = guarded([&]() -> int {
+    if (cfg->npart < 1) throw ArgError("npart must be positive");
+    if (cfg->npart > (int64_t)INT32_MAX / 2) throw ArgError("npart too large for 32-bit slots");
+    if (!(cfg->weight > 0)) throw ArgError("weight must be positive");
+    check_level(cfg->fine, "fine");
+    check_level(cfg->coarse, "coarse");
+    const vlb_smoothing_desc& S = cfg->smoothing;
+    if (S.nbdt < 1 || !S.overlap || !S.gradient || !S.nodes) throw ArgError("smoothing tables missing");
+    // the accelerated path assumes a uniform fine axis (src/accelerator.jl:262-268)
+    const double* kf = cfg->fine.knots;
+    const int nkf = cfg->fine.nknots;
+    const double h = (kf[nkf - 1] - kf[0]) / (nkf - 1);
+    for (int i = 1; i < nkf; ++i)
+      if (std::fabs((kf[i] - kf[i - 1]) - h) > 1e-9 * std::fabs(h))
+        throw ArgError("the accelerated path assumes a uniform fine grid");
+    if (cfg->coarse.knots[0] > kf[0] || cfg->coarse.knots[cfg->coarse.nknots - 1] < kf[nkf - 1])
+      throw ArgError("the fine level sticks out of the coarse level");
+    int ndev = 0;
+    VLB_CUDA(cudaGetDeviceCount(&ndev));
+    if (cfg->device < 0 || cfg->device >= ndev) throw ArgError("no such CUDA device");
+    c = new Ctx();
+    c->device = cfg->device;
+    VLB_CUDA(cudaSetDevice(c->device));
+    VLB_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
+    VLB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->N = cfg->npart;
+    c->Npad = (c->N + 63) / 64 * 64;
+    c->weight = cfg->weight;
+    setup_level(c->fine, cfg->fine, false);
+    setup_level(c->coarse, cfg->coarse, true);
+    c->x0 = kf[0];
+    c->h = h;
+    c->x0f = (float)c->x0;
+    c->hf = (float)c->h;
+    c->spacing_f = (float)S.spacing;
+    const double half = S.spacing / 2;
+    c->lo_f = (float)(kf[1] + half);
+    c->hi_f = (float)(kf[nkf - 2] - half);
+    c->nbdt = S.nbdt;
+    c->ncol = S.nbdt + 1;
+    c->overlap = upload_f(S.overlap, (size_t)c->ncol * 10);
+    c->gradient = upload_f(S.gradient, (size_t)c->ncol * 10);
+    c->nodes = upload_f(S.nodes, (size_t)c->ncol * 8);
+    const size_t P = 3 * (size_t)c->Npad;
+    for (int b = 0; b < 2; ++b) {
+      c->part[b].k = dalloc<int32_t>(P);
+      c->part[b].d = dalloc<float>(P);
+      c->part[b].pk = dalloc<int32_t>(P);
+      c->part[b].pd = dalloc<float>(P);
+      VLB_CUDA(cudaMemset(c->part[b].k, 0, P * 4));
+      VLB_CUDA(cudaMemset(c->part[b].d, 0, P * 4));
+      VLB_CUDA(cudaMemset(c->part[b].pk, 0, P * 4));
+      VLB_CUDA(cudaMemset(c->part[b].pd, 0, P * 4));
+    }
+    c->force = dalloc<float>(P);
+    VLB_CUDA(cudaMemset(c->force, 0, P * 4));
+    const int64_t N = c->N;
+    c->ncell = c->fine.nk * c->fine.nk * c->fine.nk;
+    c->keys = dalloc<uint32_t>(N);
+    c->keys_alt = dalloc<uint32_t>(N);
+    c->skeys = dalloc<uint32_t>(N);
+    c->perm = dalloc<uint32_t>(N);
+    c->vals_alt = dalloc<uint32_t>(N);
+    const int64_t ntiles = (N + 4095) / 4096;
+    c->radix_table_size = 1024 * ntiles;
+    c->radix_table = dalloc<uint32_t>(c->radix_table_size);
+    c->counts = dalloc<int32_t>(c->ncell);
+    c->cell_off = dalloc<int32_t>(c->ncell);
+    c->occupied = dalloc<int32_t>(c->ncell);
+    c->bounds = dalloc<int32_t>(c->ncell + 1);
+    c->outlist = dalloc<int32_t>(N);
+    const int64_t scan_tiles = std::max<int64_t>({(N + 4095) / 4096, (c->ncell + 4095) / 4096,
+                                                  (c->radix_table_size + 4095) / 4096}) + 1;
+    c->scan_status_size = 8 * scan_tiles;
+    c->scan_status = dalloc<unsigned long long>(c->scan_status_size);
+    const int nf = c->fine.n, nc = c->coarse.n;
+    const size_t maxg = (size_t)std::max(nf, nc) * std::max(nf, nc) * std::max(nf, nc);
+    c->rho_fixed = dalloc<unsigned long long>((size_t)nf * nf * nf);
+    c->partials = dalloc<double>(10 * (size_t)std::max(nf, nc) * std::max(nf, nc));
+    for (auto& w : c->work) w = dalloc<float>(maxg);
+    c->dsc = dalloc<DeviceScalars>(1);
+    VLB_CUDA(cudaMemset(c->dsc, 0, sizeof(DeviceScalars)));
+    VLB_CUDA(cudaMallocHost(&c->hsc, sizeof(DeviceScalars)));
+    VLB_CUDA(cudaMallocHost(&c->hin, sizeof(DeviceScalars)));
+    memset(c->hsc, 0, sizeof(DeviceScalars));
+    memset(c->hin, 0, sizeof(DeviceScalars));
+    for (auto& e : c->ev) VLB_CUDA(cudaEventCreate(&e));
+    c->evs_made = true;
+    deposit_setup(*c);
+    VLB_CUDA(cudaDeviceSynchronize());
+    return VLB_OK;
+  });
+  if (rc != VLB_OK) {
+    std::string msg = g_err;
+    destroy_ctx(c);
+    g_err = msg;
+    return rc;
+  }
+  *out = reinterpret_cast<vlb_ctx*>(c);
+  return VLB_OK;
+}
+
+int vlb_destroy(vlb_ctx* ctx) {
+  if (!ctx) return fail(VLB_ERR_ARG, "null context");
+  destroy_ctx(reinterpret_cast<Ctx*>(ctx));
+  return VLB_OK;
+}
+
+#define CTX_OR_FAIL                                              \
+  if (!ctx) return fail(VLB_ERR_ARG, "null context");            \
+  Ctx& c = *reinterpret_cast<Ctx*>(ctx);                         \
+  if (cudaSetDevice(c.device) != cudaSuccess) return fail(VLB_ERR_CUDA, "cudaSetDevice failed")
+
+int vlb_upload_particles(vlb_ctx* ctx, const int32_t* knode, const float* delta, const int32_t* pknode,
+                         const float* pdelta) {
+  CTX_OR_FAIL;
+  if (!knode || !delta || !pknode || !pdelta) return fail(VLB_ERR_ARG, "null particle array");
+  return guarded([&]() -> int {
+    Particles& P = c.part[c.cur];
+    const size_t n = (size_t)c.N;
+    for (int a = 0; a < 3; ++a) {
+      VLB_CUDA(cudaMemcpyAsync(P.k + a * c.Npad, knode + a * n, n * 4, cudaMemcpyHostToDevice, c.stream));
+      VLB_CUDA(cudaMemcpyAsync(P.d + a * c.Npad, delta + a * n, n * 4, cudaMemcpyHostToDevice, c.stream));
+      VLB_CUDA(cudaMemcpyAsync(P.pk + a * c.Npad, pknode + a * n, n * 4, cudaMemcpyHostToDevice, c.stream));
+      VLB_CUDA(cudaMemcpyAsync(P.pd + a * c.Npad, pdelta + a * n, n * 4, cudaMemcpyHostToDevice, c.stream));
+    }
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    c.sorted = false;
+    return VLB_OK;
+  });
+}
+
+int vlb_download_particles(vlb_ctx* ctx, int32_t* knode, float* delta, int32_t* pknode, float* pdelta) {
+  CTX_OR_FAIL;
+  return guarded([&]() -> int {
+    Particles& P = c.part[c.cur];
+    const size_t n = (size_t)c.N;
+    for (int a = 0; a < 3; ++a) {
+      if (knode) VLB_CUDA(cudaMemcpyAsync(knode + a * n, P.k + a * c.Npad, n * 4, cudaMemcpyDeviceToHost, c.stream));
+      if (delta) VLB_CUDA(cudaMemcpyAsync(delta + a * n, P.d + a * c.Npad, n * 4, cudaMemcpyDeviceToHost, c.stream));
+      if (pknode) VLB_CUDA(cudaMemcpyAsync(pknode + a * n, P.pk + a * c.Npad, n * 4, cudaMemcpyDeviceToHost, c.stream));
+      if (pdelta) VLB_CUDA(cudaMemcpyAsync(pdelta + a * n, P.pd + a * c.Npad, n * 4, cudaMemcpyDeviceToHost, c.stream));
+    }
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_sort(vlb_ctx* ctx, int32_t* noccupied, int32_t* outcount) {
+  CTX_OR_FAIL;
+  return guarded([&]() -> int {
+    reset_step_scalars(c);
+    launch_sort(c);
+    fetch_scalars(c);
+    if (noccupied) *noccupied = c.hsc->noccupied;
+    if (outcount) *outcount = c.hsc->outcount;
+    return status_code(c);
+  });
+}
+
+int vlb_get_sort(vlb_ctx* ctx, int32_t* perm, int32_t* occupied, int32_t* bounds, int32_t* outlist) {
+  CTX_OR_FAIL;
+  if (!c.sorted) return fail(VLB_ERR_STATE, "no sort has run on the current cloud");
+  return guarded([&]() -> int {
+    fetch_scalars(c);
+    const int nocc = c.hsc->noccupied, nout = c.hsc->outcount;
+    if (perm) VLB_CUDA(cudaMemcpyAsync(perm, c.perm, (size_t)c.N * 4, cudaMemcpyDeviceToHost, c.stream));
+    if (occupied) VLB_CUDA(cudaMemcpyAsync(occupied, c.occupied, (size_t)nocc * 4, cudaMemcpyDeviceToHost, c.stream));
+    if (bounds) VLB_CUDA(cudaMemcpyAsync(bounds, c.bounds, (size_t)(nocc + 1) * 4, cudaMemcpyDeviceToHost, c.stream));
+    if (outlist && nout)
+      VLB_CUDA(cudaMemcpyAsync(outlist, c.outlist, (size_t)nout * 4, cudaMemcpyDeviceToHost, c.stream));
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_deposit_fine(vlb_ctx* ctx, double charge, int32_t mode, int32_t* nout, double* total_charge) {
+  CTX_OR_FAIL;
+  if (mode != VLB_DEPOSIT_FLOAT32 && mode != VLB_DEPOSIT_FIXED64) return fail(VLB_ERR_ARG, "unknown deposit mode");
+  if (!c.sorted) return fail(VLB_ERR_STATE, "deposit before any sort of the current cloud");
+  return guarded([&]() -> int {
+    launch_deposit_fine(c, charge, mode);
+    fetch_scalars(c);
+    if (nout) *nout = c.hsc->nout;
+    if (total_charge) *total_charge = c.hsc->charge_raw;
+    return status_code(c);
+  });
+}
+
+int vlb_deposit_coarse(vlb_ctx* ctx, double charge) {
+  CTX_OR_FAIL;
+  return guarded([&]() -> int {
+    launch_deposit_coarse(c, charge);
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_poisson(vlb_ctx* ctx, int32_t precision) {
+  CTX_OR_FAIL;
+  if (precision != VLB_POISSON_FP32) return fail(VLB_ERR_ARG, "unsupported Poisson precision");
+  return guarded([&]() -> int {
+    launch_poisson(c);
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_coefficients(vlb_ctx* ctx, int32_t level) {
+  CTX_OR_FAIL;
+  return guarded([&]() -> int {
+    Level& L = level_of(c, level);
+    launch_coefficients(c, L, L.phi, L.csol);
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_mean_field(vlb_ctx* ctx, int32_t level, double nions, double radius) {
+  CTX_OR_FAIL;
+  return guarded([&]() -> int {
+    Level& L = level_of(c, level);
+    launch_mean_field_add(c, L, nions, radius);
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_forces(vlb_ctx* ctx, const vlb_projectile* proj, double red[4], int32_t* outcount) {
+  CTX_OR_FAIL;
+  if (!c.sorted) return fail(VLB_ERR_STATE, "forces before any sort of the current cloud");
+  return guarded([&]() -> int {
+    upload_projectile(c, proj);
+    launch_forces(c);
+    fetch_scalars(c);
+    if (red)
+      for (int i = 0; i < 4; ++i) red[i] = c.hsc->red[i];
+    if (outcount) *outcount = c.hsc->outcount;
+    return status_code(c);
+  });
+}
+
+int vlb_projectile_forces(vlb_ctx* ctx, const vlb_projectile* proj, double nions, double jellium_radius,
+                          double force[3], double* e_electrons, double* e_jellium) {
+  CTX_OR_FAIL;
+  if (!proj) return fail(VLB_ERR_ARG, "null projectile");
+  if (!c.have_forces) return fail(VLB_ERR_STATE, "projectile forces before any force evaluation");
+  // host scalar arithmetic on the sums of the last vlb_forces (src/accelerator.jl:746-756)
+  const double* P = proj->position;
+  const double q = proj->charge;
+  const double r2 = P[0] * P[0] + P[1] * P[1] + P[2] * P[2];
+  const double modf = r2 > jellium_radius * jellium_radius ? nions * q / std::pow(r2, 1.5) : q / 64.0;
+  for (int d = 0; d < 3; ++d)
+    if (force) force[d] = modf * P[d] + c.hsc->red[d];
+  if (e_electrons) *e_electrons = c.weight * q * c.hsc->red[3];
+  const double r = std::sqrt(r2);
+  if (e_jellium)
+    *e_jellium = q * (r < jellium_radius ? -nions * (3 - (r / jellium_radius) * (r / jellium_radius)) / (2 * jellium_radius)
+                                         : -nions / r);
+  return VLB_OK;
+}
+
+int vlb_push(vlb_ctx* ctx, double dt, double rcmax, double diag[5]) {
+  CTX_OR_FAIL;
+  if (!(dt > 0)) return fail(VLB_ERR_ARG, "dt must be positive");
+  return guarded([&]() -> int {
+    launch_push(c, dt, rcmax);
+    fetch_scalars(c);
+    if (diag)
+      for (int i = 0; i < 5; ++i) diag[i] = c.hsc->diag[i];
+    c.sorted = false;  // the cloud moved: the cell lists are stale
+    return VLB_OK;
+  });
+}
+
+int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, vlb_step_result* result) {
+  CTX_OR_FAIL;
+  if (!params) return fail(VLB_ERR_ARG, "null step parameters");
+  if (!(params->dt > 0)) return fail(VLB_ERR_ARG, "dt must be positive");
+  if (params->deposit_mode != VLB_DEPOSIT_FLOAT32 && params->deposit_mode != VLB_DEPOSIT_FIXED64)
+    return fail(VLB_ERR_ARG, "unknown deposit mode");
+  return guarded([&]() -> int {
+    upload_projectile(c, proj);
+    const bool graph = params->use_graph && !c.profile;
+    if (graph && c.graph_valid && same_params(c.graph_params, *params)) {
+      const int g = c.cur;
+      VLB_CUDA(cudaGraphLaunch(c.gexec[g], c.stream));
+      c.launches += c.graph_launches;
+      c.cur ^= 1;
+    } else {
+      const long long before = c.launches;
+      enqueue_step(c, *params);
+      c.graph_launches = c.launches - before;
+      if (graph) {
+        // the eager run above did this step's work; capture for the next ones
+        const long long keep = c.launches;
+        capture_graphs(c, *params);
+        c.launches = keep;
+      }
+    }
+    VLB_CUDA(cudaMemcpyAsync(c.hsc, c.dsc, sizeof(DeviceScalars), cudaMemcpyDeviceToHost, c.stream));
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    if (c.profile) {
+      for (int i = 0; i < 9; ++i) {
+        float ms = 0;
+        VLB_CUDA(cudaEventElapsedTime(&ms, c.ev[i], c.ev[i + 1]));
+        c.stage_ms[i] += ms;
+      }
+    }
+    c.sorted = false;  // after the push the lists describe the previous positions
+    c.have_forces = true;
+    const DeviceScalars& h = *c.hsc;
+    if (proj) {
+      for (int d = 0; d < 3; ++d) {
+        proj->position[d] = h.proj_pos[d];
+        proj->previous[d] = h.proj_prev[d];
+        proj->velocity[d] = h.proj_vel[d];
+      }
+    }
+    if (result) {
+      result->kinetic = h.diag[0];
+      result->escaped = h.diag[1];
+      for (int d = 0; d < 3; ++d) {
+        result->angular[d] = h.diag[2 + d];
+        result->projectile_force[d] = h.proj_force[d];
+      }
+      result->e_electrons = h.e_el;
+      result->e_jellium = h.e_jel;
+      result->enclosed_charge = c.weight * (double)h.enclosed;
+      result->total_charge = h.charge_raw;
+      result->nout = h.nout;
+      result->outcount = h.outcount;
+      result->noccupied = h.noccupied;
+      result->status = h.status;
+    }
+    if (!params->push) c.sorted = true;  // forces-only: the cloud did not move
+    return status_code(c);
+  });
+}
+
+int vlb_get_grid(vlb_ctx* ctx, int32_t which, float* host) {
+  CTX_OR_FAIL;
+  if (!host) return fail(VLB_ERR_ARG, "null host buffer");
+  return guarded([&]() -> int {
+    float* g = grid_ptr(c, which);
+    VLB_CUDA(cudaMemcpyAsync(host, g, grid_size(c, which) * 4, cudaMemcpyDeviceToHost, c.stream));
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_set_grid(vlb_ctx* ctx, int32_t which, const float* host) {
+  CTX_OR_FAIL;
+  if (!host) return fail(VLB_ERR_ARG, "null host buffer");
+  return guarded([&]() -> int {
+    float* g = grid_ptr(c, which);
+    VLB_CUDA(cudaMemcpyAsync(g, host, grid_size(c, which) * 4, cudaMemcpyHostToDevice, c.stream));
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_get_forces(vlb_ctx* ctx, float* host) {
+  CTX_OR_FAIL;
+  if (!host) return fail(VLB_ERR_ARG, "null host buffer");
+  return guarded([&]() -> int {
+    const size_t n = (size_t)c.N;
+    for (int a = 0; a < 3; ++a)
+      VLB_CUDA(cudaMemcpyAsync(host + a * n, c.force + a * c.Npad, n * 4, cudaMemcpyDeviceToHost, c.stream));
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_set_forces(vlb_ctx* ctx, const float* host) {
+  CTX_OR_FAIL;
+  if (!host) return fail(VLB_ERR_ARG, "null host buffer");
+  return guarded([&]() -> int {
+    const size_t n = (size_t)c.N;
+    for (int a = 0; a < 3; ++a)
+      VLB_CUDA(cudaMemcpyAsync(c.force + a * c.Npad, host + a * n, n * 4, cudaMemcpyHostToDevice, c.stream));
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_enclosed_charge(vlb_ctx* ctx, const double position[3], double radius, double* q) {
+  CTX_OR_FAIL;
+  if (!position || !q) return fail(VLB_ERR_ARG, "null argument");
+  return guarded([&]() -> int {
+    vlb_projectile p{};
+    for (int d = 0; d < 3; ++d) p.position[d] = position[d];
+    upload_projectile(c, &p);
+    launch_enclosed(c, radius);
+    fetch_scalars(c);
+    *q = c.weight * (double)c.hsc->enclosed;
+    return VLB_OK;
+  });
+}
+
+int vlb_profile(vlb_ctx* ctx, int32_t enable) {
+  CTX_OR_FAIL;
+  c.profile = enable != 0;
+  for (double& m : c.stage_ms) m = 0;
+  return VLB_OK;
+}
+
+int vlb_stage_count(void) { return 9; }
+
+const char* vlb_stage_name(int32_t i) { return (i >= 0 && i < kNumStages) ? kStageNames[i] : ""; }
+
+int vlb_stage_times(vlb_ctx* ctx, double* ms, int32_t n) {
+  CTX_OR_FAIL;
+  if (!ms) return fail(VLB_ERR_ARG, "null output");
+  for (int i = 0; i < std::min<int>(n, kNumStages); ++i) ms[i] = c.stage_ms[i];
+  return VLB_OK;
+}
+
+int vlb_launch_count(vlb_ctx* ctx, int64_t* count) {
+  CTX_OR_FAIL;
+  if (!count) return fail(VLB_ERR_ARG, "null output");
+  *count = c.launches;
+  return VLB_OK;
+}
+
+int vlb_stream(vlb_ctx* ctx, void** stream) {
+  CTX_OR_FAIL;
+  if (!stream) return fail(VLB_ERR_ARG, "null output");
+  *stream = (void*)c.stream;
+  return VLB_OK;
+}
+
+}  // extern "C"

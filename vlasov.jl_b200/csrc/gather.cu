@@ -1,0 +1,319 @@
+// Forces on the sorted cloud: the Gaussian-smoothed field gather with the
+// projectile fused in, and the out-of-stencil tail.
+//
+// Gather (src/kernels.jl:339-470, host reference src/fields.jl:305-347):
+// one CTA per occupied cell, taken from a dynamic work counter.  The cell's
+// 10^3 stencil of csol is staged once in shared memory; each thread takes a
+// particle, builds its three table columns from delta with the reference's
+// Float32 arithmetic, and contracts
+//
+//     F = -w ( sum c gx oy oz, sum c ox gy oz, sum c ox oy gz )
+//
+// with all sixty smoothing values in registers.  The sum over the stencil is
+// reassociated (x first, then y, then z) against the reference's order,
+// which changes rounding only.  The projectile's Gaussian force
+// (src/projectile.jl:95-108) is evaluated per particle at the position
+// rebuilt from the *cell's* (clamped) knots, as the reference does, its
+// reaction subtracted, and the four reaction sums reduced per CTA in float64.
+//
+// Tail (src/accelerator.jl:679-733): the particles whose 10^3 stencil leaves
+// the fine grid take the coarse spline gradient (src/fields.jl:358-393) in
+// float64, or nothing outside both grids, plus the ball-softened projectile
+// reaction (src/projectile.jl:79-80).  Their Gaussian reaction sums go to the
+// projectile like everyone else's.  The reference runs this part on the host
+// after a device-to-host copy; here it stays on the device.
+
+#include "vlb_internal.cuh"
+
+namespace vlb {
+
+int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
+
+namespace {
+
+constexpr int kGThreads = 128;
+
+// src/projectile.jl:86-108, Float32
+__device__ __forceinline__ float gaussian_force_kernel(float r2, float sigma) {
+  const float u2 = r2 / (sigma * sigma);
+  if (u2 <= 0.25f) {
+    const float S[7] = {1.f / 3, -1.f / 10, 1.f / 56, -1.f / 432, 1.f / 4224, -1.f / 49920, 1.f / 685440};
+    float p = 0.f;
+#pragma unroll
+    for (int k = 6; k >= 0; --k) p = S[k] + u2 * p;
+    return 0.7978845608028654f * p / (sigma * sigma * sigma);
+  }
+  const float r = sqrtf(r2);
+  const float x = r / (1.4142135623730951f * sigma);
+  return (erff(x) - 0.7978845608028654f * (r / sigma) * expf(-u2 / 2.f)) / (r2 * r);
+}
+
+struct ProjF {
+  float px, py, pz, coef, sigma;
+  bool on;
+};
+
+__device__ __forceinline__ ProjF load_proj(const DeviceScalars* dsc, double w) {
+  ProjF p;
+  p.on = dsc->proj_active != 0;
+  p.px = (float)dsc->proj_pos[0];
+  p.py = (float)dsc->proj_pos[1];
+  p.pz = (float)dsc->proj_pos[2];
+  p.coef = p.on ? (float)(-w * dsc->proj_charge) : 0.f;
+  p.sigma = p.on ? (float)dsc->proj_sigma : 1.f;
+  p.on = p.on && p.coef != 0.f;
+  return p;
+}
+
+// Gaussian projectile term at the position rebuilt from a cell's knots.
+__device__ __forceinline__ void proj_term(const ProjF& P, int kx, int ky, int kz, float dx0, float dy0, float dz0,
+                                          float x0, float h, float& fx2, float& fy2, float& fz2, float& e) {
+  const float px = fadd(fadd(x0, fmul((float)(kx - 1), h)), dx0);
+  const float py = fadd(fadd(x0, fmul((float)(ky - 1), h)), dy0);
+  const float pz = fadd(fadd(x0, fmul((float)(kz - 1), h)), dz0);
+  const float dx = P.px - px, dy = P.py - py, dz = P.pz - pz;
+  const float d2 = dx * dx + dy * dy + dz * dz;
+  const float mm = P.coef * gaussian_force_kernel(d2, P.sigma);
+  fx2 = mm * dx;
+  fy2 = mm * dy;
+  fz2 = mm * dz;
+  const float r = sqrtf(d2);
+  e = r < 1.0e-4f * P.sigma ? 0.7978845608f / P.sigma : erff(r / 1.4142135624f / P.sigma) / r;
+}
+
+__device__ __forceinline__ void load10(const float* __restrict__ tab, int col, float* v) {
+  const float2* p = reinterpret_cast<const float2*>(tab + (size_t)(col - 1) * 10);
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    const float2 t = __ldg(p + a);
+    v[2 * a] = t.x;
+    v[2 * a + 1] = t.y;
+  }
+}
+
+__device__ __forceinline__ void block_add_red(float ax, float ay, float az, float ae, double* red) {
+  __shared__ double sh[4][kGThreads / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double v[4] = {ax, ay, az, ae};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    v[c] = warp_sum(v[c]);
+    if (lane == 0) sh[c][w] = v[c];
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double s = 0;
+    for (int ww = 0; ww < kGThreads / 32; ++ww) s += sh[threadIdx.x][ww];
+    if (s != 0.0) atomicAdd(&red[threadIdx.x], s);
+  }
+}
+
+__global__ void __launch_bounds__(kGThreads, 4) k_field(
+    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds, DeviceScalars* dsc, int64_t Npad,
+    const float* __restrict__ d, const float* __restrict__ csol, int n, int nk, const float* __restrict__ ov,
+    const float* __restrict__ gr, int nbdt, int ncol, float spacing, float x0, float h, double w,
+    float* __restrict__ force) {
+  __shared__ __align__(16) float tile[1000];
+  __shared__ int s_g;
+  const int tid = threadIdx.x;
+  const int nocc = dsc->noccupied;
+  const ProjF P = load_proj(dsc, w);
+  const float wf = (float)w;
+  float ax = 0.f, ay = 0.f, az = 0.f, ae = 0.f;
+  for (;;) {
+    if (tid == 0) s_g = (int)atomicAdd(&dsc->work_gather, 1ull);
+    __syncthreads();
+    const int g = s_g;
+    if (g >= nocc) break;
+    int kx, ky, kz;
+    cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
+    if (!field_fits(kx, ky, kz, n)) {  // the tail takes these
+      __syncthreads();
+      continue;
+    }
+    const int bx = 2 * kx - 6, by = 2 * ky - 6, bz = 2 * kz - 6;  // 0-based stencil corner
+    for (int e = tid; e < 1000; e += kGThreads) {
+      const int ii = e % 10, jj = (e / 10) % 10, kk = e / 100;
+      tile[e] = csol[(size_t)(bx + ii) + (size_t)n * ((by + jj) + (size_t)n * (bz + kk))];
+    }
+    __syncthreads();
+    const int sl = bounds[g], sh = bounds[g + 1];
+    for (int s = sl + tid; s < sh; s += kGThreads) {
+      const float dx0 = d[s], dy0 = d[Npad + s], dz0 = d[2 * Npad + s];
+      const int cx = table_column(dx0, spacing, nbdt, ncol);
+      const int cy = table_column(dy0, spacing, nbdt, ncol);
+      const int cz = table_column(dz0, spacing, nbdt, ncol);
+      float ox[10], gx[10], oy[10], gy[10], oz[10], gz[10];
+      load10(ov, cx, ox);
+      load10(gr, cx, gx);
+      load10(ov, cy, oy);
+      load10(gr, cy, gy);
+      load10(ov, cz, oz);
+      load10(gr, cz, gz);
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+      for (int kk = 0; kk < 10; ++kk) {
+        float tx = 0.f, ty = 0.f, tz = 0.f;
+#pragma unroll
+        for (int jj = 0; jj < 10; ++jj) {
+          const float2* row = reinterpret_cast<const float2*>(tile + (jj + 10 * kk) * 10);
+          float dxp = 0.f, val = 0.f;
+#pragma unroll
+          for (int a = 0; a < 5; ++a) {
+            const float2 c2 = row[a];
+            dxp = fmaf(c2.x, gx[2 * a], dxp);
+            val = fmaf(c2.x, ox[2 * a], val);
+            dxp = fmaf(c2.y, gx[2 * a + 1], dxp);
+            val = fmaf(c2.y, ox[2 * a + 1], val);
+          }
+          tx = fmaf(oy[jj], dxp, tx);
+          ty = fmaf(gy[jj], val, ty);
+          tz = fmaf(oy[jj], val, tz);
+        }
+        sx = fmaf(oz[kk], tx, sx);
+        sy = fmaf(oz[kk], ty, sy);
+        sz = fmaf(gz[kk], tz, sz);
+      }
+      float fx = -wf * sx, fy = -wf * sy, fz = -wf * sz;
+      if (P.on) {
+        float fx2, fy2, fz2, e;
+        proj_term(P, kx, ky, kz, dx0, dy0, dz0, x0, h, fx2, fy2, fz2, e);
+        fx -= fx2;
+        fy -= fy2;
+        fz -= fz2;
+        ax += fx2;
+        ay += fy2;
+        az += fz2;
+        ae += e;
+      }
+      force[s] = fx;
+      force[Npad + s] = fy;
+      force[2 * Npad + s] = fz;
+    }
+    __syncthreads();
+  }
+  block_add_red(ax, ay, az, ae, dsc->red);
+}
+
+// ------------------------------------------------------------------ tail
+__device__ __forceinline__ void basis_vd(const double* g, int nk, int lin, double x, double& v, double& dv) {
+  const int knot = (lin - 1) / 2 + 1, kind = (lin - 1) & 1;
+  double a, h, s;
+  if (knot > 1 && x <= g[knot - 1]) {
+    if (x < g[knot - 2]) { v = 0; dv = 0; return; }
+    h = g[knot - 1] - g[knot - 2]; a = (x - g[knot - 2]) / h; s = -1.0;
+  } else if (knot < nk && x >= g[knot - 1]) {
+    if (x > g[knot]) { v = 0; dv = 0; return; }
+    h = g[knot] - g[knot - 1]; a = (g[knot] - x) / h; s = 1.0;
+  } else {
+    v = 0; dv = 0; return;
+  }
+  if (kind == 0) {
+    v = 3 * (a * a) - 2 * (a * a * a);
+    dv = -6 * (a - a * a) * s / h;
+  } else {
+    v = h * (a * a - a * a * a) * s;
+    dv = -2 * a + 3 * (a * a);
+  }
+}
+
+__device__ __forceinline__ int cell_index_d(const double* g, int nk, double x) {
+  if (x < g[0] || x > g[nk - 1]) return 0;
+  int lo = 0, hi = nk;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (g[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return max(1, lo);
+}
+
+__global__ void __launch_bounds__(kGThreads) k_tail(const int32_t* __restrict__ outlist, DeviceScalars* dsc,
+                                                    int64_t Npad, const int32_t* __restrict__ k,
+                                                    const float* __restrict__ d, const float* __restrict__ csolc,
+                                                    const double* __restrict__ kc, int nkc, int nc, int nk,
+                                                    float x0f, float hf, double x0, double h, double w,
+                                                    float* __restrict__ force) {
+  const int cnt = dsc->outcount;
+  const ProjF P = load_proj(dsc, w);
+  const double Px = dsc->proj_pos[0], Py = dsc->proj_pos[1], Pz = dsc->proj_pos[2];
+  const double q = dsc->proj_charge, R = dsc->proj_ball;
+  float ax = 0.f, ay = 0.f, az = 0.f, ae = 0.f;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+    const int s = outlist[t];
+    const int kxp = k[s], kyp = k[Npad + s], kzp = k[2 * Npad + s];
+    const float dx0 = d[s], dy0 = d[Npad + s], dz0 = d[2 * Npad + s];
+    double fx = 0, fy = 0, fz = 0;
+    const double px = x0 + (double)(kxp - 1) * h + (double)dx0;
+    const double py = x0 + (double)(kyp - 1) * h + (double)dy0;
+    const double pz = x0 + (double)(kzp - 1) * h + (double)dz0;
+    const int cx = cell_index_d(kc, nkc, px), cy = cell_index_d(kc, nkc, py), cz = cell_index_d(kc, nkc, pz);
+    if (cx && cy && cz) {
+      double vx[4], vy[4], vz[4], gx[4], gy[4], gz[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        basis_vd(kc, nkc, 2 * (cx - 1) + a + 1, px, vx[a], gx[a]);
+        basis_vd(kc, nkc, 2 * (cy - 1) + a + 1, py, vy[a], gy[a]);
+        basis_vd(kc, nkc, 2 * (cz - 1) + a + 1, pz, vz[a], gz[a]);
+      }
+      double ex = 0, ey = 0, ez = 0;
+      for (int ak = 0; ak < 4; ++ak)
+        for (int aj = 0; aj < 4; ++aj) {
+          const float* row =
+              csolc + (size_t)2 * (cx - 1) + (size_t)nc * ((2 * (cy - 1) + aj) + (size_t)nc * (2 * (cz - 1) + ak));
+#pragma unroll
+          for (int ai = 0; ai < 4; ++ai) {
+            const double c = row[ai];
+            ex -= c * gx[ai] * vy[aj] * vz[ak];
+            ey -= c * vx[ai] * gy[aj] * vz[ak];
+            ez -= c * vx[ai] * vy[aj] * gz[ak];
+          }
+        }
+      fx = w * ex;
+      fy = w * ey;
+      fz = w * ez;
+    }
+    if (P.on) {
+      const double dx = Px - px, dy = Py - py, dz = Pz - pz;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      const double kern = r2 > R * R ? 1.0 / (r2 * sqrt(r2)) : 1.0 / (R * R * R);
+      const double m = -w * q * kern;
+      fx -= m * dx;
+      fy -= m * dy;
+      fz -= m * dz;
+      // the Gaussian reaction on the projectile, at the clamped cell's position
+      const uint32_t cell = cell_key(kxp, kyp, kzp, nk);
+      int kx, ky, kz;
+      cell_knots(cell, nk, kx, ky, kz);
+      float fx2, fy2, fz2, e;
+      proj_term(P, kx, ky, kz, dx0, dy0, dz0, x0f, hf, fx2, fy2, fz2, e);
+      ax += fx2;
+      ay += fy2;
+      az += fz2;
+      ae += e;
+    }
+    force[s] = (float)fx;
+    force[Npad + s] = (float)fy;
+    force[2 * Npad + s] = (float)fz;
+  }
+  block_add_red(ax, ay, az, ae, dsc->red);
+}
+
+}  // namespace
+
+void launch_forces(Ctx& c) {
+  Level& F = c.fine;
+  Level& C = c.coarse;
+  Particles& P = c.part[c.cur];
+  VLB_CUDA(cudaMemsetAsync(&c.dsc->work_gather, 0, sizeof(unsigned long long), c.stream));
+  VLB_CUDA(cudaMemsetAsync(c.dsc->red, 0, sizeof(c.dsc->red), c.stream));
+  k_field<<<c.num_sms * 4, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.dsc, c.Npad, P.d, F.csol, F.n, F.nk,
+                                                     c.overlap, c.gradient, c.nbdt, c.ncol, c.spacing_f, c.x0f,
+                                                     c.hf, c.weight, c.force);
+  VLB_LAUNCHED(c);
+  k_tail<<<c.num_sms * 2, kGThreads, 0, c.stream>>>(c.outlist, c.dsc, c.Npad, P.k, P.d, C.csol, C.knots_d, C.nk,
+                                                    C.n, F.nk, c.x0f, c.hf, c.x0, c.h, c.weight, c.force);
+  VLB_LAUNCHED(c);
+  c.have_forces = true;
+}
+
+}  // namespace vlb

@@ -1,0 +1,429 @@
+// The nested tensor-product Poisson solve and the spline-coefficient
+// conversions, on the device.
+//
+// Every product of the chain is the reference's rotating mode product
+// (src/tensorsolver.jl:217-223):
+//
+//     dest[p + m*i'] = sum_i A[i', i] * src[i + n*p],    m = n^2,
+//
+// which applies A along the first axis and leaves the axes rotated, so three
+// of them restore the order.  One FP32 kernel does all of them; the stages
+// around the products are fused into its load or its store:
+//
+//   load  : plain | Poisson right-hand side with the Dirichlet lifting
+//           (src/poisson.jl:275-294) | phi + V_xc(rho) + V_jel(r) (the mean
+//           field, src/meanfield.jl:116-123, folded into the S^-1 of the
+//           total potential: S^-1 phi + S^-1 extra = S^-1 (phi + extra))
+//   store : plain | times 1/(lx+ly+lz) (src/tensorsolver.jl:291) | into the
+//           interior of phi (src/kernels.jl:804-813)
+//
+// plus the multipole moments, the multipole faces of the coarse level
+// (src/poisson.jl:55-206, src/kernels.jl:868-873) and the fine faces read
+// from the coarse spline (src/kernels.jl:888-898).
+
+#include "vlb_internal.cuh"
+
+namespace vlb {
+
+int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
+
+namespace {
+
+constexpr int kPT = 64;  // p columns per CTA
+
+enum { LOAD_PLAIN = 0, LOAD_RHS = 1, LOAD_MEANFIELD = 2 };
+enum { EPI_PLAIN = 0, EPI_INVL = 1, EPI_PHI = 2 };
+
+struct ProductArgs {
+  float* dest;
+  const float* AT;     // [n][npad]  A transposed, zero padded
+  const float* src;
+  int n, npad;
+  long long m;
+  // LOAD_RHS
+  const float* rho;    // full grid (N = n + 2)
+  const float* phi;    // full grid, faces set
+  const float* lap;    // [N*N] row-major
+  // LOAD_MEANFIELD
+  const float* colloc; // [n]
+  float nions, radius;
+  // EPI
+  const float* invl;
+};
+
+__device__ __forceinline__ float xc_potential(float rho) {
+  // src/meanfield.jl:371-386
+  const float XC_EXCHANGE = -0.9847450218426966f;       // -cbrt(3/pi)
+  const float XC_CORRELATION = -0.0333f;
+  const float XC_CORRELATION_SCALE = 18.376708275787752f;  // 11.4 cbrt(4pi/3)
+  float c = cbrtf(rho);
+  return XC_EXCHANGE * c + XC_CORRELATION * log1pf(XC_CORRELATION_SCALE * c);
+}
+__device__ __forceinline__ float sphere_potential(float Q, float R, float r) {
+  return r < R ? -Q * (3.f - (r / R) * (r / R)) / (2.f * R) : -Q / r;
+}
+
+template <int LOAD>
+__device__ __forceinline__ float load_elem(const ProductArgs& a, long long idx) {
+  if (LOAD == LOAD_PLAIN) return a.src[idx];
+  if (LOAD == LOAD_MEANFIELD) {
+    const int n = a.n;
+    const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((long long)n * n));
+    const float gx = a.colloc[i], gy = a.colloc[j], gz = a.colloc[k];
+    const float r = sqrtf(gx * gx + gy * gy + gz * gz);
+    const float extra = xc_potential(a.rho[idx]) + sphere_potential(a.nions, a.radius, r);
+    return a.src ? a.src[idx] + extra : extra;
+  }
+  // LOAD_RHS: interior point (i,j,k) of an N^3 grid, N = n + 2
+  const int n = a.n, N = n + 2;
+  const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((long long)n * n));
+  const size_t sj = N, sk = (size_t)N * N;
+  const size_t c = (size_t)(i + 1) + sj * (j + 1) + sk * (k + 1);
+  const float* D = a.lap;
+  const float* P = a.phi;
+  float v = fmul(-12.566370614359172f, a.rho[c]);
+  v = fsub(v, fmul(D[(i + 1) * N + 0], P[c - (i + 1)]));
+  v = fsub(v, fmul(D[(i + 1) * N + N - 1], P[c - (i + 1) + (N - 1)]));
+  v = fsub(v, fmul(D[(j + 1) * N + 0], P[c - sj * (j + 1)]));
+  v = fsub(v, fmul(D[(j + 1) * N + N - 1], P[c - sj * (j + 1) + sj * (N - 1)]));
+  v = fsub(v, fmul(D[(k + 1) * N + 0], P[c - sk * (k + 1)]));
+  v = fsub(v, fmul(D[(k + 1) * N + N - 1], P[c - sk * (k + 1) + sk * (N - 1)]));
+  return v;
+}
+
+template <int LOAD, int EPI>
+__global__ void __launch_bounds__(256) k_mode_product(ProductArgs a) {
+  extern __shared__ __align__(16) float sm[];
+  const int n = a.n, npad = a.npad;
+  const int lds = n | 1;
+  float* As = sm;                       // [n][npad]
+  float* Ss = sm + (size_t)n * npad;    // [kPT][lds]
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int tx = tid & 7, ty = tid >> 3;
+  const long long p0 = (long long)blockIdx.x * kPT;
+  const int cnt = (int)min((long long)kPT, a.m - p0);
+  {
+    const float4* A4 = reinterpret_cast<const float4*>(a.AT);
+    float4* As4 = reinterpret_cast<float4*>(As);
+    const int tot4 = n * npad / 4;
+    for (int e = tid; e < tot4; e += nth) As4[e] = A4[e];
+  }
+  for (int pr = 0; pr < kPT; ++pr) {
+    for (int i = tid; i < n; i += nth) {
+      float v = 0.f;
+      if (pr < cnt) v = load_elem<LOAD>(a, (p0 + pr) * n + i);
+      Ss[pr * lds + i] = v;
+    }
+  }
+  __syncthreads();
+  float acc[8][8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[r][c] = 0.f;
+  const float* arow = As + ty * 8;
+  const float* bcol = Ss + tx * lds;
+#pragma unroll 2
+  for (int kk = 0; kk < n; ++kk) {
+    const float4 a0 = *reinterpret_cast<const float4*>(arow + (size_t)kk * npad);
+    const float4 a1 = *reinterpret_cast<const float4*>(arow + (size_t)kk * npad + 4);
+    const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    float bv[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) bv[c] = bcol[c * 8 * lds + kk];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
+  }
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const int row = ty * 8 + r;
+    if (row >= n) continue;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      const int pc = tx + 8 * c;
+      if (pc >= cnt) continue;
+      const long long p = p0 + pc;
+      const long long o = p + a.m * row;
+      float v = acc[r][c];
+      if (EPI == EPI_PLAIN) {
+        a.dest[o] = v;
+      } else if (EPI == EPI_INVL) {
+        a.dest[o] = v * a.invl[o];
+      } else {
+        const int N = n + 2;
+        const int i = (int)(p % n), j = (int)(p / n);
+        a.dest[(size_t)(i + 1) + (size_t)N * ((j + 1) + (size_t)N * (row + 1))] = v;
+      }
+    }
+  }
+}
+
+size_t product_smem(int n, int npad) { return ((size_t)n * npad + (size_t)kPT * (n | 1)) * sizeof(float); }
+
+template <int LOAD, int EPI>
+void product(Ctx& c, const ProductArgs& a) {
+  const size_t smem = product_smem(a.n, a.npad);
+  static bool attr_set = false;
+  if (!attr_set) {
+    VLB_CUDA(cudaFuncSetAttribute(k_mode_product<LOAD, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(227 * 1024)));
+    attr_set = true;
+  }
+  const unsigned grid = (unsigned)((a.m + kPT - 1) / kPT);
+  k_mode_product<LOAD, EPI><<<grid, a.npad, smem, c.stream>>>(a);
+  VLB_LAUNCHED(c);
+}
+
+// ---------------------------------------------------------------- moments
+// Ten moment partials per (j,k) column (src/poisson.jl:55-93), float64.
+__global__ void k_moments(const float* __restrict__ rho, const double* __restrict__ dual, int n,
+                          double* __restrict__ partial) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = n * n;
+  if (t >= m) return;
+  const double *p0 = dual, *p1 = dual + n, *p2 = dual + 2 * n;
+  const int j = t % n, k = t / n;
+  const double a = p0[j] * p0[k], b = p1[j] * p0[k], cc = p0[j] * p1[k];
+  const double d = p2[j] * p0[k], e = p0[j] * p2[k], f = p1[j] * p1[k];
+  double s0 = 0, s1 = 0, s2 = 0;
+  const float* col = rho + (size_t)n * t;
+  for (int i = 0; i < n; ++i) {
+    const double v = col[i];
+    s0 += v * p0[i];
+    s1 += v * p1[i];
+    s2 += v * p2[i];
+  }
+  partial[0 * m + t] = s0 * a;
+  partial[1 * m + t] = s1 * a;
+  partial[2 * m + t] = s0 * b;
+  partial[3 * m + t] = s0 * cc;
+  partial[4 * m + t] = s2 * a;
+  partial[5 * m + t] = s0 * d;
+  partial[6 * m + t] = s0 * e;
+  partial[7 * m + t] = s1 * b;
+  partial[8 * m + t] = s1 * cc;
+  partial[9 * m + t] = s0 * f;
+}
+
+// One block: the ten sums in a fixed order, then the expansion in the
+// barycentre frame (src/poisson.jl:168-189).
+__global__ void __launch_bounds__(1024) k_multipole(const double* __restrict__ partial, int m, DeviceScalars* dsc) {
+  __shared__ double sh[1024];
+  __shared__ double tot[10];
+  for (int r = 0; r < 10; ++r) {
+    double s = 0;
+    for (int t = threadIdx.x; t < m; t += 1024) s += partial[(size_t)r * m + t];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 512; o > 0; o >>= 1) {
+      if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) tot[r] = sh[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double q = tot[0];
+    for (int r = 0; r < 10; ++r) dsc->moments[r] = tot[r];
+    double cx = q == 0 ? 0 : tot[1] / q, cy = q == 0 ? 0 : tot[2] / q, cz = q == 0 ? 0 : tot[3] / q;
+    const double m200 = tot[4], m020 = tot[5], m002 = tot[6], mxy = tot[7], mxz = tot[8], myz = tot[9];
+    const double b2 = cx * cx + cy * cy + cz * cz;
+    double* mp = dsc->multipole;
+    mp[0] = q;
+    mp[1] = cx; mp[2] = cy; mp[3] = cz;
+    mp[4] = (2 * m200 - m020 - m002) - q * (3 * cx * cx - b2);
+    mp[5] = (2 * m020 - m200 - m002) - q * (3 * cy * cy - b2);
+    mp[6] = (2 * m002 - m200 - m020) - q * (3 * cz * cz - b2);
+    mp[7] = 3 * mxy - 3 * q * cx * cy;
+    mp[8] = 3 * mxz - 3 * q * cx * cz;
+    mp[9] = 3 * myz - 3 * q * cy * cz;
+  }
+}
+
+// t-th surface point of an n^3 grid, 0-based (src/kernels.jl:836-859)
+__device__ __forceinline__ void face_point(int t, int n, int& i, int& j, int& k) {
+  const int cap = n * n;
+  if (t < cap) { i = t % n; j = t / n; k = 0; return; }
+  t -= cap;
+  if (t < cap) { i = t % n; j = t / n; k = n - 1; return; }
+  t -= cap;
+  const int ring = 2 * n + 2 * (n - 2);
+  k = t / ring + 1;
+  const int r = t % ring;
+  if (r < n) { i = r; j = 0; }
+  else if (r < 2 * n) { i = r - n; j = n - 1; }
+  else if (r < 2 * n + (n - 2)) { i = 0; j = r - 2 * n + 1; }
+  else { i = n - 1; j = r - 2 * n - (n - 2) + 1; }
+}
+
+// Multipole potential on the faces (src/poisson.jl:198-206)
+__global__ void k_faces_multipole(float* __restrict__ phi, const float* __restrict__ g, int n,
+                                  const DeviceScalars* dsc) {
+  const int nf = 2 * n * n + (n - 2) * (4 * n - 4);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nf) return;
+  int i, j, k;
+  face_point(t, n, i, j, k);
+  const double* mp = dsc->multipole;
+  const double px = (double)g[i] - mp[1], py = (double)g[j] - mp[2], pz = (double)g[k] - mp[3];
+  const double r2 = px * px + py * py + pz * pz;
+  const double invr = 1.0 / sqrt(r2);
+  const double quad = mp[4] * px * px + mp[5] * py * py + mp[6] * pz * pz +
+                      2 * (mp[7] * px * py + mp[8] * px * pz + mp[9] * py * pz);
+  const double i5 = invr * invr * invr * invr * invr;
+  phi[(size_t)i + (size_t)n * (j + (size_t)n * k)] = (float)(mp[0] * invr + quad * i5 / 2);
+}
+
+// Hermite basis value in float (src/splines.jl:74-122)
+__device__ __forceinline__ float basis_value(const float* g, int nk, int lin, float x) {
+  const int knot = (lin - 1) / 2 + 1, kind = (lin - 1) & 1;
+  float a, h, s;
+  if (knot > 1 && x <= g[knot - 1]) {
+    if (x < g[knot - 2]) return 0.f;
+    h = g[knot - 1] - g[knot - 2]; a = (x - g[knot - 2]) / h; s = -1.f;
+  } else if (knot < nk && x >= g[knot - 1]) {
+    if (x > g[knot]) return 0.f;
+    h = g[knot] - g[knot - 1]; a = (g[knot] - x) / h; s = 1.f;
+  } else {
+    return 0.f;
+  }
+  return kind == 0 ? 3.f * (a * a) - 2.f * (a * a * a) : h * (a * a - a * a * a) * s;
+}
+
+__device__ __forceinline__ int cell_index_f(const float* g, int nk, float x) {
+  if (x < g[0] || x > g[nk - 1]) return 0;
+  int lo = 0, hi = nk;  // first index with g[idx] >= x
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (g[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return max(1, lo);
+}
+
+// Fine faces from the coarse spline (src/kernels.jl:888-898, src/fields.jl:440-469)
+__global__ void k_faces_from_coarse(float* __restrict__ phi, const float* __restrict__ gf, int n,
+                                    const float* __restrict__ kc, int nkc, const float* __restrict__ csol, int nc) {
+  const int nf = 2 * n * n + (n - 2) * (4 * n - 4);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nf) return;
+  int i, j, k;
+  face_point(t, n, i, j, k);
+  const float px = gf[i], py = gf[j], pz = gf[k];
+  const int cx = cell_index_f(kc, nkc, px), cy = cell_index_f(kc, nkc, py), cz = cell_index_f(kc, nkc, pz);
+  float v;
+  if (!cx || !cy || !cz) {
+    v = __int_as_float(0x7fc00000);
+  } else {
+    float vx[4], vy[4], vz[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      vx[a] = basis_value(kc, nkc, 2 * (cx - 1) + a + 1, px);
+      vy[a] = basis_value(kc, nkc, 2 * (cy - 1) + a + 1, py);
+      vz[a] = basis_value(kc, nkc, 2 * (cz - 1) + a + 1, pz);
+    }
+    v = 0.f;
+    for (int ak = 0; ak < 4; ++ak)
+      for (int aj = 0; aj < 4; ++aj) {
+        const float w = vy[aj] * vz[ak];
+        const float* row = csol + (size_t)2 * (cx - 1) + (size_t)nc * ((2 * (cy - 1) + aj) + (size_t)nc * (2 * (cz - 1) + ak));
+#pragma unroll
+        for (int ai = 0; ai < 4; ++ai) v += row[ai] * vx[ai] * w;
+      }
+  }
+  phi[(size_t)i + (size_t)n * (j + (size_t)n * k)] = v;
+}
+
+__global__ void k_add(float* __restrict__ a, const float* __restrict__ b, size_t n) {
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+    a[t] += b[t];
+}
+
+ProductArgs base_args(const Level& L, bool interior) {
+  ProductArgs a{};
+  a.n = interior ? L.ni : L.n;
+  a.npad = interior ? L.nipad : L.npad;
+  a.m = (long long)a.n * a.n;
+  return a;
+}
+
+// solve_interior! with the faces already in phi (src/devicemesh.jl:133-146)
+void solve_interior(Ctx& c, Level& L) {
+  ProductArgs a = base_args(L, true);
+  a.rho = L.rho; a.phi = L.phi; a.lap = L.lap;
+  // forward: into the eigenbasis
+  a.AT = L.MinvT; a.src = nullptr; a.dest = c.work[0];
+  product<LOAD_RHS, EPI_PLAIN>(c, a);
+  a.src = c.work[0]; a.dest = c.work[1];
+  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  a.src = c.work[1]; a.dest = c.work[0]; a.invl = L.invlsum;
+  product<LOAD_PLAIN, EPI_INVL>(c, a);
+  // back
+  a.AT = L.MT;
+  a.src = c.work[0]; a.dest = c.work[1];
+  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  a.src = c.work[1]; a.dest = c.work[0];
+  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  a.src = c.work[0]; a.dest = L.phi;
+  product<LOAD_PLAIN, EPI_PHI>(c, a);
+}
+
+}  // namespace
+
+void launch_coefficients(Ctx& c, Level& L, const float* src, float* dst) {
+  ProductArgs a = base_args(L, false);
+  a.AT = L.sinvT;
+  a.src = src; a.dest = c.work[0];
+  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  a.src = c.work[0]; a.dest = c.work[1];
+  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  a.src = c.work[1]; a.dest = dst;
+  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+}
+
+void launch_mean_field_coefficients(Ctx& c, Level& L, const float* phi, float* csol, double nions,
+                                    double radius) {
+  ProductArgs a = base_args(L, false);
+  a.AT = L.sinvT;
+  a.rho = L.rho; a.colloc = L.colloc;
+  a.nions = (float)nions; a.radius = (float)radius;
+  a.src = phi; a.dest = c.work[0];
+  product<LOAD_MEANFIELD, EPI_PLAIN>(c, a);
+  a.src = c.work[0]; a.dest = c.work[1];
+  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  a.src = c.work[1]; a.dest = csol;
+  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+}
+
+// csol += S^-1 [V_xc(rho) + V_jel(r)] (src/devicemesh.jl:171-183)
+void launch_mean_field_add(Ctx& c, Level& L, double nions, double radius) {
+  launch_mean_field_coefficients(c, L, nullptr, c.work[2], nions, radius);
+  const size_t tot = (size_t)L.n * L.n * L.n;
+  k_add<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(L.csol, c.work[2], tot);
+  VLB_LAUNCHED(c);
+}
+
+void launch_poisson(Ctx& c) {
+  Level& F = c.fine;
+  Level& C = c.coarse;
+  // coarse: multipole faces + solve (src/poisson.jl:351-354)
+  const int mc = C.n * C.n;
+  k_moments<<<(mc + 127) / 128, 128, 0, c.stream>>>(C.rho, C.dual_d, C.n, c.partials);
+  VLB_LAUNCHED(c);
+  k_multipole<<<1, 1024, 0, c.stream>>>(c.partials, mc, c.dsc);
+  VLB_LAUNCHED(c);
+  const int nfc = 2 * C.n * C.n + (C.n - 2) * (4 * C.n - 4);
+  k_faces_multipole<<<(nfc + 255) / 256, 256, 0, c.stream>>>(C.phi, C.colloc, C.n, c.dsc);
+  VLB_LAUNCHED(c);
+  solve_interior(c, C);
+  // fine faces from the coarse Hartree coefficients, then the fine solve
+  launch_coefficients(c, C, C.phi, C.csol_hartree);
+  const int nff = 2 * F.n * F.n + (F.n - 2) * (4 * F.n - 4);
+  k_faces_from_coarse<<<(nff + 255) / 256, 256, 0, c.stream>>>(F.phi, F.colloc, F.n, C.knots, C.nk,
+                                                               C.csol_hartree, C.n);
+  VLB_LAUNCHED(c);
+  solve_interior(c, F);
+}
+
+}  // namespace vlb

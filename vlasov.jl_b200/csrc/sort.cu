@@ -1,0 +1,355 @@
+// Stable counting sort of the packed cloud by fine cell, on the device.
+//
+// Replaces the reference's _device_sort! (src/accelerator.jl:421-446:
+// atomic histogram, host scan, unstable atomic placement, copy back) and its
+// out-of-stencil list (src/kernels.jl:1041-1058).  The order produced here is
+// the stable order of the host cellsort! (src/sorting.jl:163-204): by cell,
+// then by index before the sort.
+//
+//   1. cell keys + warp-aggregated histogram over nk^3 cells;
+//   2. decoupled look-back scans: cell offsets, then the occupied-cell list
+//      with its bounds;
+//   3. LSD radix sort of (key, index) in passes of at most 10 bits, each
+//      pass stable (warp multi-split ranks + a scanned digit table);
+//   4. one gather of the 48-byte records into the other buffer (swap);
+//   5. a look-back scan that compacts the out-of-stencil slots.
+//
+// Every spin of the look-back is bounded: after kSpinLimit polls the tile
+// records kStatusScanTimeout in the step's status word and gives up.
+
+#include "vlb_internal.cuh"
+
+namespace vlb {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;  // 4096
+constexpr int kRadixThreads = 256;
+constexpr int kRadixWarps = kRadixThreads / 32;
+constexpr int kRadixPerWarp = 512;
+constexpr int kRadixTile = kRadixWarps * kRadixPerWarp;  // 4096
+constexpr int kMaxDigitBits = 10;
+constexpr long long kSpinLimit = 1ll << 22;
+
+constexpr unsigned long long kFlagAgg = 1ull << 62;
+constexpr unsigned long long kFlagIncl = 2ull << 62;
+constexpr unsigned long long kValMask = (1ull << 62) - 1;
+
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// ---------------------------------------------------------------- keys
+// Cell key of every particle and the histogram of cells.  The cloud is
+// nearly sorted from the previous step, so neighbouring lanes usually share
+// a cell: one atomic per group of equal keys in a warp.
+__global__ void __launch_bounds__(256) k_keys_hist(int64_t N, int64_t Npad, const int32_t* __restrict__ k,
+                                                   int nk, uint32_t* __restrict__ keys,
+                                                   int32_t* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * blockDim.x / 32;
+  for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x - lane); base < N; base += warps * 32) {
+    int64_t i = base + lane;
+    bool valid = i < N;
+    unsigned m = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+      uint32_t key = cell_key(k[i], k[Npad + i], k[2 * Npad + i], nk);
+      keys[i] = key;
+      unsigned peers = __match_any_sync(m, key);
+      int leader = __ffs(peers) - 1;
+      if (lane == leader) atomicAdd(&counts[key], __popc(peers));
+    }
+  }
+}
+
+// -------------------------------------------------------------- the scan
+// Exclusive scan of n unsigned values produced by `in`, delivered to `out`
+// as (index, exclusive prefix, value).  Single pass: tiles take tickets in
+// launch order and read their prefix from their predecessors' published
+// aggregates (decoupled look-back).  `total` receives the sum.
+struct ScanInArray { const uint32_t* a; __device__ uint32_t operator()(int64_t i) const { return a[i]; } };
+struct ScanOutArray { uint32_t* a; __device__ void operator()(int64_t i, uint32_t p, uint32_t) const { a[i] = p; } };
+
+struct ScanInCounts { const int32_t* c; __device__ uint32_t operator()(int64_t i) const { return (uint32_t)c[i]; } };
+struct ScanOutOffsets { int32_t* off; __device__ void operator()(int64_t i, uint32_t p, uint32_t) const { off[i] = (int32_t)p; } };
+
+struct ScanInOccupied { const int32_t* c; __device__ uint32_t operator()(int64_t i) const { return c[i] > 0 ? 1u : 0u; } };
+struct ScanOutOccupied {
+  int32_t* occupied; int32_t* bounds; const int32_t* off; int64_t ncell; int64_t N;
+  __device__ void operator()(int64_t i, uint32_t p, uint32_t v) const {
+    if (v) { occupied[p] = (int32_t)i; bounds[p] = off[i]; }
+    if (i == ncell - 1) bounds[p + v] = (int32_t)N;
+  }
+};
+
+struct ScanInOutside {
+  const uint32_t* skeys; int nk, n;
+  __device__ uint32_t operator()(int64_t s) const {
+    int kx, ky, kz;
+    cell_knots(skeys[s], nk, kx, ky, kz);
+    return field_fits(kx, ky, kz, n) ? 0u : 1u;
+  }
+};
+struct ScanOutOutside {
+  int32_t* outlist;
+  __device__ void operator()(int64_t s, uint32_t p, uint32_t v) const { if (v) outlist[p] = (int32_t)s; }
+};
+
+template <class In, class Out>
+__global__ void __launch_bounds__(kScanThreads) k_scan(In in, Out out, int64_t n, unsigned long long* status,
+                                                       unsigned long long* ticket, int32_t* total,
+                                                       int32_t* err) {
+  __shared__ uint32_t s_warp[kScanThreads / 32];
+  __shared__ unsigned long long s_prefix;
+  __shared__ int64_t s_tile;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (tid == 0) s_tile = (int64_t)atomicAdd(ticket, 1ull);
+  __syncthreads();
+  const int64_t tile = s_tile;
+  const int64_t base = tile * kScanTile + (int64_t)tid * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t sum = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    int64_t i = base + j;
+    v[j] = i < n ? in(i) : 0u;
+    sum += v[j];
+  }
+  // block exclusive scan of the thread sums
+  uint32_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) s_warp[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    if (lane < kScanThreads / 32) s_warp[lane] = wi - w;  // exclusive warp offsets
+    if (lane == kScanThreads / 32 - 1) {
+      unsigned long long agg = wi;  // tile aggregate
+      unsigned long long prefix = 0;
+      if (tile == 0) {
+        st_relaxed(&status[0], kFlagIncl | agg);
+      } else {
+        st_relaxed(&status[tile], kFlagAgg | agg);
+        int64_t j = tile - 1;
+        long long spins = 0;
+        while (j >= 0) {
+          unsigned long long s = ld_relaxed(&status[j]);
+          unsigned long long flag = s & ~kValMask;
+          if (flag == 0) {
+            if (++spins > kSpinLimit) { atomicOr(err, kStatusScanTimeout); break; }
+            __nanosleep(32);
+            continue;
+          }
+          prefix += s & kValMask;
+          if (flag == kFlagIncl) break;
+          --j;
+        }
+        st_relaxed(&status[tile], kFlagIncl | (prefix + agg));
+      }
+      s_prefix = prefix;
+      if (total && (tile + 1) * (int64_t)kScanTile >= n) *total = (int32_t)(prefix + agg);
+    }
+  }
+  __syncthreads();
+  uint32_t run = (uint32_t)s_prefix + s_warp[wid] + (incl - sum);
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    int64_t i = base + j;
+    if (i < n) out(i, run, v[j]);
+    run += v[j];
+  }
+}
+
+template <class In, class Out>
+void scan(Ctx& c, In in, Out out, int64_t n, int slot, int32_t* total) {
+  if (n <= 0) return;
+  int64_t tiles = (n + kScanTile - 1) / kScanTile;
+  int64_t per_slot = c.scan_status_size / 8;
+  if (tiles > per_slot) throw ArgError("scan larger than its status slot");
+  unsigned long long* st = c.scan_status + slot * per_slot;
+  k_scan<In, Out><<<(unsigned)tiles, kScanThreads, 0, c.stream>>>(in, out, n, st, &c.dsc->scan_tiles[slot],
+                                                                  total, &c.dsc->status);
+  VLB_LAUNCHED(c);
+}
+
+// ------------------------------------------------------------- radix sort
+__global__ void __launch_bounds__(kRadixThreads) k_radix_upsweep(const uint32_t* __restrict__ keys, int64_t N,
+                                                                 int shift, uint32_t mask,
+                                                                 uint32_t* __restrict__ table, int64_t ntiles) {
+  __shared__ uint32_t hist[1 << kMaxDigitBits];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int b = tid; b <= (int)mask; b += kRadixThreads) hist[b] = 0;
+  __syncthreads();
+  const int64_t tile = blockIdx.x;
+  for (int r = 0; r < kRadixPerWarp / 32; ++r) {
+    int64_t e = tile * kRadixTile + (int64_t)w * kRadixPerWarp + r * 32 + lane;
+    bool valid = e < N;
+    unsigned m = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+      uint32_t d = (keys[e] >> shift) & mask;
+      unsigned peers = __match_any_sync(m, d);
+      if (lane == __ffs(peers) - 1) atomicAdd(&hist[d], (uint32_t)__popc(peers));
+    }
+  }
+  __syncthreads();
+  for (int b = tid; b <= (int)mask; b += kRadixThreads) table[(int64_t)b * ntiles + tile] = hist[b];
+}
+
+__global__ void __launch_bounds__(kRadixThreads) k_radix_downsweep(
+    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
+    uint32_t* __restrict__ vals_out, int64_t N, int shift, uint32_t mask, const uint32_t* __restrict__ table,
+    int64_t ntiles) {
+  __shared__ uint32_t whist[kRadixWarps][1 << kMaxDigitBits];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int nb = (int)mask + 1;
+  for (int b = lane; b < nb; b += 32) whist[w][b] = 0;
+  __syncwarp();
+  const int64_t tile = blockIdx.x;
+  constexpr int R = kRadixPerWarp / 32;
+  uint32_t key[R], val[R], local[R];
+  unsigned valid_bits = 0;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    int64_t e = tile * kRadixTile + (int64_t)w * kRadixPerWarp + r * 32 + lane;
+    bool valid = e < N;
+    unsigned m = __ballot_sync(0xffffffffu, valid);
+    key[r] = valid ? keys_in[e] : 0u;
+    val[r] = valid ? (vals_in ? vals_in[e] : (uint32_t)e) : 0u;
+    local[r] = 0;
+    if (valid) {
+      valid_bits |= 1u << r;
+      uint32_t d = (key[r] >> shift) & mask;
+      unsigned peers = __match_any_sync(m, d);
+      int leader = __ffs(peers) - 1;
+      uint32_t b = 0;
+      if (lane == leader) {
+        b = whist[w][d];
+        whist[w][d] = b + (uint32_t)__popc(peers);
+      }
+      b = __shfl_sync(m, b, leader);
+      local[r] = b + (uint32_t)__popc(peers & lanemask_lt());
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // exclusive scan over warps, per digit
+  for (int b = tid; b < nb; b += kRadixThreads) {
+    uint32_t run = 0;
+#pragma unroll
+    for (int ww = 0; ww < kRadixWarps; ++ww) {
+      uint32_t t = whist[ww][b];
+      whist[ww][b] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    if (!(valid_bits & (1u << r))) continue;
+    uint32_t d = (key[r] >> shift) & mask;
+    uint32_t pos = table[(int64_t)d * ntiles + tile] + whist[w][d] + local[r];
+    if (keys_out) keys_out[pos] = key[r];
+    vals_out[pos] = val[r];
+  }
+}
+
+// ------------------------------------------------------------- the move
+// Moves the records into slot order: dst[s] = src[perm[s]], all twelve
+// component arrays.  Reads follow the permutation of a nearly sorted cloud,
+// so they stay within a few pages.
+__global__ void __launch_bounds__(256) k_gather_records(int64_t N, int64_t Npad, const uint32_t* __restrict__ perm,
+                                                        const int32_t* __restrict__ k0, const float* __restrict__ d0,
+                                                        const int32_t* __restrict__ pk0, const float* __restrict__ pd0,
+                                                        int32_t* __restrict__ k1, float* __restrict__ d1,
+                                                        int32_t* __restrict__ pk1, float* __restrict__ pd1) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < N; s += (int64_t)gridDim.x * blockDim.x) {
+    int64_t i = perm[s];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      k1[c * Npad + s] = k0[c * Npad + i];
+      d1[c * Npad + s] = d0[c * Npad + i];
+      pk1[c * Npad + s] = pk0[c * Npad + i];
+      pd1[c * Npad + s] = pd0[c * Npad + i];
+    }
+  }
+}
+
+}  // namespace
+
+int grid_for(const Ctx& c, int64_t n, int threads, int per_sm) {
+  int64_t want = (n + threads - 1) / threads;
+  int64_t cap = (int64_t)c.num_sms * per_sm;
+  return (int)std::max<int64_t>(1, std::min(want, cap));
+}
+
+void launch_sort(Ctx& c) {
+  const int64_t N = c.N;
+  const int nk = c.fine.nk, n = c.fine.n;
+  Particles& P = c.part[c.cur];
+  Particles& Q = c.part[c.cur ^ 1];
+  VLB_CUDA(cudaMemsetAsync(c.counts, 0, sizeof(int32_t) * c.ncell, c.stream));
+  VLB_CUDA(cudaMemsetAsync(c.scan_status, 0, c.scan_status_size * sizeof(unsigned long long), c.stream));
+  VLB_CUDA(cudaMemsetAsync(c.dsc->scan_tiles, 0, sizeof(c.dsc->scan_tiles), c.stream));
+  k_keys_hist<<<grid_for(c, N, 256, 8), 256, 0, c.stream>>>(N, c.Npad, P.k, nk, c.keys, c.counts);
+  VLB_LAUNCHED(c);
+  // cell offsets, then the occupied list and its bounds
+  scan(c, ScanInCounts{c.counts}, ScanOutOffsets{c.cell_off}, c.ncell, 0, nullptr);
+  scan(c, ScanInOccupied{c.counts}, ScanOutOccupied{c.occupied, c.bounds, c.cell_off, c.ncell, N}, c.ncell, 1,
+       &c.dsc->noccupied);
+  // radix passes over the key bits
+  int bits = 1;
+  while ((1ll << bits) < (long long)c.ncell) ++bits;
+  int passes = (bits + kMaxDigitBits - 1) / kMaxDigitBits;
+  if (passes > 3) throw ArgError("too many cells for the radix sort");
+  const int64_t ntiles = (N + kRadixTile - 1) / kRadixTile;
+  int shift = 0;
+  const uint32_t* kin = c.keys;
+  const uint32_t* vin = nullptr;
+  for (int p = 0; p < passes; ++p) {
+    int b = (bits - shift + (passes - p) - 1) / (passes - p);  // spread the bits evenly
+    uint32_t mask = (1u << b) - 1u;
+    bool last = p == passes - 1;
+    uint32_t* kout = last ? c.skeys : (p % 2 == 0 ? c.keys_alt : c.keys);
+    uint32_t* vout = ((passes - 1 - p) % 2 == 0) ? c.perm : c.vals_alt;
+    k_radix_upsweep<<<(unsigned)ntiles, kRadixThreads, 0, c.stream>>>(kin, N, shift, mask, c.radix_table, ntiles);
+    VLB_LAUNCHED(c);
+    scan(c, ScanInArray{c.radix_table}, ScanOutArray{c.radix_table}, (int64_t)(mask + 1) * ntiles, 2 + p, nullptr);
+    k_radix_downsweep<<<(unsigned)ntiles, kRadixThreads, 0, c.stream>>>(kin, vin, kout, vout, N, shift, mask,
+                                                                        c.radix_table, ntiles);
+    VLB_LAUNCHED(c);
+    kin = kout;
+    vin = vout;
+    shift += b;
+  }
+  k_gather_records<<<grid_for(c, N, 256, 16), 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
+                                                                   Q.pk, Q.pd);
+  VLB_LAUNCHED(c);
+  c.cur ^= 1;
+  // out-of-stencil slots, in increasing order
+  scan(c, ScanInOutside{c.skeys, nk, n}, ScanOutOutside{c.outlist}, N, 5, &c.dsc->outcount);
+  c.sorted = true;
+}
+
+}  // namespace vlb

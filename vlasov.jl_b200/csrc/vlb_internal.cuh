@@ -1,0 +1,248 @@
+// Internal declarations of the B200 library: the context, the device scalar
+// block, and the launch wrappers each kernel file exports.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/vlasov_b200.h"
+
+namespace vlb {
+
+constexpr int kWarp = 32;
+constexpr int kNumStages = 12;
+
+// Error flags raised by kernels into DeviceScalars::status.
+constexpr int kStatusScanTimeout = 1;   // decoupled look-back gave up
+constexpr int kStatusBadCell = 2;       // a particle outside the CIC domain table
+constexpr int kStatusOverflow = 4;      // fixed-point accumulator out of range
+
+// Device-resident scalars of one step.  One block, zeroed (partly) at the
+// start of a step and copied back in one transfer at its end.
+struct DeviceScalars {
+  // --- reset every step (everything up to `reset_end`) ---
+  unsigned long long work_deposit;   // dynamic work counters
+  unsigned long long work_gather;
+  unsigned long long scan_tiles[8];  // tile tickets of the look-back scans
+  int32_t nout;                      // deposit window rejections
+  int32_t outcount;                  // out-of-stencil slots
+  int32_t noccupied;
+  int32_t status;
+  double red[4];                     // projectile sums (gaussian kernel)
+  double diag[5];                    // kinetic, escaped, angular xyz
+  double moments[10];                // multipole sums (coarse)
+  double charge_raw;                 // fine charge before renormalisation
+  unsigned long long enclosed;       // particles within the capture radius
+  int32_t reset_end;
+  int32_t pad0;
+  // --- persistent ---
+  double multipole[10];              // q, centre xyz, quadrupole (xx yy zz xy xz yz)
+  double proj_pos[3], proj_prev[3], proj_vel[3], proj_force[3];
+  double proj_charge, proj_mass, proj_sigma, proj_ball;
+  int32_t proj_active;
+  int32_t pad1;
+  double e_el, e_jel;
+};
+
+struct Level {
+  int nk = 0, n = 0, ni = 0;        // knots, points, interior points per axis
+  int npad = 0, nipad = 0;          // padded row counts of the transposed matrices
+  // float32 tables
+  float* colloc = nullptr;          // [n]
+  float* knots = nullptr;           // [nk]
+  float* sinvT = nullptr;           // [n][npad]  (S^-1)^T, zero padded
+  float* MT = nullptr;              // [ni][nipad]
+  float* MinvT = nullptr;           // [ni][nipad]
+  float* lap = nullptr;             // [n*n] row-major
+  float* invlsum = nullptr;         // [ni^3]
+  float* dual = nullptr;            // [3n]
+  float* dlen = nullptr;            // [n]
+  double* dual_d = nullptr;         // [3n] float64 copy for the reductions
+  double* knots_d = nullptr;        // [nk] float64 copy for the host-tail field
+  int32_t* loc_cells = nullptr;     // [loc_ncell]
+  int loc_ncell = 0;
+  float loc_x0 = 0, loc_invw = 0;
+  // grids
+  float* rho = nullptr;
+  float* phi = nullptr;
+  float* csol = nullptr;
+  float* csol_hartree = nullptr;    // coarse only: S^-1 phi before the mean field
+  // host copies kept for reference
+  std::vector<double> h_knots, h_colloc;
+};
+
+struct Particles {
+  int32_t* k = nullptr;   // [3*Npad]
+  float* d = nullptr;
+  int32_t* pk = nullptr;
+  float* pd = nullptr;
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  int64_t N = 0, Npad = 0;
+  double weight = 0;
+  Level fine, coarse;
+  // fine-axis constants as the reference's kernels see them (Float32)
+  double x0 = 0, h = 0;
+  float x0f = 0, hf = 0, spacing_f = 0, lo_f = 0, hi_f = 0;
+  int nbdt = 0, ncol = 0;
+  float* overlap = nullptr;   // [ncol][10]
+  float* gradient = nullptr;  // [ncol][10]
+  float* nodes = nullptr;     // [ncol][8]
+  // particle state, double buffered for the sort
+  Particles part[2];
+  int cur = 0;
+  float* force = nullptr;     // [3*Npad] SoA
+  // sort
+  int ncell = 0;
+  uint32_t* keys = nullptr;      // [N] unsorted cell keys
+  uint32_t* keys_alt = nullptr;  // [N]
+  uint32_t* skeys = nullptr;     // [N] sorted cell keys (slot order)
+  uint32_t* perm = nullptr;      // [N]
+  uint32_t* vals_alt = nullptr;  // [N]
+  uint32_t* radix_table = nullptr;
+  int64_t radix_table_size = 0;
+  int32_t* counts = nullptr;     // [ncell]
+  int32_t* cell_off = nullptr;   // [ncell]
+  int32_t* occupied = nullptr;   // [ncell]
+  int32_t* bounds = nullptr;     // [ncell+1]
+  int32_t* outlist = nullptr;    // [N]
+  unsigned long long* scan_status = nullptr;  // look-back tile states
+  int64_t scan_status_size = 0;
+  // deposit
+  unsigned long long* rho_fixed = nullptr;    // [n^3] int64 accumulator
+  double* partials = nullptr;                 // [10 * n^2] reductions
+  // Poisson work buffers (max n^3)
+  float* work[3] = {nullptr, nullptr, nullptr};
+  // scalars
+  DeviceScalars* dsc = nullptr;
+  DeviceScalars* hsc = nullptr;  // pinned, results
+  DeviceScalars* hin = nullptr;  // pinned, projectile staging
+  // state
+  bool sorted = false, have_forces = false;
+  // profiling
+  bool profile = false;
+  cudaEvent_t ev[kNumStages + 1];
+  bool evs_made = false;
+  double stage_ms[kNumStages] = {0};
+  long long launches = 0;
+  // graphs of the fused step, one per parity of the sort's double buffer
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  vlb_step_params graph_params{};
+  bool graph_valid = false;
+  long long graph_launches = 0;  // kernels in one captured step
+};
+
+std::string cuda_msg(cudaError_t e, const char* what);
+int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
+
+// ---------------------------------------------------------------- kernels
+// sort.cu
+void launch_sort(Ctx& c);
+// deposit.cu
+void launch_deposit_fine(Ctx& c, double charge, int mode);
+void launch_deposit_coarse(Ctx& c, double charge);
+// poisson.cu
+void launch_poisson(Ctx& c);
+void launch_coefficients(Ctx& c, Level& L, const float* src, float* dst);
+void launch_mean_field_coefficients(Ctx& c, Level& L, const float* phi, float* csol,
+                                    double nions, double radius);
+void launch_mean_field_add(Ctx& c, Level& L, double nions, double radius);
+// gather.cu
+void launch_forces(Ctx& c);
+// push.cu
+void launch_projectile_update(Ctx& c, double dt, double nions, double jradius, int advance);
+void launch_projectile_force_only(Ctx& c, double nions, double jradius);
+void launch_push(Ctx& c, double dt, double rcmax);
+void launch_enclosed(Ctx& c, double radius);
+
+
+}  // namespace vlb
+
+// Count and check a launch.
+#define VLB_LAUNCHED(c)                                                  \
+  do {                                                                   \
+    (c).launches++;                                                      \
+    cudaError_t _e = cudaGetLastError();                                 \
+    if (_e != cudaSuccess) throw vlb::CudaError(_e, __FILE__, __LINE__); \
+  } while (0)
+
+namespace vlb {
+struct CudaError {
+  cudaError_t err;
+  const char* file;
+  int line;
+  CudaError(cudaError_t e, const char* f, int l) : err(e), file(f), line(l) {}
+};
+struct ArgError {
+  std::string msg;
+  explicit ArgError(std::string m) : msg(std::move(m)) {}
+};
+}  // namespace vlb
+
+#define VLB_CUDA(x)                                                   \
+  do {                                                                \
+    cudaError_t _e = (x);                                             \
+    if (_e != cudaSuccess) throw vlb::CudaError(_e, __FILE__, __LINE__); \
+  } while (0)
+
+// ------------------------------------------------------ device helpers
+// IEEE single-precision operations without contraction: the reference's
+// kernels compute their discrete choices (columns, cells, Verlet updates)
+// with separately rounded Float32 operations.
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+
+// table column of an offset (src/kernels.jl:414-419, 770-772)
+__device__ __forceinline__ int table_column(float d, float spacing, int nbdt, int ncol) {
+  float half = fmul(spacing, 0.5f);
+  float v = fadd(fmul(fdiv(fadd(d, half), spacing), (float)nbdt), 0.5f);
+  int c = (int)floorf(v) + 1;
+  return min(max(c, 1), ncol);
+}
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+// 0-based cell of a clamped knot triple
+__device__ __forceinline__ uint32_t cell_key(int kx, int ky, int kz, int nk) {
+  kx = clampi(kx, 1, nk);
+  ky = clampi(ky, 1, nk);
+  kz = clampi(kz, 1, nk);
+  return (uint32_t)((kx - 1) + nk * ((ky - 1) + nk * (kz - 1)));
+}
+
+__device__ __forceinline__ void cell_knots(uint32_t cell, int nk, int& kx, int& ky, int& kz) {
+  kx = (int)(cell % nk) + 1;
+  cell /= nk;
+  ky = (int)(cell % nk) + 1;
+  kz = (int)(cell / nk) + 1;
+}
+
+// 10^3 stencil of the field fits (src/kernels.jl:375-377)
+__device__ __forceinline__ bool field_fits(int kx, int ky, int kz, int n) {
+  int bx = 2 * kx - 5, by = 2 * ky - 5, bz = 2 * kz - 5;
+  return bx >= 1 && by >= 1 && bz >= 1 && bx + 9 <= n && by + 9 <= n && bz + 9 <= n;
+}
+// 8^3 stencil of the deposit fits (src/kernels.jl:106-117)
+__device__ __forceinline__ bool deposit_fits(int kx, int ky, int kz, int n) {
+  int bx = 2 * kx - 5, by = 2 * ky - 5, bz = 2 * kz - 5;
+  return bx >= 0 && by >= 0 && bz >= 0 && bx + 8 <= n && by + 8 <= n && bz + 8 <= n;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
