@@ -1,0 +1,339 @@
+"""Benchmark of the per-step pseudo-particle loop: the Na196 + Xe25+ (500 keV,
+b = 45 a0) collision with 8e6 pseudo-particles on the 130^3 fine grid, one
+fused step (sort, fine + coarse deposit, nested Poisson, mean field, smoothed
+gather with the projectile, packed Verlet push) per iteration.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).  `value` is ms/step measured with CUDA events
+on the library's stream, inputs resident in HBM (the particle state, 2 x 384 MB,
+is larger than L2).  `e2e` is the same metric through the public API with the
+cloud uploaded from and downloaded to pinned host memory inside the timed
+region.  `--impl reference` times the CPU restatement of the reference's own
+CPU path (the oracle) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+MEASURED = ROOT / "MEASURED_PEAKS.json"
+GATHER_FLOP_PER_PARTICLE = 4600.0       # 2000 FMA + 300 mul/FMA per 10^3 contraction
+PUSH_BYTES_PER_PARTICLE = 48 + 12 + 48  # read (k, d, pk, pd) + force, write the record
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--npart", type=int, default=8_000_000)
+    ap.add_argument("--nfine", type=int, default=64)
+    ap.add_argument("--profile", default="thomas-fermi", choices=["thomas-fermi", "uniform-sphere"])
+    ap.add_argument("--deposit", default="float32", choices=["float32", "fixed64"])
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+def load():
+    from __graft_entry__ import load as _load
+    return _load()
+
+
+def workload(args, vb):
+    ninner, nouter = vb.grids(args.nfine)
+    p = vb.SimulationParameters(nfine=args.nfine, ninner=ninner, nouter=nouter, rcluster=78.0, rbox=235.0,
+                                nions=196.0, nelectrons=196.0, nparticles=args.npart, nsteps=0, dt=0.5)
+    prof = vb.thomas_fermi_profile() if args.profile == "thomas-fermi" else vb.uniform_sphere_profile()
+    proj = vb.xenon_projectile(v=0.40, impact=45.0, x0=-70.0, dt=0.5)
+    return p, prof, proj
+
+
+def config_dict(args, n):
+    return {"workload": "Na196 + Xe25+ 500 keV b=45 a0 collision, one fused step",
+            "npart_per_gpu": args.npart, "fine_grid": f"{2 * args.nfine + 2}^3", "coarse_grid": f"{2 * args.nfine + 2}^3",
+            "profile": args.profile, "deposit": args.deposit, "dt": 0.5, "projectile": "Xe25+ v=0.40 x0=-70 b=45",
+            "cuda_graph": not args.no_graph, "l2": "inputs larger than L2 (2 x 384 MB particle state)",
+            "parallelism": f"replicas{n}" if n > 1 else "1 GPU"}
+
+
+class ClockSampler:
+    """SM clock and throttle reasons through NVML, sampled every 20 ms."""
+
+    def __init__(self, index):
+        self.samples = []
+        self.stop_flag = False
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.max_mhz = None
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_flag:
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((time.time(), mhz, reasons))
+            except Exception:
+                pass
+            time.sleep(0.02)
+
+    def start(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+
+    def stop(self):
+        self.stop_flag = True
+        if self.ok:
+            self.t.join()
+
+    def summary(self, t0, t1):
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        inside = [s for s in self.samples if t0 <= s[0] <= t1] or self.samples[-3:]
+        nv = self.nv
+        names = {
+            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
+            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+            "hw_power_brake_slowdown": getattr(nv, "nvmlClocksEventReasonHwPowerBrakeSlowdown", 0x80),
+        }
+        seen = sorted({n for _, _, r in inside for n, bit in names.items() if r & bit})
+        return {"sm_mhz": statistics.median(m for _, m, _ in inside) if inside else None,
+                "sm_max_mhz": self.max_mhz, "reasons": seen, "samples": len(inside)}
+
+
+def peaks():
+    try:
+        return json.loads(MEASURED.read_text()), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline(args, vb, nthreads=None):
+    """The oracle's restatement of the reference CPU step, timed on the host
+    cores.  Sample: `cpu_steps` full steps of the same workload."""
+    from oracle import oracle as orc
+    p, prof, proj = workload(args, vb)
+    meshes = vb.build_meshes(p.nfine, p.ninner, p.nouter, p.rcluster, p.rbox)
+    sm = vb.gaussian_smoothing(meshes.fine.axis)
+    w = p.nelectrons / p.nparticles
+    pos, mom = vb.sample_thomas_fermi(prof, p.nparticles, w)
+    jel = vb.Jellium.of(p.nions)
+    if nthreads:
+        orc.lib().orc_set_threads(nthreads)
+    cores = orc.lib().orc_num_threads()
+    st = orc.HostStep(meshes, sm, w, jel, p.dt, p.rcmax, proj)
+    prev = pos - p.dt * mom / w  # a step back at constant velocity (timing sample only)
+    st.step(pos, prev)           # untimed warm-up of the buffers
+    t0 = time.perf_counter()
+    for _ in range(args.cpu_steps):
+        pos, prev, _ = st.step(pos, prev)
+    dt = (time.perf_counter() - t0) / args.cpu_steps
+    return dt * 1e3, cores
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    vb = load()
+    ms, cores = None, None
+    from oracle import oracle as orc
+    p, prof, proj = workload(args, vb)
+    meshes = vb.build_meshes(p.nfine, p.ninner, p.nouter, p.rcluster, p.rbox)
+    sm = vb.gaussian_smoothing(meshes.fine.axis)
+    w = p.nelectrons / p.nparticles
+    pos, mom = vb.sample_thomas_fermi(prof, p.nparticles, w)
+    jel = vb.Jellium.of(p.nions)
+    cores = orc.lib().orc_num_threads()
+    st = orc.HostStep(meshes, sm, w, jel, p.dt, p.rcmax, proj)
+    # priming as the reference CPU path does it (src/simulation.jl:233-277)
+    half = pos - (p.dt / (2 * w)) * mom
+    force, _ = st.update_forces(half, advance=False)
+    prev = -pos + 2 * half + (p.dt / w) * force
+    for _ in range(args.warmup):
+        pos, prev, _ = st.step(pos, prev)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pos, prev, _ = st.step(pos, prev)
+    ms = (time.perf_counter() - t0) / args.steps * 1e3
+    line = {"metric": "ms/step at 8M particles, 130^3 grid", "value": ms, "unit": "ms/step", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ran2 Thomas-Fermi cloud)",
+            "config": config_dict(args, 1), "impl": "reference",
+            "cpu_baseline": {"value": ms, "unit": "ms/step", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full CPU steps of the workload (float64 restatement of the "
+                                       "reference CPU path, OpenMP contiguous chunks)"},
+            "e2e": {"value": ms, "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    vb = load()
+    L = vb._lib
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    p, prof, proj = workload(args, vb)
+    sim = vb.Simulation(p, prof, projectile=proj, device=local, fixed_point=args.deposit == "fixed64",
+                        use_graph=not args.no_graph, seed=-1 - rank)
+    acc = sim.accelerator
+    ext = torch.cuda.ExternalStream(acc.stream_handle(), device=torch.device("cuda", local))
+    for _ in range(max(args.warmup, 3)):
+        sim.step()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.1)
+    barrier()
+    launches0 = acc.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_wall0 = time.time()
+    e0.record(ext)
+    for _ in range(args.steps):
+        d = sim.step()
+    e1.record(ext)
+    e1.synchronize()
+    t_wall1 = time.time()
+    barrier()
+    launches = acc.launch_count() - launches0
+    ms = e0.elapsed_time(e1) / args.steps
+    clocks.stop()
+    ms = max_over_ranks(ms)
+    clk = clocks.summary(t_wall0, t_wall1)
+
+    # per-stage device times (eager, stage events) for the roofline
+    sim.use_graph = False
+    acc.profile(True)
+    nprof = max(3, min(args.steps, 20))
+    for _ in range(nprof):
+        sim.step()
+    stages = {k: v / nprof for k, v in acc.stage_times().items()}
+    acc.profile(False)
+    sim.use_graph = not args.no_graph
+
+    # end to end through the public API: cloud from pinned host memory, K
+    # steps, cloud back to pinned host memory
+    k, dd, pk, pd = acc.download()
+    pins = [torch.from_numpy(a).pin_memory() for a in (k, dd, pk, pd)]
+    hk, hd, hpk, hpd = (t.numpy() for t in pins)
+    outs = [torch.empty_like(t).pin_memory() for t in pins]
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(ext)
+    acc.upload(hk, hd, hpk, hpd)
+    for _ in range(args.steps):
+        sim.step()
+    L.check(L.lib().vlb_download_particles(acc.handle, L.pi(outs[0].numpy()), L.pf(outs[1].numpy()),
+                                           L.pi(outs[2].numpy()), L.pf(outs[3].numpy())))
+    f1.record(ext)
+    f1.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps)
+    cloud_bytes = 48 * args.npart
+    step_h2d = 112  # vlb_projectile in
+    step_d2h = 480  # the step's scalar block out
+
+    pk_, how = peaks()
+    fp32_peak = vb._lib.C.c_double()
+    L.check(L.lib().vlb_fp32_peak(local, vb._lib.C.byref(fp32_peak)))
+    t_forces = stages.get("forces", float("nan"))
+    achieved = GATHER_FLOP_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e12
+    t_push = stages.get("push", float("nan"))
+    push_gbs = PUSH_BYTES_PER_PARTICLE * args.npart / (t_push * 1e-3) / 1e9
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        try:
+            cms, cores = cpu_baseline(args, vb)
+            cpu = {"value": cms, "unit": "ms/step", "cores": cores, "kind": "port",
+                   "sample": f"{args.cpu_steps} full CPU steps of the same workload (float64 restatement of the "
+                             "reference CPU path, OpenMP)"}
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "ms/step", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
+    line = {
+        "metric": "ms/step at 8M particles, 130^3 grid", "value": ms, "unit": "ms/step", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded ran2 sample of the reference's Na196 Thomas-Fermi profile)",
+        "config": config_dict(args, world),
+        "particle_steps_per_s": args.npart * world / (ms * 1e-3),
+        "e2e": {"value": e2e_ms, "unit": "ms/step",
+                "h2d_bytes_per_step": step_h2d + cloud_bytes / args.steps,
+                "d2h_bytes_per_step": step_d2h + cloud_bytes / args.steps},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "k_field (smoothed gather + projectile), forces stage", "bound": "fp32",
+                     "achieved": achieved, "peak": fp32_peak.value, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak.value, "traffic": None,
+                     "peak_source": "measured FP32 FMA kernel (vlb_fp32_peak), this GPU, this run"},
+        "roofline_hbm": {"kernel": "k_push (packed Verlet)", "bound": "hbm", "achieved": push_gbs,
+                         "peak": pk_.get("hbm_gbs"), "unit": "GB/s", "frac": push_gbs / pk_.get("hbm_gbs", 1),
+                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({how})"},
+        "stages_ms": stages,
+        "clocks": clk,
+        "last_step": {"q8": d.enclosed_charge, "outcount": d.outcount, "noccupied": d.noccupied},
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    acc.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -242,6 +242,10 @@ VLB_API const char* vlb_stage_name(int32_t i);
 VLB_API int vlb_stage_times(vlb_ctx* ctx, double* ms, int32_t n);
 /* Kernel launches issued by this context so far. */
 VLB_API int vlb_launch_count(vlb_ctx* ctx, int64_t* count);
+/* FP32 FMA throughput of the device at its current clocks (TFLOP/s), the
+ * ceiling the FP32-bound kernels (gather, fine deposit) are measured against.
+ * No counterpart in the reference: a measurement helper. */
+VLB_API int vlb_fp32_peak(int32_t device, double* tflops);
 /* The context's CUDA stream (cudaStream_t), for event timing by a caller. */
 VLB_API int vlb_stream(vlb_ctx* ctx, void** stream);
 

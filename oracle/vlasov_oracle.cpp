@@ -169,15 +169,31 @@ bool spline_field(const double* g, int nk, const double* c, int n,
 
 // ------------------------------------------------------------ tensor chain
 // dest[p + m i'] = sum_i A[i'][i] src[i + n p]   (src/tensorsolver.jl:217-223)
+// Blocked over 16 columns p so that each output row segment is contiguous
+// (the reference does it as one BLAS GEMM, C = X^T A^T).
 void mode_product(double* dest, const double* A, const double* src, int n, size_t m) {
-#pragma omp parallel for schedule(static)
-  for (long long p = 0; p < (long long)m; ++p) {
-    const double* x = src + (size_t)n * p;
-    for (int r = 0; r < n; ++r) {
-      const double* a = A + (size_t)r * n;
-      double s = 0;
-      for (int i = 0; i < n; ++i) s += a[i] * x[i];
-      dest[p + m * r] = s;
+  constexpr int PB = 16;
+  const long long nblk = (long long)((m + PB - 1) / PB);
+#pragma omp parallel
+  {
+    std::vector<double> xt((size_t)n * PB);
+#pragma omp for schedule(static)
+    for (long long b = 0; b < nblk; ++b) {
+      const size_t p0 = (size_t)b * PB;
+      const int cnt = (int)std::min<size_t>(PB, m - p0);
+      for (int pp = 0; pp < PB; ++pp)
+        for (int i = 0; i < n; ++i) xt[(size_t)i * PB + pp] = pp < cnt ? src[(p0 + pp) * n + i] : 0.0;
+      for (int r = 0; r < n; ++r) {
+        const double* a = A + (size_t)r * n;
+        double acc[PB] = {0};
+        for (int i = 0; i < n; ++i) {
+          const double ai = a[i];
+          const double* x = &xt[(size_t)i * PB];
+          for (int pp = 0; pp < PB; ++pp) acc[pp] += ai * x[pp];
+        }
+        double* out = dest + p0 + m * r;
+        for (int pp = 0; pp < cnt; ++pp) out[pp] = acc[pp];
+      }
     }
   }
 }

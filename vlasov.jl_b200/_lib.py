@@ -39,7 +39,7 @@ EXPORTS = (
     "vlb_poisson", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
     "vlb_push", "vlb_step", "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
     "vlb_enclosed_charge", "vlb_profile", "vlb_stage_count", "vlb_stage_name", "vlb_stage_times",
-    "vlb_launch_count", "vlb_stream", "vlb_sample_thomas_fermi", "vlb_ran2", "vlb_pack_positions",
+    "vlb_launch_count", "vlb_fp32_peak", "vlb_stream", "vlb_sample_thomas_fermi", "vlb_ran2", "vlb_pack_positions",
     "vlb_unpack_positions",
 )
 
@@ -132,6 +132,7 @@ def lib():
             "vlb_stage_times": (C.c_int, [vp, P_D, C.c_int32]),
             "vlb_launch_count": (C.c_int, [vp, C.POINTER(C.c_int64)]),
             "vlb_stream": (C.c_int, [vp, C.POINTER(vp)]),
+            "vlb_fp32_peak": (C.c_int, [C.c_int32, P_D]),
             "vlb_sample_thomas_fermi": (C.c_int, [P_D, C.c_int32, P_D, C.c_int32, C.c_double, C.c_int64,
                                                   C.c_double, C.c_int32, C.c_int32, P_D, P_D]),
             "vlb_ran2": (C.c_int, [C.c_int32, C.c_int32, C.c_int64, P_F]),

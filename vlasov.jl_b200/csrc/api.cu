@@ -12,6 +12,7 @@
 namespace vlb {
 
 void deposit_setup(Ctx& c);
+double measure_fp32_peak(int device);
 int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
 
 namespace {
@@ -163,7 +164,7 @@ void destroy_ctx(Ctx* c) {
   dfree(c->force);
   dfree(c->keys); dfree(c->keys_alt); dfree(c->skeys); dfree(c->perm); dfree(c->vals_alt);
   dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off); dfree(c->occupied); dfree(c->bounds);
-  dfree(c->outlist); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
+  dfree(c->outlist); dfree(c->chunk_start); dfree(c->item_cell); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
   for (auto& w : c->work) dfree(w);
   dfree(c->dsc);
   if (c->hsc) cudaFreeHost(c->hsc);
@@ -388,6 +389,8 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->occupied = dalloc<int32_t>(c->ncell);
     c->bounds = dalloc<int32_t>(c->ncell + 1);
     c->outlist = dalloc<int32_t>(N);
+    c->chunk_start = dalloc<int32_t>(c->ncell);
+    c->item_cell = dalloc<int32_t>(N / kChunk + c->ncell + 1);
     const int64_t scan_tiles = std::max<int64_t>({(N + 4095) / 4096, (c->ncell + 4095) / 4096,
                                                   (c->radix_table_size + 4095) / 4096}) + 1;
     c->scan_status_size = 8 * scan_tiles;
@@ -740,6 +743,14 @@ int vlb_launch_count(vlb_ctx* ctx, int64_t* count) {
   if (!count) return fail(VLB_ERR_ARG, "null output");
   *count = c.launches;
   return VLB_OK;
+}
+
+int vlb_fp32_peak(int32_t device, double* tflops) {
+  if (!tflops) return fail(VLB_ERR_ARG, "null output");
+  return guarded([&]() -> int {
+    *tflops = measure_fp32_peak(device);
+    return VLB_OK;
+  });
 }
 
 int vlb_stream(vlb_ctx* ctx, void** stream) {

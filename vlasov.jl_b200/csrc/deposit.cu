@@ -14,8 +14,9 @@
 //
 // Coarse grid (src/kernels.jl:1207-1273, src/devicemesh.jl:93-106):
 // trilinear cloud-in-cell on the stretched collocation points, each thread
-// walking a block of consecutive sorted particles into a private 4^3 window
-// of shared memory and flushing it once.
+// walking a block of consecutive sorted particles into a private window of
+// shared memory that is added to the grid once.  The cell lookup is the
+// reference's Float32 LocateTable walk.
 
 #include "vlb_internal.cuh"
 
@@ -174,93 +175,123 @@ __global__ void k_charge_scale(float* __restrict__ rho, const unsigned long long
 }
 
 // --------------------------------------------------------------- coarse
-constexpr int kCicBlock = 64;
-constexpr int kCicTile = 4;
-constexpr int kCicThreads = 128;
+constexpr int kCicThreads = 256;
+constexpr int kCicBlock = 64;   // consecutive sorted particles per thread
+constexpr int kCicT = 4;        // private window: 4^3 coarse points
+constexpr int kCicT3 = kCicT * kCicT * kCicT;
 
-// Cell of x on the stretched collocation points (src/kernels.jl:1069-1081),
-// Float32; 0 outside.  w is the weight of the left point.
-__device__ __forceinline__ int locate_cell(const float* __restrict__ gt, int ng, float lx0, float linvw,
-                                           const int32_t* __restrict__ cells, int ncells, float x, float& w) {
+// Cell of x on the stretched collocation points (src/kernels.jl:1069-1081):
+// the Float32 LocateTable walk, tables in shared memory; 0 outside.  w is the
+// weight of the left point, with the division replaced by the interval's
+// reciprocal.
+__device__ __forceinline__ int locate_cell(const float* __restrict__ gt, const float* __restrict__ igap, int ng,
+                                           float lx0, float linvw, const int32_t* __restrict__ cells, int ncells,
+                                           float x, float& w) {
   if (x < gt[0] || x > gt[ng - 1]) { w = 0.f; return 0; }
   int b = min((int)floorf(fmul(fsub(x, lx0), linvw)) + 1, ncells);
   int c = cells[b - 1];
   const int lastc = ng - 1;
   while (c < lastc && gt[c] < x) ++c;
-  w = fdiv(fsub(gt[c], x), fsub(gt[c], gt[c - 1]));
+  w = fsub(gt[c], x) * igap[c];
   return c;
 }
 
+// Each thread walks kCicBlock consecutive sorted particles -- a handful of
+// neighbouring fine cells -- into a private 4^3 window of shared memory
+// anchored one point before its first particle, and adds the window to the
+// grid once; particles that miss the window use global atomics (the
+// reference's design, src/kernels.jl:1083-1273).  Loads are 16-byte vectors of
+// four particles.  Contributions carry charge / (wx wy wz)
+// (src/devicemesh.jl:104).
 __global__ void __launch_bounds__(kCicThreads) k_deposit_cic(
     int64_t N, int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d,
-    const float* __restrict__ gt, int ng, float lx0, float linvw, const int32_t* __restrict__ cells, int ncells,
-    float x0f, float hf, float* rho, int64_t nblock) {
-  constexpr int T = kCicTile, T3 = T * T * T;
-  __shared__ float tile[T3 * kCicThreads];
+    const float* __restrict__ gt_g, int ng, float lx0, float linvw, const int32_t* __restrict__ cells_g, int ncells,
+    const float* __restrict__ dl_g, float x0f, float hf, float charge, float* rho, int64_t nblock) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  float* tile = reinterpret_cast<float*>(smem);                 // [kCicT3][kCicThreads]
+  float* gt = tile + kCicT3 * kCicThreads;                      // [ng]
+  float* igap = gt + ng;                                        // [ng] 1 / (gt[c] - gt[c-1])
+  float* idl = igap + ng;                                       // [ng] 1 / dual length
+  int32_t* cells = reinterpret_cast<int32_t*>(idl + ng);        // [ncells]
+  for (int e = threadIdx.x; e < ng; e += kCicThreads) {
+    gt[e] = gt_g[e];
+    igap[e] = e > 0 ? 1.f / (gt_g[e] - gt_g[e - 1]) : 0.f;
+    idl[e] = 1.f / dl_g[e];
+  }
+  for (int e = threadIdx.x; e < ncells; e += kCicThreads) cells[e] = cells_g[e];
+  __syncthreads();
   const int t = threadIdx.x;
-  const int n = ng;
-  for (int64_t blk = (int64_t)blockIdx.x * kCicThreads + t;; blk += (int64_t)gridDim.x * kCicThreads) {
-    // uniform trip count across the CTA is not needed: no barrier inside
-    if (blk >= nblock) break;
-#pragma unroll 4
-    for (int p = 0; p < T3; ++p) tile[p * kCicThreads + t] = 0.f;
+  const size_t n = ng, nn = n * n;
+  for (int64_t blk = (int64_t)blockIdx.x * kCicThreads + t; blk < nblock; blk += (int64_t)gridDim.x * kCicThreads) {
+#pragma unroll
+    for (int p = 0; p < kCicT3; ++p) tile[p * kCicThreads + t] = 0.f;
     const int64_t lo = blk * kCicBlock;
     const int64_t hi = min(lo + kCicBlock, N);
     int ox = 0, oy = 0, oz = 0;
     bool anchored = false;
-    for (int64_t i = lo; i < hi; ++i) {
-      const float px = fadd(fadd(x0f, fmul((float)(k[i] - 1), hf)), d[i]);
-      const float py = fadd(fadd(x0f, fmul((float)(k[Npad + i] - 1), hf)), d[Npad + i]);
-      const float pz = fadd(fadd(x0f, fmul((float)(k[2 * Npad + i] - 1), hf)), d[2 * Npad + i]);
-      float ax, ay, az;
-      const int ix = locate_cell(gt, ng, lx0, linvw, cells, ncells, px, ax);
-      const int iy = locate_cell(gt, ng, lx0, linvw, cells, ncells, py, ay);
-      const int iz = locate_cell(gt, ng, lx0, linvw, cells, ncells, pz, az);
-      if (!(ix > 0 && iy > 0 && iz > 0)) continue;
-      if (!anchored) { ox = ix - 2; oy = iy - 2; oz = iz - 2; anchored = true; }
-      const float bx = 1.f - ax, by = 1.f - ay, bz = 1.f - az;
-      const int dx = ix - ox, dy = iy - oy, dz = iz - oz;
-      if (dx >= 1 && dx <= T - 1 && dy >= 1 && dy <= T - 1 && dz >= 1 && dz <= T - 1) {
-        const int b = (dz - 1) * T * T + (dy - 1) * T + (dx - 1);
-        tile[(b)*kCicThreads + t] += ax * ay * az;
-        tile[(b + T * T) * kCicThreads + t] += ax * ay * bz;
-        tile[(b + T) * kCicThreads + t] += ax * by * az;
-        tile[(b + T + T * T) * kCicThreads + t] += ax * by * bz;
-        tile[(b + 1) * kCicThreads + t] += bx * ay * az;
-        tile[(b + 1 + T * T) * kCicThreads + t] += bx * ay * bz;
-        tile[(b + 1 + T) * kCicThreads + t] += bx * by * az;
-        tile[(b + 1 + T + T * T) * kCicThreads + t] += bx * by * bz;
-      } else {
-        const size_t i0 = (size_t)(ix - 1) + (size_t)n * ((iy - 1) + (size_t)n * (iz - 1));
-        const size_t sj = n, sk = (size_t)n * n;
-        atomicAdd(&rho[i0], ax * ay * az);
-        atomicAdd(&rho[i0 + sk], ax * ay * bz);
-        atomicAdd(&rho[i0 + sj], ax * by * az);
-        atomicAdd(&rho[i0 + sj + sk], ax * by * bz);
-        atomicAdd(&rho[i0 + 1], bx * ay * az);
-        atomicAdd(&rho[i0 + 1 + sk], bx * ay * bz);
-        atomicAdd(&rho[i0 + 1 + sj], bx * by * az);
-        atomicAdd(&rho[i0 + 1 + sj + sk], bx * by * bz);
+    for (int64_t q = lo; q < hi; q += 4) {
+      // four particles per 16-byte load; Npad and lo are multiples of 4
+      const int4 kx4 = *reinterpret_cast<const int4*>(k + q);
+      const int4 ky4 = *reinterpret_cast<const int4*>(k + Npad + q);
+      const int4 kz4 = *reinterpret_cast<const int4*>(k + 2 * Npad + q);
+      const float4 dx4 = *reinterpret_cast<const float4*>(d + q);
+      const float4 dy4 = *reinterpret_cast<const float4*>(d + Npad + q);
+      const float4 dz4 = *reinterpret_cast<const float4*>(d + 2 * Npad + q);
+      const int kxs[4] = {kx4.x, kx4.y, kx4.z, kx4.w}, kys[4] = {ky4.x, ky4.y, ky4.z, ky4.w},
+                kzs[4] = {kz4.x, kz4.y, kz4.z, kz4.w};
+      const float dxs[4] = {dx4.x, dx4.y, dx4.z, dx4.w}, dys[4] = {dy4.x, dy4.y, dy4.z, dy4.w},
+                  dzs[4] = {dz4.x, dz4.y, dz4.z, dz4.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (q + u >= hi) break;
+        const float px = fadd(fadd(x0f, fmul((float)(kxs[u] - 1), hf)), dxs[u]);
+        const float py = fadd(fadd(x0f, fmul((float)(kys[u] - 1), hf)), dys[u]);
+        const float pz = fadd(fadd(x0f, fmul((float)(kzs[u] - 1), hf)), dzs[u]);
+        float ax, ay, az;
+        const int ix = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, px, ax);
+        const int iy = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, py, ay);
+        const int iz = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, pz, az);
+        if (!(ix > 0 && iy > 0 && iz > 0)) continue;
+        const int i0 = ix - 1, j0 = iy - 1, k0 = iz - 1;  // 0-based left points
+        if (!anchored) { ox = i0 - 1; oy = j0 - 1; oz = k0 - 1; anchored = true; }
+        const float wx0 = ax * idl[i0], wx1 = (1.f - ax) * idl[i0 + 1];
+        const float wy0 = ay * idl[j0], wy1 = (1.f - ay) * idl[j0 + 1];
+        const float wz0 = charge * az * idl[k0], wz1 = charge * (1.f - az) * idl[k0 + 1];
+        const int lx = i0 - ox, ly = j0 - oy, lz = k0 - oz;
+        if (lx >= 0 && ly >= 0 && lz >= 0 && lx + 1 < kCicT && ly + 1 < kCicT && lz + 1 < kCicT) {
+          float* b = tile + (lx + kCicT * (ly + kCicT * lz)) * kCicThreads + t;
+          constexpr int SY = kCicT * kCicThreads, SZ = kCicT * kCicT * kCicThreads, SX = kCicThreads;
+          b[0] += wx0 * wy0 * wz0;
+          b[SZ] += wx0 * wy0 * wz1;
+          b[SY] += wx0 * wy1 * wz0;
+          b[SY + SZ] += wx0 * wy1 * wz1;
+          b[SX] += wx1 * wy0 * wz0;
+          b[SX + SZ] += wx1 * wy0 * wz1;
+          b[SX + SY] += wx1 * wy1 * wz0;
+          b[SX + SY + SZ] += wx1 * wy1 * wz1;
+        } else {
+          float* b = rho + (size_t)i0 + n * j0 + nn * k0;
+          atomicAdd(b, wx0 * wy0 * wz0);
+          atomicAdd(b + nn, wx0 * wy0 * wz1);
+          atomicAdd(b + n, wx0 * wy1 * wz0);
+          atomicAdd(b + n + nn, wx0 * wy1 * wz1);
+          atomicAdd(b + 1, wx1 * wy0 * wz0);
+          atomicAdd(b + 1 + nn, wx1 * wy0 * wz1);
+          atomicAdd(b + 1 + n, wx1 * wy1 * wz0);
+          atomicAdd(b + 1 + n + nn, wx1 * wy1 * wz1);
+        }
       }
     }
     if (anchored) {
-      for (int dz = 0; dz < T; ++dz)
-        for (int dy = 0; dy < T; ++dy)
-          for (int dx = 0; dx < T; ++dx) {
-            const float v = tile[(dz * T * T + dy * T + dx) * kCicThreads + t];
-            if (v != 0.f)
-              atomicAdd(&rho[(size_t)(ox + dx) + (size_t)n * ((oy + dy) + (size_t)n * (oz + dz))], v);
-          }
+#pragma unroll 4
+      for (int p = 0; p < kCicT3; ++p) {
+        const float v = tile[p * kCicThreads + t];
+        if (v != 0.f) {
+          const int lx = p % kCicT, ly = (p / kCicT) % kCicT, lz = p / (kCicT * kCicT);
+          atomicAdd(&rho[(size_t)(ox + lx) + n * (oy + ly) + nn * (oz + lz)], v);
+        }
+      }
     }
-  }
-}
-
-// rho[i,j,k] *= charge / (wx[i] wy[j] wz[k])   (src/devicemesh.jl:104)
-__global__ void k_cic_scale(float* __restrict__ rho, const float* __restrict__ dl, int n, float charge) {
-  const size_t tot = (size_t)n * n * n;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % n), j = (int)((t / n) % n), kq = (int)(t / ((size_t)n * n));
-    rho[t] = rho[t] * fdiv(charge, fmul(fmul(dl[i], dl[j]), dl[kq]));
   }
 }
 
@@ -270,9 +301,12 @@ size_t deposit_fine_smem(const Ctx& c) {
   return (size_t)c.ncol * 8 * sizeof(float) + 3 * kDepStage * sizeof(int) + (size_t)kDepLanes * 512 * sizeof(float);
 }
 
+size_t cic_smem(const Ctx& c);
+
 void deposit_setup(Ctx& c) {
   VLB_CUDA(cudaFuncSetAttribute(k_deposit_fine, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)deposit_fine_smem(c)));
+  VLB_CUDA(cudaFuncSetAttribute(k_deposit_cic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cic_smem(c)));
 }
 
 void launch_deposit_fine(Ctx& c, double charge, int mode) {
@@ -300,6 +334,11 @@ void launch_deposit_fine(Ctx& c, double charge, int mode) {
   VLB_LAUNCHED(c);
 }
 
+size_t cic_smem(const Ctx& c) {
+  return (size_t)kCicT3 * kCicThreads * sizeof(float) + 3 * (size_t)c.coarse.n * sizeof(float) +
+         (size_t)c.coarse.loc_ncell * sizeof(int32_t);
+}
+
 void launch_deposit_coarse(Ctx& c, double charge) {
   Level& C = c.coarse;
   const size_t tot = (size_t)C.n * C.n * C.n;
@@ -307,11 +346,10 @@ void launch_deposit_coarse(Ctx& c, double charge) {
   VLB_CUDA(cudaMemsetAsync(C.rho, 0, tot * sizeof(float), c.stream));
   const int64_t nblock = (c.N + kCicBlock - 1) / kCicBlock;
   const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nblock + kCicThreads - 1) / kCicThreads,
-                                                               (int64_t)c.num_sms * 4));
-  k_deposit_cic<<<grid, kCicThreads, 0, c.stream>>>(c.N, c.Npad, P.k, P.d, C.colloc, C.n, C.loc_x0, C.loc_invw,
-                                                    C.loc_cells, C.loc_ncell, c.x0f, c.hf, C.rho, nblock);
-  VLB_LAUNCHED(c);
-  k_cic_scale<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(C.rho, C.dlen, C.n, (float)charge);
+                                                               (int64_t)c.num_sms * 3));
+  k_deposit_cic<<<grid, kCicThreads, cic_smem(c), c.stream>>>(c.N, c.Npad, P.k, P.d, C.colloc, C.n, C.loc_x0,
+                                                              C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f,
+                                                              c.hf, (float)charge, C.rho, nblock);
   VLB_LAUNCHED(c);
 }
 

@@ -31,7 +31,7 @@ int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
 
 namespace {
 
-constexpr int kGThreads = 128;
+constexpr int kGThreads = 256;
 
 // src/projectile.jl:86-108, Float32
 __device__ __forceinline__ float gaussian_force_kernel(float r2, float sigma) {
@@ -108,71 +108,98 @@ __device__ __forceinline__ void block_add_red(float ax, float ay, float az, floa
   }
 }
 
-__global__ void __launch_bounds__(kGThreads, 4) k_field(
-    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds, DeviceScalars* dsc, int64_t Npad,
+// One warp per work item (at most kChunk particles of one occupied cell),
+// items taken from a dynamic counter.  The warp stages its cell's 10^3
+// stencil in its own slice of shared memory (kept while consecutive items
+// share the cell) and takes 32 particles at a time, one per lane.  No
+// barrier but __syncwarp.  The x and y columns live in registers; the z
+// loop is not unrolled and reads its two values per step from the table
+// (L1), which keeps the contraction's code small enough for the
+// instruction cache.
+constexpr int kRow = 12;            // padded stencil row (10 values, 16-byte aligned)
+constexpr int kTile = 10 * 10 * kRow;
+
+__global__ void __launch_bounds__(kGThreads) k_field(
+    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
+    const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int64_t Npad,
     const float* __restrict__ d, const float* __restrict__ csol, int n, int nk, const float* __restrict__ ov,
     const float* __restrict__ gr, int nbdt, int ncol, float spacing, float x0, float h, double w,
     float* __restrict__ force) {
-  __shared__ __align__(16) float tile[1000];
-  __shared__ int s_g;
-  const int tid = threadIdx.x;
-  const int nocc = dsc->noccupied;
+  __shared__ __align__(16) float tiles[kGThreads / 32][kTile];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  float* tile = tiles[wid];
+  const int nitems = dsc->nitems;
   const ProjF P = load_proj(dsc, w);
   const float wf = (float)w;
   float ax = 0.f, ay = 0.f, az = 0.f, ae = 0.f;
+  int cached = -1;
   for (;;) {
-    if (tid == 0) s_g = (int)atomicAdd(&dsc->work_gather, 1ull);
-    __syncthreads();
-    const int g = s_g;
-    if (g >= nocc) break;
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(&dsc->work_gather, 1ull);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nitems) break;
+    const int g = item_cell[item];
     int kx, ky, kz;
     cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
-    if (!field_fits(kx, ky, kz, n)) {  // the tail takes these
-      __syncthreads();
-      continue;
+    if (!field_fits(kx, ky, kz, n)) continue;  // the tail takes these
+    if (g != cached) {
+      __syncwarp();
+      const int bx = 2 * kx - 6, by = 2 * ky - 6, bz = 2 * kz - 6;  // 0-based stencil corner
+      for (int e = lane; e < 1000; e += 32) {
+        const int ii = e % 10, r = e / 10;  // r = jj + 10 kk
+        const int jj = r % 10, kk = r / 10;
+        tile[r * kRow + ii] = csol[(size_t)(bx + ii) + (size_t)n * ((by + jj) + (size_t)n * (bz + kk))];
+      }
+      cached = g;
+      __syncwarp();
     }
-    const int bx = 2 * kx - 6, by = 2 * ky - 6, bz = 2 * kz - 6;  // 0-based stencil corner
-    for (int e = tid; e < 1000; e += kGThreads) {
-      const int ii = e % 10, jj = (e / 10) % 10, kk = e / 100;
-      tile[e] = csol[(size_t)(bx + ii) + (size_t)n * ((by + jj) + (size_t)n * (bz + kk))];
-    }
-    __syncthreads();
-    const int sl = bounds[g], sh = bounds[g + 1];
-    for (int s = sl + tid; s < sh; s += kGThreads) {
+    const int s0 = bounds[g] + (item - chunk_start[g]) * kChunk;
+    const int s1 = min(s0 + kChunk, bounds[g + 1]);
+    for (int s = s0 + lane; s < s1; s += 32) {
       const float dx0 = d[s], dy0 = d[Npad + s], dz0 = d[2 * Npad + s];
       const int cx = table_column(dx0, spacing, nbdt, ncol);
       const int cy = table_column(dy0, spacing, nbdt, ncol);
       const int cz = table_column(dz0, spacing, nbdt, ncol);
-      float ox[10], gx[10], oy[10], gy[10], oz[10], gz[10];
-      load10(ov, cx, ox);
-      load10(gr, cx, gx);
+      // x columns as pairs of neighbouring stencil points, for the packed FMA
+      float2 ox2[5], gx2[5];
+      {
+        const float2* po = reinterpret_cast<const float2*>(ov + (size_t)(cx - 1) * 10);
+        const float2* pg = reinterpret_cast<const float2*>(gr + (size_t)(cx - 1) * 10);
+#pragma unroll
+        for (int a = 0; a < 5; ++a) { ox2[a] = __ldg(po + a); gx2[a] = __ldg(pg + a); }
+      }
+      float oy[10], gy[10];
       load10(ov, cy, oy);
       load10(gr, cy, gy);
-      load10(ov, cz, oz);
-      load10(gr, cz, gz);
+      const float* ozp = ov + (size_t)(cz - 1) * 10;
+      const float* gzp = gr + (size_t)(cz - 1) * 10;
       float sx = 0.f, sy = 0.f, sz = 0.f;
-#pragma unroll
+#pragma unroll 1
       for (int kk = 0; kk < 10; ++kk) {
+        const float oz = __ldg(ozp + kk), gz = __ldg(gzp + kk);
         float tx = 0.f, ty = 0.f, tz = 0.f;
+        const float* plane = tile + kk * 10 * kRow;
 #pragma unroll
         for (int jj = 0; jj < 10; ++jj) {
-          const float2* row = reinterpret_cast<const float2*>(tile + (jj + 10 * kk) * 10);
-          float dxp = 0.f, val = 0.f;
+          const float4 c0 = *reinterpret_cast<const float4*>(plane + jj * kRow);
+          const float4 c1 = *reinterpret_cast<const float4*>(plane + jj * kRow + 4);
+          const float2 c2 = *reinterpret_cast<const float2*>(plane + jj * kRow + 8);
+          const float2 cp[5] = {make_float2(c0.x, c0.y), make_float2(c0.z, c0.w), make_float2(c1.x, c1.y),
+                                make_float2(c1.z, c1.w), c2};
+          float2 dxp = make_float2(0.f, 0.f), val = make_float2(0.f, 0.f);
 #pragma unroll
           for (int a = 0; a < 5; ++a) {
-            const float2 c2 = row[a];
-            dxp = fmaf(c2.x, gx[2 * a], dxp);
-            val = fmaf(c2.x, ox[2 * a], val);
-            dxp = fmaf(c2.y, gx[2 * a + 1], dxp);
-            val = fmaf(c2.y, ox[2 * a + 1], val);
+            dxp = __ffma2_rn(cp[a], gx2[a], dxp);
+            val = __ffma2_rn(cp[a], ox2[a], val);
           }
-          tx = fmaf(oy[jj], dxp, tx);
-          ty = fmaf(gy[jj], val, ty);
-          tz = fmaf(oy[jj], val, tz);
+          const float dx1 = dxp.x + dxp.y, va1 = val.x + val.y;
+          tx = fmaf(oy[jj], dx1, tx);
+          ty = fmaf(gy[jj], va1, ty);
+          tz = fmaf(oy[jj], va1, tz);
         }
-        sx = fmaf(oz[kk], tx, sx);
-        sy = fmaf(oz[kk], ty, sy);
-        sz = fmaf(gz[kk], tz, sz);
+        sx = fmaf(oz, tx, sx);
+        sy = fmaf(oz, ty, sy);
+        sz = fmaf(gz, tz, sz);
       }
       float fx = -wf * sx, fy = -wf * sy, fz = -wf * sz;
       if (P.on) {
@@ -190,7 +217,6 @@ __global__ void __launch_bounds__(kGThreads, 4) k_field(
       force[Npad + s] = fy;
       force[2 * Npad + s] = fz;
     }
-    __syncthreads();
   }
   block_add_red(ax, ay, az, ae, dsc->red);
 }
@@ -306,11 +332,12 @@ void launch_forces(Ctx& c) {
   Particles& P = c.part[c.cur];
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_gather, 0, sizeof(unsigned long long), c.stream));
   VLB_CUDA(cudaMemsetAsync(c.dsc->red, 0, sizeof(c.dsc->red), c.stream));
-  k_field<<<c.num_sms * 4, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.dsc, c.Npad, P.d, F.csol, F.n, F.nk,
+  k_field<<<c.num_sms * 3, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc,
+                                                     c.Npad, P.d, F.csol, F.n, F.nk,
                                                      c.overlap, c.gradient, c.nbdt, c.ncol, c.spacing_f, c.x0f,
                                                      c.hf, c.weight, c.force);
   VLB_LAUNCHED(c);
-  k_tail<<<c.num_sms * 2, kGThreads, 0, c.stream>>>(c.outlist, c.dsc, c.Npad, P.k, P.d, C.csol, C.knots_d, C.nk,
+  k_tail<<<c.num_sms, kGThreads, 0, c.stream>>>(c.outlist, c.dsc, c.Npad, P.k, P.d, C.csol, C.knots_d, C.nk,
                                                     C.n, F.nk, c.x0f, c.hf, c.x0, c.h, c.weight, c.force);
   VLB_LAUNCHED(c);
   c.have_forces = true;

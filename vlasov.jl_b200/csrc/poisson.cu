@@ -31,7 +31,6 @@ namespace {
 
 constexpr int kPT = 64;  // p columns per CTA
 
-enum { LOAD_PLAIN = 0, LOAD_RHS = 1, LOAD_MEANFIELD = 2 };
 enum { EPI_PLAIN = 0, EPI_INVL = 1, EPI_PHI = 2 };
 
 struct ProductArgs {
@@ -40,62 +39,37 @@ struct ProductArgs {
   const float* src;
   int n, npad;
   long long m;
-  // LOAD_RHS
-  const float* rho;    // full grid (N = n + 2)
-  const float* phi;    // full grid, faces set
-  const float* lap;    // [N*N] row-major
-  // LOAD_MEANFIELD
-  const float* colloc; // [n]
-  float nions, radius;
-  // EPI
-  const float* invl;
+  const float* invl;   // EPI_INVL
 };
 
-__device__ __forceinline__ float xc_potential(float rho) {
-  // src/meanfield.jl:371-386
-  const float XC_EXCHANGE = -0.9847450218426966f;       // -cbrt(3/pi)
-  const float XC_CORRELATION = -0.0333f;
-  const float XC_CORRELATION_SCALE = 18.376708275787752f;  // 11.4 cbrt(4pi/3)
-  float c = cbrtf(rho);
-  return XC_EXCHANGE * c + XC_CORRELATION * log1pf(XC_CORRELATION_SCALE * c);
-}
-__device__ __forceinline__ float sphere_potential(float Q, float R, float r) {
-  return r < R ? -Q * (3.f - (r / R) * (r / R)) / (2.f * R) : -Q / r;
+// row stride of the staged src tile: >= n, 16-byte rows, and == 4 (mod 8)
+// so that the 8 column groups of a warp read 8 different banks
+__host__ __device__ __forceinline__ int tile_lds(int n) {
+  int l = (n + 3) / 4 * 4;
+  if (l % 8 == 0) l += 4;
+  return l;
 }
 
-template <int LOAD>
-__device__ __forceinline__ float load_elem(const ProductArgs& a, long long idx) {
-  if (LOAD == LOAD_PLAIN) return a.src[idx];
-  if (LOAD == LOAD_MEANFIELD) {
-    const int n = a.n;
-    const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((long long)n * n));
-    const float gx = a.colloc[i], gy = a.colloc[j], gz = a.colloc[k];
-    const float r = sqrtf(gx * gx + gy * gy + gz * gz);
-    const float extra = xc_potential(a.rho[idx]) + sphere_potential(a.nions, a.radius, r);
-    return a.src ? a.src[idx] + extra : extra;
-  }
-  // LOAD_RHS: interior point (i,j,k) of an N^3 grid, N = n + 2
-  const int n = a.n, N = n + 2;
-  const int i = (int)(idx % n), j = (int)((idx / n) % n), k = (int)(idx / ((long long)n * n));
-  const size_t sj = N, sk = (size_t)N * N;
-  const size_t c = (size_t)(i + 1) + sj * (j + 1) + sk * (k + 1);
-  const float* D = a.lap;
-  const float* P = a.phi;
-  float v = fmul(-12.566370614359172f, a.rho[c]);
-  v = fsub(v, fmul(D[(i + 1) * N + 0], P[c - (i + 1)]));
-  v = fsub(v, fmul(D[(i + 1) * N + N - 1], P[c - (i + 1) + (N - 1)]));
-  v = fsub(v, fmul(D[(j + 1) * N + 0], P[c - sj * (j + 1)]));
-  v = fsub(v, fmul(D[(j + 1) * N + N - 1], P[c - sj * (j + 1) + sj * (N - 1)]));
-  v = fsub(v, fmul(D[(k + 1) * N + 0], P[c - sk * (k + 1)]));
-  v = fsub(v, fmul(D[(k + 1) * N + N - 1], P[c - sk * (k + 1) + sk * (N - 1)]));
-  return v;
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-template <int LOAD, int EPI>
+// One CTA: all output rows i' (n padded to npad) for kPT consecutive columns
+// p.  A^T and the src tile are staged with asynchronous copies (every copy in
+// flight at once), then each thread accumulates an 8 x 8 block in registers.
+template <int EPI>
 __global__ void __launch_bounds__(256) k_mode_product(ProductArgs a) {
   extern __shared__ __align__(16) float sm[];
   const int n = a.n, npad = a.npad;
-  const int lds = n | 1;
+  const int lds = tile_lds(n);
   float* As = sm;                       // [n][npad]
   float* Ss = sm + (size_t)n * npad;    // [kPT][lds]
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -103,17 +77,17 @@ __global__ void __launch_bounds__(256) k_mode_product(ProductArgs a) {
   const long long p0 = (long long)blockIdx.x * kPT;
   const int cnt = (int)min((long long)kPT, a.m - p0);
   {
-    const float4* A4 = reinterpret_cast<const float4*>(a.AT);
-    float4* As4 = reinterpret_cast<float4*>(As);
     const int tot4 = n * npad / 4;
-    for (int e = tid; e < tot4; e += nth) As4[e] = A4[e];
-  }
-  for (int pr = 0; pr < kPT; ++pr) {
-    for (int i = tid; i < n; i += nth) {
-      float v = 0.f;
-      if (pr < cnt) v = load_elem<LOAD>(a, (p0 + pr) * n + i);
-      Ss[pr * lds + i] = v;
+    for (int e = tid; e < tot4; e += nth) cp_async16(As + 4 * e, a.AT + 4 * e);
+    const int half = n / 2;  // n is even: 8-byte pieces
+    const float* base = a.src + p0 * n;
+    const int tot2 = cnt * half;
+    for (int e = tid; e < tot2; e += nth) {
+      const int pr = e / half, i2 = e - pr * half;
+      cp_async8(Ss + pr * lds + 2 * i2, base + (size_t)pr * n + 2 * i2);
     }
+    for (int e = cnt * lds + tid; e < kPT * lds; e += nth) Ss[e] = 0.f;
+    cp_async_wait_all();
   }
   __syncthreads();
   float acc[8][8];
@@ -160,20 +134,67 @@ __global__ void __launch_bounds__(256) k_mode_product(ProductArgs a) {
   }
 }
 
-size_t product_smem(int n, int npad) { return ((size_t)n * npad + (size_t)kPT * (n | 1)) * sizeof(float); }
+size_t product_smem(int n, int npad) { return ((size_t)n * npad + (size_t)kPT * tile_lds(n)) * sizeof(float); }
 
-template <int LOAD, int EPI>
+template <int EPI>
 void product(Ctx& c, const ProductArgs& a) {
   const size_t smem = product_smem(a.n, a.npad);
   static bool attr_set = false;
   if (!attr_set) {
-    VLB_CUDA(cudaFuncSetAttribute(k_mode_product<LOAD, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    VLB_CUDA(cudaFuncSetAttribute(k_mode_product<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(227 * 1024)));
     attr_set = true;
   }
   const unsigned grid = (unsigned)((a.m + kPT - 1) / kPT);
-  k_mode_product<LOAD, EPI><<<grid, a.npad, smem, c.stream>>>(a);
+  k_mode_product<EPI><<<grid, a.npad, smem, c.stream>>>(a);
   VLB_LAUNCHED(c);
+}
+
+__device__ __forceinline__ float xc_potential(float rho) {
+  // src/meanfield.jl:371-386
+  const float XC_EXCHANGE = -0.9847450218426966f;          // -cbrt(3/pi)
+  const float XC_CORRELATION = -0.0333f;
+  const float XC_CORRELATION_SCALE = 18.376708275787752f;  // 11.4 cbrt(4pi/3)
+  float c = cbrtf(rho);
+  return XC_EXCHANGE * c + XC_CORRELATION * log1pf(XC_CORRELATION_SCALE * c);
+}
+__device__ __forceinline__ float sphere_potential(float Q, float R, float r) {
+  return r < R ? -Q * (3.f - (r / R) * (r / R)) / (2.f * R) : -Q / r;
+}
+
+// Right-hand side of the interior with the Dirichlet lifting
+// (src/poisson.jl:275-294), one thread per interior point, i fastest.
+__global__ void k_rhs(float* __restrict__ rhs, const float* __restrict__ rho, const float* __restrict__ P,
+                      const float* __restrict__ D, int n) {
+  const int N = n + 2;
+  const size_t tot = (size_t)n * n * n;
+  const size_t sj = N, sk = (size_t)N * N;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % n), j = (int)((t / n) % n), k = (int)(t / ((size_t)n * n));
+    const size_t row = sj * (j + 1) + sk * (k + 1);
+    const size_t c = (size_t)(i + 1) + row;
+    float v = fmul(-12.566370614359172f, rho[c]);
+    v = fsub(v, fmul(D[(i + 1) * N], P[row]));
+    v = fsub(v, fmul(D[(i + 1) * N + N - 1], P[row + N - 1]));
+    v = fsub(v, fmul(D[(j + 1) * N], P[(i + 1) + sk * (k + 1)]));
+    v = fsub(v, fmul(D[(j + 1) * N + N - 1], P[(i + 1) + sj * (N - 1) + sk * (k + 1)]));
+    v = fsub(v, fmul(D[(k + 1) * N], P[(i + 1) + sj * (j + 1)]));
+    v = fsub(v, fmul(D[(k + 1) * N + N - 1], P[(i + 1) + sj * (j + 1) + sk * (N - 1)]));
+    rhs[t] = v;
+  }
+}
+
+// phi + V_xc(rho) + V_jel(r) at the collocation points (phi may be null)
+__global__ void k_meanfield_src(float* __restrict__ out, const float* __restrict__ phi,
+                                const float* __restrict__ rho, const float* __restrict__ g, int n, float nions,
+                                float radius) {
+  const size_t tot = (size_t)n * n * n;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % n), j = (int)((t / n) % n), k = (int)(t / ((size_t)n * n));
+    const float r = sqrtf(g[i] * g[i] + g[j] * g[j] + g[k] * g[k]);
+    const float extra = xc_potential(rho[t]) + sphere_potential(nions, radius, r);
+    out[t] = phi ? phi[t] + extra : extra;
+  }
 }
 
 // ---------------------------------------------------------------- moments
@@ -350,56 +371,64 @@ ProductArgs base_args(const Level& L, bool interior) {
 
 // solve_interior! with the faces already in phi (src/devicemesh.jl:133-146)
 void solve_interior(Ctx& c, Level& L) {
+  const int ni = L.ni;
+  k_rhs<<<grid_for(c, (int64_t)ni * ni * ni, 256, 8), 256, 0, c.stream>>>(c.work[2], L.rho, L.phi, L.lap, ni);
+  VLB_LAUNCHED(c);
   ProductArgs a = base_args(L, true);
-  a.rho = L.rho; a.phi = L.phi; a.lap = L.lap;
   // forward: into the eigenbasis
-  a.AT = L.MinvT; a.src = nullptr; a.dest = c.work[0];
-  product<LOAD_RHS, EPI_PLAIN>(c, a);
+  a.AT = L.MinvT;
+  a.src = c.work[2]; a.dest = c.work[0];
+  product<EPI_PLAIN>(c, a);
   a.src = c.work[0]; a.dest = c.work[1];
-  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  product<EPI_PLAIN>(c, a);
   a.src = c.work[1]; a.dest = c.work[0]; a.invl = L.invlsum;
-  product<LOAD_PLAIN, EPI_INVL>(c, a);
+  product<EPI_INVL>(c, a);
   // back
   a.AT = L.MT;
   a.src = c.work[0]; a.dest = c.work[1];
-  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  product<EPI_PLAIN>(c, a);
   a.src = c.work[1]; a.dest = c.work[0];
-  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  product<EPI_PLAIN>(c, a);
   a.src = c.work[0]; a.dest = L.phi;
-  product<LOAD_PLAIN, EPI_PHI>(c, a);
+  product<EPI_PHI>(c, a);
+}
+
+// three S^-1 rotations: src -> w0 -> w1 -> dst
+void coefficients(Ctx& c, Level& L, const float* src, float* w0, float* w1, float* dst) {
+  ProductArgs a = base_args(L, false);
+  a.AT = L.sinvT;
+  a.src = src; a.dest = w0;
+  product<EPI_PLAIN>(c, a);
+  a.src = w0; a.dest = w1;
+  product<EPI_PLAIN>(c, a);
+  a.src = w1; a.dest = dst;
+  product<EPI_PLAIN>(c, a);
 }
 
 }  // namespace
 
 void launch_coefficients(Ctx& c, Level& L, const float* src, float* dst) {
-  ProductArgs a = base_args(L, false);
-  a.AT = L.sinvT;
-  a.src = src; a.dest = c.work[0];
-  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
-  a.src = c.work[0]; a.dest = c.work[1];
-  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
-  a.src = c.work[1]; a.dest = dst;
-  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  coefficients(c, L, src, c.work[0], c.work[1], dst);
 }
 
+// csol = S^-1 (phi + V_xc(rho) + V_jel(r)): the Hartree coefficients and the
+// mean field of effective_potential! (src/devicemesh.jl:171-183) in one pass
 void launch_mean_field_coefficients(Ctx& c, Level& L, const float* phi, float* csol, double nions,
                                     double radius) {
-  ProductArgs a = base_args(L, false);
-  a.AT = L.sinvT;
-  a.rho = L.rho; a.colloc = L.colloc;
-  a.nions = (float)nions; a.radius = (float)radius;
-  a.src = phi; a.dest = c.work[0];
-  product<LOAD_MEANFIELD, EPI_PLAIN>(c, a);
-  a.src = c.work[0]; a.dest = c.work[1];
-  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
-  a.src = c.work[1]; a.dest = csol;
-  product<LOAD_PLAIN, EPI_PLAIN>(c, a);
+  const size_t tot = (size_t)L.n * L.n * L.n;
+  k_meanfield_src<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(c.work[2], phi, L.rho, L.colloc, L.n,
+                                                                            (float)nions, (float)radius);
+  VLB_LAUNCHED(c);
+  coefficients(c, L, c.work[2], c.work[0], c.work[1], csol);
 }
 
 // csol += S^-1 [V_xc(rho) + V_jel(r)] (src/devicemesh.jl:171-183)
 void launch_mean_field_add(Ctx& c, Level& L, double nions, double radius) {
-  launch_mean_field_coefficients(c, L, nullptr, c.work[2], nions, radius);
   const size_t tot = (size_t)L.n * L.n * L.n;
+  k_meanfield_src<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(c.work[2], nullptr, L.rho, L.colloc,
+                                                                            L.n, (float)nions, (float)radius);
+  VLB_LAUNCHED(c);
+  coefficients(c, L, c.work[2], c.work[0], c.work[1], c.work[2]);
   k_add<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(L.csol, c.work[2], tot);
   VLB_LAUNCHED(c);
 }

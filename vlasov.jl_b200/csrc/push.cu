@@ -122,7 +122,49 @@ __global__ void __launch_bounds__(256) k_enclosed(int64_t N, int64_t Npad, const
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&dsc->enclosed, cnt);
 }
 
+// Long chains of independent FMAs: the FP32 pipe's ceiling at the current
+// clocks, the denominator of the gather's and deposit's roofline.
+__global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a, float b) {
+  float x[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) x[j] = threadIdx.x * 1e-7f + j;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) x[j] = fmaf(x[j], a, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += x[j];
+  if (s == 1234.5f) out[blockIdx.x] = s;  // keeps the chains alive
+}
+
 }  // namespace
+
+double measure_fp32_peak(int device) {
+  VLB_CUDA(cudaSetDevice(device));
+  int sms = 0;
+  VLB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  float* out = nullptr;
+  VLB_CUDA(cudaMalloc(&out, sizeof(float) * sms * 8));
+  cudaEvent_t e0, e1;
+  VLB_CUDA(cudaEventCreate(&e0));
+  VLB_CUDA(cudaEventCreate(&e1));
+  const int iters = 4096, blocks = sms * 8, threads = 256;
+  k_fma_peak<<<blocks, threads>>>(out, iters / 8, 0.999f, 1e-3f);  // warm-up
+  VLB_CUDA(cudaEventRecord(e0));
+  k_fma_peak<<<blocks, threads>>>(out, iters, 0.999f, 1e-3f);
+  VLB_CUDA(cudaEventRecord(e1));
+  VLB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  VLB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  const double flops = 2.0 * 16 * 8 * (double)iters * blocks * threads;
+  return flops / (ms * 1e-3) / 1e12;
+}
 
 void launch_push(Ctx& c, double dt, double rcmax) {
   Particles& P = c.part[c.cur];

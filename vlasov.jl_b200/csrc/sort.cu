@@ -107,6 +107,30 @@ struct ScanOutOutside {
   __device__ void operator()(int64_t s, uint32_t p, uint32_t v) const { if (v) outlist[p] = (int32_t)s; }
 };
 
+// Chunks of at most kChunk particles of each occupied cell: the gather's
+// work items.
+struct ScanInChunks {
+  const int32_t* bounds; const DeviceScalars* dsc;
+  __device__ uint32_t operator()(int64_t g) const {
+    if (g >= dsc->noccupied) return 0u;
+    return (uint32_t)((bounds[g + 1] - bounds[g] + kChunk - 1) / kChunk);
+  }
+};
+struct ScanOutChunks {
+  int32_t* start;
+  __device__ void operator()(int64_t g, uint32_t p, uint32_t) const { start[g] = (int32_t)p; }
+};
+
+__global__ void k_items(const int32_t* __restrict__ bounds, const int32_t* __restrict__ start, const DeviceScalars* dsc,
+                        int32_t* __restrict__ item_cell) {
+  const int nocc = dsc->noccupied;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nocc; g += gridDim.x * blockDim.x) {
+    const int nch = (bounds[g + 1] - bounds[g] + kChunk - 1) / kChunk;
+    const int s0 = start[g];
+    for (int ch = 0; ch < nch; ++ch) item_cell[s0 + ch] = g;
+  }
+}
+
 template <class In, class Out>
 __global__ void __launch_bounds__(kScanThreads) k_scan(In in, Out out, int64_t n, unsigned long long* status,
                                                        unsigned long long* ticket, int32_t* total,
@@ -349,6 +373,10 @@ void launch_sort(Ctx& c) {
   c.cur ^= 1;
   // out-of-stencil slots, in increasing order
   scan(c, ScanInOutside{c.skeys, nk, n}, ScanOutOutside{c.outlist}, N, 5, &c.dsc->outcount);
+  // the gather's work items
+  scan(c, ScanInChunks{c.bounds, c.dsc}, ScanOutChunks{c.chunk_start}, c.ncell, 6, &c.dsc->nitems);
+  k_items<<<grid_for(c, c.ncell, 256, 4), 256, 0, c.stream>>>(c.bounds, c.chunk_start, c.dsc, c.item_cell);
+  VLB_LAUNCHED(c);
   c.sorted = true;
 }
 

@@ -13,6 +13,7 @@ namespace vlb {
 
 constexpr int kWarp = 32;
 constexpr int kNumStages = 12;
+constexpr int kChunk = 128;  // particles per gather work item
 
 // Error flags raised by kernels into DeviceScalars::status.
 constexpr int kStatusScanTimeout = 1;   // decoupled look-back gave up
@@ -35,6 +36,9 @@ struct DeviceScalars {
   double moments[10];                // multipole sums (coarse)
   double charge_raw;                 // fine charge before renormalisation
   unsigned long long enclosed;       // particles within the capture radius
+  unsigned long long work_cic;
+  int32_t nitems;                    // cell chunks of the gather
+  int32_t pad_items;
   int32_t reset_end;
   int32_t pad0;
   // --- persistent ---
@@ -112,6 +116,8 @@ struct Ctx {
   int32_t* occupied = nullptr;   // [ncell]
   int32_t* bounds = nullptr;     // [ncell+1]
   int32_t* outlist = nullptr;    // [N]
+  int32_t* chunk_start = nullptr;  // [ncell] first chunk of occupied cell g
+  int32_t* item_cell = nullptr;    // [N / kChunk + ncell] occupied cell of each chunk
   unsigned long long* scan_status = nullptr;  // look-back tile states
   int64_t scan_status_size = 0;
   // deposit

@@ -427,6 +427,7 @@ class StepDiagnostics:
     noccupied: int
     projectile_force: tuple
     total_charge: float
+    status: int = 0
 
 
 class Simulation:
@@ -495,7 +496,7 @@ class Simulation:
                                                                       capture=self.capture_radius))
         self.steps_done += 1
         return StepDiagnostics(r.kinetic, r.escaped, tuple(r.angular), r.enclosed_charge, r.nout, r.outcount,
-                               r.noccupied, tuple(r.projectile_force), r.total_charge)
+                               r.noccupied, tuple(r.projectile_force), r.total_charge, r.status)
 
     def run(self, nsteps: int | None = None, callback=None):
         nsteps = self.params.nsteps if nsteps is None else nsteps
