@@ -249,6 +249,23 @@ VLB_API int vlb_fp32_peak(int32_t device, double* tflops);
 /* The context's CUDA stream (cudaStream_t), for event timing by a caller. */
 VLB_API int vlb_stream(vlb_ctx* ctx, void** stream);
 
+/* Total charge sum_ijk rho[i,j,k] m0[i] m0[j] m0[k] of a density the caller
+ * holds on the device, for callers that cannot allocate device memory: a host
+ * capturing a CUDA graph, where an allocation is an unsafe call that fails; an
+ * embedding runtime whose pool has already claimed the GPU's memory; a loop
+ * that must not stall on cudaMalloc's synchronisation.  It allocates nothing:
+ * the scratch (one float64 per (j,k) column) is a fixed 512 KiB of static
+ * device memory that every GPU loading the library keeps until exit, so n is
+ * at most 256 points per axis; larger n returns VLB_ERR_ARG.
+ * rho: device float32 [n*n*n], i fastest; m0: device float64 [n] (order-0 dual
+ * moments); q: device float64 [1], written; stream: a cudaStream_t, or NULL.
+ * Runs on the current device.  The first call on a device resolves the
+ * scratch's device address; make it before any stream capture.  Calls share
+ * the scratch: calls that overlap on the GPU race, so keep them on one stream.
+ * No counterpart in the reference (its total_charge allocates through its
+ * backend); the reduction is the one vlb_deposit_fine applies. */
+VLB_API int vlb_total_charge_noalloc(const float* rho, const double* m0, int32_t n, double* q, void* stream);
+
 /* ---- host-side set-up helpers (no GPU needed) ---- */
 
 /* sample_thomas_fermi(profile::RadialProfile, npart, weight; rng = Ran2(seed))

@@ -40,7 +40,7 @@ EXPORTS = (
     "vlb_push", "vlb_step", "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
     "vlb_enclosed_charge", "vlb_profile", "vlb_stage_count", "vlb_stage_name", "vlb_stage_times",
     "vlb_launch_count", "vlb_fp32_peak", "vlb_stream", "vlb_sample_thomas_fermi", "vlb_ran2", "vlb_pack_positions",
-    "vlb_unpack_positions",
+    "vlb_unpack_positions", "vlb_total_charge_noalloc",
 )
 
 P_D = C.POINTER(C.c_double)
@@ -138,6 +138,7 @@ def lib():
             "vlb_ran2": (C.c_int, [C.c_int32, C.c_int32, C.c_int64, P_F]),
             "vlb_pack_positions": (C.c_int, [C.c_int64, P_D, C.c_double, C.c_double, P_I, P_F]),
             "vlb_unpack_positions": (C.c_int, [C.c_int64, P_I, P_F, C.c_double, C.c_double, P_D]),
+            "vlb_total_charge_noalloc": (C.c_int, [vp, vp, C.c_int32, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

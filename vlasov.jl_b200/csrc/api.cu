@@ -301,6 +301,8 @@ void capture_graphs(Ctx& c, const vlb_step_params& p) {
 
 }  // namespace
 
+void set_last_error(const std::string& msg) { g_err = msg; }
+
 std::string cuda_msg(cudaError_t e, const char* what) {
   return std::string(what) + ": " + cudaGetErrorString(e);
 }

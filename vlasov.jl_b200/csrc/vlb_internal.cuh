@@ -145,6 +145,7 @@ struct Ctx {
 };
 
 std::string cuda_msg(cudaError_t e, const char* what);
+void set_last_error(const std::string& msg);
 int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
 
 // ---------------------------------------------------------------- kernels
