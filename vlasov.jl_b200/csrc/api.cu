@@ -258,9 +258,9 @@ void enqueue_step(Ctx& c, const vlb_step_params& p) {
   stage_mark(c, 6);
   launch_projectile_update(c, p.dt, p.jellium_nions, p.jellium_radius, p.advance_projectile);
   stage_mark(c, 7);
-  if (p.push) launch_push(c, p.dt, p.rcmax);
+  if (p.push) launch_push(c, p.dt, p.rcmax, p.capture_radius);
   stage_mark(c, 8);
-  if (p.capture_radius > 0) launch_enclosed(c, p.capture_radius);
+  if (!p.push && p.capture_radius > 0) launch_enclosed(c, p.capture_radius);
   stage_mark(c, 9);
 }
 
@@ -513,6 +513,7 @@ int vlb_deposit_fine(vlb_ctx* ctx, double charge, int32_t mode, int32_t* nout, d
 
 int vlb_deposit_coarse(vlb_ctx* ctx, double charge) {
   CTX_OR_FAIL;
+  if (!c.sorted) return fail(VLB_ERR_STATE, "deposit before any sort of the current cloud");
   return guarded([&]() -> int {
     launch_deposit_coarse(c, charge);
     VLB_CUDA(cudaStreamSynchronize(c.stream));
@@ -588,7 +589,7 @@ int vlb_push(vlb_ctx* ctx, double dt, double rcmax, double diag[5]) {
   CTX_OR_FAIL;
   if (!(dt > 0)) return fail(VLB_ERR_ARG, "dt must be positive");
   return guarded([&]() -> int {
-    launch_push(c, dt, rcmax);
+    launch_push(c, dt, rcmax, 0.0);
     fetch_scalars(c);
     if (diag)
       for (int i = 0; i < 5; ++i) diag[i] = c.hsc->diag[i];

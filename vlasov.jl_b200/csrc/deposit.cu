@@ -27,12 +27,18 @@ int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
 namespace {
 
 constexpr int kDepThreads = 256;
-constexpr int kDepLanes = 16;      // particle lanes per CTA
+constexpr int kDepLanes = 32;      // particle lanes per CTA, 8 threads (one z row each) per lane
 constexpr int kDepStage = 256;     // particles whose columns are staged at once
+constexpr int kDepRow = 68;        // floats per (lane, z row) in the reduction buffer: 64 + 4 against bank conflicts
 constexpr double kFixedScale = 1099511627776.0;        // 2^40
 constexpr double kFixedInv = 1.0 / 1099511627776.0;
 
-__global__ void __launch_bounds__(kDepThreads) k_deposit_fine(
+// One CTA per occupied cell at a time (dynamic counter).  Columns of 256
+// particles are staged in shared memory while the k/d loads of the next 256
+// are in flight.  Thread (lane, q) owns the z row q of its lane's 8^3 sum:
+// 64 float32 accumulators as float2 pairs along x, so one packed FMA covers two
+// outputs.  Lane partials are summed over the lanes in a fixed order.
+__global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
     const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds, DeviceScalars* dsc,
     int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ nodes,
     int nk, int n, float x0, float h, float lo, float hi, float spacing, int nbdt, int ncol, float* rho,
@@ -40,15 +46,14 @@ __global__ void __launch_bounds__(kDepThreads) k_deposit_fine(
   extern __shared__ __align__(16) unsigned char smem[];
   float* nodes_s = reinterpret_cast<float*>(smem);                      // [ncol][8]
   int* cols_s = reinterpret_cast<int*>(nodes_s + (size_t)ncol * 8);      // [3][kDepStage]
-  float* red_s = reinterpret_cast<float*>(cols_s + 3 * kDepStage);       // [kDepLanes][512]
+  float* red_s = reinterpret_cast<float*>(cols_s + 3 * kDepStage);       // [kDepLanes][8][kDepRow]
   __shared__ int s_g;
   __shared__ int s_nout;
   const int tid = threadIdx.x;
   for (int e = tid; e < ncol * 8; e += kDepThreads) nodes_s[e] = nodes[e];
   if (tid == 0) s_nout = 0;
   const int nocc = dsc->noccupied;
-  const int pl = tid / 16, q = tid % 16;
-  const int j0 = 2 * (q % 4), k0 = 2 * (q / 4);
+  const int pl = tid / 8, q = tid % 8;
   int my_nout = 0;
   __syncthreads();
   for (;;) {
@@ -61,21 +66,27 @@ __global__ void __launch_bounds__(kDepThreads) k_deposit_fine(
     int kx, ky, kz;
     cell_knots((uint32_t)cell, nk, kx, ky, kz);
     const bool fits = deposit_fits(kx, ky, kz, n);
-    float acc[32];
+    float2 acc[32];
 #pragma unroll
-    for (int a = 0; a < 32; ++a) acc[a] = 0.f;
+    for (int a = 0; a < 32; ++a) acc[a] = make_float2(0.f, 0.f);
+    int kk[3] = {0, 0, 0};
+    float dd[3] = {0.f, 0.f, 0.f};
+    if (sl + tid < sh) {
+#pragma unroll
+      for (int ax = 0; ax < 3; ++ax) {
+        kk[ax] = k[ax * Npad + sl + tid];
+        dd[ax] = d[ax * Npad + sl + tid];
+      }
+    }
     for (int base = sl; base < sh; base += kDepStage) {
-      const int s = base + tid;
-      if (s < sh) {
+      if (base + tid < sh) {
         bool inside = true;
         int cc[3];
 #pragma unroll
         for (int ax = 0; ax < 3; ++ax) {
-          const int kk = k[ax * Npad + s];
-          const float dd = d[ax * Npad + s];
-          const float p = fadd(fadd(x0, fmul((float)(kk - 1), h)), dd);
+          const float p = fadd(fadd(x0, fmul((float)(kk[ax] - 1), h)), dd[ax]);
           inside = inside && (lo <= p) && (p <= hi);
-          cc[ax] = table_column(dd, spacing, nbdt, ncol);
+          cc[ax] = table_column(dd[ax], spacing, nbdt, ncol);
         }
         if (!inside) { cc[0] = cc[1] = cc[2] = 1; ++my_nout; }
         cols_s[tid] = cc[0];
@@ -83,42 +94,58 @@ __global__ void __launch_bounds__(kDepThreads) k_deposit_fine(
         cols_s[2 * kDepStage + tid] = cc[2];
       }
       __syncthreads();
+      const int nb = base + kDepStage;
+      if (nb + tid < sh) {
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+          kk[ax] = k[ax * Npad + nb + tid];
+          dd[ax] = d[ax * Npad + nb + tid];
+        }
+      }
       if (fits) {
         const int cnt = min(kDepStage, sh - base);
         for (int t = pl; t < cnt; t += kDepLanes) {
           const float* vx = nodes_s + (size_t)(cols_s[t] - 1) * 8;
           const float* vy = nodes_s + (size_t)(cols_s[kDepStage + t] - 1) * 8;
-          const float* vz = nodes_s + (size_t)(cols_s[2 * kDepStage + t] - 1) * 8;
+          const float z = nodes_s[(size_t)(cols_s[2 * kDepStage + t] - 1) * 8 + q];
           const float4 xa = *reinterpret_cast<const float4*>(vx);
           const float4 xb = *reinterpret_cast<const float4*>(vx + 4);
-          const float2 y = *reinterpret_cast<const float2*>(vy + j0);
-          const float2 z = *reinterpret_cast<const float2*>(vz + k0);
-          const float x[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
-          const float w[4] = {y.x * z.x, y.y * z.x, y.x * z.y, y.y * z.y};
+          const float4 ya = *reinterpret_cast<const float4*>(vy);
+          const float4 yb = *reinterpret_cast<const float4*>(vy + 4);
+          const float2 x2[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w), make_float2(xb.x, xb.y),
+                                make_float2(xb.z, xb.w)};
+          const float y[8] = {ya.x, ya.y, ya.z, ya.w, yb.x, yb.y, yb.z, yb.w};
 #pragma unroll
-          for (int m = 0; m < 4; ++m)
+          for (int j = 0; j < 8; ++j) {
+            const float w = y[j] * z;
+            const float2 w2 = make_float2(w, w);
 #pragma unroll
-            for (int a = 0; a < 8; ++a) acc[8 * m + a] = fmaf(x[a], w[m], acc[8 * m + a]);
+            for (int a = 0; a < 4; ++a) acc[4 * j + a] = __ffma2_rn(x2[a], w2, acc[4 * j + a]);
+          }
         }
       }
       __syncthreads();
     }
     if (fits) {
-      // lane partials -> shared, then a fixed-order sum over the 16 lanes
+      // lane partials -> shared, then a fixed-order sum over the lanes that
+      // received particles
+      float* row = red_s + (size_t)(pl * 8 + q) * kDepRow;
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const int jj = j0 + (m & 1), kk = k0 + (m >> 1);
-#pragma unroll
-        for (int a = 0; a < 8; ++a) red_s[pl * 512 + a + 8 * (jj + 8 * kk)] = acc[8 * m + a];
+      for (int j = 0; j < 8; ++j) {
+        *reinterpret_cast<float4*>(row + 8 * j) = make_float4(acc[4 * j].x, acc[4 * j].y, acc[4 * j + 1].x,
+                                                              acc[4 * j + 1].y);
+        *reinterpret_cast<float4*>(row + 8 * j + 4) = make_float4(acc[4 * j + 2].x, acc[4 * j + 2].y,
+                                                                  acc[4 * j + 3].x, acc[4 * j + 3].y);
       }
       __syncthreads();
+      const int nl = min(kDepLanes, sh - sl);
       const int bx = 2 * kx - 5, by = 2 * ky - 5, bz = 2 * kz - 5;
       for (int o = tid; o < 512; o += kDepThreads) {
+        const int a = o & 7, jj = (o >> 3) & 7, kq = o >> 6;
+        const float* src = red_s + (size_t)kq * kDepRow + 8 * jj + a;
         float v = 0.f;
-#pragma unroll
-        for (int l = 0; l < kDepLanes; ++l) v += red_s[l * 512 + o];
-        const int a = o & 7, jj = (o >> 3) & 7, kk = o >> 6;
-        const size_t addr = (size_t)(bx + a) + (size_t)n * ((by + jj) + (size_t)n * (bz + kk));
+        for (int l = 0; l < nl; ++l) v += src[(size_t)l * 8 * kDepRow];
+        const size_t addr = (size_t)(bx + a) + (size_t)n * ((by + jj) + (size_t)n * (bz + kq));
         if (mode == VLB_DEPOSIT_FIXED64) {
           const long long iv = llrint((double)v * kFixedScale);
           if (iv) atomicAdd(&rho_fixed[addr], (unsigned long long)iv);
@@ -176,9 +203,8 @@ __global__ void k_charge_scale(float* __restrict__ rho, const unsigned long long
 
 // --------------------------------------------------------------- coarse
 constexpr int kCicThreads = 256;
-constexpr int kCicBlock = 64;   // consecutive sorted particles per thread
-constexpr int kCicT = 4;        // private window: 4^3 coarse points
-constexpr int kCicT3 = kCicT * kCicT * kCicT;
+constexpr int kCicW = 4;                        // window points per axis
+constexpr int kCicW3 = kCicW * kCicW * kCicW;   // 64 accumulators per lane
 
 // Cell of x on the stretched collocation points (src/kernels.jl:1069-1081):
 // the Float32 LocateTable walk, tables in shared memory; 0 outside.  w is the
@@ -196,20 +222,32 @@ __device__ __forceinline__ int locate_cell(const float* __restrict__ gt, const f
   return c;
 }
 
-// Each thread walks kCicBlock consecutive sorted particles -- a handful of
-// neighbouring fine cells -- into a private 4^3 window of shared memory
-// anchored one point before its first particle, and adds the window to the
-// grid once; particles that miss the window use global atomics (the
-// reference's design, src/kernels.jl:1083-1273).  Loads are 16-byte vectors of
-// four particles.  Contributions carry charge / (wx wy wz)
-// (src/devicemesh.jl:104).
-__global__ void __launch_bounds__(kCicThreads) k_deposit_cic(
-    int64_t N, int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d,
-    const float* __restrict__ gt_g, int ng, float lx0, float linvw, const int32_t* __restrict__ cells_g, int ncells,
-    const float* __restrict__ dl_g, float x0f, float hf, float charge, float* rho, int64_t nblock) {
+// The two weights of one axis spread over the window's four points: the left
+// point sits at offset l in [0, 2].
+__device__ __forceinline__ void window_axis(int l, float w0, float w1, float (&f)[kCicW]) {
+#pragma unroll
+  for (int e = 0; e < kCicW; ++e) f[e] = e == l ? w0 : (e == l + 1 ? w1 : 0.f);
+}
+
+// One warp per work item of the cell sort (a run of at most kChunk particles
+// of one fine cell).  Each lane adds its particles' eight trilinear
+// contributions into a 4^3 register window anchored at the coarse point left
+// of the fine cell's lower edge: the fine cell is one knot spacing wide, and
+// the collocation gaps of the coarse grid are wide enough that its particles'
+// left points lie within three of the anchor.  A particle whose left point
+// does not (a cell clamped at the edge of the fine grid) adds its corners with
+// global atomics.  The window is summed over the warp and added to the grid
+// once per item.  Contributions carry charge / (wx wy wz)
+// (src/devicemesh.jl:104); the walk is the reference's
+// (src/kernels.jl:1083-1273) with the scatter grouped by cell.
+__global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
+    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
+    const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int nk,
+    int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ gt_g, int ng,
+    float lx0, float linvw, const int32_t* __restrict__ cells_g, int ncells, const float* __restrict__ dl_g,
+    float x0f, float hf, float charge, float* rho) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float* tile = reinterpret_cast<float*>(smem);                 // [kCicT3][kCicThreads]
-  float* gt = tile + kCicT3 * kCicThreads;                      // [ng]
+  float* gt = reinterpret_cast<float*>(smem);                   // [ng]
   float* igap = gt + ng;                                        // [ng] 1 / (gt[c] - gt[c-1])
   float* idl = igap + ng;                                       // [ng] 1 / dual length
   int32_t* cells = reinterpret_cast<int32_t*>(idl + ng);        // [ncells]
@@ -220,76 +258,123 @@ __global__ void __launch_bounds__(kCicThreads) k_deposit_cic(
   }
   for (int e = threadIdx.x; e < ncells; e += kCicThreads) cells[e] = cells_g[e];
   __syncthreads();
-  const int t = threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int nitems = dsc->nitems;
   const size_t n = ng, nn = n * n;
-  for (int64_t blk = (int64_t)blockIdx.x * kCicThreads + t; blk < nblock; blk += (int64_t)gridDim.x * kCicThreads) {
+  const float halfh = 0.5f * hf;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(&dsc->work_cic, 1ull);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nitems) break;
+    const int g = item_cell[item];
+    const int s0 = bounds[g] + (item - chunk_start[g]) * kChunk;
+    const int s1 = min(s0 + kChunk, bounds[g + 1]);
+    int kx, ky, kz;
+    cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
+    int anc[3];
+    {
+      const int kc[3] = {kx, ky, kz};
 #pragma unroll
-    for (int p = 0; p < kCicT3; ++p) tile[p * kCicThreads + t] = 0.f;
-    const int64_t lo = blk * kCicBlock;
-    const int64_t hi = min(lo + kCicBlock, N);
-    int ox = 0, oy = 0, oz = 0;
-    bool anchored = false;
-    for (int64_t q = lo; q < hi; q += 4) {
-      // four particles per 16-byte load; Npad and lo are multiples of 4
-      const int4 kx4 = *reinterpret_cast<const int4*>(k + q);
-      const int4 ky4 = *reinterpret_cast<const int4*>(k + Npad + q);
-      const int4 kz4 = *reinterpret_cast<const int4*>(k + 2 * Npad + q);
-      const float4 dx4 = *reinterpret_cast<const float4*>(d + q);
-      const float4 dy4 = *reinterpret_cast<const float4*>(d + Npad + q);
-      const float4 dz4 = *reinterpret_cast<const float4*>(d + 2 * Npad + q);
-      const int kxs[4] = {kx4.x, kx4.y, kx4.z, kx4.w}, kys[4] = {ky4.x, ky4.y, ky4.z, ky4.w},
-                kzs[4] = {kz4.x, kz4.y, kz4.z, kz4.w};
-      const float dxs[4] = {dx4.x, dx4.y, dx4.z, dx4.w}, dys[4] = {dy4.x, dy4.y, dy4.z, dy4.w},
-                  dzs[4] = {dz4.x, dz4.y, dz4.z, dz4.w};
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (q + u >= hi) break;
-        const float px = fadd(fadd(x0f, fmul((float)(kxs[u] - 1), hf)), dxs[u]);
-        const float py = fadd(fadd(x0f, fmul((float)(kys[u] - 1), hf)), dys[u]);
-        const float pz = fadd(fadd(x0f, fmul((float)(kzs[u] - 1), hf)), dzs[u]);
-        float ax, ay, az;
-        const int ix = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, px, ax);
-        const int iy = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, py, ay);
-        const int iz = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, pz, az);
-        if (!(ix > 0 && iy > 0 && iz > 0)) continue;
-        const int i0 = ix - 1, j0 = iy - 1, k0 = iz - 1;  // 0-based left points
-        if (!anchored) { ox = i0 - 1; oy = j0 - 1; oz = k0 - 1; anchored = true; }
-        const float wx0 = ax * idl[i0], wx1 = (1.f - ax) * idl[i0 + 1];
-        const float wy0 = ay * idl[j0], wy1 = (1.f - ay) * idl[j0 + 1];
-        const float wz0 = charge * az * idl[k0], wz1 = charge * (1.f - az) * idl[k0 + 1];
-        const int lx = i0 - ox, ly = j0 - oy, lz = k0 - oz;
-        if (lx >= 0 && ly >= 0 && lz >= 0 && lx + 1 < kCicT && ly + 1 < kCicT && lz + 1 < kCicT) {
-          float* b = tile + (lx + kCicT * (ly + kCicT * lz)) * kCicThreads + t;
-          constexpr int SY = kCicT * kCicThreads, SZ = kCicT * kCicT * kCicThreads, SX = kCicThreads;
-          b[0] += wx0 * wy0 * wz0;
-          b[SZ] += wx0 * wy0 * wz1;
-          b[SY] += wx0 * wy1 * wz0;
-          b[SY + SZ] += wx0 * wy1 * wz1;
-          b[SX] += wx1 * wy0 * wz0;
-          b[SX + SZ] += wx1 * wy0 * wz1;
-          b[SX + SY] += wx1 * wy1 * wz0;
-          b[SX + SY + SZ] += wx1 * wy1 * wz1;
-        } else {
-          float* b = rho + (size_t)i0 + n * j0 + nn * k0;
-          atomicAdd(b, wx0 * wy0 * wz0);
-          atomicAdd(b + nn, wx0 * wy0 * wz1);
-          atomicAdd(b + n, wx0 * wy1 * wz0);
-          atomicAdd(b + n + nn, wx0 * wy1 * wz1);
-          atomicAdd(b + 1, wx1 * wy0 * wz0);
-          atomicAdd(b + 1 + nn, wx1 * wy0 * wz1);
-          atomicAdd(b + 1 + n, wx1 * wy1 * wz0);
-          atomicAdd(b + 1 + n + nn, wx1 * wy1 * wz1);
-        }
+      for (int ax = 0; ax < 3; ++ax) {
+        float wdummy;
+        const float edge = fsub(fadd(x0f, fmul((float)(kc[ax] - 1), hf)), halfh);
+        const int c = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, edge, wdummy);
+        anc[ax] = c > 0 ? c - 1 : -1000;
       }
     }
-    if (anchored) {
-#pragma unroll 4
-      for (int p = 0; p < kCicT3; ++p) {
-        const float v = tile[p * kCicThreads + t];
-        if (v != 0.f) {
-          const int lx = p % kCicT, ly = (p / kCicT) % kCicT, lz = p / (kCicT * kCicT);
-          atomicAdd(&rho[(size_t)(ox + lx) + n * (oy + ly) + nn * (oz + lz)], v);
-        }
+    float acc[kCicW3];
+#pragma unroll
+    for (int e = 0; e < kCicW3; ++e) acc[e] = 0.f;
+    for (int s = s0 + lane; s < s1; s += 32) {
+      const float px = fadd(fadd(x0f, fmul((float)(k[s] - 1), hf)), d[s]);
+      const float py = fadd(fadd(x0f, fmul((float)(k[Npad + s] - 1), hf)), d[Npad + s]);
+      const float pz = fadd(fadd(x0f, fmul((float)(k[2 * Npad + s] - 1), hf)), d[2 * Npad + s]);
+      float ax, ay, az;
+      const int ix = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, px, ax);
+      const int iy = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, py, ay);
+      const int iz = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, pz, az);
+      if (!(ix > 0 && iy > 0 && iz > 0)) continue;
+      const int i0 = ix - 1, j0 = iy - 1, k0 = iz - 1;  // 0-based left points
+      const float wx0 = ax * idl[i0], wx1 = (1.f - ax) * idl[i0 + 1];
+      const float wy0 = ay * idl[j0], wy1 = (1.f - ay) * idl[j0 + 1];
+      const float wz0 = charge * az * idl[k0], wz1 = charge * (1.f - az) * idl[k0 + 1];
+      const int lx = i0 - anc[0], ly = j0 - anc[1], lz = k0 - anc[2];
+      if ((unsigned)lx <= kCicW - 2 && (unsigned)ly <= kCicW - 2 && (unsigned)lz <= kCicW - 2) {
+        float fx[kCicW], fy[kCicW], fz[kCicW];
+        window_axis(lx, wx0, wx1, fx);
+        window_axis(ly, wy0, wy1, fy);
+        window_axis(lz, wz0, wz1, fz);
+#pragma unroll
+        for (int ey = 0; ey < kCicW; ++ey)
+#pragma unroll
+          for (int ex = 0; ex < kCicW; ++ex) {
+            const float fxy = fx[ex] * fy[ey];
+#pragma unroll
+            for (int ez = 0; ez < kCicW; ++ez) acc[ex + kCicW * (ey + kCicW * ez)] += fxy * fz[ez];
+          }
+      } else {
+        float* b = rho + (size_t)i0 + n * j0 + nn * k0;
+        atomicAdd(b, wx0 * wy0 * wz0);
+        atomicAdd(b + nn, wx0 * wy0 * wz1);
+        atomicAdd(b + n, wx0 * wy1 * wz0);
+        atomicAdd(b + n + nn, wx0 * wy1 * wz1);
+        atomicAdd(b + 1, wx1 * wy0 * wz0);
+        atomicAdd(b + 1 + nn, wx1 * wy0 * wz1);
+        atomicAdd(b + 1 + n, wx1 * wy1 * wz0);
+        atomicAdd(b + 1 + n + nn, wx1 * wy1 * wz1);
+      }
+    }
+    // recursive halving over the warp: after the five steps lane l holds the
+    // totals of entries l and 32 + l
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const bool up = lane & 16;
+      const float send = up ? acc[i] : acc[i + 32];
+      const float keep = up ? acc[i + 32] : acc[i];
+      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+    // acc[i], i < 32, is entry i + 32 * (lane has bit 4); pair the halves
+    // of the remaining 32 over bits 3..0, then move the kept pair together
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const bool up = lane & 8;
+      const float send = up ? acc[i] : acc[i + 16];
+      const float keep = up ? acc[i + 16] : acc[i];
+      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const bool up = lane & 4;
+      const float send = up ? acc[i] : acc[i + 8];
+      const float keep = up ? acc[i + 8] : acc[i];
+      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const bool up = lane & 2;
+      const float send = up ? acc[i] : acc[i + 4];
+      const float keep = up ? acc[i + 4] : acc[i];
+      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const bool up = lane & 1;
+      const float send = up ? acc[i] : acc[i + 2];
+      const float keep = up ? acc[i + 2] : acc[i];
+      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+    }
+    // lane l now holds, in acc[0] and acc[1], entries e0 = 32 b4 + 16 b3 +
+    // 8 b2 + 4 b1 + 2 b0 and e0 + 1, b the bits of l
+    const int e0 = 32 * ((lane >> 4) & 1) + 16 * ((lane >> 3) & 1) + 8 * ((lane >> 2) & 1) + 4 * ((lane >> 1) & 1) +
+                   2 * (lane & 1);
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const float v = acc[r];
+      if (v != 0.f) {
+        const int e = e0 + r;
+        const int ex = e % kCicW, ey = (e / kCicW) % kCicW, ez = e / (kCicW * kCicW);
+        atomicAdd(&rho[(size_t)(anc[0] + ex) + n * (anc[1] + ey) + nn * (anc[2] + ez)], v);
       }
     }
   }
@@ -298,7 +383,8 @@ __global__ void __launch_bounds__(kCicThreads) k_deposit_cic(
 }  // namespace
 
 size_t deposit_fine_smem(const Ctx& c) {
-  return (size_t)c.ncol * 8 * sizeof(float) + 3 * kDepStage * sizeof(int) + (size_t)kDepLanes * 512 * sizeof(float);
+  return (size_t)c.ncol * 8 * sizeof(float) + 3 * kDepStage * sizeof(int) +
+         (size_t)kDepLanes * 8 * kDepRow * sizeof(float);
 }
 
 size_t cic_smem(const Ctx& c);
@@ -319,7 +405,7 @@ void launch_deposit_fine(Ctx& c, double charge, int mode) {
     VLB_CUDA(cudaMemsetAsync(F.rho, 0, tot * sizeof(float), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_deposit, 0, sizeof(unsigned long long), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->nout, 0, sizeof(int32_t), c.stream));
-  const int grid = c.num_sms * 3;
+  const int grid = c.num_sms * 2;
   k_deposit_fine<<<grid, kDepThreads, deposit_fine_smem(c), c.stream>>>(
       c.occupied, c.bounds, c.dsc, c.Npad, P.k, P.d, c.nodes, F.nk, F.n, c.x0f, c.hf, c.lo_f, c.hi_f, c.spacing_f,
       c.nbdt, c.ncol, F.rho, c.rho_fixed, mode);
@@ -335,8 +421,7 @@ void launch_deposit_fine(Ctx& c, double charge, int mode) {
 }
 
 size_t cic_smem(const Ctx& c) {
-  return (size_t)kCicT3 * kCicThreads * sizeof(float) + 3 * (size_t)c.coarse.n * sizeof(float) +
-         (size_t)c.coarse.loc_ncell * sizeof(int32_t);
+  return 3 * (size_t)c.coarse.n * sizeof(float) + (size_t)c.coarse.loc_ncell * sizeof(int32_t);
 }
 
 void launch_deposit_coarse(Ctx& c, double charge) {
@@ -344,12 +429,10 @@ void launch_deposit_coarse(Ctx& c, double charge) {
   const size_t tot = (size_t)C.n * C.n * C.n;
   Particles& P = c.part[c.cur];
   VLB_CUDA(cudaMemsetAsync(C.rho, 0, tot * sizeof(float), c.stream));
-  const int64_t nblock = (c.N + kCicBlock - 1) / kCicBlock;
-  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((nblock + kCicThreads - 1) / kCicThreads,
-                                                               (int64_t)c.num_sms * 3));
-  k_deposit_cic<<<grid, kCicThreads, cic_smem(c), c.stream>>>(c.N, c.Npad, P.k, P.d, C.colloc, C.n, C.loc_x0,
-                                                              C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f,
-                                                              c.hf, (float)charge, C.rho, nblock);
+  VLB_CUDA(cudaMemsetAsync(&c.dsc->work_cic, 0, sizeof(unsigned long long), c.stream));
+  k_deposit_cic<<<c.num_sms * 4, kCicThreads, cic_smem(c), c.stream>>>(
+      c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.fine.nk, c.Npad, P.k, P.d, C.colloc, C.n,
+      C.loc_x0, C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho);
   VLB_LAUNCHED(c);
 }
 

@@ -31,40 +31,85 @@ __device__ __forceinline__ void verlet1(int kq, float dq, int ok, float od, floa
   gap = fadd(fmul((float)(kn - ok), h), fsub(dn, od));
 }
 
+// Four consecutive particles per thread, 16-byte loads and stores of every
+// component array (Npad is a multiple of 64).  When `r2cap` > 0 the same pass
+// counts the particles within sqrt(r2cap) of the projectile after the step
+// (enclosed_charge, float64 positions), which the reference reads after
+// step! on the host.
 __global__ void __launch_bounds__(256) k_push(int64_t N, int64_t Npad, int32_t* __restrict__ k, float* __restrict__ d,
                                               int32_t* __restrict__ pk, float* __restrict__ pd,
                                               const float* __restrict__ force, float a, float h, float x0, float pfac,
-                                              float r2max, float inv2M, double* diag) {
+                                              float r2max, float inv2M, double* diag, double r2cap, double x0d,
+                                              double hd, DeviceScalars* dsc) {
   double ek = 0, eo = 0, lx = 0, ly = 0, lz = 0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
-    int kq[3], ko[3], kn[3];
-    float dq[3], od[3], dn[3], gap[3], q[3];
+  unsigned cnt = 0;
+  const double P0 = dsc->proj_pos[0], P1 = dsc->proj_pos[1], P2 = dsc->proj_pos[2];
+  const int64_t nq = (N + 3) / 4;
+  for (int64_t qi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; qi < nq; qi += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i0 = 4 * qi;
+    int kq[3][4], ko[3][4], kn[3][4];
+    float dq[3][4], od[3][4], dn[3][4], gap[3][4], ff[3][4];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      kq[c] = k[c * Npad + i];
-      dq[c] = d[c * Npad + i];
-      ko[c] = pk[c * Npad + i];
-      od[c] = pd[c * Npad + i];
-      verlet1(kq[c], dq[c], ko[c], od[c], a, force[c * Npad + i], h, kn[c], dn[c], gap[c]);
-      q[c] = fadd(fadd(x0, fmul((float)(kq[c] - 1), h)), dq[c]);
+      const int4 a4 = *reinterpret_cast<const int4*>(k + c * Npad + i0);
+      const float4 b4 = *reinterpret_cast<const float4*>(d + c * Npad + i0);
+      const int4 c4 = *reinterpret_cast<const int4*>(pk + c * Npad + i0);
+      const float4 d4 = *reinterpret_cast<const float4*>(pd + c * Npad + i0);
+      const float4 f4 = *reinterpret_cast<const float4*>(force + c * Npad + i0);
+      kq[c][0] = a4.x; kq[c][1] = a4.y; kq[c][2] = a4.z; kq[c][3] = a4.w;
+      dq[c][0] = b4.x; dq[c][1] = b4.y; dq[c][2] = b4.z; dq[c][3] = b4.w;
+      ko[c][0] = c4.x; ko[c][1] = c4.y; ko[c][2] = c4.z; ko[c][3] = c4.w;
+      od[c][0] = d4.x; od[c][1] = d4.y; od[c][2] = d4.z; od[c][3] = d4.w;
+      ff[c][0] = f4.x; ff[c][1] = f4.y; ff[c][2] = f4.z; ff[c][3] = f4.w;
     }
-    const float px = fmul(gap[0], pfac), py = fmul(gap[1], pfac), pz = fmul(gap[2], pfac);
-    const float e = fmul(fadd(fadd(fmul(px, px), fmul(py, py)), fmul(pz, pz)), inv2M);
-    ek += e;
-    const float r2 = fadd(fadd(fmul(q[0], q[0]), fmul(q[1], q[1])), fmul(q[2], q[2]));
-    if (r2 > r2max) eo += e;
-    lx += (double)fsub(fmul(q[1], pz), fmul(q[2], py));
-    ly += (double)fsub(fmul(q[2], px), fmul(q[0], pz));
-    lz += (double)fsub(fmul(q[0], py), fmul(q[1], px));
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      float q[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        verlet1(kq[c][u], dq[c][u], ko[c][u], od[c][u], a, ff[c][u], h, kn[c][u], dn[c][u], gap[c][u]);
+        q[c] = fadd(fadd(x0, fmul((float)(kq[c][u] - 1), h)), dq[c][u]);
+      }
+      if (i0 + u < N) {
+        const float px = fmul(gap[0][u], pfac), py = fmul(gap[1][u], pfac), pz = fmul(gap[2][u], pfac);
+        const float e = fmul(fadd(fadd(fmul(px, px), fmul(py, py)), fmul(pz, pz)), inv2M);
+        ek += e;
+        const float r2 = fadd(fadd(fmul(q[0], q[0]), fmul(q[1], q[1])), fmul(q[2], q[2]));
+        if (r2 > r2max) eo += e;
+        lx += (double)fsub(fmul(q[1], pz), fmul(q[2], py));
+        ly += (double)fsub(fmul(q[2], px), fmul(q[0], pz));
+        lz += (double)fsub(fmul(q[0], py), fmul(q[1], px));
+        if (r2cap > 0) {
+          const double ex = x0d + (double)(kn[0][u] - 1) * hd + (double)dn[0][u] - P0;
+          const double ey = x0d + (double)(kn[1][u] - 1) * hd + (double)dn[1][u] - P1;
+          const double ez = x0d + (double)(kn[2][u] - 1) * hd + (double)dn[2][u] - P2;
+          if (ex * ex + ey * ey + ez * ez < r2cap) ++cnt;
+        }
+      } else {
+        // padding slots past N keep their (unused) contents
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { kn[c][u] = kq[c][u]; dn[c][u] = dq[c][u]; }
+      }
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      k[c * Npad + i] = kn[c];
-      d[c * Npad + i] = dn[c];
-      pk[c * Npad + i] = kq[c];
-      pd[c * Npad + i] = dq[c];
+      if (i0 + 3 < N) {
+        *reinterpret_cast<int4*>(k + c * Npad + i0) = make_int4(kn[c][0], kn[c][1], kn[c][2], kn[c][3]);
+        *reinterpret_cast<float4*>(d + c * Npad + i0) = make_float4(dn[c][0], dn[c][1], dn[c][2], dn[c][3]);
+        *reinterpret_cast<int4*>(pk + c * Npad + i0) = make_int4(kq[c][0], kq[c][1], kq[c][2], kq[c][3]);
+        *reinterpret_cast<float4*>(pd + c * Npad + i0) = make_float4(dq[c][0], dq[c][1], dq[c][2], dq[c][3]);
+      } else {
+        for (int u = 0; u < 4 && i0 + u < N; ++u) {
+          k[c * Npad + i0 + u] = kn[c][u];
+          d[c * Npad + i0 + u] = dn[c][u];
+          pk[c * Npad + i0 + u] = kq[c][u];
+          pd[c * Npad + i0 + u] = dq[c][u];
+        }
+      }
     }
   }
   __shared__ double sh[5][8];
+  __shared__ unsigned shc[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double v[5] = {ek, eo, lx, ly, lz};
 #pragma unroll
@@ -72,11 +117,17 @@ __global__ void __launch_bounds__(256) k_push(int64_t N, int64_t Npad, int32_t* 
     v[c] = warp_sum(v[c]);
     if (lane == 0) sh[c][w] = v[c];
   }
+  cnt = __reduce_add_sync(0xffffffffu, cnt);
+  if (lane == 0) shc[w] = cnt;
   __syncthreads();
   if (threadIdx.x < 5) {
     double s = 0;
     for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww) s += sh[threadIdx.x][ww];
     atomicAdd(&diag[threadIdx.x], s);
+  } else if (threadIdx.x == 5 && r2cap > 0) {
+    unsigned long long s = 0;
+    for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww) s += shc[ww];
+    if (s) atomicAdd(&dsc->enclosed, s);
   }
 }
 
@@ -166,13 +217,15 @@ double measure_fp32_peak(int device) {
   return flops / (ms * 1e-3) / 1e12;
 }
 
-void launch_push(Ctx& c, double dt, double rcmax) {
+void launch_push(Ctx& c, double dt, double rcmax, double capture_radius) {
   Particles& P = c.part[c.cur];
   const double M = c.weight;  // ELECTRON_MASS * weight
   VLB_CUDA(cudaMemsetAsync(c.dsc->diag, 0, sizeof(c.dsc->diag), c.stream));
-  k_push<<<grid_for(c, c.N, 256, 8), 256, 0, c.stream>>>(
+  if (capture_radius > 0) VLB_CUDA(cudaMemsetAsync(&c.dsc->enclosed, 0, sizeof(unsigned long long), c.stream));
+  k_push<<<grid_for(c, (c.N + 3) / 4, 256, 8), 256, 0, c.stream>>>(
       c.N, c.Npad, P.k, P.d, P.pk, P.pd, c.force, (float)(dt * dt / M), c.hf, c.x0f, (float)(M / (2 * dt)),
-      (float)(rcmax * rcmax), (float)(1 / (2 * M)), c.dsc->diag);
+      (float)(rcmax * rcmax), (float)(1 / (2 * M)), c.dsc->diag,
+      capture_radius > 0 ? capture_radius * capture_radius : 0.0, c.x0, c.h, c.dsc);
   VLB_LAUNCHED(c);
 }
 

@@ -165,7 +165,7 @@ void launch_forces(Ctx& c);
 // push.cu
 void launch_projectile_update(Ctx& c, double dt, double nions, double jradius, int advance);
 void launch_projectile_force_only(Ctx& c, double nions, double jradius);
-void launch_push(Ctx& c, double dt, double rcmax);
+void launch_push(Ctx& c, double dt, double rcmax, double capture_radius);
 void launch_enclosed(Ctx& c, double radius);
 
 
