@@ -13,5 +13,6 @@ from .simulation import (SimulationParameters, Jellium, BallSoftening, GaussianS
                          sample_thomas_fermi, ran2, pack_positions, unpack_positions, DeviceAccelerator,
                          Simulation, StepDiagnostics, xenon_projectile)
 from . import _lib
+from . import xenon
 
 __all__ = [n for n in dir() if not n.startswith("_")]

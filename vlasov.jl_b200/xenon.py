@@ -1,0 +1,91 @@
+"""The Na196 + Xe25+ collision of scripts/xenon.jl, run on the B200 library.
+
+Same setup as the reference's script (scripts/xenon.jl:293-420): Na196 cluster
+sampled from the Thomas-Fermi profile with Ran2(-1), rcluster = 78, rbox = 235,
+dt = 0.5, Xe25+ of mass 131.3*1836.154 at v = 0.40 from x = -70 with b = 45
+and a ball softening of radius 5, ceil(140 / (v dt)) = 700 steps.  It prints
+the reference's table -- q(<8 a0) and the out-of-stencil count every 50 steps
+-- and the charge carried away.  The film (GLMakie/Cairo) is not produced.
+
+    python -c 'import __graft_entry__ as g; g.load().xenon.main()' --particules 8000000 --nfine 64
+
+(from the repository root; the package directory is imported as vlasov_b200).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import sys
+import time
+
+
+def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point: bool = False,
+        uniform: bool = False, nsteps: int | None = None, device: int = 0, seed: int = -1, quiet: bool = False):
+    """Runs the crossing; returns a dict with the capture curve (q(<8) and
+    outcount after every step), the final charge and the timing."""
+    import numpy as np
+    from . import simulation as S
+
+    dt, v, x0 = 0.5, 0.40, -70.0
+    total = math.ceil((abs(x0) + 70.0) / (v * dt))
+    nsteps = total if nsteps is None else nsteps
+    p = S.SimulationParameters.for_grid(nfine, rcluster=78.0, rbox=235.0, nparticles=npart, dt=dt)
+    prof = S.uniform_sphere_profile() if uniform else S.thomas_fermi_profile()
+    t0 = time.time()
+    sim = S.Simulation(p, prof, projectile=S.xenon_projectile(v=v, x0=x0, dt=dt), seed=seed,
+                       fixed_point=fixed_point, device=device)
+    built = time.time() - t0
+    if not quiet:
+        print(f"Na196 + Xe25+, 500 keV, b = 45 a0 | {npart:.1e} particles, grid {2 * nfine + 2}^3")
+        print(f"built in {built:.1f} s\n")
+        print("   step     t (fs)    x_ion (a0)   q(<8 a0)        out    ms/step")
+        sys.stdout.flush()
+    fs = 41.341373335  # atomic units of time per femtosecond
+    q, out, xs = np.zeros(nsteps), np.zeros(nsteps, dtype=np.int64), np.zeros(nsteps)
+    acc = sim.accelerator
+    t_run = time.time()
+    tprev = t_run
+    for s in range(1, nsteps + 1):
+        d = sim.step()
+        q[s - 1] = d.enclosed_charge
+        out[s - 1] = d.outcount
+        xs[s - 1] = sim.projectile.position[0]
+        if not quiet and (s % every == 0 or s == nsteps):
+            now = time.time()
+            print(f"{s:7d} {s * dt / fs:10.2f} {sim.projectile.position[0]:12.1f} {d.enclosed_charge:10.3f} "
+                  f"{d.outcount:10d} {1000 * (now - tprev) / every:10.1f}")
+            sys.stdout.flush()
+            tprev = now
+        if d.status != 0:
+            raise RuntimeError(f"device status {d.status} at step {s}")
+    elapsed = time.time() - t_run
+    acc.close()
+    if not quiet:
+        print(f"\n{nsteps} steps in {elapsed:.1f} s -- {1000 * elapsed / nsteps:.2f} ms/step (wall clock, "
+              f"including the per-step read of the step's scalars)")
+        print(f"charge carried away by the ion: {q[-1]:.3f} electrons")
+    return {"npart": npart, "nfine": nfine, "nsteps": nsteps, "q8": q.tolist(), "outcount": out.tolist(),
+            "x_ion": xs.tolist(), "final_q8": float(q[-1]), "final_outcount": int(out[-1]),
+            "wall_s": elapsed, "built_s": built, "fixed_point": fixed_point, "uniform": uniform}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--particules", type=int, default=8_000_000)
+    ap.add_argument("--nfine", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--fixed-point", action="store_true")
+    ap.add_argument("--uniform", action="store_true", help="uniform-sphere cloud instead of Thomas-Fermi")
+    ap.add_argument("--json", default=None, help="write the capture curve here")
+    a = ap.parse_args(argv)
+    if a.nfine % 2:
+        ap.error("--nfine must be even")
+    r = run(a.particules, a.nfine, fixed_point=a.fixed_point, uniform=a.uniform, nsteps=a.steps)
+    if a.json:
+        with open(a.json, "w") as f:
+            json.dump(r, f)
+
+
+if __name__ == "__main__":
+    main()
