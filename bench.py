@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--nfine", type=int, default=64)
     ap.add_argument("--profile", default="thomas-fermi", choices=["thomas-fermi", "uniform-sphere"])
     ap.add_argument("--deposit", default="float32", choices=["float32", "fixed64"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "3xtf32"],
+                    help="mode products on the CUDA cores (fp32) or split-precision on the tensor cores")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
@@ -68,7 +70,7 @@ def workload(args, vb):
 def config_dict(args, n):
     return {"workload": "Na196 + Xe25+ 500 keV b=45 a0 collision, one fused step",
             "npart_per_gpu": args.npart, "fine_grid": f"{2 * args.nfine + 2}^3", "coarse_grid": f"{2 * args.nfine + 2}^3",
-            "profile": args.profile, "deposit": args.deposit, "dt": 0.5, "projectile": "Xe25+ v=0.40 x0=-70 b=45",
+            "profile": args.profile, "deposit": args.deposit, "mode_products": args.precision, "dt": 0.5, "projectile": "Xe25+ v=0.40 x0=-70 b=45",
             "cuda_graph": not args.no_graph, "l2": "inputs larger than L2 (2 x 384 MB particle state)",
             "parallelism": f"replicas{n}" if n > 1 else "1 GPU"}
 
@@ -226,6 +228,7 @@ def main():
 
     p, prof, proj = workload(args, vb)
     sim = vb.Simulation(p, prof, projectile=proj, device=local, fixed_point=args.deposit == "fixed64",
+                        precision=vb._lib.VLB_POISSON_3XTF32 if args.precision == "3xtf32" else vb._lib.VLB_POISSON_FP32,
                         use_graph=not args.no_graph, seed=-1 - rank)
     acc = sim.accelerator
     ext = torch.cuda.ExternalStream(acc.stream_handle(), device=torch.device("cuda", local))

@@ -117,6 +117,7 @@ typedef struct vlb_step_params {
   int32_t advance_projectile;  /* 0 during priming (src/simulation.jl:254) */
   int32_t push;                /* 0: forces only, no Verlet (priming) */
   int32_t use_graph;           /* 1: replay the step as one captured CUDA graph */
+  int32_t poisson_precision;   /* VLB_POISSON_FP32 or VLB_POISSON_3XTF32, every mode product of the step */
 } vlb_step_params;
 
 #define VLB_DEPOSIT_FLOAT32 0
@@ -145,8 +146,11 @@ typedef struct vlb_step_result {
 #define VLB_GRID_CSOL_FINE 4
 #define VLB_GRID_CSOL_COARSE 5
 
-/* Precision of the Poisson mode products. */
+/* Precision of the mode products (the tensor solves and the S^-1 conversions):
+ * FP32 on the CUDA cores, or split-precision 3xTF32 on the tensor cores with
+ * FP32 accumulation (even n <= 144 points per axis). */
 #define VLB_POISSON_FP32 0
+#define VLB_POISSON_3XTF32 1
 
 VLB_API const char* vlb_last_error(void);
 VLB_API const char* vlb_version(void);
@@ -191,6 +195,11 @@ VLB_API int vlb_deposit_coarse(vlb_ctx* ctx, double charge);
 /* poisson!(phis, rhos, dms) (src/devicemesh.jl:160-169): coarse multipole
  * faces + solve, fine faces from the coarse spline + solve. */
 VLB_API int vlb_poisson(vlb_ctx* ctx, int32_t precision);
+
+/* Precision of the mode products of vlb_coefficients and vlb_mean_field
+ * (vlb_poisson and vlb_step set it too).  No counterpart in the reference,
+ * whose products are SGEMM on CUDA devices. */
+VLB_API int vlb_set_precision(vlb_ctx* ctx, int32_t precision);
 
 /* spline_coefficients!(csol, phi, dm) (src/devicemesh.jl:126-127) into the
  * level's csol grid.  level: 0 fine, 1 coarse. */

@@ -31,12 +31,13 @@ VLB_GRID_CSOL_FINE = 4
 VLB_GRID_CSOL_COARSE = 5
 
 VLB_POISSON_FP32 = 0
+VLB_POISSON_3XTF32 = 1
 
 # every symbol include/vlasov_b200.h declares
 EXPORTS = (
     "vlb_last_error", "vlb_version", "vlb_create", "vlb_destroy", "vlb_upload_particles",
     "vlb_download_particles", "vlb_sort", "vlb_get_sort", "vlb_deposit_fine", "vlb_deposit_coarse",
-    "vlb_poisson", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
+    "vlb_poisson", "vlb_set_precision", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
     "vlb_push", "vlb_step", "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
     "vlb_enclosed_charge", "vlb_profile", "vlb_stage_count", "vlb_stage_name", "vlb_stage_times",
     "vlb_launch_count", "vlb_fp32_peak", "vlb_stream", "vlb_sample_thomas_fermi", "vlb_ran2", "vlb_pack_positions",
@@ -74,7 +75,8 @@ class ProjectileDesc(C.Structure):
 class StepParams(C.Structure):
     _fields_ = [("dt", C.c_double), ("rcmax", C.c_double), ("jellium_nions", C.c_double),
                 ("jellium_radius", C.c_double), ("capture_radius", C.c_double), ("deposit_mode", C.c_int32),
-                ("advance_projectile", C.c_int32), ("push", C.c_int32), ("use_graph", C.c_int32)]
+                ("advance_projectile", C.c_int32), ("push", C.c_int32), ("use_graph", C.c_int32),
+                ("poisson_precision", C.c_int32)]
 
 
 class StepResult(C.Structure):
@@ -114,6 +116,7 @@ def lib():
             "vlb_deposit_fine": (C.c_int, [vp, C.c_double, C.c_int32, P_I, P_D]),
             "vlb_deposit_coarse": (C.c_int, [vp, C.c_double]),
             "vlb_poisson": (C.c_int, [vp, C.c_int32]),
+            "vlb_set_precision": (C.c_int, [vp, C.c_int32]),
             "vlb_coefficients": (C.c_int, [vp, C.c_int32]),
             "vlb_mean_field": (C.c_int, [vp, C.c_int32, C.c_double, C.c_double]),
             "vlb_forces": (C.c_int, [vp, C.POINTER(ProjectileDesc), P_D, P_I]),

@@ -108,6 +108,9 @@ void setup_level(Level& D, const vlb_level_desc& L, bool coarse) {
   D.sinvT = upload_transposed(L.sinv, n, D.npad);
   D.MT = upload_transposed(L.eigvec, ni, D.nipad);
   D.MinvT = upload_transposed(L.eigvec_inv, ni, D.nipad);
+  D.tc_sinv = make_tc_image(L.sinv, n);
+  D.tc_M = make_tc_image(L.eigvec, ni);
+  D.tc_Minv = make_tc_image(L.eigvec_inv, ni);
   D.lap = upload_f(L.laplacian, (size_t)n * n);
   {
     std::vector<float> il((size_t)ni * ni * ni);
@@ -143,6 +146,7 @@ void setup_level(Level& D, const vlb_level_desc& L, bool coarse) {
 
 void free_level(Level& D) {
   dfree(D.colloc); dfree(D.knots); dfree(D.knots_d); dfree(D.sinvT); dfree(D.MT); dfree(D.MinvT);
+  dfree(D.tc_sinv.img); dfree(D.tc_M.img); dfree(D.tc_Minv.img);
   dfree(D.lap); dfree(D.invlsum); dfree(D.dual); dfree(D.dual_d); dfree(D.dlen); dfree(D.loc_cells);
   dfree(D.rho); dfree(D.phi); dfree(D.csol); dfree(D.csol_hartree);
 }
@@ -166,6 +170,7 @@ void destroy_ctx(Ctx* c) {
   dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off); dfree(c->occupied); dfree(c->bounds);
   dfree(c->outlist); dfree(c->chunk_start); dfree(c->item_cell); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
   for (auto& w : c->work) dfree(w);
+  dfree(c->tc_sync);
   dfree(c->dsc);
   if (c->hsc) cudaFreeHost(c->hsc);
   if (c->hin) cudaFreeHost(c->hin);
@@ -226,6 +231,8 @@ void fetch_scalars(Ctx& c) {
 int status_code(Ctx& c) {
   int s = c.hsc->status;
   if (s & kStatusScanTimeout) return fail(VLB_ERR_TIMEOUT, "a device scan gave up waiting on a predecessor tile");
+  if (s & kStatusMmaTimeout)
+    return fail(VLB_ERR_TIMEOUT, "a tensor-core mode product gave up waiting on its copies or MMAs");
   if (s) return fail(VLB_ERR_STATE, "device status flags set: " + std::to_string(s));
   return VLB_OK;
 }
@@ -267,7 +274,8 @@ void enqueue_step(Ctx& c, const vlb_step_params& p) {
 bool same_params(const vlb_step_params& a, const vlb_step_params& b) {
   return a.dt == b.dt && a.rcmax == b.rcmax && a.jellium_nions == b.jellium_nions &&
          a.jellium_radius == b.jellium_radius && a.capture_radius == b.capture_radius &&
-         a.deposit_mode == b.deposit_mode && a.advance_projectile == b.advance_projectile && a.push == b.push;
+         a.deposit_mode == b.deposit_mode && a.advance_projectile == b.advance_projectile && a.push == b.push &&
+         a.poisson_precision == b.poisson_precision;
 }
 
 // Two graphs, one per parity of the sort's double buffer: the step moves
@@ -411,6 +419,7 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     for (auto& e : c->ev) VLB_CUDA(cudaEventCreate(&e));
     c->evs_made = true;
     deposit_setup(*c);
+    tc_setup(*c);
     VLB_CUDA(cudaDeviceSynchronize());
     return VLB_OK;
   });
@@ -521,13 +530,32 @@ int vlb_deposit_coarse(vlb_ctx* ctx, double charge) {
   });
 }
 
+namespace {
+int check_precision(const Ctx& c, int32_t precision) {
+  if (precision == VLB_POISSON_FP32) return VLB_OK;
+  if (precision != VLB_POISSON_3XTF32) return fail(VLB_ERR_ARG, "unknown mode-product precision");
+  if (!c.fine.tc_sinv.img || !c.fine.tc_M.img || !c.coarse.tc_sinv.img || !c.coarse.tc_M.img)
+    return fail(VLB_ERR_ARG, "3xTF32 mode products need an even n <= 144 points per axis on both levels");
+  return VLB_OK;
+}
+}  // namespace
+
+int vlb_set_precision(vlb_ctx* ctx, int32_t precision) {
+  CTX_OR_FAIL;
+  if (int rc = check_precision(c, precision)) return rc;
+  c.mode_precision = precision;
+  return VLB_OK;
+}
+
 int vlb_poisson(vlb_ctx* ctx, int32_t precision) {
   CTX_OR_FAIL;
-  if (precision != VLB_POISSON_FP32) return fail(VLB_ERR_ARG, "unsupported Poisson precision");
+  if (int rc = check_precision(c, precision)) return rc;
+  c.mode_precision = precision;
   return guarded([&]() -> int {
+    VLB_CUDA(cudaMemsetAsync(&c.dsc->status, 0, sizeof(int32_t), c.stream));
     launch_poisson(c);
-    VLB_CUDA(cudaStreamSynchronize(c.stream));
-    return VLB_OK;
+    fetch_scalars(c);
+    return status_code(c);
   });
 }
 
@@ -535,9 +563,10 @@ int vlb_coefficients(vlb_ctx* ctx, int32_t level) {
   CTX_OR_FAIL;
   return guarded([&]() -> int {
     Level& L = level_of(c, level);
+    VLB_CUDA(cudaMemsetAsync(&c.dsc->status, 0, sizeof(int32_t), c.stream));
     launch_coefficients(c, L, L.phi, L.csol);
-    VLB_CUDA(cudaStreamSynchronize(c.stream));
-    return VLB_OK;
+    fetch_scalars(c);
+    return status_code(c);
   });
 }
 
@@ -545,9 +574,10 @@ int vlb_mean_field(vlb_ctx* ctx, int32_t level, double nions, double radius) {
   CTX_OR_FAIL;
   return guarded([&]() -> int {
     Level& L = level_of(c, level);
+    VLB_CUDA(cudaMemsetAsync(&c.dsc->status, 0, sizeof(int32_t), c.stream));
     launch_mean_field_add(c, L, nions, radius);
-    VLB_CUDA(cudaStreamSynchronize(c.stream));
-    return VLB_OK;
+    fetch_scalars(c);
+    return status_code(c);
   });
 }
 
@@ -604,6 +634,8 @@ int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, 
   if (!(params->dt > 0)) return fail(VLB_ERR_ARG, "dt must be positive");
   if (params->deposit_mode != VLB_DEPOSIT_FLOAT32 && params->deposit_mode != VLB_DEPOSIT_FIXED64)
     return fail(VLB_ERR_ARG, "unknown deposit mode");
+  if (int rc = check_precision(c, params->poisson_precision)) return rc;
+  c.mode_precision = params->poisson_precision;
   return guarded([&]() -> int {
     upload_projectile(c, proj);
     const bool graph = params->use_graph && !c.profile;

@@ -161,19 +161,24 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
   if (tid == 0 && s_nout) atomicAdd(&dsc->nout, s_nout);
 }
 
-// Per (j,k) column: sum_i rho[i,j,k] m0[i], times m0[j] m0[k].
-__global__ void k_charge_columns(const float* __restrict__ rho, const unsigned long long* __restrict__ fixed,
-                                 const double* __restrict__ m0, int n, double* __restrict__ partial) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// Per (j,k) column: sum_i rho[i,j,k] m0[i], times m0[j] m0[k].  One warp
+// per column: lane l sums i = l, l+32, ... in order, then the fixed
+// butterfly over the lanes.
+__global__ void __launch_bounds__(256) k_charge_columns(const float* __restrict__ rho,
+                                                        const unsigned long long* __restrict__ fixed,
+                                                        const double* __restrict__ m0, int n,
+                                                        double* __restrict__ partial) {
+  const int t = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (t >= n * n) return;
   const int j = t % n, kq = t / n;
   double s = 0;
   if (fixed) {
-    for (int i = 0; i < n; ++i) s += (double)(long long)fixed[(size_t)t * n + i] * kFixedInv * m0[i];
+    for (int i = lane; i < n; i += 32) s += (double)(long long)fixed[(size_t)t * n + i] * kFixedInv * m0[i];
   } else {
-    for (int i = 0; i < n; ++i) s += (double)rho[(size_t)t * n + i] * m0[i];
+    for (int i = lane; i < n; i += 32) s += (double)rho[(size_t)t * n + i] * m0[i];
   }
-  partial[t] = s * m0[j] * m0[kq];
+  s = warp_sum(s);
+  if (lane == 0) partial[t] = s * m0[j] * m0[kq];
 }
 
 // One block: the fixed-order sum of the column partials.
@@ -412,7 +417,7 @@ void launch_deposit_fine(Ctx& c, double charge, int mode) {
   VLB_LAUNCHED(c);
   const unsigned long long* fx = mode == VLB_DEPOSIT_FIXED64 ? c.rho_fixed : nullptr;
   const int cols = F.n * F.n;
-  k_charge_columns<<<(cols + 127) / 128, 128, 0, c.stream>>>(F.rho, fx, F.dual_d, F.n, c.partials);
+  k_charge_columns<<<(cols + 7) / 8, 256, 0, c.stream>>>(F.rho, fx, F.dual_d, F.n, c.partials);
   VLB_LAUNCHED(c);
   k_charge_total<<<1, 1024, 0, c.stream>>>(c.partials, cols, &c.dsc->charge_raw);
   VLB_LAUNCHED(c);

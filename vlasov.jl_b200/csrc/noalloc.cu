@@ -45,15 +45,18 @@ static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxN * kNoAll
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
-// Per (j,k) column: sum_i rho[i,j,k] m0[i], times m0[j] m0[k].
-__global__ void k_noalloc_columns(const float* __restrict__ rho, const double* __restrict__ m0, int n,
-                                  double* __restrict__ partial) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// Per (j,k) column: sum_i rho[i,j,k] m0[i], times m0[j] m0[k].  One warp
+// per column: lane l sums i = l, l+32, ... in order, then the fixed
+// butterfly over the lanes.
+__global__ void __launch_bounds__(256) k_noalloc_columns(const float* __restrict__ rho, const double* __restrict__ m0,
+                                                         int n, double* __restrict__ partial) {
+  const int t = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (t >= n * n) return;
   const int j = t % n, k = t / n;
   double s = 0;
-  for (int i = 0; i < n; ++i) s += (double)rho[(size_t)t * n + i] * m0[i];
-  partial[t] = s * m0[j] * m0[k];
+  for (int i = lane; i < n; i += 32) s += (double)rho[(size_t)t * n + i] * m0[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) partial[t] = s * m0[j] * m0[k];
 }
 
 // One block: the fixed-order sum of the column partials.
@@ -106,7 +109,7 @@ extern "C" int vlb_total_charge_noalloc(const float* rho, const double* m0, int3
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const int cols = n * n;
-  k_noalloc_columns<<<(cols + 127) / 128, 128, 0, s>>>(rho, m0, n, partials);
+  k_noalloc_columns<<<(cols + 7) / 8, 256, 0, s>>>(rho, m0, n, partials);
   k_noalloc_total<<<1, 1024, 0, s>>>(partials, cols, q);
   e = cudaGetLastError();
   if (e != cudaSuccess) return noalloc_fail(VLB_ERR_CUDA, cuda_msg(e, "vlb_total_charge_noalloc launch"));

@@ -110,6 +110,20 @@ __global__ void __launch_bounds__(256) k_mode_product(ProductArgs a) {
 #pragma unroll
       for (int c = 0; c < 8; ++c) acc[r][c] = fmaf(av[r], bv[c], acc[r][c]);
   }
+  if (EPI == EPI_INVL) {
+    // every factor in flight before the first store (dest and invl could
+    // alias as far as the compiler knows)
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int row = ty * 8 + r;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const int pc = tx + 8 * c;
+        const bool in = row < n && pc < cnt;
+        acc[r][c] *= in ? __ldg(a.invl + (p0 + pc) + a.m * row) : 0.f;
+      }
+    }
+  }
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     const int row = ty * 8 + r;
@@ -121,10 +135,8 @@ __global__ void __launch_bounds__(256) k_mode_product(ProductArgs a) {
       const long long p = p0 + pc;
       const long long o = p + a.m * row;
       float v = acc[r][c];
-      if (EPI == EPI_PLAIN) {
+      if (EPI != EPI_PHI) {
         a.dest[o] = v;
-      } else if (EPI == EPI_INVL) {
-        a.dest[o] = v * a.invl[o];
       } else {
         const int N = n + 2;
         const int i = (int)(p % n), j = (int)(p / n);
@@ -164,13 +176,14 @@ __device__ __forceinline__ float sphere_potential(float Q, float R, float r) {
 
 // Right-hand side of the interior with the Dirichlet lifting
 // (src/poisson.jl:275-294), one thread per interior point, i fastest.
+// One block per (j, k) line of the interior, threads along i.
 __global__ void k_rhs(float* __restrict__ rhs, const float* __restrict__ rho, const float* __restrict__ P,
                       const float* __restrict__ D, int n) {
   const int N = n + 2;
-  const size_t tot = (size_t)n * n * n;
   const size_t sj = N, sk = (size_t)N * N;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % n), j = (int)((t / n) % n), k = (int)(t / ((size_t)n * n));
+  const int j = blockIdx.y, k = blockIdx.z;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const size_t t = (size_t)i + (size_t)n * (j + (size_t)n * k);
     const size_t row = sj * (j + 1) + sk * (k + 1);
     const size_t c = (size_t)(i + 1) + row;
     float v = fmul(-12.566370614359172f, rho[c]);
@@ -188,9 +201,9 @@ __global__ void k_rhs(float* __restrict__ rhs, const float* __restrict__ rho, co
 __global__ void k_meanfield_src(float* __restrict__ out, const float* __restrict__ phi,
                                 const float* __restrict__ rho, const float* __restrict__ g, int n, float nions,
                                 float radius) {
-  const size_t tot = (size_t)n * n * n;
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % n), j = (int)((t / n) % n), k = (int)(t / ((size_t)n * n));
+  const int j = blockIdx.y, k = blockIdx.z;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const size_t t = (size_t)i + (size_t)n * (j + (size_t)n * k);
     const float r = sqrtf(g[i] * g[i] + g[j] * g[j] + g[k] * g[k]);
     const float extra = xc_potential(rho[t]) + sphere_potential(nions, radius, r);
     out[t] = phi ? phi[t] + extra : extra;
@@ -198,69 +211,82 @@ __global__ void k_meanfield_src(float* __restrict__ out, const float* __restrict
 }
 
 // ---------------------------------------------------------------- moments
-// Ten moment partials per (j,k) column (src/poisson.jl:55-93), float64.
-__global__ void k_moments(const float* __restrict__ rho, const double* __restrict__ dual, int n,
-                          double* __restrict__ partial) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+constexpr int kMomBlocks = 256;   // block partials of the ten moments
+
+// Ten moments of the density (src/poisson.jl:55-93), float64: one warp per
+// (j,k) column at a time (coalesced along i), summed per warp, then per
+// block in a fixed order into partial[r * kMomBlocks + block].
+__global__ void __launch_bounds__(256) k_moments(const float* __restrict__ rho, const double* __restrict__ dual,
+                                                 int n, double* __restrict__ partial) {
+  __shared__ double sh[10][8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int m = n * n;
-  if (t >= m) return;
   const double *p0 = dual, *p1 = dual + n, *p2 = dual + 2 * n;
-  const int j = t % n, k = t / n;
-  const double a = p0[j] * p0[k], b = p1[j] * p0[k], cc = p0[j] * p1[k];
-  const double d = p2[j] * p0[k], e = p0[j] * p2[k], f = p1[j] * p1[k];
-  double s0 = 0, s1 = 0, s2 = 0;
-  const float* col = rho + (size_t)n * t;
-  for (int i = 0; i < n; ++i) {
-    const double v = col[i];
-    s0 += v * p0[i];
-    s1 += v * p1[i];
-    s2 += v * p2[i];
+  double acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int t = blockIdx.x * 8 + w; t < m; t += gridDim.x * 8) {
+    const float* col = rho + (size_t)n * t;
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int i = lane; i < n; i += 32) {
+      const double v = col[i];
+      s0 += v * p0[i];
+      s1 += v * p1[i];
+      s2 += v * p2[i];
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    s2 = warp_sum(s2);
+    const int j = t % n, k = t / n;
+    const double a = p0[j] * p0[k], b = p1[j] * p0[k], cc = p0[j] * p1[k];
+    const double d = p2[j] * p0[k], e = p0[j] * p2[k], f = p1[j] * p1[k];
+    acc[0] += s0 * a;
+    acc[1] += s1 * a;
+    acc[2] += s0 * b;
+    acc[3] += s0 * cc;
+    acc[4] += s2 * a;
+    acc[5] += s0 * d;
+    acc[6] += s0 * e;
+    acc[7] += s1 * b;
+    acc[8] += s1 * cc;
+    acc[9] += s0 * f;
   }
-  partial[0 * m + t] = s0 * a;
-  partial[1 * m + t] = s1 * a;
-  partial[2 * m + t] = s0 * b;
-  partial[3 * m + t] = s0 * cc;
-  partial[4 * m + t] = s2 * a;
-  partial[5 * m + t] = s0 * d;
-  partial[6 * m + t] = s0 * e;
-  partial[7 * m + t] = s1 * b;
-  partial[8 * m + t] = s1 * cc;
-  partial[9 * m + t] = s0 * f;
+  if (lane == 0)
+    for (int r = 0; r < 10; ++r) sh[r][w] = acc[r];
+  __syncthreads();
+  if (threadIdx.x < 10) {
+    double s = 0;
+    for (int ww = 0; ww < 8; ++ww) s += sh[threadIdx.x][ww];
+    partial[(size_t)threadIdx.x * kMomBlocks + blockIdx.x] = s;
+  }
 }
 
-// One block: the ten sums in a fixed order, then the expansion in the
-// barycentre frame (src/poisson.jl:168-189).
-__global__ void __launch_bounds__(1024) k_multipole(const double* __restrict__ partial, int m, DeviceScalars* dsc) {
-  __shared__ double sh[1024];
-  __shared__ double tot[10];
-  for (int r = 0; r < 10; ++r) {
-    double s = 0;
-    for (int t = threadIdx.x; t < m; t += 1024) s += partial[(size_t)r * m + t];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = 512; o > 0; o >>= 1) {
-      if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) tot[r] = sh[0];
+// Block r: the sum of moment r over the block partials, in a fixed order.
+__global__ void __launch_bounds__(256) k_moment_sums(const double* __restrict__ partial, DeviceScalars* dsc) {
+  __shared__ double sh[256];
+  const int r = blockIdx.x;
+  sh[threadIdx.x] = threadIdx.x < kMomBlocks ? partial[(size_t)r * kMomBlocks + threadIdx.x] : 0.0;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    const double q = tot[0];
-    for (int r = 0; r < 10; ++r) dsc->moments[r] = tot[r];
-    double cx = q == 0 ? 0 : tot[1] / q, cy = q == 0 ? 0 : tot[2] / q, cz = q == 0 ? 0 : tot[3] / q;
-    const double m200 = tot[4], m020 = tot[5], m002 = tot[6], mxy = tot[7], mxz = tot[8], myz = tot[9];
-    const double b2 = cx * cx + cy * cy + cz * cz;
-    double* mp = dsc->multipole;
-    mp[0] = q;
-    mp[1] = cx; mp[2] = cy; mp[3] = cz;
-    mp[4] = (2 * m200 - m020 - m002) - q * (3 * cx * cx - b2);
-    mp[5] = (2 * m020 - m200 - m002) - q * (3 * cy * cy - b2);
-    mp[6] = (2 * m002 - m200 - m020) - q * (3 * cz * cz - b2);
-    mp[7] = 3 * mxy - 3 * q * cx * cy;
-    mp[8] = 3 * mxz - 3 * q * cx * cz;
-    mp[9] = 3 * myz - 3 * q * cy * cz;
-  }
+  if (threadIdx.x == 0) dsc->moments[r] = sh[0];
+}
+
+// Monopole, barycentre and traceless quadrupole in the barycentre frame
+// (src/poisson.jl:168-189) from the ten moments.
+__device__ __forceinline__ void multipole_of(const double* tot, double* mp) {
+  const double q = tot[0];
+  const double cx = q == 0 ? 0 : tot[1] / q, cy = q == 0 ? 0 : tot[2] / q, cz = q == 0 ? 0 : tot[3] / q;
+  const double m200 = tot[4], m020 = tot[5], m002 = tot[6], mxy = tot[7], mxz = tot[8], myz = tot[9];
+  const double b2 = cx * cx + cy * cy + cz * cz;
+  mp[0] = q;
+  mp[1] = cx; mp[2] = cy; mp[3] = cz;
+  mp[4] = (2 * m200 - m020 - m002) - q * (3 * cx * cx - b2);
+  mp[5] = (2 * m020 - m200 - m002) - q * (3 * cy * cy - b2);
+  mp[6] = (2 * m002 - m200 - m020) - q * (3 * cz * cz - b2);
+  mp[7] = 3 * mxy - 3 * q * cx * cy;
+  mp[8] = 3 * mxz - 3 * q * cx * cz;
+  mp[9] = 3 * myz - 3 * q * cy * cz;
 }
 
 // t-th surface point of an n^3 grid, 0-based (src/kernels.jl:836-859)
@@ -281,13 +307,16 @@ __device__ __forceinline__ void face_point(int t, int n, int& i, int& j, int& k)
 
 // Multipole potential on the faces (src/poisson.jl:198-206)
 __global__ void k_faces_multipole(float* __restrict__ phi, const float* __restrict__ g, int n,
-                                  const DeviceScalars* dsc) {
+                                  DeviceScalars* dsc) {
   const int nf = 2 * n * n + (n - 2) * (4 * n - 4);
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double mp[10];
+  multipole_of(dsc->moments, mp);
+  if (t == 0)
+    for (int r = 0; r < 10; ++r) dsc->multipole[r] = mp[r];
   if (t >= nf) return;
   int i, j, k;
   face_point(t, n, i, j, k);
-  const double* mp = dsc->multipole;
   const double px = (double)g[i] - mp[1], py = (double)g[j] - mp[2], pz = (double)g[k] - mp[3];
   const double r2 = px * px + py * py + pz * pz;
   const double invr = 1.0 / sqrt(r2);
@@ -372,9 +401,21 @@ ProductArgs base_args(const Level& L, bool interior) {
 // solve_interior! with the faces already in phi (src/devicemesh.jl:133-146)
 void solve_interior(Ctx& c, Level& L) {
   const int ni = L.ni;
-  k_rhs<<<grid_for(c, (int64_t)ni * ni * ni, 256, 8), 256, 0, c.stream>>>(c.work[2], L.rho, L.phi, L.lap, ni);
+  k_rhs<<<dim3(1, ni, ni), std::min(1024, (ni + 31) / 32 * 32), 0, c.stream>>>(c.work[2], L.rho, L.phi, L.lap, ni);
   VLB_LAUNCHED(c);
   ProductArgs a = base_args(L, true);
+  if (c.mode_precision == VLB_POISSON_3XTF32) {
+    // two chains of three products on the tensor cores
+    const float* s1[3] = {c.work[2], c.work[0], c.work[1]};
+    float* d1[3] = {c.work[0], c.work[1], c.work[0]};
+    const int e1[3] = {EPI_PLAIN, EPI_PLAIN, EPI_INVL};
+    launch_mode_chain_tc(c, L.tc_Minv, 3, s1, d1, e1, a.m, L.invlsum);
+    const float* s2[3] = {c.work[0], c.work[1], c.work[0]};
+    float* d2[3] = {c.work[1], c.work[0], L.phi};
+    const int e2[3] = {EPI_PLAIN, EPI_PLAIN, EPI_PHI};
+    launch_mode_chain_tc(c, L.tc_M, 3, s2, d2, e2, a.m, nullptr);
+    return;
+  }
   // forward: into the eigenbasis
   a.AT = L.MinvT;
   a.src = c.work[2]; a.dest = c.work[0];
@@ -396,6 +437,13 @@ void solve_interior(Ctx& c, Level& L) {
 // three S^-1 rotations: src -> w0 -> w1 -> dst
 void coefficients(Ctx& c, Level& L, const float* src, float* w0, float* w1, float* dst) {
   ProductArgs a = base_args(L, false);
+  if (c.mode_precision == VLB_POISSON_3XTF32) {
+    const float* s[3] = {src, w0, w1};
+    float* d[3] = {w0, w1, dst};
+    const int e[3] = {EPI_PLAIN, EPI_PLAIN, EPI_PLAIN};
+    launch_mode_chain_tc(c, L.tc_sinv, 3, s, d, e, a.m, nullptr);
+    return;
+  }
   a.AT = L.sinvT;
   a.src = src; a.dest = w0;
   product<EPI_PLAIN>(c, a);
@@ -415,8 +463,7 @@ void launch_coefficients(Ctx& c, Level& L, const float* src, float* dst) {
 // mean field of effective_potential! (src/devicemesh.jl:171-183) in one pass
 void launch_mean_field_coefficients(Ctx& c, Level& L, const float* phi, float* csol, double nions,
                                     double radius) {
-  const size_t tot = (size_t)L.n * L.n * L.n;
-  k_meanfield_src<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(c.work[2], phi, L.rho, L.colloc, L.n,
+  k_meanfield_src<<<dim3(1, L.n, L.n), std::min(1024, (L.n + 31) / 32 * 32), 0, c.stream>>>(c.work[2], phi, L.rho, L.colloc, L.n,
                                                                             (float)nions, (float)radius);
   VLB_LAUNCHED(c);
   coefficients(c, L, c.work[2], c.work[0], c.work[1], csol);
@@ -425,7 +472,7 @@ void launch_mean_field_coefficients(Ctx& c, Level& L, const float* phi, float* c
 // csol += S^-1 [V_xc(rho) + V_jel(r)] (src/devicemesh.jl:171-183)
 void launch_mean_field_add(Ctx& c, Level& L, double nions, double radius) {
   const size_t tot = (size_t)L.n * L.n * L.n;
-  k_meanfield_src<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(c.work[2], nullptr, L.rho, L.colloc,
+  k_meanfield_src<<<dim3(1, L.n, L.n), std::min(1024, (L.n + 31) / 32 * 32), 0, c.stream>>>(c.work[2], nullptr, L.rho, L.colloc,
                                                                             L.n, (float)nions, (float)radius);
   VLB_LAUNCHED(c);
   coefficients(c, L, c.work[2], c.work[0], c.work[1], c.work[2]);
@@ -438,9 +485,10 @@ void launch_poisson(Ctx& c) {
   Level& C = c.coarse;
   // coarse: multipole faces + solve (src/poisson.jl:351-354)
   const int mc = C.n * C.n;
-  k_moments<<<(mc + 127) / 128, 128, 0, c.stream>>>(C.rho, C.dual_d, C.n, c.partials);
+  (void)mc;
+  k_moments<<<kMomBlocks, 256, 0, c.stream>>>(C.rho, C.dual_d, C.n, c.partials);
   VLB_LAUNCHED(c);
-  k_multipole<<<1, 1024, 0, c.stream>>>(c.partials, mc, c.dsc);
+  k_moment_sums<<<10, 256, 0, c.stream>>>(c.partials, c.dsc);
   VLB_LAUNCHED(c);
   const int nfc = 2 * C.n * C.n + (C.n - 2) * (4 * C.n - 4);
   k_faces_multipole<<<(nfc + 255) / 256, 256, 0, c.stream>>>(C.phi, C.colloc, C.n, c.dsc);

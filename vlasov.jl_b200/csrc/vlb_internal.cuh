@@ -19,6 +19,14 @@ constexpr int kChunk = 128;  // particles per gather work item
 constexpr int kStatusScanTimeout = 1;   // decoupled look-back gave up
 constexpr int kStatusBadCell = 2;       // a particle outside the CIC domain table
 constexpr int kStatusOverflow = 4;      // fixed-point accumulator out of range
+constexpr int kStatusMmaTimeout = 8;    // a tensor-core product gave up waiting on its copies or MMAs
+
+// A matrix split into TF32 head and tail for the tensor-core mode product:
+// [hi | lo], each npad16 x kpad8 in the canonical K-major no-swizzle layout.
+struct TcImage {
+  float* img = nullptr;
+  int n = 0, npad16 = 0, kpad8 = 0;
+};
 
 // Device-resident scalars of one step.  One block, zeroed (partly) at the
 // start of a step and copied back in one transfer at its end.
@@ -59,6 +67,7 @@ struct Level {
   float* sinvT = nullptr;           // [n][npad]  (S^-1)^T, zero padded
   float* MT = nullptr;              // [ni][nipad]
   float* MinvT = nullptr;           // [ni][nipad]
+  TcImage tc_sinv, tc_M, tc_Minv;   // the same matrices for the 3xTF32 products
   float* lap = nullptr;             // [n*n] row-major
   float* invlsum = nullptr;         // [ni^3]
   float* dual = nullptr;            // [3n]
@@ -125,6 +134,8 @@ struct Ctx {
   double* partials = nullptr;                 // [10 * n^2] reductions
   // Poisson work buffers (max n^3)
   float* work[3] = {nullptr, nullptr, nullptr};
+  int mode_precision = 0;     // VLB_POISSON_FP32 or VLB_POISSON_3XTF32
+  unsigned* tc_sync = nullptr;  // grid-barrier counter of the tensor-core chains
   // scalars
   DeviceScalars* dsc = nullptr;
   DeviceScalars* hsc = nullptr;  // pinned, results
@@ -156,6 +167,12 @@ void launch_deposit_fine(Ctx& c, double charge, int mode);
 void launch_deposit_coarse(Ctx& c, double charge);
 // poisson.cu
 void launch_poisson(Ctx& c);
+// mode_tc.cu
+bool tc_supported(int n);
+TcImage make_tc_image(const double* A, int n);
+void tc_setup(Ctx& c);
+void launch_mode_chain_tc(Ctx& c, const TcImage& A, int nst, const float* const* src, float* const* dest,
+                          const int* epi, long long m, const float* invl);
 void launch_coefficients(Ctx& c, Level& L, const float* src, float* dst);
 void launch_mean_field_coefficients(Ctx& c, Level& L, const float* phi, float* csol,
                                     double nions, double radius);

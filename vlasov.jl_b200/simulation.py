@@ -329,8 +329,14 @@ class DeviceAccelerator:
     def deposit_cic(self, charge: float):
         L.check(L.lib().vlb_deposit_coarse(self._h, charge))
 
-    def poisson(self):
-        L.check(L.lib().vlb_poisson(self._h, L.VLB_POISSON_FP32))
+    def poisson(self, precision: int = L.VLB_POISSON_FP32):
+        """poisson!(phi, rho, meshes); precision VLB_POISSON_FP32 (CUDA cores) or
+        VLB_POISSON_3XTF32 (split-precision tensor cores).  Later coefficient
+        conversions use the same precision."""
+        L.check(L.lib().vlb_poisson(self._h, precision))
+
+    def set_precision(self, precision: int):
+        L.check(L.lib().vlb_set_precision(self._h, precision))
 
     def spline_coefficients(self, level: int):
         L.check(L.lib().vlb_coefficients(self._h, level))
@@ -437,7 +443,8 @@ class Simulation:
 
     def __init__(self, p: SimulationParameters, profile: RadialProfile, *, projectile: Projectile | None = None,
                  seed: int = -1, consistent_startup: bool = False, device: int = 0,
-                 fixed_point: bool = False, use_graph: bool = True, capture_radius: float = 8.0):
+                 fixed_point: bool = False, use_graph: bool = True, capture_radius: float = 8.0,
+                 precision: int = L.VLB_POISSON_FP32):
         self.params = p
         self.meshes = build_meshes(p.nfine, p.ninner, p.nouter, p.rcluster, p.rbox)
         self.smoothing = gaussian_smoothing(self.meshes.fine.axis)
@@ -445,6 +452,7 @@ class Simulation:
         self.weight = p.nelectrons / p.nparticles
         self.projectile = projectile
         self.fixed_point = fixed_point
+        self.precision = precision
         self.use_graph = use_graph
         self.capture_radius = capture_radius
         positions, momenta = sample_thomas_fermi(profile, p.nparticles, self.weight, seed=seed)
@@ -468,6 +476,7 @@ class Simulation:
         sp.advance_projectile = int(advance)
         sp.push = int(push)
         sp.use_graph = int(self.use_graph and push)
+        sp.poisson_precision = self.precision
         return sp
 
     def prime_leapfrog(self, positions, momenta, consistent: bool = False):
