@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--nfine", type=int, default=64)
     ap.add_argument("--profile", default="thomas-fermi", choices=["thomas-fermi", "uniform-sphere"])
     ap.add_argument("--deposit", default="float32", choices=["float32", "fixed64"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "3xtf32"],
+    ap.add_argument("--precision", default="3xtf32", choices=["fp32", "3xtf32"],
                     help="mode products on the CUDA cores (fp32) or split-precision on the tensor cores")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -24,9 +24,10 @@ PUBLISHED_Q350, PUBLISHED_OUT350 = 0.635, 74_061   # README.md:94
 PUBLISHED_OUT700 = 216_829            # README.md:96
 
 
-@pytest.mark.parametrize("fixed_point", [False, True], ids=["float32", "fixed64"])
-def test_capture_curve_at_8e6_matches_the_published_run(cuda_device, fixed_point):
-    r = vb.xenon.run(8_000_000, 64, fixed_point=fixed_point, device=cuda_device, quiet=True)
+@pytest.mark.parametrize("fixed_point,precision", [(False, "fp32"), (True, "fp32"), (False, "3xtf32")],
+                         ids=["float32", "fixed64", "float32-3xtf32"])
+def test_capture_curve_at_8e6_matches_the_published_run(cuda_device, fixed_point, precision):
+    r = vb.xenon.run(8_000_000, 64, fixed_point=fixed_point, device=cuda_device, quiet=True, precision=precision)
     assert r["nsteps"] == 700
     q, out = r["q8"], r["outcount"]
     assert min(abs(q[-1] - p) for p in PUBLISHED_Q700) <= 0.005, q[-1]

@@ -10,7 +10,7 @@
 //     F = -w ( sum c gx oy oz, sum c ox gy oz, sum c ox oy gz )
 //
 // with all sixty smoothing values in registers.  The sum over the stencil is
-// reassociated (x first, then y, then z) against the reference's order,
+// reassociated (y first, then x, then z) against the reference's order,
 // which changes rounding only.  The projectile's Gaussian force
 // (src/projectile.jl:95-108) is evaluated per particle at the position
 // rebuilt from the *cell's* (clamped) knots, as the reference does, its
@@ -112,10 +112,9 @@ __device__ __forceinline__ void block_add_red(float ax, float ay, float az, floa
 // items taken from a dynamic counter.  The warp stages its cell's 10^3
 // stencil in its own slice of shared memory (kept while consecutive items
 // share the cell) and takes 32 particles at a time, one per lane.  No
-// barrier but __syncwarp.  The x and y columns live in registers; the z
-// loop is not unrolled and reads its two values per step from the table
-// (L1), which keeps the contraction's code small enough for the
-// instruction cache.
+// barrier but __syncwarp.  All sixty table values of the particle live in
+// registers; every stencil row read from shared memory (a broadcast: the
+// whole warp reads the same row) feeds ten independent packed FMAs.
 constexpr int kRow = 12;            // padded stencil row (10 values, 16-byte aligned)
 constexpr int kTile = 10 * 10 * kRow;
 
@@ -160,7 +159,8 @@ __global__ void __launch_bounds__(kGThreads) k_field(
       const int cx = table_column(dx0, spacing, nbdt, ncol);
       const int cy = table_column(dy0, spacing, nbdt, ncol);
       const int cz = table_column(dz0, spacing, nbdt, ncol);
-      // x columns as pairs of neighbouring stencil points, for the packed FMA
+      // x columns as pairs of neighbouring stencil points; y values as
+      // broadcast pairs, for the packed FMA
       float2 ox2[5], gx2[5];
       {
         const float2* po = reinterpret_cast<const float2*>(ov + (size_t)(cx - 1) * 10);
@@ -168,17 +168,27 @@ __global__ void __launch_bounds__(kGThreads) k_field(
 #pragma unroll
         for (int a = 0; a < 5; ++a) { ox2[a] = __ldg(po + a); gx2[a] = __ldg(pg + a); }
       }
-      float oy[10], gy[10];
-      load10(ov, cy, oy);
-      load10(gr, cy, gy);
-      const float* ozp = ov + (size_t)(cz - 1) * 10;
-      const float* gzp = gr + (size_t)(cz - 1) * 10;
+      float2 oy2[10], gy2[10];
+      {
+        float oy[10], gy[10];
+        load10(ov, cy, oy);
+        load10(gr, cy, gy);
+#pragma unroll
+        for (int j = 0; j < 10; ++j) { oy2[j] = make_float2(oy[j], oy[j]); gy2[j] = make_float2(gy[j], gy[j]); }
+      }
+      float ozr[10], gzr[10];
+      load10(ov, cz, ozr);
+      load10(gr, cz, gzr);
       float sx = 0.f, sy = 0.f, sz = 0.f;
-#pragma unroll 1
+#pragma unroll
       for (int kk = 0; kk < 10; ++kk) {
-        const float oz = __ldg(ozp + kk), gz = __ldg(gzp + kk);
-        float tx = 0.f, ty = 0.f, tz = 0.f;
+        const float oz = ozr[kk], gz = gzr[kk];
         const float* plane = tile + kk * 10 * kRow;
+        // y first: Yo[a] = sum_j c[a,j] oy_j, Yg[a] = sum_j c[a,j] gy_j, ten
+        // independent packed accumulators per row
+        float2 yo[5], yg[5];
+#pragma unroll
+        for (int a = 0; a < 5; ++a) { yo[a] = make_float2(0.f, 0.f); yg[a] = make_float2(0.f, 0.f); }
 #pragma unroll
         for (int jj = 0; jj < 10; ++jj) {
           const float4 c0 = *reinterpret_cast<const float4*>(plane + jj * kRow);
@@ -186,20 +196,23 @@ __global__ void __launch_bounds__(kGThreads) k_field(
           const float2 c2 = *reinterpret_cast<const float2*>(plane + jj * kRow + 8);
           const float2 cp[5] = {make_float2(c0.x, c0.y), make_float2(c0.z, c0.w), make_float2(c1.x, c1.y),
                                 make_float2(c1.z, c1.w), c2};
-          float2 dxp = make_float2(0.f, 0.f), val = make_float2(0.f, 0.f);
 #pragma unroll
           for (int a = 0; a < 5; ++a) {
-            dxp = __ffma2_rn(cp[a], gx2[a], dxp);
-            val = __ffma2_rn(cp[a], ox2[a], val);
+            yo[a] = __ffma2_rn(cp[a], oy2[jj], yo[a]);
+            yg[a] = __ffma2_rn(cp[a], gy2[jj], yg[a]);
           }
-          const float dx1 = dxp.x + dxp.y, va1 = val.x + val.y;
-          tx = fmaf(oy[jj], dx1, tx);
-          ty = fmaf(gy[jj], va1, ty);
-          tz = fmaf(oy[jj], va1, tz);
         }
-        sx = fmaf(oz, tx, sx);
-        sy = fmaf(oz, ty, sy);
-        sz = fmaf(gz, tz, sz);
+        // then x: tx = sum_a gx_a Yo[a], ty = sum_a ox_a Yg[a], tz = sum_a ox_a Yo[a]
+        float2 tx2 = make_float2(0.f, 0.f), ty2 = make_float2(0.f, 0.f), tz2 = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int a = 0; a < 5; ++a) {
+          tx2 = __ffma2_rn(gx2[a], yo[a], tx2);
+          ty2 = __ffma2_rn(ox2[a], yg[a], ty2);
+          tz2 = __ffma2_rn(ox2[a], yo[a], tz2);
+        }
+        sx = fmaf(oz, tx2.x + tx2.y, sx);
+        sy = fmaf(oz, ty2.x + ty2.y, sy);
+        sz = fmaf(gz, tz2.x + tz2.y, sz);
       }
       float fx = -wf * sx, fy = -wf * sy, fz = -wf * sz;
       if (P.on) {

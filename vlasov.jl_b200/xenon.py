@@ -21,7 +21,8 @@ import time
 
 
 def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point: bool = False,
-        uniform: bool = False, nsteps: int | None = None, device: int = 0, seed: int = -1, quiet: bool = False):
+        uniform: bool = False, nsteps: int | None = None, device: int = 0, seed: int = -1, quiet: bool = False,
+        precision: str = "fp32"):
     """Runs the crossing; returns a dict with the capture curve (q(<8) and
     outcount after every step), the final charge and the timing."""
     import numpy as np
@@ -33,8 +34,10 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
     p = S.SimulationParameters.for_grid(nfine, rcluster=78.0, rbox=235.0, nparticles=npart, dt=dt)
     prof = S.uniform_sphere_profile() if uniform else S.thomas_fermi_profile()
     t0 = time.time()
+    from . import _lib as L
+    prec = {"fp32": L.VLB_POISSON_FP32, "3xtf32": L.VLB_POISSON_3XTF32}[precision]
     sim = S.Simulation(p, prof, projectile=S.xenon_projectile(v=v, x0=x0, dt=dt), seed=seed,
-                       fixed_point=fixed_point, device=device)
+                       fixed_point=fixed_point, device=device, precision=prec)
     built = time.time() - t0
     if not quiet:
         print(f"Na196 + Xe25+, 500 keV, b = 45 a0 | {npart:.1e} particles, grid {2 * nfine + 2}^3")
@@ -67,7 +70,8 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
         print(f"charge carried away by the ion: {q[-1]:.3f} electrons")
     return {"npart": npart, "nfine": nfine, "nsteps": nsteps, "q8": q.tolist(), "outcount": out.tolist(),
             "x_ion": xs.tolist(), "final_q8": float(q[-1]), "final_outcount": int(out[-1]),
-            "wall_s": elapsed, "built_s": built, "fixed_point": fixed_point, "uniform": uniform}
+            "wall_s": elapsed, "built_s": built, "fixed_point": fixed_point, "uniform": uniform,
+            "precision": precision}
 
 
 def main(argv=None):
@@ -77,11 +81,14 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--fixed-point", action="store_true")
     ap.add_argument("--uniform", action="store_true", help="uniform-sphere cloud instead of Thomas-Fermi")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "3xtf32"],
+                    help="mode products on the CUDA cores or split-precision on the tensor cores")
     ap.add_argument("--json", default=None, help="write the capture curve here")
     a = ap.parse_args(argv)
     if a.nfine % 2:
         ap.error("--nfine must be even")
-    r = run(a.particules, a.nfine, fixed_point=a.fixed_point, uniform=a.uniform, nsteps=a.steps)
+    r = run(a.particules, a.nfine, fixed_point=a.fixed_point, uniform=a.uniform, nsteps=a.steps,
+            precision=a.precision)
     if a.json:
         with open(a.json, "w") as f:
             json.dump(r, f)
