@@ -92,3 +92,28 @@ def test_capture_of_a_slow_projectile_is_a_charge(cuda_device):
     assert 0 <= d.enclosed_charge <= 196
     assert d.noccupied > 100 and d.status == 0
     assert abs(d.enclosed_charge - sim.enclosed_charge(8.0)) < 1e-12
+
+
+def test_upload_after_graph_steps_rebuilds_the_cell_keys(cuda_device):
+    """The captured step takes its cell keys from the previous step's push; a
+    cloud uploaded after graph steps must go through the eager step, which
+    computes them, and give what a fresh context gives (to the noise of the
+    float32 atomics of the coarse deposit, as in the graph test above; stale
+    keys would scramble the sort instead)."""
+    a = make_sim(fixed=True, graph=False)
+    snap = a.accelerator.download()
+    proj0 = (a.projectile.position.copy(), a.projectile.previous.copy(), a.projectile.velocity.copy())
+    b = make_sim(fixed=True, graph=True)
+    for _ in range(3):
+        b.step()
+    b.accelerator.upload(*snap)
+    b.projectile.position, b.projectile.previous, b.projectile.velocity = (x.copy() for x in proj0)
+    for _ in range(2):
+        da, db = a.step(), b.step()
+        assert da.outcount == db.outcount and da.nout == db.nout and da.noccupied == db.noccupied
+        assert abs(da.kinetic - db.kinetic) < 1e-6 * da.kinetic
+    ka, dka, pka, pdka = a.accelerator.download()
+    kb, dkb, pkb, pdkb = b.accelerator.download()
+    # the same stable sort order: the previous positions are the same records
+    assert np.array_equal(pka, pkb) and np.max(np.abs(pdka - pdkb)) < 1e-5
+    assert np.mean(np.all(ka == kb, axis=0)) > 0.9999 and np.max(np.abs(dka - dkb)) < 1e-5

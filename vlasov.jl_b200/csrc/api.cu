@@ -265,7 +265,7 @@ void enqueue_step(Ctx& c, const vlb_step_params& p) {
   stage_mark(c, 6);
   launch_projectile_update(c, p.dt, p.jellium_nions, p.jellium_radius, p.advance_projectile);
   stage_mark(c, 7);
-  if (p.push) launch_push(c, p.dt, p.rcmax, p.capture_radius);
+  if (p.push) launch_push(c, p.dt, p.rcmax, p.capture_radius, true);
   stage_mark(c, 8);
   if (!p.push && p.capture_radius > 0) launch_enclosed(c, p.capture_radius);
   stage_mark(c, 9);
@@ -459,6 +459,7 @@ int vlb_upload_particles(vlb_ctx* ctx, const int32_t* knode, const float* delta,
     }
     VLB_CUDA(cudaStreamSynchronize(c.stream));
     c.sorted = false;
+    c.keys_ready = false;
     return VLB_OK;
   });
 }
@@ -619,7 +620,7 @@ int vlb_push(vlb_ctx* ctx, double dt, double rcmax, double diag[5]) {
   CTX_OR_FAIL;
   if (!(dt > 0)) return fail(VLB_ERR_ARG, "dt must be positive");
   return guarded([&]() -> int {
-    launch_push(c, dt, rcmax, 0.0);
+    launch_push(c, dt, rcmax, 0.0, false);
     fetch_scalars(c);
     if (diag)
       for (int i = 0; i < 5; ++i) diag[i] = c.hsc->diag[i];
@@ -639,7 +640,8 @@ int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, 
   return guarded([&]() -> int {
     upload_projectile(c, proj);
     const bool graph = params->use_graph && !c.profile;
-    if (graph && c.graph_valid && same_params(c.graph_params, *params)) {
+    // the captured step starts from keys written by the previous push
+    if (graph && c.graph_valid && c.keys_ready && same_params(c.graph_params, *params)) {
       const int g = c.cur;
       VLB_CUDA(cudaGraphLaunch(c.gexec[g], c.stream));
       c.launches += c.graph_launches;

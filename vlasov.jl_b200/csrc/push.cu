@@ -35,12 +35,16 @@ __device__ __forceinline__ void verlet1(int kq, float dq, int ok, float od, floa
 // component array (Npad is a multiple of 64).  When `r2cap` > 0 the same pass
 // counts the particles within sqrt(r2cap) of the projectile after the step
 // (enclosed_charge, float64 positions), which the reference reads after
-// step! on the host.
+// step! on the host.  When `keys` is set it also writes the cell key of
+// every new position and adds it to the cell histogram (zero on entry) --
+// the first stage of the next step's sort, done while the positions are in
+// registers.
 __global__ void __launch_bounds__(256) k_push(int64_t N, int64_t Npad, int32_t* __restrict__ k, float* __restrict__ d,
                                               int32_t* __restrict__ pk, float* __restrict__ pd,
                                               const float* __restrict__ force, float a, float h, float x0, float pfac,
                                               float r2max, float inv2M, double* diag, double r2cap, double x0d,
-                                              double hd, DeviceScalars* dsc) {
+                                              double hd, DeviceScalars* dsc, uint32_t* __restrict__ keys,
+                                              int32_t* __restrict__ counts, int nk) {
   double ek = 0, eo = 0, lx = 0, ly = 0, lz = 0;
   unsigned cnt = 0;
   const double P0 = dsc->proj_pos[0], P1 = dsc->proj_pos[1], P2 = dsc->proj_pos[2];
@@ -89,6 +93,21 @@ __global__ void __launch_bounds__(256) k_push(int64_t N, int64_t Npad, int32_t* 
         // padding slots past N keep their (unused) contents
 #pragma unroll
         for (int c = 0; c < 3; ++c) { kn[c][u] = kq[c][u]; dn[c][u] = dq[c][u]; }
+      }
+    }
+    if (keys) {
+      // warp-aggregated histogram: the cloud is sorted, so lanes mostly share
+      // cells; one atomic per group of equal keys for each of the 4 slots
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const bool valid = i0 + u < N;
+        const unsigned m = __ballot_sync(__activemask(), valid);
+        if (valid) {
+          const uint32_t key = cell_key(kn[0][u], kn[1][u], kn[2][u], nk);
+          keys[i0 + u] = key;
+          const unsigned peers = __match_any_sync(m, key);
+          if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counts[key], __popc(peers));
+        }
       }
     }
 #pragma unroll
@@ -217,7 +236,7 @@ double measure_fp32_peak(int device) {
   return flops / (ms * 1e-3) / 1e12;
 }
 
-void launch_push(Ctx& c, double dt, double rcmax, double capture_radius) {
+void launch_push(Ctx& c, double dt, double rcmax, double capture_radius, bool keys) {
   Particles& P = c.part[c.cur];
   const double M = c.weight;  // ELECTRON_MASS * weight
   VLB_CUDA(cudaMemsetAsync(c.dsc->diag, 0, sizeof(c.dsc->diag), c.stream));
@@ -225,8 +244,10 @@ void launch_push(Ctx& c, double dt, double rcmax, double capture_radius) {
   k_push<<<grid_for(c, (c.N + 3) / 4, 256, 8), 256, 0, c.stream>>>(
       c.N, c.Npad, P.k, P.d, P.pk, P.pd, c.force, (float)(dt * dt / M), c.hf, c.x0f, (float)(M / (2 * dt)),
       (float)(rcmax * rcmax), (float)(1 / (2 * M)), c.dsc->diag,
-      capture_radius > 0 ? capture_radius * capture_radius : 0.0, c.x0, c.h, c.dsc);
+      capture_radius > 0 ? capture_radius * capture_radius : 0.0, c.x0, c.h, c.dsc, keys ? c.keys : nullptr,
+      c.counts, c.fine.nk);
   VLB_LAUNCHED(c);
+  c.keys_ready = keys;
 }
 
 void launch_projectile_update(Ctx& c, double dt, double nions, double jradius, int advance) {

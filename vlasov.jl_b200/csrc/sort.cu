@@ -7,12 +7,15 @@
 // then by index before the sort.
 //
 //   1. cell keys + warp-aggregated histogram over nk^3 cells;
-//   2. decoupled look-back scans: cell offsets, then the occupied-cell list
-//      with its bounds;
-//   3. LSD radix sort of (key, index) in passes of at most 10 bits, each
+//   2. a decoupled look-back scan that compacts the occupied cells;
+//   3. one CTA scans the occupied cells (a few thousand): their bounds, the
+//      gather's work items (chunks of at most kChunk particles) and the
+//      out-of-stencil slots, all functions of the cell alone; one warp per
+//      occupied cell then writes the item list and the out-of-stencil list
+//      (increasing slot order);
+//   4. LSD radix sort of (key, index) in passes of at most 10 bits, each
 //      pass stable (warp multi-split ranks + a scanned digit table);
-//   4. one gather of the 48-byte records into the other buffer (swap);
-//   5. a look-back scan that compacts the out-of-stencil slots.
+//   5. one gather of the 48-byte records into the other buffer (swap).
 //
 // Every spin of the look-back is bounded: after kSpinLimit polls the tile
 // records kStatusScanTimeout in the step's status word and gives up.
@@ -82,52 +85,116 @@ __global__ void __launch_bounds__(256) k_keys_hist(int64_t N, int64_t Npad, cons
 struct ScanInArray { const uint32_t* a; __device__ uint32_t operator()(int64_t i) const { return a[i]; } };
 struct ScanOutArray { uint32_t* a; __device__ void operator()(int64_t i, uint32_t p, uint32_t) const { a[i] = p; } };
 
-struct ScanInCounts { const int32_t* c; __device__ uint32_t operator()(int64_t i) const { return (uint32_t)c[i]; } };
-struct ScanOutOffsets { int32_t* off; __device__ void operator()(int64_t i, uint32_t p, uint32_t) const { off[i] = (int32_t)p; } };
-
 struct ScanInOccupied { const int32_t* c; __device__ uint32_t operator()(int64_t i) const { return c[i] > 0 ? 1u : 0u; } };
 struct ScanOutOccupied {
-  int32_t* occupied; int32_t* bounds; const int32_t* off; int64_t ncell; int64_t N;
+  int32_t* occupied;
   __device__ void operator()(int64_t i, uint32_t p, uint32_t v) const {
-    if (v) { occupied[p] = (int32_t)i; bounds[p] = off[i]; }
-    if (i == ncell - 1) bounds[p + v] = (int32_t)N;
+    if (v) occupied[p] = (int32_t)i;
   }
 };
 
-struct ScanInOutside {
-  const uint32_t* skeys; int nk, n;
-  __device__ uint32_t operator()(int64_t s) const {
-    int kx, ky, kz;
-    cell_knots(skeys[s], nk, kx, ky, kz);
-    return field_fits(kx, ky, kz, n) ? 0u : 1u;
-  }
-};
-struct ScanOutOutside {
-  int32_t* outlist;
-  __device__ void operator()(int64_t s, uint32_t p, uint32_t v) const { if (v) outlist[p] = (int32_t)s; }
-};
+// One CTA over the occupied cells g < nocc (in increasing cell order), each
+// thread a contiguous run of them: exclusive prefixes of the particle count
+// (bounds), of the number of work items (ceil(count / kChunk)) and of the
+// particles of cells whose 10^3 stencil leaves the fine grid (out_start, -1
+// for the others); totals into bounds[nocc], nitems and outcount.
+constexpr int kListThreads = 1024;
 
-// Chunks of at most kChunk particles of each occupied cell: the gather's
-// work items.
-struct ScanInChunks {
-  const int32_t* bounds; const DeviceScalars* dsc;
-  __device__ uint32_t operator()(int64_t g) const {
-    if (g >= dsc->noccupied) return 0u;
-    return (uint32_t)((bounds[g + 1] - bounds[g] + kChunk - 1) / kChunk);
+__device__ __forceinline__ void block_scan3(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t* tot) {
+  // exclusive scan of three counters over the CTA; tot receives the sums
+  __shared__ uint32_t sh[3][kListThreads / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t v[3] = {a, b, c}, incl[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    uint32_t x = v[q];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    incl[q] = x;
+    if (lane == 31) sh[q][w] = x;
   }
-};
-struct ScanOutChunks {
-  int32_t* start;
-  __device__ void operator()(int64_t g, uint32_t p, uint32_t) const { start[g] = (int32_t)p; }
-};
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      uint32_t x = sh[q][lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      sh[q][lane] = x;  // inclusive over warps
+    }
+  }
+  __syncthreads();
+  const uint32_t wb[3] = {w ? sh[0][w - 1] : 0u, w ? sh[1][w - 1] : 0u, w ? sh[2][w - 1] : 0u};
+  a = wb[0] + incl[0] - v[0];
+  b = wb[1] + incl[1] - v[1];
+  c = wb[2] + incl[2] - v[2];
+  tot[0] = sh[0][31];
+  tot[1] = sh[1][31];
+  tot[2] = sh[2][31];
+}
 
-__global__ void k_items(const int32_t* __restrict__ bounds, const int32_t* __restrict__ start, const DeviceScalars* dsc,
-                        int32_t* __restrict__ item_cell) {
+__global__ void __launch_bounds__(kListThreads) k_cell_lists(const int32_t* __restrict__ counts,
+                                                             const int32_t* __restrict__ occupied, DeviceScalars* dsc,
+                                                             int nk, int n, int32_t* __restrict__ bounds,
+                                                             int32_t* __restrict__ chunk_start,
+                                                             int32_t* __restrict__ out_start) {
   const int nocc = dsc->noccupied;
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nocc; g += gridDim.x * blockDim.x) {
-    const int nch = (bounds[g + 1] - bounds[g] + kChunk - 1) / kChunk;
-    const int s0 = start[g];
-    for (int ch = 0; ch < nch; ++ch) item_cell[s0 + ch] = g;
+  const int per = (nocc + kListThreads - 1) / kListThreads;
+  const int g0 = min((int)threadIdx.x * per, nocc), g1 = min(g0 + per, nocc);
+  uint32_t sc = 0, sch = 0, so = 0;
+  for (int g = g0; g < g1; ++g) {
+    const int cell = occupied[g];
+    const uint32_t c = (uint32_t)counts[cell];
+    int kx, ky, kz;
+    cell_knots((uint32_t)cell, nk, kx, ky, kz);
+    sc += c;
+    sch += (c + kChunk - 1) / kChunk;
+    if (!field_fits(kx, ky, kz, n)) so += c;
+  }
+  uint32_t tot[3];
+  block_scan3(sc, sch, so, tot);
+  for (int g = g0; g < g1; ++g) {
+    const int cell = occupied[g];
+    const uint32_t c = (uint32_t)counts[cell];
+    int kx, ky, kz;
+    cell_knots((uint32_t)cell, nk, kx, ky, kz);
+    const bool fits = field_fits(kx, ky, kz, n);
+    bounds[g] = (int32_t)sc;
+    chunk_start[g] = (int32_t)sch;
+    out_start[g] = fits ? -1 : (int32_t)so;
+    sc += c;
+    sch += (c + kChunk - 1) / kChunk;
+    if (!fits) so += c;
+  }
+  if (threadIdx.x == 0) {
+    bounds[nocc] = (int32_t)tot[0];
+    dsc->nitems = (int32_t)tot[1];
+    dsc->outcount = (int32_t)tot[2];
+  }
+}
+
+// One warp per occupied cell: its work items and, for cells whose stencil
+// leaves the fine grid, its slots in the out-of-stencil list.
+__global__ void __launch_bounds__(256) k_expand_lists(const int32_t* __restrict__ bounds,
+                                                      const int32_t* __restrict__ chunk_start,
+                                                      const int32_t* __restrict__ out_start, const DeviceScalars* dsc,
+                                                      int32_t* __restrict__ item_cell, int32_t* __restrict__ outlist) {
+  const int nocc = dsc->noccupied;
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nocc; g += warps) {
+    const int b0 = bounds[g], cnt = bounds[g + 1] - b0;
+    const int nch = (cnt + kChunk - 1) / kChunk, c0 = chunk_start[g];
+    for (int ch = lane; ch < nch; ch += 32) item_cell[c0 + ch] = g;
+    const int o0 = out_start[g];
+    if (o0 >= 0)
+      for (int j = lane; j < cnt; j += 32) outlist[o0 + j] = b0 + j;
   }
 }
 
@@ -301,15 +368,44 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_downsweep(
 
 // ------------------------------------------------------------- the move
 // Moves the records into slot order: dst[s] = src[perm[s]], all twelve
-// component arrays.  Reads follow the permutation of a nearly sorted cloud,
-// so they stay within a few pages.
+// component arrays.  Four consecutive slots per thread: one 16-byte load of
+// their permutation entries, the 48 gathered loads all in flight, then one
+// 16-byte store per component array (Npad is a multiple of 64).  Reads
+// follow the permutation of a nearly sorted cloud, so they stay within a
+// few pages.
 __global__ void __launch_bounds__(256) k_gather_records(int64_t N, int64_t Npad, const uint32_t* __restrict__ perm,
                                                         const int32_t* __restrict__ k0, const float* __restrict__ d0,
                                                         const int32_t* __restrict__ pk0, const float* __restrict__ pd0,
                                                         int32_t* __restrict__ k1, float* __restrict__ d1,
                                                         int32_t* __restrict__ pk1, float* __restrict__ pd1) {
-  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < N; s += (int64_t)gridDim.x * blockDim.x) {
-    int64_t i = perm[s];
+  const int64_t nq = N / 4;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = 4 * q;
+    const uint4 pv = *reinterpret_cast<const uint4*>(perm + s);
+    const int64_t i[4] = {pv.x, pv.y, pv.z, pv.w};
+    int kv[3][4], pkv[3][4];
+    float dv[3][4], pdv[3][4];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        kv[c][u] = __ldg(k0 + c * Npad + i[u]);
+        dv[c][u] = __ldg(d0 + c * Npad + i[u]);
+        pkv[c][u] = __ldg(pk0 + c * Npad + i[u]);
+        pdv[c][u] = __ldg(pd0 + c * Npad + i[u]);
+      }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      *reinterpret_cast<int4*>(k1 + c * Npad + s) = make_int4(kv[c][0], kv[c][1], kv[c][2], kv[c][3]);
+      *reinterpret_cast<float4*>(d1 + c * Npad + s) = make_float4(dv[c][0], dv[c][1], dv[c][2], dv[c][3]);
+      *reinterpret_cast<int4*>(pk1 + c * Npad + s) = make_int4(pkv[c][0], pkv[c][1], pkv[c][2], pkv[c][3]);
+      *reinterpret_cast<float4*>(pd1 + c * Npad + s) = make_float4(pdv[c][0], pdv[c][1], pdv[c][2], pdv[c][3]);
+    }
+  }
+  // the last N mod 4 slots
+  for (int64_t s = 4 * nq + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < N;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = perm[s];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       k1[c * Npad + s] = k0[c * Npad + i];
@@ -333,15 +429,25 @@ void launch_sort(Ctx& c) {
   const int nk = c.fine.nk, n = c.fine.n;
   Particles& P = c.part[c.cur];
   Particles& Q = c.part[c.cur ^ 1];
-  VLB_CUDA(cudaMemsetAsync(c.counts, 0, sizeof(int32_t) * c.ncell, c.stream));
   VLB_CUDA(cudaMemsetAsync(c.scan_status, 0, c.scan_status_size * sizeof(unsigned long long), c.stream));
   VLB_CUDA(cudaMemsetAsync(c.dsc->scan_tiles, 0, sizeof(c.dsc->scan_tiles), c.stream));
-  k_keys_hist<<<grid_for(c, N, 256, 8), 256, 0, c.stream>>>(N, c.Npad, P.k, nk, c.keys, c.counts);
+  if (!c.keys_ready) {
+    VLB_CUDA(cudaMemsetAsync(c.counts, 0, sizeof(int32_t) * c.ncell, c.stream));
+    k_keys_hist<<<grid_for(c, N, 256, 8), 256, 0, c.stream>>>(N, c.Npad, P.k, nk, c.keys, c.counts);
+    VLB_LAUNCHED(c);
+  }
+  // the occupied cells, then their bounds, work items and out-of-stencil
+  // slots (cell_off holds the out-of-stencil start of each occupied cell)
+  scan(c, ScanInOccupied{c.counts}, ScanOutOccupied{c.occupied}, c.ncell, 1, &c.dsc->noccupied);
+  k_cell_lists<<<1, kListThreads, 0, c.stream>>>(c.counts, c.occupied, c.dsc, nk, n, c.bounds, c.chunk_start,
+                                                 c.cell_off);
   VLB_LAUNCHED(c);
-  // cell offsets, then the occupied list and its bounds
-  scan(c, ScanInCounts{c.counts}, ScanOutOffsets{c.cell_off}, c.ncell, 0, nullptr);
-  scan(c, ScanInOccupied{c.counts}, ScanOutOccupied{c.occupied, c.bounds, c.cell_off, c.ncell, N}, c.ncell, 1,
-       &c.dsc->noccupied);
+  k_expand_lists<<<c.num_sms * 4, 256, 0, c.stream>>>(c.bounds, c.chunk_start, c.cell_off, c.dsc, c.item_cell,
+                                                      c.outlist);
+  VLB_LAUNCHED(c);
+  // the histogram is spent: zero it for the push that may refill it
+  VLB_CUDA(cudaMemsetAsync(c.counts, 0, sizeof(int32_t) * c.ncell, c.stream));
+  c.keys_ready = false;
   // radix passes over the key bits
   int bits = 1;
   while ((1ll << bits) < (long long)c.ncell) ++bits;
@@ -367,16 +473,10 @@ void launch_sort(Ctx& c) {
     vin = vout;
     shift += b;
   }
-  k_gather_records<<<grid_for(c, N, 256, 16), 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
+  k_gather_records<<<grid_for(c, (N + 3) / 4, 256, 8), 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
                                                                    Q.pk, Q.pd);
   VLB_LAUNCHED(c);
   c.cur ^= 1;
-  // out-of-stencil slots, in increasing order
-  scan(c, ScanInOutside{c.skeys, nk, n}, ScanOutOutside{c.outlist}, N, 5, &c.dsc->outcount);
-  // the gather's work items
-  scan(c, ScanInChunks{c.bounds, c.dsc}, ScanOutChunks{c.chunk_start}, c.ncell, 6, &c.dsc->nitems);
-  k_items<<<grid_for(c, c.ncell, 256, 4), 256, 0, c.stream>>>(c.bounds, c.chunk_start, c.dsc, c.item_cell);
-  VLB_LAUNCHED(c);
   c.sorted = true;
 }
 

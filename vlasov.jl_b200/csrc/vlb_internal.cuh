@@ -142,6 +142,9 @@ struct Ctx {
   DeviceScalars* hin = nullptr;  // pinned, projectile staging
   // state
   bool sorted = false, have_forces = false;
+  // keys[] and counts[] hold the cell keys and histogram of part[cur] in slot
+  // order (written by the push of a fused step): the next sort skips them
+  bool keys_ready = false;
   // profiling
   bool profile = false;
   cudaEvent_t ev[kNumStages + 1];
@@ -182,7 +185,7 @@ void launch_forces(Ctx& c);
 // push.cu
 void launch_projectile_update(Ctx& c, double dt, double nions, double jradius, int advance);
 void launch_projectile_force_only(Ctx& c, double nions, double jradius);
-void launch_push(Ctx& c, double dt, double rcmax, double capture_radius);
+void launch_push(Ctx& c, double dt, double rcmax, double capture_radius, bool keys);
 void launch_enclosed(Ctx& c, double radius);
 
 
