@@ -71,8 +71,10 @@ def config_dict(args, n):
     return {"workload": "Na196 + Xe25+ 500 keV b=45 a0 collision, one fused step",
             "npart_per_gpu": args.npart, "fine_grid": f"{2 * args.nfine + 2}^3", "coarse_grid": f"{2 * args.nfine + 2}^3",
             "profile": args.profile, "deposit": args.deposit, "mode_products": args.precision, "dt": 0.5, "projectile": "Xe25+ v=0.40 x0=-70 b=45",
-            "cuda_graph": not args.no_graph, "l2": "inputs larger than L2 (2 x 384 MB particle state)",
-            "parallelism": f"replicas{n}" if n > 1 else "1 GPU"}
+            "cuda_graph": (not args.no_graph) if n == 1 else "per-phase eager (collectives between phases)",
+            "l2": "inputs larger than L2 (2 x 384 MB particle state)",
+            "parallelism": (f"{n} particle shards, NCCL all-reduce of the deposited grids and the projectile's "
+                            "reaction sums" if n > 1 else "1 GPU")}
 
 
 class ClockSampler:
@@ -227,9 +229,17 @@ def main():
         return float(t.item())
 
     p, prof, proj = workload(args, vb)
-    sim = vb.Simulation(p, prof, projectile=proj, device=local, fixed_point=args.deposit == "fixed64",
-                        precision=vb._lib.VLB_POISSON_3XTF32 if args.precision == "3xtf32" else vb._lib.VLB_POISSON_FP32,
-                        use_graph=not args.no_graph, seed=-1 - rank)
+    precision = vb._lib.VLB_POISSON_3XTF32 if args.precision == "3xtf32" else vb._lib.VLB_POISSON_FP32
+    if world > 1:
+        # weak scaling: npart per GPU, one cloud of world * npart particles
+        # sharded over the ranks (each rank draws its own slice)
+        p.nparticles = args.npart * world
+        sim = vb.sharded.ShardedSimulation(p, prof, comm=vb.sharded.TorchComm(), device=local, projectile=proj,
+                                           fixed_point=args.deposit == "fixed64", precision=precision,
+                                           sampling="per-rank", seed=-1)
+    else:
+        sim = vb.Simulation(p, prof, projectile=proj, device=local, fixed_point=args.deposit == "fixed64",
+                            precision=precision, use_graph=not args.no_graph, seed=-1)
     acc = sim.accelerator
     ext = torch.cuda.ExternalStream(acc.stream_handle(), device=torch.device("cuda", local))
     for _ in range(max(args.warmup, 3)):
@@ -256,14 +266,16 @@ def main():
     clk = clocks.summary(t_wall0, t_wall1)
 
     # per-stage device times (eager, stage events) for the roofline
-    sim.use_graph = False
+    if world == 1:
+        sim.use_graph = False
     acc.profile(True)
     nprof = max(3, min(args.steps, 20))
     for _ in range(nprof):
         sim.step()
     stages = {k: v / nprof for k, v in acc.stage_times().items()}
     acc.profile(False)
-    sim.use_graph = not args.no_graph
+    if world == 1:
+        sim.use_graph = not args.no_graph
 
     # end to end through the public API: cloud from pinned host memory, K
     # steps, cloud back to pinned host memory

@@ -231,6 +231,49 @@ VLB_API int vlb_push(vlb_ctx* ctx, double dt, double rcmax, double diag[5]);
 VLB_API int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params,
              vlb_step_result* result);
 
+/* ---- the same step sharded over several contexts (one per GPU), each
+ * holding a slice of the cloud.  No counterpart in the reference, which runs
+ * one device.  The step is the three phases below; between them the caller
+ * sums the exchange buffers over the shards, in place, on the context's
+ * stream (an all-reduce):
+ *   vlb_step_deposit  : sort, raw fine deposit, coarse deposit;
+ *                       then sum rho_fine, rho_coarse and scalars;
+ *   vlb_step_fields   : renormalise with the whole cloud's count, nested
+ *                       Poisson solve, mean field (identical on every shard),
+ *                       forces on this shard's particles;
+ *                       then sum reaction (the projectile's reaction sums);
+ *   vlb_step_advance  : projectile step (identical on every shard), push,
+ *                       capture count; results are this shard's (sum the
+ *                       kinetic, escaped, angular, enclosed and counts).
+ * With the fixed-point deposit the summed fine density does not depend on
+ * the order of the sum.  One context alone is vlb_step. */
+#define VLB_DTYPE_FLOAT32 0
+#define VLB_DTYPE_INT64 1
+
+typedef struct vlb_exchange {
+  void* rho_fine;             /* n^3 of rho_fine_dtype: the raw fine deposit */
+  int32_t rho_fine_dtype;     /* VLB_DTYPE_INT64 (fixed point) or VLB_DTYPE_FLOAT32 */
+  int32_t pad0_;
+  int64_t rho_fine_count;
+  float* rho_coarse;          /* n^3 float32: the coarse deposit */
+  int64_t rho_coarse_count;
+  double* scalars;            /* float64: [0] particles outside the deposit window */
+  int32_t scalars_count;
+  int32_t pad1_;
+  double* reaction;           /* float64 [4]: the projectile's reaction sums */
+  int32_t reaction_count;
+  int32_t pad2_;
+  void* stream;               /* the context's cudaStream_t */
+} vlb_exchange;
+
+/* Device addresses of the exchange buffers (valid for the context's life). */
+VLB_API int vlb_exchange_buffers(vlb_ctx* ctx, int32_t deposit_mode, vlb_exchange* out);
+VLB_API int vlb_step_deposit(vlb_ctx* ctx, const vlb_projectile* proj, const vlb_step_params* params);
+/* npart_global: particles in all shards together. */
+VLB_API int vlb_step_fields(vlb_ctx* ctx, const vlb_step_params* params, int64_t npart_global);
+VLB_API int vlb_step_advance(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params,
+                     vlb_step_result* result);
+
 /* sync_host! (src/simulation.jl:544-552) for one grid, and its inverse. */
 VLB_API int vlb_get_grid(vlb_ctx* ctx, int32_t which, float* host);
 VLB_API int vlb_set_grid(vlb_ctx* ctx, int32_t which, const float* host);

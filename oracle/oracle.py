@@ -74,6 +74,7 @@ def lib():
             "orc_outside": (ll, [ll, P_I, i32, P_I]),
             "orc_columns": (ll, [ll, P_I, P_F, f32, f32, f32, f32, f32, i32, i32, P_I]),
             "orc_deposit_sorted": (dbl, [pl, ps, ll, P_I, P_I, P_I, i32, ll, dbl, P_D]),
+            "orc_deposit_sorted_raw": (dbl, [pl, ps, ll, P_I, P_I, P_I, i32, P_D]),
             "orc_deposit_cic_device": (None, [pl, ll, P_I, P_F, f32, f32, dbl, P_D]),
             "orc_forces_device": (ll, [pl, pl, ps, ll, P_I, P_F, P_I, P_I, i32, P_D, P_D, dbl, dbl, dbl, pp,
                                        P_D, P_D]),

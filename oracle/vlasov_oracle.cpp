@@ -550,9 +550,25 @@ long long orc_columns(long long N, const int32_t* knode, const float* delta, flo
 // _deposit_sorted_kernel! (src/kernels.jl:601-726) accumulated in float64,
 // then the renormalisation of deposit_smoothed!(..., acc) (src/accelerator.jl:554-557).
 // Returns the charge before scaling.
+// The same deposit without the renormalisation (the raw density, which the
+// shards of a sharded step sum); returns its total charge.
+double orc_deposit_sorted_raw(const orc_level* F, const orc_smoothing* sm, long long N,
+                              const int32_t* cols, const int32_t* occupied, const int32_t* bounds,
+                              int32_t nocc, double* rho);
+
 double orc_deposit_sorted(const orc_level* F, const orc_smoothing* sm, long long N,
                           const int32_t* cols, const int32_t* occupied, const int32_t* bounds,
                           int32_t nocc, long long nout, double charge, double* rho) {
+  double q = orc_deposit_sorted_raw(F, sm, N, cols, occupied, bounds, nocc, rho);
+  const size_t tot = (size_t)F->n * F->n * F->n;
+  double scale = (double)(N - nout) * charge / q;
+  for (size_t t = 0; t < tot; ++t) rho[t] *= scale;
+  return q;
+}
+
+double orc_deposit_sorted_raw(const orc_level* F, const orc_smoothing* sm, long long N,
+                              const int32_t* cols, const int32_t* occupied, const int32_t* bounds,
+                              int32_t nocc, double* rho) {
   int n = F->n, nk = F->nk;
   size_t tot = (size_t)n * n * n;
   std::fill(rho, rho + tot, 0.0);
@@ -578,10 +594,7 @@ double orc_deposit_sorted(const orc_level* F, const orc_smoothing* sm, long long
         for (int a = 0; a < 8; ++a)
           rho[(bx + a) + (size_t)n * ((by + b) + (size_t)n * (bz + c))] += acc[a + 8 * (b + 8 * c)];
   }
-  double q = total_charge(rho, *F);
-  double scale = (double)(N - nout) * charge / q;
-  for (size_t t = 0; t < tot; ++t) rho[t] *= scale;
-  return q;
+  return total_charge(rho, *F);
 }
 
 // Coarse CIC deposit of the device path (src/kernels.jl:1207-1273,

@@ -14,5 +14,6 @@ from .simulation import (SimulationParameters, Jellium, BallSoftening, GaussianS
                          Simulation, StepDiagnostics, xenon_projectile)
 from . import _lib
 from . import xenon
+from . import sharded
 
 __all__ = [n for n in dir() if not n.startswith("_")]

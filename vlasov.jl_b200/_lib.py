@@ -38,7 +38,8 @@ EXPORTS = (
     "vlb_last_error", "vlb_version", "vlb_create", "vlb_destroy", "vlb_upload_particles",
     "vlb_download_particles", "vlb_sort", "vlb_get_sort", "vlb_deposit_fine", "vlb_deposit_coarse",
     "vlb_poisson", "vlb_set_precision", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
-    "vlb_push", "vlb_step", "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
+    "vlb_push", "vlb_step", "vlb_exchange_buffers", "vlb_step_deposit", "vlb_step_fields", "vlb_step_advance",
+    "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
     "vlb_enclosed_charge", "vlb_profile", "vlb_stage_count", "vlb_stage_name", "vlb_stage_times",
     "vlb_launch_count", "vlb_fp32_peak", "vlb_stream", "vlb_sample_thomas_fermi", "vlb_ran2", "vlb_pack_positions",
     "vlb_unpack_positions", "vlb_total_charge_noalloc",
@@ -86,6 +87,18 @@ class StepResult(C.Structure):
                 ("outcount", C.c_int32), ("noccupied", C.c_int32), ("status", C.c_int32)]
 
 
+class Exchange(C.Structure):
+    _fields_ = [("rho_fine", C.c_void_p), ("rho_fine_dtype", C.c_int32), ("pad0_", C.c_int32),
+                ("rho_fine_count", C.c_int64), ("rho_coarse", C.c_void_p), ("rho_coarse_count", C.c_int64),
+                ("scalars", C.c_void_p), ("scalars_count", C.c_int32), ("pad1_", C.c_int32),
+                ("reaction", C.c_void_p), ("reaction_count", C.c_int32), ("pad2_", C.c_int32),
+                ("stream", C.c_void_p)]
+
+
+VLB_DTYPE_FLOAT32 = 0
+VLB_DTYPE_INT64 = 1
+
+
 class VlbError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"vlb error {code}: {msg}")
@@ -124,6 +137,11 @@ def lib():
                                                 P_D, P_D]),
             "vlb_push": (C.c_int, [vp, C.c_double, C.c_double, P_D]),
             "vlb_step": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams), C.POINTER(StepResult)]),
+            "vlb_exchange_buffers": (C.c_int, [vp, C.c_int32, C.POINTER(Exchange)]),
+            "vlb_step_deposit": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams)]),
+            "vlb_step_fields": (C.c_int, [vp, C.POINTER(StepParams), C.c_int64]),
+            "vlb_step_advance": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams),
+                                           C.POINTER(StepResult)]),
             "vlb_get_grid": (C.c_int, [vp, C.c_int32, P_F]),
             "vlb_set_grid": (C.c_int, [vp, C.c_int32, P_F]),
             "vlb_get_forces": (C.c_int, [vp, P_F]),

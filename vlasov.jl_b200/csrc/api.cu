@@ -247,15 +247,24 @@ void reset_step_scalars(Ctx& c) {
 
 // The fused step: everything on the stream, no host synchronisation.
 // Stage events are recorded only when profiling (never inside a capture).
-void enqueue_step(Ctx& c, const vlb_step_params& p) {
+// It runs in three phases; a sharded step exchanges between them (the raw
+// deposits and the deposit-window count after the first, the projectile's
+// reaction sums after the second).  normalize_npart > 0: renormalise the
+// fine density inside the phase (the whole cloud is in this context).
+void enqueue_phase_deposit(Ctx& c, const vlb_step_params& p, int64_t normalize_npart) {
   reset_step_scalars(c);
   stage_mark(c, 0);
   launch_sort(c);
   stage_mark(c, 1);
-  launch_deposit_fine(c, c.weight, p.deposit_mode);
+  launch_deposit_fine_raw(c, p.deposit_mode);
+  if (normalize_npart > 0) launch_deposit_fine_normalize(c, c.weight, p.deposit_mode, normalize_npart);
   stage_mark(c, 2);
   launch_deposit_coarse(c, c.weight);
   stage_mark(c, 3);
+}
+
+void enqueue_phase_fields(Ctx& c, const vlb_step_params& p, int64_t normalize_npart) {
+  if (normalize_npart > 0) launch_deposit_fine_normalize(c, c.weight, p.deposit_mode, normalize_npart);
   launch_poisson(c);
   stage_mark(c, 4);
   launch_mean_field_coefficients(c, c.fine, c.fine.phi, c.fine.csol, p.jellium_nions, p.jellium_radius);
@@ -263,12 +272,21 @@ void enqueue_step(Ctx& c, const vlb_step_params& p) {
   stage_mark(c, 5);
   launch_forces(c);
   stage_mark(c, 6);
+}
+
+void enqueue_phase_advance(Ctx& c, const vlb_step_params& p) {
   launch_projectile_update(c, p.dt, p.jellium_nions, p.jellium_radius, p.advance_projectile);
   stage_mark(c, 7);
   if (p.push) launch_push(c, p.dt, p.rcmax, p.capture_radius, true);
   stage_mark(c, 8);
   if (!p.push && p.capture_radius > 0) launch_enclosed(c, p.capture_radius);
   stage_mark(c, 9);
+}
+
+void enqueue_step(Ctx& c, const vlb_step_params& p) {
+  enqueue_phase_deposit(c, p, c.N);
+  enqueue_phase_fields(c, p, 0);
+  enqueue_phase_advance(c, p);
 }
 
 bool same_params(const vlb_step_params& a, const vlb_step_params& b) {
@@ -629,15 +647,63 @@ int vlb_push(vlb_ctx* ctx, double dt, double rcmax, double diag[5]) {
   });
 }
 
-int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, vlb_step_result* result) {
-  CTX_OR_FAIL;
+namespace {
+int check_step_params(Ctx& c, const vlb_step_params* params) {
   if (!params) return fail(VLB_ERR_ARG, "null step parameters");
   if (!(params->dt > 0)) return fail(VLB_ERR_ARG, "dt must be positive");
   if (params->deposit_mode != VLB_DEPOSIT_FLOAT32 && params->deposit_mode != VLB_DEPOSIT_FIXED64)
     return fail(VLB_ERR_ARG, "unknown deposit mode");
-  if (int rc = check_precision(c, params->poisson_precision)) return rc;
+  return check_precision(c, params->poisson_precision);
+}
+
+// Scalars back to the host after a step (synchronises the stream), the
+// projectile out, the step's results.
+void finish_step(Ctx& c, vlb_projectile* proj, const vlb_step_params* params, vlb_step_result* result) {
+  VLB_CUDA(cudaMemcpyAsync(c.hsc, c.dsc, sizeof(DeviceScalars), cudaMemcpyDeviceToHost, c.stream));
+  VLB_CUDA(cudaStreamSynchronize(c.stream));
+  if (c.profile) {
+    for (int i = 0; i < 9; ++i) {
+      float ms = 0;
+      VLB_CUDA(cudaEventElapsedTime(&ms, c.ev[i], c.ev[i + 1]));
+      c.stage_ms[i] += ms;
+    }
+  }
+  c.sorted = false;  // after the push the lists describe the previous positions
+  c.have_forces = true;
+  const DeviceScalars& h = *c.hsc;
+  if (proj) {
+    for (int d = 0; d < 3; ++d) {
+      proj->position[d] = h.proj_pos[d];
+      proj->previous[d] = h.proj_prev[d];
+      proj->velocity[d] = h.proj_vel[d];
+    }
+  }
+  if (result) {
+    result->kinetic = h.diag[0];
+    result->escaped = h.diag[1];
+    for (int d = 0; d < 3; ++d) {
+      result->angular[d] = h.diag[2 + d];
+      result->projectile_force[d] = h.proj_force[d];
+    }
+    result->e_electrons = h.e_el;
+    result->e_jellium = h.e_jel;
+    result->enclosed_charge = c.weight * (double)h.enclosed;
+    result->total_charge = h.charge_raw;
+    result->nout = h.nout;
+    result->outcount = h.outcount;
+    result->noccupied = h.noccupied;
+    result->status = h.status;
+  }
+  if (!params->push) c.sorted = true;  // forces-only: the cloud did not move
+}
+}  // namespace
+
+int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, vlb_step_result* result) {
+  CTX_OR_FAIL;
+  if (int rc = check_step_params(c, params)) return rc;
   c.mode_precision = params->poisson_precision;
   return guarded([&]() -> int {
+    c.shard_phase = 0;
     upload_projectile(c, proj);
     const bool graph = params->use_graph && !c.profile;
     // the captured step starts from keys written by the previous push
@@ -657,42 +723,69 @@ int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, 
         c.launches = keep;
       }
     }
-    VLB_CUDA(cudaMemcpyAsync(c.hsc, c.dsc, sizeof(DeviceScalars), cudaMemcpyDeviceToHost, c.stream));
-    VLB_CUDA(cudaStreamSynchronize(c.stream));
-    if (c.profile) {
-      for (int i = 0; i < 9; ++i) {
-        float ms = 0;
-        VLB_CUDA(cudaEventElapsedTime(&ms, c.ev[i], c.ev[i + 1]));
-        c.stage_ms[i] += ms;
-      }
-    }
-    c.sorted = false;  // after the push the lists describe the previous positions
-    c.have_forces = true;
-    const DeviceScalars& h = *c.hsc;
-    if (proj) {
-      for (int d = 0; d < 3; ++d) {
-        proj->position[d] = h.proj_pos[d];
-        proj->previous[d] = h.proj_prev[d];
-        proj->velocity[d] = h.proj_vel[d];
-      }
-    }
-    if (result) {
-      result->kinetic = h.diag[0];
-      result->escaped = h.diag[1];
-      for (int d = 0; d < 3; ++d) {
-        result->angular[d] = h.diag[2 + d];
-        result->projectile_force[d] = h.proj_force[d];
-      }
-      result->e_electrons = h.e_el;
-      result->e_jellium = h.e_jel;
-      result->enclosed_charge = c.weight * (double)h.enclosed;
-      result->total_charge = h.charge_raw;
-      result->nout = h.nout;
-      result->outcount = h.outcount;
-      result->noccupied = h.noccupied;
-      result->status = h.status;
-    }
-    if (!params->push) c.sorted = true;  // forces-only: the cloud did not move
+    finish_step(c, proj, params, result);
+    return status_code(c);
+  });
+}
+
+int vlb_exchange_buffers(vlb_ctx* ctx, int32_t deposit_mode, vlb_exchange* out) {
+  CTX_OR_FAIL;
+  if (!out) return fail(VLB_ERR_ARG, "null exchange descriptor");
+  if (deposit_mode != VLB_DEPOSIT_FLOAT32 && deposit_mode != VLB_DEPOSIT_FIXED64)
+    return fail(VLB_ERR_ARG, "unknown deposit mode");
+  const int64_t nf = (int64_t)c.fine.n * c.fine.n * c.fine.n, nc = (int64_t)c.coarse.n * c.coarse.n * c.coarse.n;
+  *out = vlb_exchange{};
+  if (deposit_mode == VLB_DEPOSIT_FIXED64) {
+    out->rho_fine = c.rho_fixed;
+    out->rho_fine_dtype = VLB_DTYPE_INT64;
+  } else {
+    out->rho_fine = c.fine.rho;
+    out->rho_fine_dtype = VLB_DTYPE_FLOAT32;
+  }
+  out->rho_fine_count = nf;
+  out->rho_coarse = c.coarse.rho;
+  out->rho_coarse_count = nc;
+  out->scalars = c.dsc->xch;
+  out->scalars_count = 1;
+  out->reaction = c.dsc->red;
+  out->reaction_count = 4;
+  out->stream = c.stream;
+  return VLB_OK;
+}
+
+int vlb_step_deposit(vlb_ctx* ctx, const vlb_projectile* proj, const vlb_step_params* params) {
+  CTX_OR_FAIL;
+  if (int rc = check_step_params(c, params)) return rc;
+  c.mode_precision = params->poisson_precision;
+  return guarded([&]() -> int {
+    upload_projectile(c, proj);
+    enqueue_phase_deposit(c, *params, 0);
+    c.shard_phase = 1;
+    return VLB_OK;
+  });
+}
+
+int vlb_step_fields(vlb_ctx* ctx, const vlb_step_params* params, int64_t npart_global) {
+  CTX_OR_FAIL;
+  if (int rc = check_step_params(c, params)) return rc;
+  if (c.shard_phase != 1) return fail(VLB_ERR_STATE, "vlb_step_fields before vlb_step_deposit");
+  if (npart_global < c.N) return fail(VLB_ERR_ARG, "the whole cloud cannot be smaller than this shard");
+  c.mode_precision = params->poisson_precision;
+  return guarded([&]() -> int {
+    enqueue_phase_fields(c, *params, npart_global);
+    c.shard_phase = 2;
+    return VLB_OK;
+  });
+}
+
+int vlb_step_advance(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, vlb_step_result* result) {
+  CTX_OR_FAIL;
+  if (int rc = check_step_params(c, params)) return rc;
+  if (c.shard_phase != 2) return fail(VLB_ERR_STATE, "vlb_step_advance before vlb_step_fields");
+  return guarded([&]() -> int {
+    enqueue_phase_advance(c, *params);
+    c.shard_phase = 0;
+    finish_step(c, proj, params, result);
     return status_code(c);
   });
 }

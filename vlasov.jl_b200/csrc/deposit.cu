@@ -196,10 +196,13 @@ __global__ void __launch_bounds__(1024) k_charge_total(const double* __restrict_
 }
 
 // rho *= (N - nout) w / q, converting from fixed point when needed.
+// rho = raw * (N - nout) w / q with N and nout over the whole cloud (all
+// shards): nout is read from xch[0], where the deposit published its own
+// count and a sharded step the sum over the shards.
 __global__ void k_charge_scale(float* __restrict__ rho, const unsigned long long* __restrict__ fixed, size_t tot,
                                const DeviceScalars* dsc, int64_t N, double w) {
   const double q = dsc->charge_raw;
-  const float sc = (float)((double)(N - dsc->nout) * w / q);
+  const float sc = (float)(((double)N - dsc->xch[0]) * w / q);
   for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x) {
     const float v = fixed ? (float)((double)(long long)fixed[t] * kFixedInv) : rho[t];
     rho[t] = v * sc;
@@ -400,7 +403,11 @@ void deposit_setup(Ctx& c) {
   VLB_CUDA(cudaFuncSetAttribute(k_deposit_cic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cic_smem(c)));
 }
 
-void launch_deposit_fine(Ctx& c, double charge, int mode) {
+__global__ void k_publish_nout(DeviceScalars* dsc) { dsc->xch[0] = (double)dsc->nout; }
+
+// The raw deposit of this context's particles (no renormalisation): the part
+// of a step that the shards sum.
+void launch_deposit_fine_raw(Ctx& c, int mode) {
   Level& F = c.fine;
   const size_t tot = (size_t)F.n * F.n * F.n;
   Particles& P = c.part[c.cur];
@@ -415,14 +422,29 @@ void launch_deposit_fine(Ctx& c, double charge, int mode) {
       c.occupied, c.bounds, c.dsc, c.Npad, P.k, P.d, c.nodes, F.nk, F.n, c.x0f, c.hf, c.lo_f, c.hi_f, c.spacing_f,
       c.nbdt, c.ncol, F.rho, c.rho_fixed, mode);
   VLB_LAUNCHED(c);
+  k_publish_nout<<<1, 1, 0, c.stream>>>(c.dsc);
+  VLB_LAUNCHED(c);
+}
+
+// Total charge of the (summed) raw density and the renormalisation to
+// (npart_global - nout) * charge (src/accelerator.jl:554-557).
+void launch_deposit_fine_normalize(Ctx& c, double charge, int mode, int64_t npart_global) {
+  Level& F = c.fine;
+  const size_t tot = (size_t)F.n * F.n * F.n;
   const unsigned long long* fx = mode == VLB_DEPOSIT_FIXED64 ? c.rho_fixed : nullptr;
   const int cols = F.n * F.n;
   k_charge_columns<<<(cols + 7) / 8, 256, 0, c.stream>>>(F.rho, fx, F.dual_d, F.n, c.partials);
   VLB_LAUNCHED(c);
   k_charge_total<<<1, 1024, 0, c.stream>>>(c.partials, cols, &c.dsc->charge_raw);
   VLB_LAUNCHED(c);
-  k_charge_scale<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(F.rho, fx, tot, c.dsc, c.N, charge);
+  k_charge_scale<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(F.rho, fx, tot, c.dsc, npart_global,
+                                                                           charge);
   VLB_LAUNCHED(c);
+}
+
+void launch_deposit_fine(Ctx& c, double charge, int mode) {
+  launch_deposit_fine_raw(c, mode);
+  launch_deposit_fine_normalize(c, charge, mode, c.N);
 }
 
 size_t cic_smem(const Ctx& c) {

@@ -47,6 +47,7 @@ struct DeviceScalars {
   unsigned long long work_cic;
   int32_t nitems;                    // cell chunks of the gather
   int32_t pad_items;
+  double xch[4];                     // exchanged between the shards of a step: [0] deposit-window rejections
   int32_t reset_end;
   int32_t pad0;
   // --- persistent ---
@@ -145,6 +146,7 @@ struct Ctx {
   // keys[] and counts[] hold the cell keys and histogram of part[cur] in slot
   // order (written by the push of a fused step): the next sort skips them
   bool keys_ready = false;
+  int shard_phase = 0;  // phases of a sharded step done: 1 deposit, 2 fields
   // profiling
   bool profile = false;
   cudaEvent_t ev[kNumStages + 1];
@@ -167,6 +169,8 @@ int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
 void launch_sort(Ctx& c);
 // deposit.cu
 void launch_deposit_fine(Ctx& c, double charge, int mode);
+void launch_deposit_fine_raw(Ctx& c, int mode);
+void launch_deposit_fine_normalize(Ctx& c, double charge, int mode, int64_t npart_global);
 void launch_deposit_coarse(Ctx& c, double charge);
 // poisson.cu
 void launch_poisson(Ctx& c);

@@ -375,6 +375,30 @@ class DeviceAccelerator:
         self._nocc, self._outc = res.noccupied, res.outcount
         return res
 
+    # -- the step in three phases, for a cloud sharded over several contexts
+    def exchange(self, deposit_mode: int) -> L.Exchange:
+        """Device addresses of the buffers the shards sum between phases."""
+        x = L.Exchange()
+        L.check(L.lib().vlb_exchange_buffers(self._h, deposit_mode, C.byref(x)))
+        return x
+
+    def step_deposit(self, projectile: Projectile | None, params: L.StepParams):
+        desc = projectile.to_desc() if projectile is not None else None
+        L.check(L.lib().vlb_step_deposit(self._h, C.byref(desc) if desc is not None else None, C.byref(params)))
+
+    def step_fields(self, params: L.StepParams, npart_global: int):
+        L.check(L.lib().vlb_step_fields(self._h, C.byref(params), int(npart_global)))
+
+    def step_advance(self, projectile: Projectile | None, params: L.StepParams) -> L.StepResult:
+        res = L.StepResult()
+        desc = projectile.to_desc() if projectile is not None else None
+        L.check(L.lib().vlb_step_advance(self._h, C.byref(desc) if desc is not None else None, C.byref(params),
+                                         C.byref(res)))
+        if projectile is not None:
+            projectile.from_desc(desc)
+        self._nocc, self._outc = res.noccupied, res.outcount
+        return res
+
     def grid(self, which: int) -> np.ndarray:
         n = self.nf if which % 2 == 0 else self.nc
         out = np.empty((n, n, n), np.float32)  # [k][j][i]: i fastest
