@@ -32,7 +32,7 @@ import numpy as np  # noqa: E402
 
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 GATHER_FLOP_PER_PARTICLE = 4600.0       # 2000 FMA + 300 mul/FMA per 10^3 contraction
-PUSH_BYTES_PER_PARTICLE = 48 + 12 + 48  # read (k, d, pk, pd) + force, write the record
+PUSH_BYTES_PER_PARTICLE = 48 + 12 + 48 + 4  # read (k, d, pk, pd) + force; write the record + the next sort's cell key
 
 
 def parse():
