@@ -266,6 +266,39 @@ typedef struct vlb_exchange {
   void* stream;               /* the context's cudaStream_t */
 } vlb_exchange;
 
+/* ---- launch shapes.  No counterpart in the reference (whose kernels take
+ * fixed workgroup sizes, src/accelerator.jl:253-259).  chunk: particles per
+ * work item of the gather and the coarse deposit (a multiple of 32, 32 to
+ * 4096); the others: CTAs per SM of the persistent grids.  Results do not
+ * depend on them except for the order of float32 atomic sums.  Setting them
+ * drops the captured step; the next step re-sorts. */
+typedef struct vlb_tuning {
+  int32_t chunk;              /* 128 */
+  int32_t field_ctas_per_sm;  /* 3: the smoothed gather */
+  int32_t cic_ctas_per_sm;    /* 4: the coarse deposit */
+  int32_t push_ctas_per_sm;   /* 8: the Verlet push */
+  int32_t move_ctas_per_sm;   /* 8: the record move of the sort */
+  int32_t reserved[3];
+} vlb_tuning;
+
+VLB_API int vlb_set_tuning(vlb_ctx* ctx, const vlb_tuning* tuning);
+VLB_API int vlb_get_tuning(vlb_ctx* ctx, vlb_tuning* tuning);
+
+/* ---- batches: several independent runs (contexts on one device, e.g. an
+ * impact-parameter / projectile sweep with clouds of different sizes)
+ * stepped together.  No counterpart in the reference, which runs one
+ * collision per process.  vlb_batch_step advances every context by one
+ * step (projs[i] and results[i] belong to the i-th context; params are
+ * shared), each on its own stream, forked from and joined to the batch's
+ * stream; with params->use_graph the whole batch step is captured once as
+ * one CUDA graph and replayed.  params->push must be 1 (priming goes
+ * through vlb_step). */
+typedef struct vlb_batch vlb_batch;
+VLB_API int vlb_batch_create(vlb_ctx* const* ctxs, int32_t n, vlb_batch** out);
+VLB_API int vlb_batch_step(vlb_batch* batch, vlb_projectile* projs, const vlb_step_params* params,
+                   vlb_step_result* results);
+VLB_API int vlb_batch_destroy(vlb_batch* batch);
+
 /* Device addresses of the exchange buffers (valid for the context's life). */
 VLB_API int vlb_exchange_buffers(vlb_ctx* ctx, int32_t deposit_mode, vlb_exchange* out);
 VLB_API int vlb_step_deposit(vlb_ctx* ctx, const vlb_projectile* proj, const vlb_step_params* params);

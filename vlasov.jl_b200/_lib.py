@@ -38,7 +38,8 @@ EXPORTS = (
     "vlb_last_error", "vlb_version", "vlb_create", "vlb_destroy", "vlb_upload_particles",
     "vlb_download_particles", "vlb_sort", "vlb_get_sort", "vlb_deposit_fine", "vlb_deposit_coarse",
     "vlb_poisson", "vlb_set_precision", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
-    "vlb_push", "vlb_step", "vlb_exchange_buffers", "vlb_step_deposit", "vlb_step_fields", "vlb_step_advance",
+    "vlb_push", "vlb_step", "vlb_set_tuning", "vlb_get_tuning", "vlb_batch_create", "vlb_batch_step",
+    "vlb_batch_destroy", "vlb_exchange_buffers", "vlb_step_deposit", "vlb_step_fields", "vlb_step_advance",
     "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
     "vlb_enclosed_charge", "vlb_profile", "vlb_stage_count", "vlb_stage_name", "vlb_stage_times",
     "vlb_launch_count", "vlb_fp32_peak", "vlb_stream", "vlb_sample_thomas_fermi", "vlb_ran2", "vlb_pack_positions",
@@ -99,6 +100,14 @@ VLB_DTYPE_FLOAT32 = 0
 VLB_DTYPE_INT64 = 1
 
 
+class Tuning(C.Structure):
+    _fields_ = [("chunk", C.c_int32), ("field_ctas_per_sm", C.c_int32), ("cic_ctas_per_sm", C.c_int32),
+                ("push_ctas_per_sm", C.c_int32), ("move_ctas_per_sm", C.c_int32), ("reserved", C.c_int32 * 3)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
+
+
 class VlbError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"vlb error {code}: {msg}")
@@ -138,6 +147,11 @@ def lib():
             "vlb_push": (C.c_int, [vp, C.c_double, C.c_double, P_D]),
             "vlb_step": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams), C.POINTER(StepResult)]),
             "vlb_exchange_buffers": (C.c_int, [vp, C.c_int32, C.POINTER(Exchange)]),
+            "vlb_set_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),
+            "vlb_get_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),
+            "vlb_batch_create": (C.c_int, [C.POINTER(vp), C.c_int32, C.POINTER(vp)]),
+            "vlb_batch_step": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams), C.POINTER(StepResult)]),
+            "vlb_batch_destroy": (C.c_int, [vp]),
             "vlb_step_deposit": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams)]),
             "vlb_step_fields": (C.c_int, [vp, C.POINTER(StepParams), C.c_int64]),
             "vlb_step_advance": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams),

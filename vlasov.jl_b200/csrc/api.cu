@@ -418,7 +418,7 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->bounds = dalloc<int32_t>(c->ncell + 1);
     c->outlist = dalloc<int32_t>(N);
     c->chunk_start = dalloc<int32_t>(c->ncell);
-    c->item_cell = dalloc<int32_t>(N / kChunk + c->ncell + 1);
+    c->item_cell = dalloc<int32_t>(N / kMinChunk + c->ncell + 1);
     const int64_t scan_tiles = std::max<int64_t>({(N + 4095) / 4096, (c->ncell + 4095) / 4096,
                                                   (c->radix_table_size + 4095) / 4096}) + 1;
     c->scan_status_size = 8 * scan_tiles;
@@ -658,9 +658,16 @@ int check_step_params(Ctx& c, const vlb_step_params* params) {
 
 // Scalars back to the host after a step (synchronises the stream), the
 // projectile out, the step's results.
+void collect_step(Ctx& c, vlb_projectile* proj, const vlb_step_params* params, vlb_step_result* result);
+
 void finish_step(Ctx& c, vlb_projectile* proj, const vlb_step_params* params, vlb_step_result* result) {
   VLB_CUDA(cudaMemcpyAsync(c.hsc, c.dsc, sizeof(DeviceScalars), cudaMemcpyDeviceToHost, c.stream));
   VLB_CUDA(cudaStreamSynchronize(c.stream));
+  collect_step(c, proj, params, result);
+}
+
+// The host side of a finished step, from the scalars already in c.hsc.
+void collect_step(Ctx& c, vlb_projectile* proj, const vlb_step_params* params, vlb_step_result* result) {
   if (c.profile) {
     for (int i = 0; i < 9; ++i) {
       float ms = 0;
@@ -725,6 +732,228 @@ int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, 
     }
     finish_step(c, proj, params, result);
     return status_code(c);
+  });
+}
+
+// ------------------------------------------------------------ tuning
+int vlb_set_tuning(vlb_ctx* ctx, const vlb_tuning* t) {
+  CTX_OR_FAIL;
+  if (!t) return fail(VLB_ERR_ARG, "null tuning");
+  if (t->chunk < kMinChunk || t->chunk > 4096 || t->chunk % 32)
+    return fail(VLB_ERR_ARG, "chunk must be a multiple of 32 in [32, 4096]");
+  const int32_t cps[4] = {t->field_ctas_per_sm, t->cic_ctas_per_sm, t->push_ctas_per_sm, t->move_ctas_per_sm};
+  for (int32_t v : cps)
+    if (v < 1 || v > 32) return fail(VLB_ERR_ARG, "CTAs per SM must be in [1, 32]");
+  c.chunk = t->chunk;
+  c.field_cps = t->field_ctas_per_sm;
+  c.cic_cps = t->cic_ctas_per_sm;
+  c.push_cps = t->push_ctas_per_sm;
+  c.move_cps = t->move_ctas_per_sm;
+  c.graph_valid = false;  // the captured step has the old launch shapes
+  c.sorted = false;       // the work items follow the chunk
+  return VLB_OK;
+}
+
+int vlb_get_tuning(vlb_ctx* ctx, vlb_tuning* t) {
+  CTX_OR_FAIL;
+  if (!t) return fail(VLB_ERR_ARG, "null tuning");
+  *t = vlb_tuning{};
+  t->chunk = c.chunk;
+  t->field_ctas_per_sm = c.field_cps;
+  t->cic_ctas_per_sm = c.cic_cps;
+  t->push_ctas_per_sm = c.push_cps;
+  t->move_ctas_per_sm = c.move_cps;
+  return VLB_OK;
+}
+
+// ------------------------------------------------------------- batches
+struct vlb_batch {
+  std::vector<Ctx*> ctx;
+  int device = 0;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  std::vector<int> cur0;       // the contexts' sort parities that gexec[0] starts from
+  vlb_step_params params{};
+  bool valid = false;
+};
+
+namespace {
+
+// One step of every context of the batch, each on its own stream, forked
+// from and joined back to the batch's stream.
+void enqueue_batch(vlb_batch& b, const vlb_step_params& p) {
+  VLB_CUDA(cudaEventRecord(b.fork, b.origin));
+  for (size_t i = 0; i < b.ctx.size(); ++i) {
+    Ctx& c = *b.ctx[i];
+    VLB_CUDA(cudaStreamWaitEvent(c.stream, b.fork, 0));
+    enqueue_step(c, p);
+    VLB_CUDA(cudaEventRecord(b.join[i], c.stream));
+    VLB_CUDA(cudaStreamWaitEvent(b.origin, b.join[i], 0));
+  }
+}
+
+void destroy_batch_graphs(vlb_batch& b) {
+  for (auto& g : b.gexec) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
+  b.valid = false;
+}
+
+// Two graphs: from the contexts' current parities, and from all flipped.
+void capture_batch(vlb_batch& b, const vlb_step_params& p) {
+  destroy_batch_graphs(b);
+  std::vector<int> saved(b.ctx.size());
+  for (size_t i = 0; i < b.ctx.size(); ++i) saved[i] = b.ctx[i]->cur;
+  b.cur0 = saved;
+  for (int g = 0; g < 2; ++g) {
+    for (size_t i = 0; i < b.ctx.size(); ++i) {
+      b.ctx[i]->cur = saved[i] ^ g;
+      b.ctx[i]->keys_ready = true;  // the captured step follows a step whose push wrote them
+    }
+    cudaGraph_t graph = nullptr;
+    VLB_CUDA(cudaStreamBeginCapture(b.origin, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue_batch(b, p);
+    } catch (...) {
+      cudaStreamEndCapture(b.origin, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      for (size_t i = 0; i < b.ctx.size(); ++i) b.ctx[i]->cur = saved[i];
+      throw;
+    }
+    VLB_CUDA(cudaStreamEndCapture(b.origin, &graph));
+    cudaError_t e = cudaGraphInstantiate(&b.gexec[g], graph, 0);
+    cudaGraphDestroy(graph);
+    VLB_CUDA(e);
+  }
+  for (size_t i = 0; i < b.ctx.size(); ++i) {
+    b.ctx[i]->cur = saved[i];
+    b.ctx[i]->keys_ready = true;
+  }
+  b.params = p;
+  b.valid = true;
+}
+
+}  // namespace
+
+int vlb_batch_create(vlb_ctx* const* ctxs, int32_t n, vlb_batch** out) {
+  if (!ctxs || !out || n < 1) return fail(VLB_ERR_ARG, "a batch needs at least one context");
+  *out = nullptr;
+  auto* b = new (std::nothrow) vlb_batch();
+  if (!b) return fail(VLB_ERR_NOMEM, "batch");
+  for (int32_t i = 0; i < n; ++i) {
+    if (!ctxs[i]) {
+      delete b;
+      return fail(VLB_ERR_ARG, "null context in the batch");
+    }
+    Ctx* c = reinterpret_cast<Ctx*>(ctxs[i]);
+    for (Ctx* o : b->ctx)
+      if (o == c) {
+        delete b;
+        return fail(VLB_ERR_ARG, "a context appears twice in the batch");
+      }
+    if (i > 0 && c->device != b->ctx[0]->device) {
+      delete b;
+      return fail(VLB_ERR_ARG, "the contexts of a batch must share one device");
+    }
+    b->ctx.push_back(c);
+  }
+  b->device = b->ctx[0]->device;
+  int rc = guarded([&]() -> int {
+    VLB_CUDA(cudaSetDevice(b->device));
+    VLB_CUDA(cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking));
+    VLB_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    b->join.assign(b->ctx.size(), nullptr);
+    for (auto& e : b->join) VLB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return VLB_OK;
+  });
+  if (rc != VLB_OK) {
+    vlb_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return VLB_OK;
+}
+
+int vlb_batch_destroy(vlb_batch* b) {
+  if (!b) return VLB_OK;
+  cudaSetDevice(b->device);
+  if (b->origin) cudaStreamSynchronize(b->origin);
+  destroy_batch_graphs(*b);
+  for (auto& e : b->join)
+    if (e) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->origin) cudaStreamDestroy(b->origin);
+  delete b;
+  return VLB_OK;
+}
+
+int vlb_batch_step(vlb_batch* b, vlb_projectile* projs, const vlb_step_params* params, vlb_step_result* results) {
+  if (!b) return fail(VLB_ERR_ARG, "null batch");
+  if (cudaSetDevice(b->device) != cudaSuccess) return fail(VLB_ERR_CUDA, "cudaSetDevice failed");
+  for (Ctx* c : b->ctx) {
+    if (int rc = check_step_params(*c, params)) return rc;
+    if (c->profile) return fail(VLB_ERR_STATE, "a batch step cannot be profiled");
+  }
+  if (!params->push) return fail(VLB_ERR_ARG, "a batch step pushes the clouds");
+  return guarded([&]() -> int {
+    const size_t n = b->ctx.size();
+    for (size_t i = 0; i < n; ++i) {
+      Ctx& c = *b->ctx[i];
+      c.mode_precision = params->poisson_precision;
+      c.shard_phase = 0;
+      upload_projectile(c, projs ? &projs[i] : nullptr);
+      VLB_CUDA(cudaEventRecord(b->join[i], c.stream));
+      VLB_CUDA(cudaStreamWaitEvent(b->origin, b->join[i], 0));
+    }
+    // the captured steps start from keys written by the previous pushes and
+    // from the parities they were captured at
+    bool replay = params->use_graph && b->valid && same_params(b->params, *params);
+    int g = -1;
+    if (replay) {
+      bool same = true, flipped = true;
+      for (size_t i = 0; i < n; ++i) {
+        const Ctx& c = *b->ctx[i];
+        replay = replay && c.keys_ready;
+        same = same && c.cur == b->cur0[i];
+        flipped = flipped && c.cur == (b->cur0[i] ^ 1);
+      }
+      g = same ? 0 : (flipped ? 1 : -1);
+      replay = replay && g >= 0;
+    }
+    if (replay) {
+      VLB_CUDA(cudaGraphLaunch(b->gexec[g], b->origin));
+      for (Ctx* c : b->ctx) {
+        c->cur ^= 1;
+        c->keys_ready = true;
+        c->launches += c->graph_launches;
+      }
+    } else {
+      std::vector<long long> before(n);
+      for (size_t i = 0; i < n; ++i) before[i] = b->ctx[i]->launches;
+      enqueue_batch(*b, *params);
+      for (size_t i = 0; i < n; ++i) b->ctx[i]->graph_launches = b->ctx[i]->launches - before[i];
+      if (params->use_graph) {
+        std::vector<long long> keep(n);
+        for (size_t i = 0; i < n; ++i) keep[i] = b->ctx[i]->launches;
+        capture_batch(*b, *params);
+        for (size_t i = 0; i < n; ++i) b->ctx[i]->launches = keep[i];
+      }
+    }
+    for (Ctx* c : b->ctx)
+      VLB_CUDA(cudaMemcpyAsync(c->hsc, c->dsc, sizeof(DeviceScalars), cudaMemcpyDeviceToHost, b->origin));
+    VLB_CUDA(cudaEventRecord(b->fork, b->origin));
+    for (Ctx* c : b->ctx) VLB_CUDA(cudaStreamWaitEvent(c->stream, b->fork, 0));  // later work on a context follows
+    VLB_CUDA(cudaStreamSynchronize(b->origin));
+    int rc = VLB_OK;
+    for (size_t i = 0; i < n; ++i) {
+      Ctx& c = *b->ctx[i];
+      collect_step(c, projs ? &projs[i] : nullptr, params, results ? &results[i] : nullptr);
+      if (int r = status_code(c)) rc = r;
+    }
+    return rc;
   });
 }
 

@@ -237,7 +237,7 @@ __device__ __forceinline__ void window_axis(int l, float w0, float w1, float (&f
   for (int e = 0; e < kCicW; ++e) f[e] = e == l ? w0 : (e == l + 1 ? w1 : 0.f);
 }
 
-// One warp per work item of the cell sort (a run of at most kChunk particles
+// One warp per work item of the cell sort (a run of at most `chunk` particles
 // of one fine cell).  Each lane adds its particles' eight trilinear
 // contributions into a 4^3 register window anchored at the coarse point left
 // of the fine cell's lower edge: the fine cell is one knot spacing wide, and
@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
     const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int nk,
     int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ gt_g, int ng,
     float lx0, float linvw, const int32_t* __restrict__ cells_g, int ncells, const float* __restrict__ dl_g,
-    float x0f, float hf, float charge, float* rho) {
+    float x0f, float hf, float charge, float* rho, int chunk) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* gt = reinterpret_cast<float*>(smem);                   // [ng]
   float* igap = gt + ng;                                        // [ng] 1 / (gt[c] - gt[c-1])
@@ -276,8 +276,8 @@ __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= nitems) break;
     const int g = item_cell[item];
-    const int s0 = bounds[g] + (item - chunk_start[g]) * kChunk;
-    const int s1 = min(s0 + kChunk, bounds[g + 1]);
+    const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
+    const int s1 = min(s0 + chunk, bounds[g + 1]);
     int kx, ky, kz;
     cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
     int anc[3];
@@ -457,9 +457,9 @@ void launch_deposit_coarse(Ctx& c, double charge) {
   Particles& P = c.part[c.cur];
   VLB_CUDA(cudaMemsetAsync(C.rho, 0, tot * sizeof(float), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_cic, 0, sizeof(unsigned long long), c.stream));
-  k_deposit_cic<<<c.num_sms * 4, kCicThreads, cic_smem(c), c.stream>>>(
+  k_deposit_cic<<<c.num_sms * c.cic_cps, kCicThreads, cic_smem(c), c.stream>>>(
       c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.fine.nk, c.Npad, P.k, P.d, C.colloc, C.n,
-      C.loc_x0, C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho);
+      C.loc_x0, C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho, c.chunk);
   VLB_LAUNCHED(c);
 }
 

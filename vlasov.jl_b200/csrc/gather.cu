@@ -108,7 +108,7 @@ __device__ __forceinline__ void block_add_red(float ax, float ay, float az, floa
   }
 }
 
-// One warp per work item (at most kChunk particles of one occupied cell),
+// One warp per work item (at most `chunk` particles of one occupied cell),
 // items taken from a dynamic counter.  The warp stages its cell's 10^3
 // stencil in its own slice of shared memory (kept while consecutive items
 // share the cell) and takes 32 particles at a time, one per lane.  No
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kGThreads) k_field(
     const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int64_t Npad,
     const float* __restrict__ d, const float* __restrict__ csol, int n, int nk, const float* __restrict__ ov,
     const float* __restrict__ gr, int nbdt, int ncol, float spacing, float x0, float h, double w,
-    float* __restrict__ force) {
+    float* __restrict__ force, int chunk) {
   __shared__ __align__(16) float tiles[kGThreads / 32][kTile];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   float* tile = tiles[wid];
@@ -152,8 +152,8 @@ __global__ void __launch_bounds__(kGThreads) k_field(
       cached = g;
       __syncwarp();
     }
-    const int s0 = bounds[g] + (item - chunk_start[g]) * kChunk;
-    const int s1 = min(s0 + kChunk, bounds[g + 1]);
+    const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
+    const int s1 = min(s0 + chunk, bounds[g + 1]);
     for (int s = s0 + lane; s < s1; s += 32) {
       const float dx0 = d[s], dy0 = d[Npad + s], dz0 = d[2 * Npad + s];
       const int cx = table_column(dx0, spacing, nbdt, ncol);
@@ -345,10 +345,10 @@ void launch_forces(Ctx& c) {
   Particles& P = c.part[c.cur];
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_gather, 0, sizeof(unsigned long long), c.stream));
   VLB_CUDA(cudaMemsetAsync(c.dsc->red, 0, sizeof(c.dsc->red), c.stream));
-  k_field<<<c.num_sms * 3, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc,
+  k_field<<<c.num_sms * c.field_cps, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc,
                                                      c.Npad, P.d, F.csol, F.n, F.nk,
                                                      c.overlap, c.gradient, c.nbdt, c.ncol, c.spacing_f, c.x0f,
-                                                     c.hf, c.weight, c.force);
+                                                     c.hf, c.weight, c.force, c.chunk);
   VLB_LAUNCHED(c);
   k_tail<<<c.num_sms, kGThreads, 0, c.stream>>>(c.outlist, c.dsc, c.Npad, P.k, P.d, C.csol, C.knots_d, C.nk,
                                                     C.n, F.nk, c.x0f, c.hf, c.x0, c.h, c.weight, c.force);

@@ -241,7 +241,7 @@ void launch_push(Ctx& c, double dt, double rcmax, double capture_radius, bool ke
   const double M = c.weight;  // ELECTRON_MASS * weight
   VLB_CUDA(cudaMemsetAsync(c.dsc->diag, 0, sizeof(c.dsc->diag), c.stream));
   if (capture_radius > 0) VLB_CUDA(cudaMemsetAsync(&c.dsc->enclosed, 0, sizeof(unsigned long long), c.stream));
-  k_push<<<grid_for(c, (c.N + 3) / 4, 256, 8), 256, 0, c.stream>>>(
+  k_push<<<grid_for(c, (c.N + 3) / 4, 256, c.push_cps), 256, 0, c.stream>>>(
       c.N, c.Npad, P.k, P.d, P.pk, P.pd, c.force, (float)(dt * dt / M), c.hf, c.x0f, (float)(M / (2 * dt)),
       (float)(rcmax * rcmax), (float)(1 / (2 * M)), c.dsc->diag,
       capture_radius > 0 ? capture_radius * capture_radius : 0.0, c.x0, c.h, c.dsc, keys ? c.keys : nullptr,

@@ -9,7 +9,7 @@
 //   1. cell keys + warp-aggregated histogram over nk^3 cells;
 //   2. a decoupled look-back scan that compacts the occupied cells;
 //   3. one CTA scans the occupied cells (a few thousand): their bounds, the
-//      gather's work items (chunks of at most kChunk particles) and the
+//      gather's work items (chunks of at most `chunk` particles) and the
 //      out-of-stencil slots, all functions of the cell alone; one warp per
 //      occupied cell then writes the item list and the out-of-stencil list
 //      (increasing slot order);
@@ -95,7 +95,7 @@ struct ScanOutOccupied {
 
 // One CTA over the occupied cells g < nocc (in increasing cell order), each
 // thread a contiguous run of them: exclusive prefixes of the particle count
-// (bounds), of the number of work items (ceil(count / kChunk)) and of the
+// (bounds), of the number of work items (ceil(count / chunk)) and of the
 // particles of cells whose 10^3 stencil leaves the fine grid (out_start, -1
 // for the others); totals into bounds[nocc], nitems and outcount.
 constexpr int kListThreads = 1024;
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kListThreads) k_cell_lists(const int32_t* __re
                                                              const int32_t* __restrict__ occupied, DeviceScalars* dsc,
                                                              int nk, int n, int32_t* __restrict__ bounds,
                                                              int32_t* __restrict__ chunk_start,
-                                                             int32_t* __restrict__ out_start) {
+                                                             int32_t* __restrict__ out_start, int chunk) {
   const int nocc = dsc->noccupied;
   const int per = (nocc + kListThreads - 1) / kListThreads;
   const int g0 = min((int)threadIdx.x * per, nocc), g1 = min(g0 + per, nocc);
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(kListThreads) k_cell_lists(const int32_t* __re
     int kx, ky, kz;
     cell_knots((uint32_t)cell, nk, kx, ky, kz);
     sc += c;
-    sch += (c + kChunk - 1) / kChunk;
+    sch += (c + chunk - 1) / chunk;
     if (!field_fits(kx, ky, kz, n)) so += c;
   }
   uint32_t tot[3];
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kListThreads) k_cell_lists(const int32_t* __re
     chunk_start[g] = (int32_t)sch;
     out_start[g] = fits ? -1 : (int32_t)so;
     sc += c;
-    sch += (c + kChunk - 1) / kChunk;
+    sch += (c + chunk - 1) / chunk;
     if (!fits) so += c;
   }
   if (threadIdx.x == 0) {
@@ -184,13 +184,14 @@ __global__ void __launch_bounds__(kListThreads) k_cell_lists(const int32_t* __re
 __global__ void __launch_bounds__(256) k_expand_lists(const int32_t* __restrict__ bounds,
                                                       const int32_t* __restrict__ chunk_start,
                                                       const int32_t* __restrict__ out_start, const DeviceScalars* dsc,
-                                                      int32_t* __restrict__ item_cell, int32_t* __restrict__ outlist) {
+                                                      int32_t* __restrict__ item_cell, int32_t* __restrict__ outlist,
+                                                      int chunk) {
   const int nocc = dsc->noccupied;
   const int lane = threadIdx.x & 31;
   const int warps = gridDim.x * (blockDim.x >> 5);
   for (int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); g < nocc; g += warps) {
     const int b0 = bounds[g], cnt = bounds[g + 1] - b0;
-    const int nch = (cnt + kChunk - 1) / kChunk, c0 = chunk_start[g];
+    const int nch = (cnt + chunk - 1) / chunk, c0 = chunk_start[g];
     for (int ch = lane; ch < nch; ch += 32) item_cell[c0 + ch] = g;
     const int o0 = out_start[g];
     if (o0 >= 0)
@@ -440,10 +441,10 @@ void launch_sort(Ctx& c) {
   // slots (cell_off holds the out-of-stencil start of each occupied cell)
   scan(c, ScanInOccupied{c.counts}, ScanOutOccupied{c.occupied}, c.ncell, 1, &c.dsc->noccupied);
   k_cell_lists<<<1, kListThreads, 0, c.stream>>>(c.counts, c.occupied, c.dsc, nk, n, c.bounds, c.chunk_start,
-                                                 c.cell_off);
+                                                 c.cell_off, c.chunk);
   VLB_LAUNCHED(c);
   k_expand_lists<<<c.num_sms * 4, 256, 0, c.stream>>>(c.bounds, c.chunk_start, c.cell_off, c.dsc, c.item_cell,
-                                                      c.outlist);
+                                                      c.outlist, c.chunk);
   VLB_LAUNCHED(c);
   // the histogram is spent: zero it for the push that may refill it
   VLB_CUDA(cudaMemsetAsync(c.counts, 0, sizeof(int32_t) * c.ncell, c.stream));
@@ -473,7 +474,7 @@ void launch_sort(Ctx& c) {
     vin = vout;
     shift += b;
   }
-  k_gather_records<<<grid_for(c, (N + 3) / 4, 256, 8), 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
+  k_gather_records<<<grid_for(c, (N + 3) / 4, 256, c.move_cps), 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
                                                                    Q.pk, Q.pd);
   VLB_LAUNCHED(c);
   c.cur ^= 1;

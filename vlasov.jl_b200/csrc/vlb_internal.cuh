@@ -13,7 +13,8 @@ namespace vlb {
 
 constexpr int kWarp = 32;
 constexpr int kNumStages = 12;
-constexpr int kChunk = 128;  // particles per gather work item
+constexpr int kChunk = 128;       // default particles per work item of the gather and CIC
+constexpr int kMinChunk = 32;     // smallest chunk a tuning may set (sizes the item list)
 
 // Error flags raised by kernels into DeviceScalars::status.
 constexpr int kStatusScanTimeout = 1;   // decoupled look-back gave up
@@ -136,6 +137,9 @@ struct Ctx {
   // Poisson work buffers (max n^3)
   float* work[3] = {nullptr, nullptr, nullptr};
   int mode_precision = 0;     // VLB_POISSON_FP32 or VLB_POISSON_3XTF32
+  // launch shapes (vlb_set_tuning): particles per work item, persistent-grid
+  // CTAs per SM of the gather, the coarse deposit, the push and the record move
+  int chunk = kChunk, field_cps = 3, cic_cps = 4, push_cps = 8, move_cps = 8;
   unsigned* tc_sync = nullptr;  // grid-barrier counter of the tensor-core chains
   // scalars
   DeviceScalars* dsc = nullptr;
