@@ -15,5 +15,7 @@ from .simulation import (SimulationParameters, Jellium, BallSoftening, GaussianS
 from . import _lib
 from . import xenon
 from . import sharded
+from . import autotune
+from . import sweep
 
 __all__ = [n for n in dir() if not n.startswith("_")]

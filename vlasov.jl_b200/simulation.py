@@ -258,6 +258,7 @@ class DeviceAccelerator:
         handle = C.c_void_p()
         L.check(L.lib().vlb_create(C.byref(cfg), C.byref(handle)))
         self._h = handle
+        self.device = int(device)
         self.npart = int(npart)
         self.weight = float(weight)
         self.meshes = meshes
@@ -425,6 +426,23 @@ class DeviceAccelerator:
         L.check(L.lib().vlb_enclosed_charge(self._h, L.pd(P), radius, C.byref(q)))
         return q.value
 
+    # -- launch shapes (vlb_set_tuning)
+    def tuning(self) -> dict:
+        t = L.Tuning()
+        L.check(L.lib().vlb_get_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        """Changes some launch shapes (chunk, field_ctas_per_sm,
+        cic_ctas_per_sm, push_ctas_per_sm, move_ctas_per_sm)."""
+        cur = self.tuning()
+        unknown = set(kw) - set(cur)
+        if unknown:
+            raise ValueError(f"unknown launch shapes {sorted(unknown)}")
+        cur.update(kw)
+        t = L.Tuning(**cur)
+        L.check(L.lib().vlb_set_tuning(self._h, C.byref(t)))
+
     def launch_count(self) -> int:
         n = C.c_int64()
         L.check(L.lib().vlb_launch_count(self._h, C.byref(n)))
@@ -540,6 +558,19 @@ class Simulation:
             if callback is not None:
                 callback(i, d)
         return out
+
+    def snapshot(self):
+        """The state a step changes: the cloud and the projectile."""
+        pr = self.projectile
+        proj = None if pr is None else (pr.position.copy(), pr.previous.copy(), pr.velocity.copy())
+        return self.accelerator.download(), proj, self.steps_done
+
+    def restore(self, snap):
+        cloud, proj, steps = snap
+        self.accelerator.upload(*cloud)
+        if proj is not None:
+            self.projectile.position, self.projectile.previous, self.projectile.velocity = (x.copy() for x in proj)
+        self.steps_done = steps
 
     def positions(self):
         k, d, pk, pd = self.accelerator.download()
