@@ -118,6 +118,7 @@ typedef struct vlb_step_params {
   int32_t push;                /* 0: forces only, no Verlet (priming) */
   int32_t use_graph;           /* 1: replay the step as one captured CUDA graph */
   int32_t poisson_precision;   /* VLB_POISSON_FP32 or VLB_POISSON_3XTF32, every mode product of the step */
+  int32_t denoise;             /* 1: the learned denoiser on the fine density (vlb_set_denoiser) */
 } vlb_step_params;
 
 #define VLB_DEPOSIT_FLOAT32 0
@@ -136,6 +137,8 @@ typedef struct vlb_step_result {
   int32_t outcount;            /* 10^3 stencil leaves the fine grid */
   int32_t noccupied;           /* occupied fine cells */
   int32_t status;              /* device-side error flags, 0 when clean */
+  int32_t denoised;            /* 1: the step used the denoiser's density, 0: the deposit's */
+  int32_t pad_;
 } vlb_step_result;
 
 /* Grid selectors for vlb_get_grid / vlb_set_grid. */
@@ -265,6 +268,42 @@ typedef struct vlb_exchange {
   int32_t pad2_;
   void* stream;               /* the context's cudaStream_t */
 } vlb_exchange;
+
+/* ---- the learned denoiser of the fine density.  No counterpart in the
+ * reference.  A 3-D convolutional network (four 3^3 layers, 1-16-16-16-3
+ * channels, ReLU, no biases; BF16 weights, float32 arithmetic; weights of
+ * layer l as [27][cin][cout], tap = dx + 3 dy + 9 dz).  Its three outputs are
+ * a charge flux F = f(s rho) and the density it gives is
+ * out = rho + div F / s, with no flux through the grid's faces: the network
+ * moves charge between neighbouring voxels and adds none.  It is trained on
+ * pairs of densities of the method itself (an 8e6-particle run's deposit
+ * against a run with ten times the particles, at the same instant).
+ *
+ * In the step (vlb_step_params.denoise): after the renormalised fine
+ * deposit, the network's density replaces the deposit's when their charges
+ * differ by at most charge_tolerance (electrons), renormalised to the
+ * deposit's charge; otherwise the deposit stays (vlb_step_result.denoised).
+ * The building blocks below (device pointers, the caller's stream) are what
+ * a training loop needs: the forward pass, the loss gradient against a
+ * target density, an Adam update. */
+VLB_API int vlb_dn_weight_count(void);
+VLB_API int vlb_set_denoiser(vlb_ctx* ctx, const float* weights, int32_t count, double input_scale,
+                     double charge_tolerance);
+VLB_API int vlb_clear_denoiser(vlb_ctx* ctx);
+
+typedef struct vlb_denoiser vlb_denoiser;
+VLB_API int vlb_dn_create(int32_t nx, int32_t ny, int32_t nz, int32_t device, vlb_denoiser** out);
+VLB_API int vlb_dn_destroy(vlb_denoiser* dn);
+/* out = x + div f(scale x) / scale over an nx*ny*nz float32 grid (device pointers) */
+VLB_API int vlb_dn_forward(vlb_denoiser* dn, const float* x, float scale, const float* weights, float* out,
+                   void* stream);
+/* grad = d loss / d weights, loss = mean over voxels of (scale (out - target))^2 (host, may be null) */
+VLB_API int vlb_dn_gradient(vlb_denoiser* dn, const float* x, const float* target, float scale,
+                    const float* weights, float* grad, double* loss, void* stream);
+VLB_API int vlb_dn_adam(vlb_denoiser* dn, float* weights, const float* grad, float* m, float* v, float lr,
+                int32_t step, void* stream);
+/* tiles of 8^3 voxels the last pass computed (the others are empty) */
+VLB_API int vlb_dn_active_tiles(vlb_denoiser* dn, int32_t* n);
 
 /* ---- launch shapes.  No counterpart in the reference (whose kernels take
  * fixed workgroup sizes, src/accelerator.jl:253-259).  chunk: particles per

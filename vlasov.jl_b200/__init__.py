@@ -17,5 +17,6 @@ from . import xenon
 from . import sharded
 from . import autotune
 from . import sweep
+from . import denoiser
 
 __all__ = [n for n in dir() if not n.startswith("_")]

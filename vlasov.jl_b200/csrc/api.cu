@@ -170,6 +170,7 @@ void destroy_ctx(Ctx* c) {
   dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off); dfree(c->occupied); dfree(c->bounds);
   dfree(c->outlist); dfree(c->chunk_start); dfree(c->item_cell); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
   for (auto& w : c->work) dfree(w);
+  free_denoiser(*c);
   dfree(c->tc_sync);
   dfree(c->dsc);
   if (c->hsc) cudaFreeHost(c->hsc);
@@ -257,14 +258,20 @@ void enqueue_phase_deposit(Ctx& c, const vlb_step_params& p, int64_t normalize_n
   launch_sort(c);
   stage_mark(c, 1);
   launch_deposit_fine_raw(c, p.deposit_mode);
-  if (normalize_npart > 0) launch_deposit_fine_normalize(c, c.weight, p.deposit_mode, normalize_npart);
+  if (normalize_npart > 0) {
+    launch_deposit_fine_normalize(c, c.weight, p.deposit_mode, normalize_npart);
+    if (p.denoise) launch_denoise(c, normalize_npart);
+  }
   stage_mark(c, 2);
   launch_deposit_coarse(c, c.weight);
   stage_mark(c, 3);
 }
 
 void enqueue_phase_fields(Ctx& c, const vlb_step_params& p, int64_t normalize_npart) {
-  if (normalize_npart > 0) launch_deposit_fine_normalize(c, c.weight, p.deposit_mode, normalize_npart);
+  if (normalize_npart > 0) {
+    launch_deposit_fine_normalize(c, c.weight, p.deposit_mode, normalize_npart);
+    if (p.denoise) launch_denoise(c, normalize_npart);
+  }
   launch_poisson(c);
   stage_mark(c, 4);
   launch_mean_field_coefficients(c, c.fine, c.fine.phi, c.fine.csol, p.jellium_nions, p.jellium_radius);
@@ -293,7 +300,7 @@ bool same_params(const vlb_step_params& a, const vlb_step_params& b) {
   return a.dt == b.dt && a.rcmax == b.rcmax && a.jellium_nions == b.jellium_nions &&
          a.jellium_radius == b.jellium_radius && a.capture_radius == b.capture_radius &&
          a.deposit_mode == b.deposit_mode && a.advance_projectile == b.advance_projectile && a.push == b.push &&
-         a.poisson_precision == b.poisson_precision;
+         a.poisson_precision == b.poisson_precision && a.denoise == b.denoise;
 }
 
 // Two graphs, one per parity of the sort's double buffer: the step moves
@@ -653,6 +660,7 @@ int check_step_params(Ctx& c, const vlb_step_params* params) {
   if (!(params->dt > 0)) return fail(VLB_ERR_ARG, "dt must be positive");
   if (params->deposit_mode != VLB_DEPOSIT_FLOAT32 && params->deposit_mode != VLB_DEPOSIT_FIXED64)
     return fail(VLB_ERR_ARG, "unknown deposit mode");
+  if (params->denoise && !c.dn) return fail(VLB_ERR_STATE, "denoise asked for, and no denoiser is set");
   return check_precision(c, params->poisson_precision);
 }
 
@@ -700,6 +708,7 @@ void collect_step(Ctx& c, vlb_projectile* proj, const vlb_step_params* params, v
     result->outcount = h.outcount;
     result->noccupied = h.noccupied;
     result->status = h.status;
+    result->denoised = h.denoised;
   }
   if (!params->push) c.sorted = true;  // forces-only: the cloud did not move
 }
@@ -735,6 +744,47 @@ int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, 
   });
 }
 
+// ----------------------------------------------------------- denoiser
+int vlb_set_denoiser(vlb_ctx* ctx, const float* weights, int32_t count, double input_scale,
+                     double charge_tolerance) {
+  CTX_OR_FAIL;
+  if (!weights || count != vlb_dn_weight_count())
+    return fail(VLB_ERR_ARG, "vlb_set_denoiser: expected " + std::to_string(vlb_dn_weight_count()) + " weights");
+  if (!(input_scale > 0) || !(charge_tolerance >= 0)) return fail(VLB_ERR_ARG, "vlb_set_denoiser: bad scale or tolerance");
+  return guarded([&]() -> int {
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    free_denoiser(c);
+    ++c.config_epoch;
+    const int n = c.fine.n;
+    c.dn = dn_create(n, n, n, c.device, c.num_sms);
+    std::vector<float> w(weights, weights + count);
+    for (float& f : w) {  // round to BF16, ties to even
+      uint32_t u;
+      std::memcpy(&u, &f, 4);
+      u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+      std::memcpy(&f, &u, 4);
+    }
+    c.dn_weights = dalloc<float>(w.size());
+    VLB_CUDA(cudaMemcpy(c.dn_weights, w.data(), w.size() * 4, cudaMemcpyHostToDevice));
+    c.dn_pred = dalloc<float>((size_t)n * n * n);
+    c.dn_scale = input_scale;
+    c.dn_tol = charge_tolerance;
+    c.graph_valid = false;
+    return VLB_OK;
+  });
+}
+
+int vlb_clear_denoiser(vlb_ctx* ctx) {
+  CTX_OR_FAIL;
+  return guarded([&]() -> int {
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    free_denoiser(c);
+    ++c.config_epoch;
+    c.graph_valid = false;
+    return VLB_OK;
+  });
+}
+
 // ------------------------------------------------------------ tuning
 int vlb_set_tuning(vlb_ctx* ctx, const vlb_tuning* t) {
   CTX_OR_FAIL;
@@ -750,6 +800,7 @@ int vlb_set_tuning(vlb_ctx* ctx, const vlb_tuning* t) {
   c.push_cps = t->push_ctas_per_sm;
   c.move_cps = t->move_ctas_per_sm;
   c.graph_valid = false;  // the captured step has the old launch shapes
+  ++c.config_epoch;
   c.sorted = false;       // the work items follow the chunk
   return VLB_OK;
 }
@@ -775,6 +826,7 @@ struct vlb_batch {
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   std::vector<int> cur0;       // the contexts' sort parities that gexec[0] starts from
+  std::vector<uint64_t> epoch0;  // the contexts' configuration epochs the graphs were captured at
   vlb_step_params params{};
   bool valid = false;
 };
@@ -832,6 +884,8 @@ void capture_batch(vlb_batch& b, const vlb_step_params& p) {
     b.ctx[i]->cur = saved[i];
     b.ctx[i]->keys_ready = true;
   }
+  b.epoch0.resize(b.ctx.size());
+  for (size_t i = 0; i < b.ctx.size(); ++i) b.epoch0[i] = b.ctx[i]->config_epoch;
   b.params = p;
   b.valid = true;
 }
@@ -916,7 +970,7 @@ int vlb_batch_step(vlb_batch* b, vlb_projectile* projs, const vlb_step_params* p
       bool same = true, flipped = true;
       for (size_t i = 0; i < n; ++i) {
         const Ctx& c = *b->ctx[i];
-        replay = replay && c.keys_ready;
+        replay = replay && c.keys_ready && c.config_epoch == b->epoch0[i];
         same = same && c.cur == b->cur0[i];
         flipped = flipped && c.cur == (b->cur0[i] ^ 1);
       }

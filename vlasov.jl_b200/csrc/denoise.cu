@@ -1,0 +1,715 @@
+// The learned denoiser of the fine density: training and inference kernels.
+//
+// The network (fixed shape): four 3^3 convolutions, 1 -> 16 -> 16 -> 16 -> 3
+// channels, ReLU after the first three, no biases, zero padding at the
+// grid's faces.  The three output channels are a charge flux F = f(s rho)
+// (s a fixed input scale), and the output is its divergence added to the
+// input:
+//
+//     out[v] = rho[v] + (1/s) sum_axes (F~a[v] - F~a[v - e_a]),
+//
+// F~a the flux with no flow through the grid's faces (zero on the last
+// plane of its axis and before the first).  The correction moves charge
+// between neighbouring voxels and adds none: the sum of out equals the sum
+// of rho.  Without biases f(0) = 0 and f is positively homogeneous, so empty
+// space stays empty and the correction scales with the density.  Weights are
+// BF16 (kept as float32 values that BF16 represents exactly), every product
+// and sum is float32.
+//
+// Activations are channel-last float32 ([z][y][x][c], i fastest as the
+// grids).  The volume is cut into 8^3 tiles; a tile whose input within four
+// voxels (the network's reach) is zero has zero activations at every layer
+// and is skipped, forward and backward alike -- exactly, not as an
+// approximation.
+//
+//   k_conv<CIN, COUT>     one layer (also the input-gradient pass, with the
+//                         weights flipped and transposed), 256 threads per
+//                         tile, two voxels per thread sharing the weight reads
+//   k_conv_wgrad<..>      weight gradient, per-CTA partial sums over tiles,
+//                         reduced in a fixed order by k_reduce_partials
+//   k_divergence          out = rho + div F~ / s
+//   k_loss, k_div_adjoint mean squared error against the target and its
+//                         gradient at the flux
+//   k_adam                Adam update of the float32 master weights
+//
+// The same kernels serve the training loop (vlb_dn_*) and the in-step
+// inference (vlb_set_denoiser + vlb_step_params.denoise).
+
+#include <cstring>
+#include <vector>
+
+#include "vlb_internal.cuh"
+
+namespace vlb {
+
+namespace {
+
+constexpr int kT = 8;                  // tile edge (voxels)
+constexpr int kH = kT + 2;             // halo edge
+constexpr int kConvThreads = 256;      // two voxels per thread
+constexpr int kLayers = 4;
+constexpr int kLayerIn[kLayers] = {1, 16, 16, 16};
+constexpr int kLayerOut[kLayers] = {16, 16, 16, 3};
+
+__host__ __device__ constexpr int pad_stride(int c) { return c == 16 ? 20 : c; }  // float stride per halo voxel
+
+struct Vol {
+  int nx, ny, nz;
+  int tx, ty, tz;  // tiles per axis
+};
+
+__device__ __forceinline__ void tile_origin(const Vol& v, int tile, int& x0, int& y0, int& z0) {
+  x0 = (tile % v.tx) * kT;
+  y0 = ((tile / v.tx) % v.ty) * kT;
+  z0 = (tile / (v.tx * v.ty)) * kT;
+}
+
+// ---------------------------------------------------------------- tiles
+// flags[t] = 1 if tile t holds a nonzero input voxel.
+__global__ void k_tile_flags(const float* __restrict__ x, Vol v, int32_t* __restrict__ flags) {
+  const int tile = blockIdx.x;
+  int x0, y0, z0;
+  tile_origin(v, tile, x0, y0, z0);
+  int any = 0;
+  for (int e = threadIdx.x; e < kT * kT * kT; e += blockDim.x) {
+    const int i = x0 + e % kT, j = y0 + (e / kT) % kT, k = z0 + e / (kT * kT);
+    if (i < v.nx && j < v.ny && k < v.nz && x[(size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)] != 0.f) any = 1;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) flags[tile] = any;
+}
+
+// Active tiles: a flagged tile or a neighbour of one (the reach, four
+// voxels, is less than a tile), compacted in tile order.
+__global__ void k_tile_active(const int32_t* __restrict__ flags, Vol v, int32_t* __restrict__ list,
+                              int32_t* __restrict__ count) {
+  const int ntiles = v.tx * v.ty * v.tz;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    const int a = t % v.tx, b = (t / v.tx) % v.ty, c = t / (v.tx * v.ty);
+    int on = 0;
+    for (int dc = -1; dc <= 1 && !on; ++dc)
+      for (int db = -1; db <= 1 && !on; ++db)
+        for (int da = -1; da <= 1 && !on; ++da) {
+          const int aa = a + da, bb = b + db, cc = c + dc;
+          if (aa < 0 || bb < 0 || cc < 0 || aa >= v.tx || bb >= v.ty || cc >= v.tz) continue;
+          on = flags[aa + v.tx * (bb + v.ty * cc)];
+        }
+    if (on) list[atomicAdd(count, 1)] = t;
+  }
+}
+
+// -------------------------------------------------------------- the conv
+// y[v][co] = sum_tap sum_ci w[tap][ci][co] * scale_in * x[v + tap - 1][ci]
+// (zero outside the volume), then y = max(y, 0) when `relu`, and y = 0 where
+// mask[v][co] <= 0 when `mask` is given (the input-gradient pass through a
+// ReLU).  Tiles not in `list` are left as they are (the caller zeroes them).
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kConvThreads) k_conv(const float* __restrict__ x, const float* __restrict__ w,
+                                                       float* __restrict__ y, Vol v, const int32_t* __restrict__ list,
+                                                       const int32_t* __restrict__ count, int relu,
+                                                       const float* __restrict__ mask, float scale_in) {
+  constexpr int PS = pad_stride(CIN);
+  extern __shared__ __align__(16) float sm[];
+  float* ws = sm;                                   // [27][CIN][COUT]
+  float* xs = sm + 27 * CIN * COUT;                 // [kH^3][PS]
+  for (int e = threadIdx.x; e < 27 * CIN * COUT; e += kConvThreads) ws[e] = w[e];
+  const int n = *count;
+  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+    int x0, y0, z0;
+    tile_origin(v, list[li], x0, y0, z0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < kH * kH * kH * CIN; e += kConvThreads) {
+      const int ci = e % CIN, hv = e / CIN;
+      const int i = x0 - 1 + hv % kH, j = y0 - 1 + (hv / kH) % kH, k = z0 - 1 + hv / (kH * kH);
+      float val = 0.f;
+      if (i >= 0 && j >= 0 && k >= 0 && i < v.nx && j < v.ny && k < v.nz)
+        val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
+      xs[hv * PS + ci] = val;
+    }
+    __syncthreads();
+    // thread: voxel (a, b, c) and (a, b, c + 4)
+    const int a = threadIdx.x % kT, b = (threadIdx.x / kT) % kT, c = threadIdx.x / (kT * kT);
+    float acc0[COUT], acc1[COUT];
+#pragma unroll
+    for (int co = 0; co < COUT; ++co) { acc0[co] = 0.f; acc1[co] = 0.f; }
+    for (int tap = 0; tap < 27; ++tap) {
+      const int da = tap % 3, db = (tap / 3) % 3, dc = tap / 9;
+      const float* p0 = xs + ((a + da) + kH * ((b + db) + kH * (c + dc))) * PS;
+      const float* p1 = p0 + 4 * kH * kH * PS;
+      float xv0[CIN], xv1[CIN];
+      if constexpr (CIN % 4 == 0) {
+#pragma unroll
+        for (int q = 0; q < CIN / 4; ++q) {
+          const float4 t0 = *reinterpret_cast<const float4*>(p0 + 4 * q);
+          const float4 t1 = *reinterpret_cast<const float4*>(p1 + 4 * q);
+          xv0[4 * q] = t0.x; xv0[4 * q + 1] = t0.y; xv0[4 * q + 2] = t0.z; xv0[4 * q + 3] = t0.w;
+          xv1[4 * q] = t1.x; xv1[4 * q + 1] = t1.y; xv1[4 * q + 2] = t1.z; xv1[4 * q + 3] = t1.w;
+        }
+      } else {
+#pragma unroll
+        for (int ci = 0; ci < CIN; ++ci) { xv0[ci] = p0[ci]; xv1[ci] = p1[ci]; }
+      }
+      const float* wt = ws + tap * CIN * COUT;
+#pragma unroll
+      for (int ci = 0; ci < CIN; ++ci) {
+        if constexpr (COUT % 4 == 0) {
+#pragma unroll
+          for (int q = 0; q < COUT / 4; ++q) {
+            const float4 wv = *reinterpret_cast<const float4*>(wt + ci * COUT + 4 * q);
+            acc0[4 * q] = fmaf(xv0[ci], wv.x, acc0[4 * q]);
+            acc0[4 * q + 1] = fmaf(xv0[ci], wv.y, acc0[4 * q + 1]);
+            acc0[4 * q + 2] = fmaf(xv0[ci], wv.z, acc0[4 * q + 2]);
+            acc0[4 * q + 3] = fmaf(xv0[ci], wv.w, acc0[4 * q + 3]);
+            acc1[4 * q] = fmaf(xv1[ci], wv.x, acc1[4 * q]);
+            acc1[4 * q + 1] = fmaf(xv1[ci], wv.y, acc1[4 * q + 1]);
+            acc1[4 * q + 2] = fmaf(xv1[ci], wv.z, acc1[4 * q + 2]);
+            acc1[4 * q + 3] = fmaf(xv1[ci], wv.w, acc1[4 * q + 3]);
+          }
+        } else {
+#pragma unroll
+          for (int co = 0; co < COUT; ++co) {
+            acc0[co] = fmaf(xv0[ci], wt[ci * COUT + co], acc0[co]);
+            acc1[co] = fmaf(xv1[ci], wt[ci * COUT + co], acc1[co]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      const int i = x0 + a, j = y0 + b, k = z0 + c + 4 * s;
+      if (i >= v.nx || j >= v.ny || k >= v.nz) continue;
+      const size_t vox = (size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k);
+      float* acc = s ? acc1 : acc0;
+#pragma unroll
+      for (int co = 0; co < COUT; ++co) {
+        float r = acc[co];
+        if (relu) r = fmaxf(r, 0.f);
+        if (mask && !(mask[vox * COUT + co] > 0.f)) r = 0.f;
+        y[vox * COUT + co] = r;
+      }
+    }
+  }
+}
+
+// gw[tap][ci][co] = sum_v x[v + tap - 1][ci] * g[v][co] over the active
+// tiles; each CTA sums its tiles into partial[blockIdx.x][27 * CIN * COUT].
+// Thread t owns (tap, ci) pairs t and t + 256 (432 pairs at CIN = 16).
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kConvThreads) k_conv_wgrad(const float* __restrict__ x, const float* __restrict__ g,
+                                                             Vol v, const int32_t* __restrict__ list,
+                                                             const int32_t* __restrict__ count,
+                                                             float* __restrict__ partial, float scale_in) {
+  constexpr int PS = pad_stride(CIN);
+  constexpr int NP = 27 * CIN;           // (tap, ci) pairs
+  constexpr int PER = (NP + kConvThreads - 1) / kConvThreads;
+  extern __shared__ __align__(16) float sm[];
+  float* xs = sm;                         // [kH^3][PS]
+  float* gs = sm + kH * kH * kH * PS;     // [kT^3][COUT]
+  float acc[PER][COUT];
+#pragma unroll
+  for (int p = 0; p < PER; ++p)
+#pragma unroll
+    for (int co = 0; co < COUT; ++co) acc[p][co] = 0.f;
+  const int n = *count;
+  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+    int x0, y0, z0;
+    tile_origin(v, list[li], x0, y0, z0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < kH * kH * kH * CIN; e += kConvThreads) {
+      const int ci = e % CIN, hv = e / CIN;
+      const int i = x0 - 1 + hv % kH, j = y0 - 1 + (hv / kH) % kH, k = z0 - 1 + hv / (kH * kH);
+      float val = 0.f;
+      if (i >= 0 && j >= 0 && k >= 0 && i < v.nx && j < v.ny && k < v.nz)
+        val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
+      xs[hv * PS + ci] = val;
+    }
+    for (int e = threadIdx.x; e < kT * kT * kT * COUT; e += kConvThreads) {
+      const int co = e % COUT, tv = e / COUT;
+      const int i = x0 + tv % kT, j = y0 + (tv / kT) % kT, k = z0 + tv / (kT * kT);
+      float val = 0.f;
+      if (i < v.nx && j < v.ny && k < v.nz) val = g[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * COUT + co];
+      gs[tv * COUT + co] = val;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int pair = threadIdx.x + p * kConvThreads;
+      if (pair >= NP) continue;
+      const int tap = pair / CIN, ci = pair % CIN;
+      const int da = tap % 3, db = (tap / 3) % 3, dc = tap / 9;
+      for (int tv = 0; tv < kT * kT * kT; ++tv) {
+        const int a = tv % kT, b = (tv / kT) % kT, c = tv / (kT * kT);
+        const float xv = xs[((a + da) + kH * ((b + db) + kH * (c + dc))) * PS + ci];
+        const float* gr = gs + tv * COUT;
+#pragma unroll
+        for (int co = 0; co < COUT; ++co) acc[p][co] = fmaf(xv, gr[co], acc[p][co]);
+      }
+    }
+  }
+  float* out = partial + (size_t)blockIdx.x * NP * COUT;
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int pair = threadIdx.x + p * kConvThreads;
+    if (pair >= NP) continue;
+#pragma unroll
+    for (int co = 0; co < COUT; ++co) out[pair * COUT + co] = acc[p][co];
+  }
+}
+
+// out[e] = sum_b partial[b][e], b in order.
+__global__ void k_reduce_partials(const float* __restrict__ partial, int nb, int m, float* __restrict__ out) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int b = 0; b < nb; ++b) s += partial[(size_t)b * m + e];
+    out[e] = s;
+  }
+}
+
+// div F~ at voxel e = (i, j, k): F~a[u] = F[u][a] except on the last plane
+// of axis a, and zero before the first.
+__device__ __forceinline__ float flux_divergence(const float* __restrict__ F, const Vol& v, size_t e) {
+  const int i = (int)(e % v.nx), j = (int)((e / v.nx) % v.ny), k = (int)(e / ((size_t)v.nx * v.ny));
+  const size_t sy = v.nx, sz = (size_t)v.nx * v.ny;
+  float div = 0.f;
+  if (i < v.nx - 1) div += F[e * 3 + 0];
+  if (i > 0) div -= F[(e - 1) * 3 + 0];
+  if (j < v.ny - 1) div += F[e * 3 + 1];
+  if (j > 0) div -= F[(e - sy) * 3 + 1];
+  if (k < v.nz - 1) div += F[e * 3 + 2];
+  if (k > 0) div -= F[(e - sz) * 3 + 2];
+  return div;
+}
+
+// out = x + div F~ / s.
+__global__ void k_divergence(const float* __restrict__ x, const float* __restrict__ F, Vol v, float inv_s,
+                             float* __restrict__ out) {
+  const size_t n = (size_t)v.nx * v.ny * v.nz;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    out[e] = x[e] + flux_divergence(F, v, e) * inv_s;
+}
+
+// The loss: d = s x + div F~ - s t (the scaled output error); g = 2 d / nvox
+// (its gradient); per-block partial sums of d^2 (float64).
+__global__ void k_loss(const float* __restrict__ x, const float* __restrict__ F, const float* __restrict__ t,
+                       float s, Vol v, float* __restrict__ g, double* __restrict__ partial) {
+  __shared__ double sh[256];
+  double acc = 0;
+  const size_t nvox = (size_t)v.nx * v.ny * v.nz;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nvox; e += (size_t)gridDim.x * blockDim.x) {
+    const float d = s * x[e] + flux_divergence(F, v, e) - s * t[e];
+    g[e] = 2.f * d / (float)nvox;
+    acc += (double)d * d;
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+// Gradient at the flux from the gradient g at the output (the adjoint of
+// the divergence): G[u][a] = g[u] - g[u + e_a] below the last plane of
+// axis a, 0 on it.
+__global__ void k_div_adjoint(const float* __restrict__ g, Vol v, float* __restrict__ G) {
+  const size_t n = (size_t)v.nx * v.ny * v.nz, sy = v.nx, sz = (size_t)v.nx * v.ny;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % v.nx), j = (int)((e / v.nx) % v.ny), k = (int)(e / sz);
+    const float ge = g[e];
+    G[e * 3 + 0] = i < v.nx - 1 ? ge - g[e + 1] : 0.f;
+    G[e * 3 + 1] = j < v.ny - 1 ? ge - g[e + sy] : 0.f;
+    G[e * 3 + 2] = k < v.nz - 1 ? ge - g[e + sz] : 0.f;
+  }
+}
+
+__global__ void k_sum_double(const double* __restrict__ partial, int n, double* out, double scale) {
+  __shared__ double sh[256];
+  double s = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0] * scale;
+}
+
+// Round to the nearest BF16 value, ties to even (kept as float32).
+__device__ __forceinline__ float bf16_round(float f) {
+  unsigned u = __float_as_uint(f);
+  u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+  return __uint_as_float(u);
+}
+
+__global__ void k_bf16_round(const float* __restrict__ src, float* __restrict__ dst, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = bf16_round(src[i]);
+}
+
+// w'[tap'][co][ci] = w[tap][ci][co], tap' = 26 - tap: the weights of the
+// input-gradient pass (a correlation with the flipped, transposed kernel).
+__global__ void k_flip_weights(const float* __restrict__ w, float* __restrict__ wt, int cin, int cout) {
+  const int m = 27 * cin * cout;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
+    const int co = e % cout, ci = (e / cout) % cin, tap = e / (cin * cout);
+    wt[((26 - tap) * cout + co) * cin + ci] = w[e];
+  }
+}
+
+__global__ void k_adam(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+template <int CIN, int COUT>
+size_t conv_smem() { return (size_t)(27 * CIN * COUT + kH * kH * kH * pad_stride(CIN)) * sizeof(float); }
+template <int CIN, int COUT>
+size_t wgrad_smem() { return (size_t)(kH * kH * kH * pad_stride(CIN) + kT * kT * kT * COUT) * sizeof(float); }
+
+size_t layer_offset(int l) {
+  size_t o = 0;
+  for (int i = 0; i < l; ++i) o += 27 * (size_t)kLayerIn[i] * kLayerOut[i];
+  return o;
+}
+
+}  // namespace
+
+constexpr int kDnWeights = 27 * (1 * 16 + 16 * 16 + 16 * 16 + 16 * 3);  // 15,552
+
+// Workspaces of the network on one volume.
+struct Denoiser {
+  Vol v{};
+  int device = 0;
+  int nblocks = 0;              // CTAs of the conv grids (persistent over tiles)
+  int32_t* flags = nullptr;     // [tiles]
+  int32_t* list = nullptr;      // [tiles]
+  int32_t* count = nullptr;     // [1]
+  float* act[kLayers] = {};     // output of layer l: [vox][kLayerOut[l]]
+  float* gbuf[2] = {};          // gradients, [vox][16]
+  float* gout = nullptr;        // gradient at the output, [vox]
+  float* wr = nullptr;          // BF16-rounded weights used by the passes
+  float* wt = nullptr;          // flipped/transposed weights of one layer
+  float* partial = nullptr;     // [nblocks][27*16*16]
+  double* lpart = nullptr;      // loss partials
+  double* loss = nullptr;       // [1]
+};
+
+void dn_free(Denoiser* d) {
+  if (!d) return;
+  cudaSetDevice(d->device);
+  cudaFree(d->flags); cudaFree(d->list); cudaFree(d->count);
+  for (auto& a : d->act) cudaFree(a);
+  for (auto& g : d->gbuf) cudaFree(g);
+  cudaFree(d->gout);
+  cudaFree(d->wr); cudaFree(d->wt); cudaFree(d->partial); cudaFree(d->lpart); cudaFree(d->loss);
+  delete d;
+}
+
+Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms) {
+  auto* d = new Denoiser();
+  d->device = device;
+  d->v = Vol{nx, ny, nz, (nx + kT - 1) / kT, (ny + kT - 1) / kT, (nz + kT - 1) / kT};
+  const size_t ntiles = (size_t)d->v.tx * d->v.ty * d->v.tz, nvox = (size_t)nx * ny * nz;
+  d->nblocks = num_sms * 2;
+  auto alloc = [](void** p, size_t bytes) { VLB_CUDA(cudaMalloc(p, std::max<size_t>(bytes, 16))); };
+  try {
+    alloc((void**)&d->flags, ntiles * 4);
+    alloc((void**)&d->list, ntiles * 4);
+    alloc((void**)&d->count, 4);
+    for (int l = 0; l < kLayers; ++l) alloc((void**)&d->act[l], nvox * kLayerOut[l] * 4);
+    for (auto& g : d->gbuf) alloc((void**)&g, nvox * 16 * 4);
+    alloc((void**)&d->gout, nvox * 4);
+    alloc((void**)&d->wr, kDnWeights * 4);
+    alloc((void**)&d->wt, 27 * 16 * 16 * 4);
+    alloc((void**)&d->partial, (size_t)d->nblocks * 27 * 16 * 16 * 4);
+    alloc((void**)&d->lpart, 1024 * 8);
+    alloc((void**)&d->loss, 8);
+  } catch (...) {
+    dn_free(d);
+    throw;
+  }
+  static bool attrs = false;
+  if (!attrs) {
+    VLB_CUDA(cudaFuncSetAttribute(k_conv<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<1, 16>()));
+    VLB_CUDA(cudaFuncSetAttribute(k_conv<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<16, 16>()));
+    VLB_CUDA(cudaFuncSetAttribute(k_conv<16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<16, 3>()));
+    VLB_CUDA(cudaFuncSetAttribute(k_conv<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<3, 16>()));
+    VLB_CUDA(cudaFuncSetAttribute(k_conv_wgrad<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)wgrad_smem<1, 16>()));
+    VLB_CUDA(cudaFuncSetAttribute(k_conv_wgrad<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)wgrad_smem<16, 16>()));
+    VLB_CUDA(cudaFuncSetAttribute(k_conv_wgrad<16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)wgrad_smem<16, 3>()));
+    attrs = true;
+  }
+  return d;
+}
+
+namespace {
+
+void conv(Denoiser& d, int cin, int cout, const float* x, const float* w, float* y, bool relu, const float* mask,
+          float scale_in, cudaStream_t s) {
+  const int g = d.nblocks;
+  if (cin == 1 && cout == 16)
+    k_conv<1, 16><<<g, kConvThreads, conv_smem<1, 16>(), s>>>(x, w, y, d.v, d.list, d.count, relu, mask, scale_in);
+  else if (cin == 16 && cout == 16)
+    k_conv<16, 16><<<g, kConvThreads, conv_smem<16, 16>(), s>>>(x, w, y, d.v, d.list, d.count, relu, mask, scale_in);
+  else if (cin == 16 && cout == 3)
+    k_conv<16, 3><<<g, kConvThreads, conv_smem<16, 3>(), s>>>(x, w, y, d.v, d.list, d.count, relu, mask, scale_in);
+  else if (cin == 3 && cout == 16)
+    k_conv<3, 16><<<g, kConvThreads, conv_smem<3, 16>(), s>>>(x, w, y, d.v, d.list, d.count, relu, mask, scale_in);
+  else
+    throw ArgError("unsupported conv shape");
+  VLB_CUDA(cudaGetLastError());
+}
+
+void wgrad(Denoiser& d, int cin, int cout, const float* x, const float* g, float* gw, float scale_in,
+           cudaStream_t s) {
+  const int nb = d.nblocks, m = 27 * cin * cout;
+  if (cin == 1 && cout == 16)
+    k_conv_wgrad<1, 16><<<nb, kConvThreads, wgrad_smem<1, 16>(), s>>>(x, g, d.v, d.list, d.count, d.partial,
+                                                                       scale_in);
+  else if (cin == 16 && cout == 16)
+    k_conv_wgrad<16, 16><<<nb, kConvThreads, wgrad_smem<16, 16>(), s>>>(x, g, d.v, d.list, d.count, d.partial,
+                                                                         scale_in);
+  else if (cin == 16 && cout == 3)
+    k_conv_wgrad<16, 3><<<nb, kConvThreads, wgrad_smem<16, 3>(), s>>>(x, g, d.v, d.list, d.count, d.partial,
+                                                                       scale_in);
+  else
+    throw ArgError("unsupported conv shape");
+  VLB_CUDA(cudaGetLastError());
+  k_reduce_partials<<<(m + 255) / 256, 256, 0, s>>>(d.partial, nb, m, gw);
+  VLB_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+constexpr int kForwardLaunches = 3 + kLayers;  // kernels dn_forward launches
+
+// Active tiles of input x, BF16 rounding of the weights, and the forward
+// pass: act[3] = F = f(s x) (three channels); act[l] zeroed outside active
+// tiles.
+void dn_forward(Denoiser& d, const float* x, float s, const float* w_master, cudaStream_t st) {
+  const size_t ntiles = (size_t)d.v.tx * d.v.ty * d.v.tz, nvox = (size_t)d.v.nx * d.v.ny * d.v.nz;
+  k_tile_flags<<<(unsigned)ntiles, 256, 0, st>>>(x, d.v, d.flags);
+  VLB_CUDA(cudaGetLastError());
+  VLB_CUDA(cudaMemsetAsync(d.count, 0, 4, st));
+  k_tile_active<<<(unsigned)((ntiles + 255) / 256), 256, 0, st>>>(d.flags, d.v, d.list, d.count);
+  VLB_CUDA(cudaGetLastError());
+  k_bf16_round<<<(kDnWeights + 255) / 256, 256, 0, st>>>(w_master, d.wr, kDnWeights);
+  VLB_CUDA(cudaGetLastError());
+  for (int l = 0; l < kLayers; ++l) {
+    VLB_CUDA(cudaMemsetAsync(d.act[l], 0, nvox * kLayerOut[l] * 4, st));
+    conv(d, kLayerIn[l], kLayerOut[l], l == 0 ? x : d.act[l - 1], d.wr + layer_offset(l), d.act[l], l < 3, nullptr,
+         l == 0 ? s : 1.f, st);
+  }
+}
+
+// Loss against target t (same scale s) and the gradient of the master
+// weights into gw (after dn_forward on the same x).
+void dn_backward(Denoiser& d, const float* x, const float* t, float s, float* gw, cudaStream_t st) {
+  const size_t nvox = (size_t)d.v.nx * d.v.ny * d.v.nz;
+  const int lb = 1024;
+  k_loss<<<lb, 256, 0, st>>>(x, d.act[3], t, s, d.v, d.gout, d.lpart);
+  VLB_CUDA(cudaGetLastError());
+  k_sum_double<<<1, 256, 0, st>>>(d.lpart, lb, d.loss, 1.0 / (double)nvox);
+  VLB_CUDA(cudaGetLastError());
+  k_div_adjoint<<<lb, 256, 0, st>>>(d.gout, d.v, d.gbuf[0]);
+  VLB_CUDA(cudaGetLastError());
+  int cur = 0;  // gbuf[cur]: gradient at the output of layer l
+  for (int l = kLayers - 1; l >= 0; --l) {
+    const int cin = kLayerIn[l], cout = kLayerOut[l];
+    const float* in = l == 0 ? x : d.act[l - 1];
+    wgrad(d, cin, cout, in, d.gbuf[cur], gw + layer_offset(l), l == 0 ? s : 1.f, st);
+    if (l == 0) break;
+    // gradient at the input of layer l = conv^T(g) masked by the ReLU of layer l-1
+    k_flip_weights<<<(27 * cin * cout + 255) / 256, 256, 0, st>>>(d.wr + layer_offset(l), d.wt, cin, cout);
+    VLB_CUDA(cudaGetLastError());
+    VLB_CUDA(cudaMemsetAsync(d.gbuf[cur ^ 1], 0, nvox * cin * 4, st));
+    conv(d, cout, cin, d.gbuf[cur], d.wt, d.gbuf[cur ^ 1], false, d.act[l - 1], 1.f, st);
+    cur ^= 1;
+  }
+}
+
+void dn_adam(Denoiser& d, float* w, const float* g, float* m, float* v, float lr, int step, cudaStream_t st) {
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
+  k_adam<<<(kDnWeights + 255) / 256, 256, 0, st>>>(w, g, m, v, kDnWeights, lr, b1, b2, 1e-8f, c1, c2);
+  VLB_CUDA(cudaGetLastError());
+}
+
+const float* dn_output(const Denoiser& d) { return d.act[3]; }
+double* dn_loss_ptr(const Denoiser& d) { return d.loss; }
+int dn_active_tiles(const Denoiser& d) {
+  int n = 0;
+  cudaMemcpy(&n, d.count, 4, cudaMemcpyDeviceToHost);
+  return n;
+}
+
+}  // namespace vlb
+
+// ------------------------------------------------------------- in the step
+namespace vlb {
+namespace {
+
+// The deposit's charge is (N - nout) w after its renormalisation; keep the
+// prediction (renormalised to that charge) when its own charge is within
+// `tol` of it, else keep the deposit.
+__global__ void k_denoise_select(float* __restrict__ rho, const float* __restrict__ pred, size_t n,
+                                 DeviceScalars* dsc, double npart_global, double w, double tol) {
+  const double q_dep = (npart_global - dsc->xch[0]) * w;
+  const double q_pred = dsc->xch[1];
+  const bool use = fabs(q_pred - q_dep) <= tol && q_pred > 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) dsc->denoised = use ? 1 : 0;
+  if (!use) return;
+  const float sc = (float)(q_dep / q_pred);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    rho[i] = pred[i] * sc;
+}
+
+}  // namespace
+
+void launch_denoise(Ctx& c, int64_t npart_global) {
+  Level& F = c.fine;
+  const size_t tot = (size_t)F.n * F.n * F.n;
+  Denoiser& d = *c.dn;
+  dn_forward(d, F.rho, (float)c.dn_scale, c.dn_weights, c.stream);
+  c.launches += kForwardLaunches;
+  k_divergence<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(F.rho, dn_output(d), d.v,
+                                                                         (float)(1.0 / c.dn_scale), c.dn_pred);
+  VLB_LAUNCHED(c);
+  launch_grid_charge(c, F, c.dn_pred, &c.dsc->xch[1]);
+  k_denoise_select<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(F.rho, c.dn_pred, tot, c.dsc,
+                                                                             (double)npart_global, c.weight, c.dn_tol);
+  VLB_LAUNCHED(c);
+}
+
+void free_denoiser(Ctx& c) {
+  if (c.dn) dn_free(c.dn);
+  c.dn = nullptr;
+  if (c.dn_weights) cudaFree(c.dn_weights);
+  if (c.dn_pred) cudaFree(c.dn_pred);
+  c.dn_weights = nullptr;
+  c.dn_pred = nullptr;
+}
+
+}  // namespace vlb
+
+// --------------------------------------------------------------- C ABI
+using namespace vlb;
+
+struct vlb_denoiser {
+  Denoiser* d = nullptr;
+};
+
+namespace {
+int dn_fail(int code, const std::string& m) {
+  set_last_error(m);
+  return code;
+}
+template <class F>
+int dn_guard(F&& f) {
+  try {
+    return f();
+  } catch (const CudaError& e) {
+    return dn_fail(VLB_ERR_CUDA, cuda_msg(e.err, "denoiser"));
+  } catch (const ArgError& e) {
+    return dn_fail(VLB_ERR_ARG, e.msg);
+  } catch (const std::bad_alloc&) {
+    return dn_fail(VLB_ERR_NOMEM, "host allocation failed");
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int vlb_dn_weight_count(void) { return kDnWeights; }
+
+int vlb_dn_create(int32_t nx, int32_t ny, int32_t nz, int32_t device, vlb_denoiser** out) {
+  if (!out || nx < 1 || ny < 1 || nz < 1) return dn_fail(VLB_ERR_ARG, "vlb_dn_create: bad volume");
+  *out = nullptr;
+  return dn_guard([&]() -> int {
+    VLB_CUDA(cudaSetDevice(device));
+    int sms = 148;
+    VLB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    auto* h = new vlb_denoiser();
+    try {
+      h->d = dn_create(nx, ny, nz, device, sms);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+    return VLB_OK;
+  });
+}
+
+int vlb_dn_destroy(vlb_denoiser* h) {
+  if (!h) return VLB_OK;
+  dn_free(h->d);
+  delete h;
+  return VLB_OK;
+}
+
+int vlb_dn_forward(vlb_denoiser* h, const float* x, float scale, const float* weights, float* out, void* stream) {
+  if (!h || !x || !weights || !out || !(scale > 0)) return dn_fail(VLB_ERR_ARG, "vlb_dn_forward: bad arguments");
+  return dn_guard([&]() -> int {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Denoiser& d = *h->d;
+    VLB_CUDA(cudaSetDevice(d.device));
+    dn_forward(d, x, scale, weights, s);
+    const size_t n = (size_t)d.v.nx * d.v.ny * d.v.nz;
+    k_divergence<<<(unsigned)std::min<size_t>((n + 255) / 256, 65535), 256, 0, s>>>(x, dn_output(d), d.v, 1.f / scale,
+                                                                                      out);
+    VLB_CUDA(cudaGetLastError());
+    return VLB_OK;
+  });
+}
+
+int vlb_dn_gradient(vlb_denoiser* h, const float* x, const float* target, float scale, const float* weights,
+                    float* grad, double* loss, void* stream) {
+  if (!h || !x || !target || !weights || !grad || !(scale > 0))
+    return dn_fail(VLB_ERR_ARG, "vlb_dn_gradient: bad arguments");
+  return dn_guard([&]() -> int {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Denoiser& d = *h->d;
+    VLB_CUDA(cudaSetDevice(d.device));
+    dn_forward(d, x, scale, weights, s);
+    dn_backward(d, x, target, scale, grad, s);
+    if (loss) {
+      VLB_CUDA(cudaMemcpyAsync(loss, dn_loss_ptr(d), sizeof(double), cudaMemcpyDeviceToHost, s));
+      VLB_CUDA(cudaStreamSynchronize(s));
+    }
+    return VLB_OK;
+  });
+}
+
+int vlb_dn_adam(vlb_denoiser* h, float* weights, const float* grad, float* m, float* v, float lr, int32_t step,
+                void* stream) {
+  if (!h || !weights || !grad || !m || !v || step < 1) return dn_fail(VLB_ERR_ARG, "vlb_dn_adam: bad arguments");
+  return dn_guard([&]() -> int {
+    VLB_CUDA(cudaSetDevice(h->d->device));
+    dn_adam(*h->d, weights, grad, m, v, lr, step, static_cast<cudaStream_t>(stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_dn_active_tiles(vlb_denoiser* h, int32_t* n) {
+  if (!h || !n) return dn_fail(VLB_ERR_ARG, "vlb_dn_active_tiles: bad arguments");
+  return dn_guard([&]() -> int {
+    VLB_CUDA(cudaSetDevice(h->d->device));
+    VLB_CUDA(cudaDeviceSynchronize());
+    *n = dn_active_tiles(*h->d);
+    return VLB_OK;
+  });
+}
+
+}  // extern "C"

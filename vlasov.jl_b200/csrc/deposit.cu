@@ -442,6 +442,15 @@ void launch_deposit_fine_normalize(Ctx& c, double charge, int mode, int64_t npar
   VLB_LAUNCHED(c);
 }
 
+// The charge sum rho m0x m0y m0z of a float32 grid of level L into *out.
+void launch_grid_charge(Ctx& c, Level& L, const float* rho, double* out) {
+  const int cols = L.n * L.n;
+  k_charge_columns<<<(cols + 7) / 8, 256, 0, c.stream>>>(rho, nullptr, L.dual_d, L.n, c.partials);
+  VLB_LAUNCHED(c);
+  k_charge_total<<<1, 1024, 0, c.stream>>>(c.partials, cols, out);
+  VLB_LAUNCHED(c);
+}
+
 void launch_deposit_fine(Ctx& c, double charge, int mode) {
   launch_deposit_fine_raw(c, mode);
   launch_deposit_fine_normalize(c, charge, mode, c.N);

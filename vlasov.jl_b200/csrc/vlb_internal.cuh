@@ -48,7 +48,10 @@ struct DeviceScalars {
   unsigned long long work_cic;
   int32_t nitems;                    // cell chunks of the gather
   int32_t pad_items;
-  double xch[4];                     // exchanged between the shards of a step: [0] deposit-window rejections
+  double xch[4];                     // exchanged between the shards of a step: [0] deposit-window rejections;
+                                     // [1] charge of the denoiser's prediction (not exchanged)
+  int32_t denoised;                  // 1: the step used the denoiser's density
+  int32_t pad_dn;
   int32_t reset_end;
   int32_t pad0;
   // --- persistent ---
@@ -94,6 +97,8 @@ struct Particles {
   int32_t* pk = nullptr;
   float* pd = nullptr;
 };
+
+struct Denoiser;
 
 struct Ctx {
   int device = 0;
@@ -141,6 +146,11 @@ struct Ctx {
   // CTAs per SM of the gather, the coarse deposit, the push and the record move
   int chunk = kChunk, field_cps = 3, cic_cps = 4, push_cps = 8, move_cps = 8;
   unsigned* tc_sync = nullptr;  // grid-barrier counter of the tensor-core chains
+  // the learned denoiser of the fine density (vlb_set_denoiser)
+  Denoiser* dn = nullptr;
+  float* dn_weights = nullptr;  // BF16-rounded weights on the device
+  float* dn_pred = nullptr;     // [n^3] its prediction
+  double dn_scale = 1, dn_tol = 1e-3;
   // scalars
   DeviceScalars* dsc = nullptr;
   DeviceScalars* hsc = nullptr;  // pinned, results
@@ -161,6 +171,7 @@ struct Ctx {
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   vlb_step_params graph_params{};
   bool graph_valid = false;
+  uint64_t config_epoch = 0;         // bumped by every change a captured graph bakes in (shapes, denoiser)
   long long graph_launches = 0;  // kernels in one captured step
 };
 
@@ -178,6 +189,12 @@ void launch_deposit_fine_normalize(Ctx& c, double charge, int mode, int64_t npar
 void launch_deposit_coarse(Ctx& c, double charge);
 // poisson.cu
 void launch_poisson(Ctx& c);
+void launch_grid_charge(Ctx& c, Level& L, const float* rho, double* out);
+// denoise.cu
+Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms);
+void dn_free(Denoiser* d);
+void launch_denoise(Ctx& c, int64_t npart_global);
+void free_denoiser(Ctx& c);
 // mode_tc.cu
 bool tc_supported(int n);
 TcImage make_tc_image(const double* A, int n);

@@ -476,6 +476,7 @@ class StepDiagnostics:
     projectile_force: tuple
     total_charge: float
     status: int = 0
+    denoised: int = 0            # 1: the step's fine density came from the learned denoiser
 
 
 class Simulation:
@@ -497,6 +498,7 @@ class Simulation:
         self.precision = precision
         self.use_graph = use_graph
         self.capture_radius = capture_radius
+        self.denoise = False       # set by denoiser.attach()
         positions, momenta = sample_thomas_fermi(profile, p.nparticles, self.weight, seed=seed)
         self.accelerator = DeviceAccelerator(self.meshes, self.smoothing, p.nparticles, self.weight, device)
         self.x0, self.h = self.accelerator.x0, self.accelerator.h
@@ -519,6 +521,7 @@ class Simulation:
         sp.push = int(push)
         sp.use_graph = int(self.use_graph and push)
         sp.poisson_precision = self.precision
+        sp.denoise = int(self.denoise and push)
         return sp
 
     def prime_leapfrog(self, positions, momenta, consistent: bool = False):
@@ -547,7 +550,7 @@ class Simulation:
                                                                       capture=self.capture_radius))
         self.steps_done += 1
         return StepDiagnostics(r.kinetic, r.escaped, tuple(r.angular), r.enclosed_charge, r.nout, r.outcount,
-                               r.noccupied, tuple(r.projectile_force), r.total_charge, r.status)
+                               r.noccupied, tuple(r.projectile_force), r.total_charge, r.status, r.denoised)
 
     def run(self, nsteps: int | None = None, callback=None):
         nsteps = self.params.nsteps if nsteps is None else nsteps
