@@ -274,8 +274,10 @@ typedef struct vlb_exchange {
  * channels, ReLU, no biases; BF16 weights, float32 arithmetic; weights of
  * layer l as [27][cin][cout], tap = dx + 3 dy + 9 dz).  Its three outputs are
  * a charge flux F = f(s rho) and the density it gives is
- * out = rho + div F / s, with no flux through the grid's faces: the network
- * moves charge between neighbouring voxels and adds none.  It is trained on
+ * out = rho + div F^ / s, F^ the flux with none through the grid's faces
+ * and limited so that no voxel gives more charge than it holds: the network
+ * moves charge between neighbouring voxels, adds none and makes no negative
+ * density.  It is trained on
  * pairs of densities of the method itself (an 8e6-particle run's deposit
  * against a run with ten times the particles, at the same instant).
  *

@@ -10,9 +10,13 @@ against, and its own gradient is pinned by finite differences of its own loss
 
 Network: four 3^3 convolutions, 1 -> 16 -> 16 -> 16 -> 3 channels, ReLU after
 the first three, no biases, zero padding.  The three outputs are a flux
-F = f(s x) and out = x + div F~ / s, F~ the flux with no flow through the
-grid's faces (F~a = 0 on the last plane of axis a and before the first), so
-that sum(out) = sum(x).  Weights of
+F = f(s x) and out = x + div F^ / s, F~ the flux with no flow through the
+grid's faces (F~a = 0 on the last plane of axis a and before the first) and
+F^ that flux limited so that no voxel gives more than it holds: the face
+flux p = F~a[u] leaves its donor (u + e_a when p > 0, u when p < 0); a donor
+with charge c = s x and outflow O = sum of its |p| scales them all by
+lam = 1 (O <= c), c / O (O > c > 0), 0 (c <= 0).  So sum(out) = sum(x) and
+out >= min(x, 0).  Weights of
 layer l are stored flat as [27][cin][cout], tap = da + 3 db + 9 dc reading the
 input at (i + da - 1, j + db - 1, k + dc - 1).  The passes use the weights
 rounded to BF16 (nearest, ties to even); the gradient of the master weights is
@@ -78,6 +82,71 @@ def conv_weight_grad(x, g):
     return gw
 
 
+AXES = ((0, 2), (1, 1), (2, 0))   # flux channel -> array axis (x, y, z)
+
+
+def _shift(arr, ax, k):
+    """arr at index + k along axis ax, zero outside."""
+    out = np.zeros_like(arr)
+    n = arr.shape[ax]
+    src, dst = [slice(None)] * arr.ndim, [slice(None)] * arr.ndim
+    if k > 0:
+        src[ax], dst[ax] = slice(k, n), slice(0, n - k)
+    else:
+        src[ax], dst[ax] = slice(0, n + k), slice(-k, n)
+    out[tuple(dst)] = arr[tuple(src)]
+    return out
+
+
+def face_flux(F):
+    """F~: the flux with the last plane of each channel's axis zeroed."""
+    Ft = np.array(F, dtype=np.float64)
+    for a, ax in AXES:
+        sl = [slice(None)] * 3
+        sl[ax] = -1
+        Ft[tuple(sl) + (a,)] = 0.0
+    return Ft
+
+
+def limiter(Ft, c):
+    """(lam, O) of every voxel as a donor, for face fluxes Ft and charges c."""
+    O = np.zeros(c.shape)
+    for a, ax in AXES:
+        p = Ft[..., a]
+        O += np.maximum(-p, 0.0) + _shift(np.maximum(p, 0.0), ax, -1)
+    safe = np.where(O > 0, O, 1.0)
+    lam = np.where(O <= c, 1.0, np.where(c > 0, c / safe, 0.0))
+    return lam, O
+
+
+def _donor(arr, p, ax):
+    """arr at the donor of each face flux p (index + 1 along ax when p > 0)."""
+    return np.where(p > 0, _shift(arr, ax, 1), arr)
+
+
+def limited_flux(Ft, lam):
+    Fh = np.empty_like(Ft)
+    for a, ax in AXES:
+        p = Ft[..., a]
+        Fh[..., a] = p * _donor(lam, p, ax)
+    return Fh
+
+
+def limited_flux_adjoint(G, Ft, lam, O, c):
+    """dL/dF~ from G = dL/dF^ (lam, O functions of F~, c held)."""
+    T = np.zeros(c.shape)
+    for a, ax in AXES:
+        p, Ga = Ft[..., a], G[..., a]
+        T += np.where(p < 0, Ga * p, 0.0) + _shift(np.where(p > 0, Ga * p, 0.0), ax, -1)
+    out = np.zeros_like(Ft)
+    for a, ax in AXES:
+        p, Ga = Ft[..., a], G[..., a]
+        ld, Od, cd, Td = (_donor(z, p, ax) for z in (lam, O, c, T))
+        lim = (Od > cd) & (cd > 0) & (p != 0)
+        out[..., a] = ld * Ga - np.where(lim, ld / np.where(lim, Od, 1.0) * np.sign(p) * Td, 0.0)
+    return out
+
+
 def divergence(F):
     """div F~ of a (nz, ny, nx, 3) flux (channel a along axis x, y, z)."""
     out = np.zeros(F.shape[:3])
@@ -101,27 +170,33 @@ def divergence_adjoint(g):
     return G
 
 
-def forward(x, weights, scale, rounding=True):
+def forward(x, weights, scale, rounding=True, details=False):
     """Activations of every layer (inputs included; the last is the flux F)
-    and out = x + div F~ / scale.  rounding=False uses the weights as given
-    (float64), for finite differences."""
+    and out = x + div F^ / scale (with the limiter's (Ft, lam, O) when
+    `details`).  rounding=False uses the weights as given (float64), for
+    finite differences."""
     ws = split(bf16_round(weights) if rounding else weights)
-    a = [scale * np.asarray(x, dtype=np.float64)[..., None]]
+    x = np.asarray(x, dtype=np.float64)
+    a = [scale * x[..., None]]
     for l, w in enumerate(ws):
         z = conv(a[-1], w)
         a.append(np.maximum(z, 0.0) if l < 3 else z)
-    return a, np.asarray(x, dtype=np.float64) + divergence(a[-1]) / scale
+    Ft = face_flux(a[-1])
+    lam, O = limiter(Ft, scale * x)
+    out = x + divergence(limited_flux(Ft, lam)) / scale
+    return (a, out, (Ft, lam, O)) if details else (a, out)
 
 
 def loss_and_grad(x, target, weights, scale, rounding=True):
     """loss = mean over voxels of (scale (out - target))^2 and its gradient
     with respect to the weights (flat, straight-through the BF16 rounding)."""
     ws = split(bf16_round(weights) if rounding else weights)
-    a, out = forward(x, weights, scale, rounding)
+    a, out, (Ft, lam, O) = forward(x, weights, scale, rounding, details=True)
     d = scale * (out - np.asarray(target, dtype=np.float64))
     nvox = d.size
     loss = float(np.sum(d * d) / nvox)
-    g = divergence_adjoint(2.0 * d / nvox)
+    G = divergence_adjoint(2.0 * d / nvox)
+    g = face_flux(limited_flux_adjoint(G, Ft, lam, O, scale * np.asarray(x, dtype=np.float64)))
     grads = [None] * 4
     for l in range(3, -1, -1):
         grads[l] = conv_weight_grad(a[l], g)

@@ -31,7 +31,10 @@ def test_divergence_adds_no_charge_and_has_its_adjoint():
 def test_weight_gradient_matches_finite_differences():
     rng = np.random.default_rng(5)
     x, t, w = _case(rng)
+    w[-27 * 16 * 3:] *= 4.0                  # strong fluxes: the limiter acts
     scale = 2.0
+    _, _, (Ft, lam, O) = D.forward(x, w, scale, rounding=False, details=True)
+    assert np.sum((lam > 0) & (lam < 1)) > 5 and np.sum((lam == 0) & (O > 0)) > 5
     _, g = D.loss_and_grad(x, t, w, scale, rounding=False)
     offs = np.cumsum([0] + [27 * a * b for a, b in D.LAYERS])
     picks = np.concatenate([rng.integers(offs[l], offs[l + 1], 12) for l in range(4)])
@@ -62,6 +65,15 @@ def test_bf16_rounding_matches_torch():
     assert np.array_equal(D.bf16_round(w), ref)
 
 
+def test_limiter_keeps_the_density_nonnegative():
+    rng = np.random.default_rng(13)
+    x, _, w = _case(rng, (12, 12, 12))
+    w[-27 * 16 * 3:] *= 20.0
+    _, out, (_, lam, _) = D.forward(x, w, 3.0, details=True)
+    assert np.min(lam) < 0.5                      # it had work to do
+    assert np.min(out) >= -1e-12 and abs(out.sum() - x.sum()) < 1e-9 * x.sum()
+
+
 def test_empty_space_stays_empty():
     rng = np.random.default_rng(11)
     x, _, w = _case(rng, (20, 20, 20))
@@ -74,3 +86,19 @@ def test_empty_space_stays_empty():
     assert np.all(out[far] == 0)
     assert abs(out.sum() - x.sum()) < 1e-9 * x.sum()
     assert D.active_tiles(x) == 8          # tile (0,0,0) and its neighbours in a 3^3 tile grid
+
+
+def test_committed_network_loads():
+    """The trained network in the package: the right count, BF16 values,
+    a positive input scale; on a small noisy blob it conserves the charge
+    and makes no negative density."""
+    from conftest import load_package
+    DN = load_package().denoiser
+    w, scale, meta = DN.load_weights()
+    assert w.shape == (D.WEIGHT_COUNT,) and scale > 0 and meta["low"] * 10 == meta["high"]
+    assert np.array_equal(w, D.bf16_round(w))
+    rng = np.random.default_rng(17)
+    x = np.zeros((16, 16, 16))
+    x[4:12, 4:12, 4:12] = rng.poisson(30.0, (8, 8, 8)) / (30.0 * scale)
+    _, out = D.forward(x, w, scale)
+    assert np.min(out) >= -1e-12 and abs(out.sum() - x.sum()) < 1e-9 * x.sum()

@@ -6,12 +6,15 @@
 // (s a fixed input scale), and the output is its divergence added to the
 // input:
 //
-//     out[v] = rho[v] + (1/s) sum_axes (F~a[v] - F~a[v - e_a]),
+//     out[v] = rho[v] + (1/s) sum_axes (F^a[v] - F^a[v - e_a]),
 //
 // F~a the flux with no flow through the grid's faces (zero on the last
-// plane of its axis and before the first).  The correction moves charge
-// between neighbouring voxels and adds none: the sum of out equals the sum
-// of rho.  Without biases f(0) = 0 and f is positively homogeneous, so empty
+// plane of its axis and before the first), F^ that flux limited so that no
+// voxel gives more charge than it holds (k_flux_limit).  The correction
+// moves charge between neighbouring voxels and adds none: the sum of out
+// equals the sum of rho, and out >= min(rho, 0) (the exchange-correlation
+// potential of the step needs rho > -1.6e-4; the network can make no new
+// negative density).  Without biases f(0) = 0 and f is positively homogeneous, so empty
 // space stays empty and the correction scales with the density.  Weights are
 // BF16 (kept as float32 values that BF16 represents exactly), every product
 // and sum is float32.
@@ -27,9 +30,10 @@
 //                         tile, two voxels per thread sharing the weight reads
 //   k_conv_wgrad<..>      weight gradient, per-CTA partial sums over tiles,
 //                         reduced in a fixed order by k_reduce_partials
-//   k_divergence          out = rho + div F~ / s
-//   k_loss, k_div_adjoint mean squared error against the target and its
-//                         gradient at the flux
+//   k_flux_limit          the positivity limiter of the flux
+//   k_divergence          out = rho + div F^ / s (F^ the limited flux)
+//   k_loss, k_limit_tsum, mean squared error against the target and its
+//   k_div_adjoint         gradient at the flux, through the limiter
 //   k_adam                Adam update of the float32 master weights
 //
 // The same kernels serve the training loop (vlb_dn_*) and the in-step
@@ -265,38 +269,80 @@ __global__ void k_reduce_partials(const float* __restrict__ partial, int nb, int
   }
 }
 
-// div F~ at voxel e = (i, j, k): F~a[u] = F[u][a] except on the last plane
-// of axis a, and zero before the first.
-__device__ __forceinline__ float flux_divergence(const float* __restrict__ F, const Vol& v, size_t e) {
-  const int i = (int)(e % v.nx), j = (int)((e / v.nx) % v.ny), k = (int)(e / ((size_t)v.nx * v.ny));
-  const size_t sy = v.nx, sz = (size_t)v.nx * v.ny;
+// Voxel e's coordinates, the grid's extents and strides, by axis.
+struct Cell {
+  int ijk[3], n[3];
+  size_t st[3];
+  __device__ Cell(const Vol& v, size_t e) {
+    n[0] = v.nx; n[1] = v.ny; n[2] = v.nz;
+    st[0] = 1; st[1] = (size_t)v.nx; st[2] = (size_t)v.nx * v.ny;
+    ijk[0] = (int)(e % v.nx); ijk[1] = (int)((e / v.nx) % v.ny); ijk[2] = (int)(e / st[2]);
+  }
+};
+
+// The flux limiter.  The face flux p = F~a[u] (between u and u + e_a) moves
+// charge from u + e_a into u when p > 0 and from u into u + e_a when p < 0:
+// its donor is the voxel it leaves.  Voxel e gives at most its own charge
+// c = s x[e]: with O its outflow (the sum of |p| over the faces it donates
+// through), every flux it donates is scaled by
+//     lam = 1 (O <= c),  c / O (O > c > 0),  0 (c <= 0),
+// so that out >= min(x, 0) everywhere; the limited fluxes still cancel in
+// pairs (no charge is added).
+__global__ void k_flux_limit(const float* __restrict__ F, const float* __restrict__ x, float s, Vol v,
+                             float* __restrict__ lam, float* __restrict__ outflow) {
+  const size_t nvox = (size_t)v.nx * v.ny * v.nz;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nvox; e += (size_t)gridDim.x * blockDim.x) {
+    const Cell q(v, e);
+    float O = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (q.ijk[a] < q.n[a] - 1) O += fmaxf(-F[e * 3 + a], 0.f);        // face (e, e + e_a)
+      if (q.ijk[a] > 0) O += fmaxf(F[(e - q.st[a]) * 3 + a], 0.f);      // face (e - e_a, e)
+    }
+    const float c = s * x[e];
+    lam[e] = O <= c ? 1.f : (c > 0.f ? c / O : 0.f);
+    outflow[e] = O;
+  }
+}
+
+// div F^ at voxel e, F^ = the limited flux.
+__device__ __forceinline__ float limited_divergence(const float* __restrict__ F, const float* __restrict__ lam,
+                                                    const Vol& v, size_t e) {
+  const Cell q(v, e);
   float div = 0.f;
-  if (i < v.nx - 1) div += F[e * 3 + 0];
-  if (i > 0) div -= F[(e - 1) * 3 + 0];
-  if (j < v.ny - 1) div += F[e * 3 + 1];
-  if (j > 0) div -= F[(e - sy) * 3 + 1];
-  if (k < v.nz - 1) div += F[e * 3 + 2];
-  if (k > 0) div -= F[(e - sz) * 3 + 2];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (q.ijk[a] < q.n[a] - 1) {
+      const float p = F[e * 3 + a];
+      div += p * (p > 0.f ? lam[e + q.st[a]] : lam[e]);
+    }
+    if (q.ijk[a] > 0) {
+      const size_t u = e - q.st[a];
+      const float p = F[u * 3 + a];
+      div -= p * (p > 0.f ? lam[e] : lam[u]);
+    }
+  }
   return div;
 }
 
-// out = x + div F~ / s.
-__global__ void k_divergence(const float* __restrict__ x, const float* __restrict__ F, Vol v, float inv_s,
-                             float* __restrict__ out) {
+// out = x + div F^ / s.
+__global__ void k_divergence(const float* __restrict__ x, const float* __restrict__ F, const float* __restrict__ lam,
+                             Vol v, float inv_s, float* __restrict__ out) {
   const size_t n = (size_t)v.nx * v.ny * v.nz;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
-    out[e] = x[e] + flux_divergence(F, v, e) * inv_s;
+    out[e] = x[e] + limited_divergence(F, lam, v, e) * inv_s;
 }
 
-// The loss: d = s x + div F~ - s t (the scaled output error); g = 2 d / nvox
+// The loss: d = s x + div F^ - s t (the scaled output error); g = 2 d / nvox
 // (its gradient); per-block partial sums of d^2 (float64).
-__global__ void k_loss(const float* __restrict__ x, const float* __restrict__ F, const float* __restrict__ t,
-                       float s, Vol v, float* __restrict__ g, double* __restrict__ partial) {
+__global__ void k_loss(const float* __restrict__ x, const float* __restrict__ F, const float* __restrict__ lam,
+                       const float* __restrict__ t, float s, Vol v, float* __restrict__ g,
+                       double* __restrict__ partial) {
   __shared__ double sh[256];
   double acc = 0;
   const size_t nvox = (size_t)v.nx * v.ny * v.nz;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nvox; e += (size_t)gridDim.x * blockDim.x) {
-    const float d = s * x[e] + flux_divergence(F, v, e) - s * t[e];
+    const float d = s * x[e] + limited_divergence(F, lam, v, e) - s * t[e];
     g[e] = 2.f * d / (float)nvox;
     acc += (double)d * d;
   }
@@ -309,17 +355,54 @@ __global__ void k_loss(const float* __restrict__ x, const float* __restrict__ F,
   if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
 }
 
-// Gradient at the flux from the gradient g at the output (the adjoint of
-// the divergence): G[u][a] = g[u] - g[u + e_a] below the last plane of
-// axis a, 0 on it.
-__global__ void k_div_adjoint(const float* __restrict__ g, Vol v, float* __restrict__ G) {
-  const size_t n = (size_t)v.nx * v.ny * v.nz, sy = v.nx, sz = (size_t)v.nx * v.ny;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(e % v.nx), j = (int)((e / v.nx) % v.ny), k = (int)(e / sz);
-    const float ge = g[e];
-    G[e * 3 + 0] = i < v.nx - 1 ? ge - g[e + 1] : 0.f;
-    G[e * 3 + 1] = j < v.ny - 1 ? ge - g[e + sy] : 0.f;
-    G[e * 3 + 2] = k < v.nz - 1 ? ge - g[e + sz] : 0.f;
+// Backward through the limiter, first pass: T[e] = sum over the faces e
+// donates through of G p, G = g[u] - g[u + e_a] the gradient at the
+// limited flux of face (u, u + e_a).
+__global__ void k_limit_tsum(const float* __restrict__ g, const float* __restrict__ F, Vol v,
+                             float* __restrict__ tsum) {
+  const size_t nvox = (size_t)v.nx * v.ny * v.nz;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nvox; e += (size_t)gridDim.x * blockDim.x) {
+    const Cell q(v, e);
+    float T = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (q.ijk[a] < q.n[a] - 1) {
+        const float p = F[e * 3 + a];
+        if (p < 0.f) T += (g[e] - g[e + q.st[a]]) * p;
+      }
+      if (q.ijk[a] > 0) {
+        const size_t u = e - q.st[a];
+        const float p = F[u * 3 + a];
+        if (p > 0.f) T += (g[u] - g[e]) * p;
+      }
+    }
+    tsum[e] = T;
+  }
+}
+
+// Gradient at the network's flux F (the adjoint of the limited divergence):
+// for face p = F~a[u] with donor d,
+//     dL/dp = lam[d] G - [d limited] (lam[d] / O[d]) sign(p) T[d],
+// d limited when O[d] > c[d] > 0; 0 on the last plane of axis a.
+__global__ void k_div_adjoint(const float* __restrict__ g, const float* __restrict__ F, const float* __restrict__ x,
+                              float s, const float* __restrict__ lam, const float* __restrict__ outflow,
+                              const float* __restrict__ tsum, Vol v, float* __restrict__ G) {
+  const size_t nvox = (size_t)v.nx * v.ny * v.nz;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nvox; e += (size_t)gridDim.x * blockDim.x) {
+    const Cell q(v, e);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      float r = 0.f;
+      if (q.ijk[a] < q.n[a] - 1) {
+        const size_t up = e + q.st[a];
+        const float p = F[e * 3 + a];
+        const size_t d = p > 0.f ? up : e;
+        const float l = lam[d], O = outflow[d], c = s * x[d];
+        r = l * (g[e] - g[up]);
+        if (O > c && c > 0.f && p != 0.f) r -= (l / O) * (p > 0.f ? 1.f : -1.f) * tsum[d];
+      }
+      G[e * 3 + a] = r;
+    }
   }
 }
 
@@ -395,6 +478,9 @@ struct Denoiser {
   float* act[kLayers] = {};     // output of layer l: [vox][kLayerOut[l]]
   float* gbuf[2] = {};          // gradients, [vox][16]
   float* gout = nullptr;        // gradient at the output, [vox]
+  float* lam = nullptr;         // flux limiter of each donor voxel, [vox]
+  float* outflow = nullptr;     // its unlimited outflow, [vox]
+  float* tsum = nullptr;        // limiter backward sums, [vox]
   float* wr = nullptr;          // BF16-rounded weights used by the passes
   float* wt = nullptr;          // flipped/transposed weights of one layer
   float* partial = nullptr;     // [nblocks][27*16*16]
@@ -408,7 +494,7 @@ void dn_free(Denoiser* d) {
   cudaFree(d->flags); cudaFree(d->list); cudaFree(d->count);
   for (auto& a : d->act) cudaFree(a);
   for (auto& g : d->gbuf) cudaFree(g);
-  cudaFree(d->gout);
+  cudaFree(d->gout); cudaFree(d->lam); cudaFree(d->outflow); cudaFree(d->tsum);
   cudaFree(d->wr); cudaFree(d->wt); cudaFree(d->partial); cudaFree(d->lpart); cudaFree(d->loss);
   delete d;
 }
@@ -427,6 +513,9 @@ Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms) {
     for (int l = 0; l < kLayers; ++l) alloc((void**)&d->act[l], nvox * kLayerOut[l] * 4);
     for (auto& g : d->gbuf) alloc((void**)&g, nvox * 16 * 4);
     alloc((void**)&d->gout, nvox * 4);
+    alloc((void**)&d->lam, nvox * 4);
+    alloc((void**)&d->outflow, nvox * 4);
+    alloc((void**)&d->tsum, nvox * 4);
     alloc((void**)&d->wr, kDnWeights * 4);
     alloc((void**)&d->wt, 27 * 16 * 16 * 4);
     alloc((void**)&d->partial, (size_t)d->nblocks * 27 * 16 * 16 * 4);
@@ -492,11 +581,11 @@ void wgrad(Denoiser& d, int cin, int cout, const float* x, const float* g, float
 
 }  // namespace
 
-constexpr int kForwardLaunches = 3 + kLayers;  // kernels dn_forward launches
+constexpr int kForwardLaunches = 4 + kLayers;  // kernels dn_forward launches
 
-// Active tiles of input x, BF16 rounding of the weights, and the forward
-// pass: act[3] = F = f(s x) (three channels); act[l] zeroed outside active
-// tiles.
+// Active tiles of input x, BF16 rounding of the weights, the forward pass
+// (act[3] = F = f(s x), three channels; act[l] zeroed outside active tiles)
+// and the flux limiter.
 void dn_forward(Denoiser& d, const float* x, float s, const float* w_master, cudaStream_t st) {
   const size_t ntiles = (size_t)d.v.tx * d.v.ty * d.v.tz, nvox = (size_t)d.v.nx * d.v.ny * d.v.nz;
   k_tile_flags<<<(unsigned)ntiles, 256, 0, st>>>(x, d.v, d.flags);
@@ -511,6 +600,9 @@ void dn_forward(Denoiser& d, const float* x, float s, const float* w_master, cud
     conv(d, kLayerIn[l], kLayerOut[l], l == 0 ? x : d.act[l - 1], d.wr + layer_offset(l), d.act[l], l < 3, nullptr,
          l == 0 ? s : 1.f, st);
   }
+  k_flux_limit<<<(unsigned)std::min<size_t>((nvox + 255) / 256, 65535), 256, 0, st>>>(d.act[3], x, s, d.v, d.lam,
+                                                                                       d.outflow);
+  VLB_CUDA(cudaGetLastError());
 }
 
 // Loss against target t (same scale s) and the gradient of the master
@@ -518,11 +610,13 @@ void dn_forward(Denoiser& d, const float* x, float s, const float* w_master, cud
 void dn_backward(Denoiser& d, const float* x, const float* t, float s, float* gw, cudaStream_t st) {
   const size_t nvox = (size_t)d.v.nx * d.v.ny * d.v.nz;
   const int lb = 1024;
-  k_loss<<<lb, 256, 0, st>>>(x, d.act[3], t, s, d.v, d.gout, d.lpart);
+  k_loss<<<lb, 256, 0, st>>>(x, d.act[3], d.lam, t, s, d.v, d.gout, d.lpart);
   VLB_CUDA(cudaGetLastError());
   k_sum_double<<<1, 256, 0, st>>>(d.lpart, lb, d.loss, 1.0 / (double)nvox);
   VLB_CUDA(cudaGetLastError());
-  k_div_adjoint<<<lb, 256, 0, st>>>(d.gout, d.v, d.gbuf[0]);
+  k_limit_tsum<<<lb, 256, 0, st>>>(d.gout, d.act[3], d.v, d.tsum);
+  VLB_CUDA(cudaGetLastError());
+  k_div_adjoint<<<lb, 256, 0, st>>>(d.gout, d.act[3], x, s, d.lam, d.outflow, d.tsum, d.v, d.gbuf[0]);
   VLB_CUDA(cudaGetLastError());
   int cur = 0;  // gbuf[cur]: gradient at the output of layer l
   for (int l = kLayers - 1; l >= 0; --l) {
@@ -583,7 +677,7 @@ void launch_denoise(Ctx& c, int64_t npart_global) {
   Denoiser& d = *c.dn;
   dn_forward(d, F.rho, (float)c.dn_scale, c.dn_weights, c.stream);
   c.launches += kForwardLaunches;
-  k_divergence<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(F.rho, dn_output(d), d.v,
+  k_divergence<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(F.rho, dn_output(d), d.lam, d.v,
                                                                          (float)(1.0 / c.dn_scale), c.dn_pred);
   VLB_LAUNCHED(c);
   launch_grid_charge(c, F, c.dn_pred, &c.dsc->xch[1]);
@@ -667,8 +761,8 @@ int vlb_dn_forward(vlb_denoiser* h, const float* x, float scale, const float* we
     VLB_CUDA(cudaSetDevice(d.device));
     dn_forward(d, x, scale, weights, s);
     const size_t n = (size_t)d.v.nx * d.v.ny * d.v.nz;
-    k_divergence<<<(unsigned)std::min<size_t>((n + 255) / 256, 65535), 256, 0, s>>>(x, dn_output(d), d.v, 1.f / scale,
-                                                                                      out);
+    k_divergence<<<(unsigned)std::min<size_t>((n + 255) / 256, 65535), 256, 0, s>>>(x, dn_output(d), d.lam, d.v,
+                                                                                      1.f / scale, out);
     VLB_CUDA(cudaGetLastError());
     return VLB_OK;
   });

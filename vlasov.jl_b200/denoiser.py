@@ -47,9 +47,9 @@ CHARGE_TOLERANCE = 1e-3                                  # electrons
 DEFAULT_WEIGHTS = Path(__file__).resolve().parent / "data" / "denoiser_xe25_130.npz"
 
 
-def init_weights(seed: int = 0, flux_gain: float = 0.05) -> np.ndarray:
-    """He-normal weights (fan-in 27 cin), the flux layer scaled down so that
-    the untrained network starts near the identity."""
+def init_weights(seed: int = 0, flux_gain: float = 0.0) -> np.ndarray:
+    """He-normal weights (fan-in 27 cin), the flux layer scaled by
+    `flux_gain`: at 0 the untrained network is the identity (no flux)."""
     rng = np.random.default_rng(seed)
     parts = []
     for l, (a, b) in enumerate(LAYERS):
@@ -195,13 +195,15 @@ def input_scale(x) -> float:
 
 
 # ------------------------------------------------------------ training
-def train(inputs, targets, *, steps: int = 3000, batch: int = 4, lr: float = 2e-3, seed: int = 0,
-          scale: float | None = None, log_every: int = 100, weights=None, log=print,
-          time_limit: float | None = None):
+def train(inputs, targets, *, steps: int = 3000, batch: int = 4, lr: float = 1e-3, warmup: int = 100,
+          seed: int = 0, scale: float | None = None, log_every: int = 100, weights=None, log=print,
+          time_limit: float | None = None, val_inputs=None, val_targets=None):
     """Adam on the mean squared error of the network's density against the
-    targets, pairs drawn at random, cosine learning-rate decay; on the GPU
-    with vlb_dn_gradient / vlb_dn_adam.  Stops early after `time_limit`
-    seconds.  Returns (weights, scale, history)."""
+    targets, pairs drawn at random, linear warm-up then cosine decay of the
+    learning rate; on the GPU with vlb_dn_gradient / vlb_dn_adam.  With a
+    validation set, the weights of the lowest validation loss (checked every
+    `log_every` steps) are returned.  Stops early after `time_limit` seconds.
+    Returns (weights, scale, history of (step, train loss, val loss, s))."""
     import torch
     dev = inputs.device
     scale = input_scale(inputs) if scale is None else scale
@@ -211,6 +213,14 @@ def train(inputs, targets, *, steps: int = 3000, batch: int = 4, lr: float = 2e-
     m, v, g, gs = (torch.zeros_like(w) for _ in range(4))
     rng = np.random.default_rng(seed)
     hist = []
+    best = (math.inf, w.clone())
+
+    def val_loss():
+        if val_inputs is None:
+            return float("nan")
+        return float(np.mean([net.gradient(x, t, w, scale, g, want_loss=True)
+                              for x, t in zip(val_inputs, val_targets)]))
+
     t0 = time.perf_counter()
     try:
         for it in range(1, steps + 1):
@@ -222,20 +232,26 @@ def train(inputs, targets, *, steps: int = 3000, batch: int = 4, lr: float = 2e-
                 losses.append(net.gradient(inputs[p], targets[p], w, scale, g, want_loss=want))
                 gs.add_(g)
             gs.div_(batch)
-            lr_t = lr * 0.5 * (1.0 + math.cos(math.pi * (it - 1) / steps))
+            ramp = min(1.0, it / warmup) if warmup > 0 else 1.0
+            lr_t = lr * ramp * 0.5 * (1.0 + math.cos(math.pi * (it - 1) / steps))
             net.adam(w, gs, m, v, lr_t, it)
-            if want:
-                hist.append((it, float(np.mean(losses)), time.perf_counter() - t0))
+            if want or it == steps:
+                vl = val_loss()
+                if vl < best[0]:
+                    best = (vl, w.clone())
+                hist.append((it, float(np.nanmean([x for x in losses if x is not None] or [np.nan])), vl,
+                             time.perf_counter() - t0))
                 if log:
-                    log(f"step {it:5d}  loss {hist[-1][1]:.4e}  lr {lr_t:.2e}  {hist[-1][2]:.1f} s")
-                if time_limit is not None and hist[-1][2] > time_limit:
+                    log(f"step {it:5d}  loss {hist[-1][1]:.4e}  val {vl:.4e}  lr {lr_t:.2e}  {hist[-1][3]:.1f} s")
+                if time_limit is not None and hist[-1][3] > time_limit:
                     if log:
                         log(f"stopped at step {it}: time limit")
                     break
         torch.cuda.synchronize(dev)
     finally:
         net.close()
-    return w.cpu().numpy(), scale, hist
+    wf = best[1] if val_inputs is not None and math.isfinite(best[0]) else w
+    return wf.cpu().numpy(), scale, hist
 
 
 def errors(inputs, targets, weights, scale: float):
@@ -286,7 +302,7 @@ def main(argv=None):
     ap.add_argument("--high", type=int, default=HIGH)
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=4)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--time-limit", type=float, default=None, help="seconds of training at most")
     ap.add_argument("--weights", default=None, help="saved network (evaluate)")
     ap.add_argument("--out", default=None, help="where train saves the network")
@@ -298,12 +314,18 @@ def main(argv=None):
     out = {"command": a.command}
     if a.command == "train":
         xs, ts = _collect_pairs(TRAIN_IMPACTS, a.steps, a.every, a.low, a.high, a.device, log)
-        w, scale, hist = train(xs, ts, steps=a.train_steps, batch=a.batch, lr=a.lr, log=log,
-                               time_limit=a.time_limit)
-        plain, learned = errors(xs, ts, w, scale)
+        # every 8th pair is kept aside for validation
+        import torch
+        val = torch.arange(len(xs), device=xs.device) % 8 == 7
+        w, scale, hist = train(xs[~val], ts[~val], steps=a.train_steps, batch=a.batch, lr=a.lr, log=log,
+                               time_limit=a.time_limit, val_inputs=xs[val], val_targets=ts[val])
+        plain, learned = errors(xs[~val], ts[~val], w, scale)
+        vplain, vlearned = errors(xs[val], ts[val], w, scale)
         out.update(pairs=len(xs), scale=scale, history=hist, train_err_plain=float(plain.mean()),
-                   train_err_learned=float(learned.mean()))
-        log(f"training pairs: relative L2 error {plain.mean():.4f} plain, {learned.mean():.4f} denoised")
+                   train_err_learned=float(learned.mean()), val_err_plain=float(vplain.mean()),
+                   val_err_learned=float(vlearned.mean()))
+        log(f"training pairs: relative L2 error {plain.mean():.4f} plain, {learned.mean():.4f} denoised; "
+            f"validation {vplain.mean():.4f} plain, {vlearned.mean():.4f} denoised")
         if a.out:
             save_weights(a.out, w, scale, {"impacts": TRAIN_IMPACTS, "low": a.low, "high": a.high,
                                            "data_steps": a.steps, "every": a.every, "train_steps": a.train_steps,
