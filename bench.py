@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-learned", action="store_true", help="skip the step with the learned denoiser")
     return ap.parse_args()
 
 
@@ -187,7 +188,7 @@ def run_reference(args):
     for _ in range(args.steps):
         pos, prev, _ = st.step(pos, prev)
     ms = (time.perf_counter() - t0) / args.steps * 1e3
-    line = {"metric": "ms/step at 8M particles, 130^3 grid", "value": ms, "unit": "ms/step", "n_gpus": args.gpus,
+    line = {"metric": "ms/step at 8M particles, 130^3 grid; learned vs plain at equal capture error", "value": ms, "unit": "ms/step", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ran2 Thomas-Fermi cloud)",
             "config": config_dict(args, 1), "impl": "reference",
@@ -299,6 +300,26 @@ def main():
     step_h2d = 112  # vlb_projectile in
     step_d2h = 480  # the step's scalar block out
 
+    # the same steps with the learned denoiser after the fine deposit
+    learned = None
+    if world == 1 and not args.no_learned and args.nfine == 64:
+        w_dn, s_dn, meta_dn = vb.denoiser.load_weights()
+        vb.denoiser.attach(sim, w_dn, s_dn)
+        for _ in range(max(args.warmup, 3)):
+            sim.step()
+        used = 0
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(ext)
+        for _ in range(args.steps):
+            used += sim.step().denoised
+        g1.record(ext)
+        g1.synchronize()
+        learned_ms = g0.elapsed_time(g1) / args.steps
+        vb.denoiser.detach(sim)
+        learned = {"ms_per_step": learned_ms, "vs_plain": learned_ms / ms, "denoised_steps": used,
+                   "steps": args.steps, "network": "vlasov.jl_b200/data/denoiser_xe25_130.npz",
+                   "trained_on": meta_dn}
+
     pk_, how = peaks()
     fp32_peak = vb._lib.C.c_double()
     L.check(L.lib().vlb_fp32_peak(local, vb._lib.C.byref(fp32_peak)))
@@ -321,7 +342,7 @@ def main():
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "ms/step", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
     line = {
-        "metric": "ms/step at 8M particles, 130^3 grid", "value": ms, "unit": "ms/step", "n_gpus": world,
+        "metric": "ms/step at 8M particles, 130^3 grid; learned vs plain at equal capture error", "value": ms, "unit": "ms/step", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded ran2 sample of the reference's Na196 Thomas-Fermi profile)",
@@ -342,6 +363,8 @@ def main():
         "clocks": clk,
         "last_step": {"q8": d.enclosed_charge, "outcount": d.outcount, "noccupied": d.noccupied},
     }
+    if learned:
+        line["learned"] = learned
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)

@@ -304,7 +304,9 @@ VLB_API int vlb_dn_gradient(vlb_denoiser* dn, const float* x, const float* targe
                     const float* weights, float* grad, double* loss, void* stream);
 VLB_API int vlb_dn_adam(vlb_denoiser* dn, float* weights, const float* grad, float* m, float* v, float lr,
                 int32_t step, void* stream);
-/* tiles of 8^3 voxels the last pass computed (the others are empty) */
+/* tiles of 8^3 voxels the last pass computed: those within one tile of a
+ * tile whose largest |x| exceeds 1e-3 of the volume's (the others pass
+ * through unchanged) */
 VLB_API int vlb_dn_active_tiles(vlb_denoiser* dn, int32_t* n);
 
 /* ---- launch shapes.  No counterpart in the reference (whose kernels take

@@ -22,6 +22,11 @@ input at (i + da - 1, j + db - 1, k + dc - 1).  The passes use the weights
 rounded to BF16 (nearest, ties to even); the gradient of the master weights is
 the gradient with respect to the rounded ones (straight-through).
 
+The network is evaluated on the active tiles of 8^3 voxels: a tile is
+flagged when its largest |x| exceeds TILE_THRESHOLD times the volume's, the
+active tiles are the flagged ones and their neighbours, and every layer's
+activations (the input included) are zero outside them.
+
 Volumes are numpy arrays of shape (nz, ny, nx) (x fastest, as the grids).
 """
 from __future__ import annotations
@@ -29,6 +34,8 @@ from __future__ import annotations
 import numpy as np
 
 LAYERS = ((1, 16), (16, 16), (16, 16), (16, 3))
+TILE = 8
+TILE_THRESHOLD = np.float32(1e-3)
 WEIGHT_COUNT = sum(27 * a * b for a, b in LAYERS)  # 15,552
 
 
@@ -176,10 +183,11 @@ def forward(x, weights, scale, rounding=True, details=False):
     `details`).  rounding=False uses the weights as given (float64), for
     finite differences."""
     ws = split(bf16_round(weights) if rounding else weights)
+    M = voxel_mask(x)[..., None]
     x = np.asarray(x, dtype=np.float64)
-    a = [scale * x[..., None]]
+    a = [scale * x[..., None] * M]
     for l, w in enumerate(ws):
-        z = conv(a[-1], w)
+        z = conv(a[-1], w) * M
         a.append(np.maximum(z, 0.0) if l < 3 else z)
     Ft = face_flux(a[-1])
     lam, O = limiter(Ft, scale * x)
@@ -197,6 +205,7 @@ def loss_and_grad(x, target, weights, scale, rounding=True):
     loss = float(np.sum(d * d) / nvox)
     G = divergence_adjoint(2.0 * d / nvox)
     g = face_flux(limited_flux_adjoint(G, Ft, lam, O, scale * np.asarray(x, dtype=np.float64)))
+    g = g * voxel_mask(x)[..., None]
     grads = [None] * 4
     for l in range(3, -1, -1):
         grads[l] = conv_weight_grad(a[l], g)
@@ -213,19 +222,35 @@ def adam(w, g, m, v, lr, step, b1=0.9, b2=0.999, eps=1e-8):
     return w, m, v
 
 
-def active_tiles(x, tile=8):
-    """Tiles of `tile`^3 voxels within one tile of a tile holding a nonzero input."""
-    nz, ny, nx = x.shape
+def active_map(x, tile=TILE, threshold=TILE_THRESHOLD):
+    """Boolean map of the active tiles (tz, ty, tx)."""
+    ax = np.abs(np.asarray(x, dtype=np.float32))
+    nz, ny, nx = ax.shape
     tz, ty, tx = -(-nz // tile), -(-ny // tile), -(-nx // tile)
-    flags = np.zeros((tz, ty, tx), dtype=bool)
+    tmax = np.zeros((tz, ty, tx), dtype=np.float32)
     for c in range(tz):
         for b in range(ty):
             for a in range(tx):
-                flags[c, b, a] = np.any(x[c * tile:(c + 1) * tile, b * tile:(b + 1) * tile, a * tile:(a + 1) * tile])
+                blk = ax[c * tile:(c + 1) * tile, b * tile:(b + 1) * tile, a * tile:(a + 1) * tile]
+                tmax[c, b, a] = blk.max() if blk.size else 0.0
+    tau = np.float32(threshold) * tmax.max()
+    flags = (tmax > tau) & (tmax > 0)
     p = np.pad(flags, 1)
     on = np.zeros_like(flags)
     for dc in range(3):
         for db in range(3):
             for da in range(3):
                 on |= p[dc:dc + tz, db:db + ty, da:da + tx]
-    return int(on.sum())
+    return on
+
+
+def voxel_mask(x, tile=TILE, threshold=TILE_THRESHOLD):
+    on = active_map(x, tile, threshold)
+    nz, ny, nx = np.shape(x)
+    m = np.repeat(np.repeat(np.repeat(on, tile, 0), tile, 1), tile, 2)
+    return m[:nz, :ny, :nx]
+
+
+def active_tiles(x, tile=TILE, threshold=TILE_THRESHOLD):
+    """Number of active tiles."""
+    return int(active_map(x, tile, threshold).sum())

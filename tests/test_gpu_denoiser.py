@@ -63,6 +63,25 @@ def test_forward_matches_oracle(cuda_device):
         net.close()
 
 
+def test_faint_tiles_match_oracle(cuda_device):
+    """Specks below and above the tile threshold, far from the blob."""
+    rng = np.random.default_rng(21)
+    x, t = _blob_volume(rng)
+    x[17, 22, 44] = 1e-5 * x.max()
+    x[2, 24, 40] = 3e-2 * x.max()
+    w = DN.init_weights(3, flux_gain=0.5)
+    net = DN.Network(x.shape)
+    try:
+        xt, wt = _tensors(x, w)
+        out = net.forward(xt, wt, 250.0).cpu().numpy()
+        _, ref = D.forward(x, w, 250.0)
+        assert np.max(np.abs(out - ref)) <= 2e-5 * np.max(np.abs(ref))
+        assert out[17, 22, 44] == x[17, 22, 44] and out[2, 24, 40] != x[2, 24, 40]
+        assert net.active_tiles() == D.active_tiles(x)
+    finally:
+        net.close()
+
+
 def test_gradient_matches_oracle(cuda_device):
     import torch
     rng = np.random.default_rng(2)

@@ -102,3 +102,18 @@ def test_committed_network_loads():
     x[4:12, 4:12, 4:12] = rng.poisson(30.0, (8, 8, 8)) / (30.0 * scale)
     _, out = D.forward(x, w, scale)
     assert np.min(out) >= -1e-12 and abs(out.sum() - x.sum()) < 1e-9 * x.sum()
+
+
+def test_faint_tiles_pass_through():
+    """A speck below the tile threshold (1e-3 of the peak) is left as it is;
+    one above it is denoised like the rest."""
+    rng = np.random.default_rng(19)
+    x, _, w = _case(rng, (24, 24, 40))
+    w[-27 * 16 * 3:] *= 4.0
+    x[20, 20, 35] = 1e-5 * x.max()
+    _, out = D.forward(x, w, 2.0)
+    assert out[20, 20, 35] == x[20, 20, 35] and np.all(out[16:, 16:, 32:][x[16:, 16:, 32:] == 0] == 0)
+    assert D.active_tiles(x) == D.active_tiles(np.where(x > 1e-5, x, 0))
+    x[20, 20, 35] = 1e-2 * x.max()
+    _, out = D.forward(x, w, 2.0)
+    assert out[20, 20, 35] != x[20, 20, 35]

@@ -20,10 +20,14 @@
 // and sum is float32.
 //
 // Activations are channel-last float32 ([z][y][x][c], i fastest as the
-// grids).  The volume is cut into 8^3 tiles; a tile whose input within four
-// voxels (the network's reach) is zero has zero activations at every layer
-// and is skipped, forward and backward alike -- exactly, not as an
-// approximation.
+// grids).  The volume is cut into 8^3 tiles.  A tile is flagged when its
+// largest |rho| exceeds kTileThreshold times the volume's; the active tiles
+// are the flagged ones and their neighbours, and the network is defined on
+// them: every layer's activations (its input included) are zero outside the
+// active tiles.  With the threshold at zero this is exact (the network's
+// reach, four voxels, is less than a tile); above it, the faint density of a
+// few escaped electrons (a pseudo-particle deposits ~1e-8 against a peak of
+// ~4e-3) passes through unchanged instead of filling the grid with tiles.
 //
 //   k_conv<CIN, COUT>     one layer (also the input-gradient pass, with the
 //                         weights flipped and transposed), 256 threads per
@@ -54,6 +58,7 @@ constexpr int kConvThreads = 256;      // two voxels per thread
 constexpr int kLayers = 4;
 constexpr int kLayerIn[kLayers] = {1, 16, 16, 16};
 constexpr int kLayerOut[kLayers] = {16, 16, 16, 3};
+constexpr float kTileThreshold = 1e-3f;   // of the volume's largest |rho|
 
 __host__ __device__ constexpr int pad_stride(int c) { return c == 16 ? 20 : c; }  // float stride per halo voxel
 
@@ -69,25 +74,46 @@ __device__ __forceinline__ void tile_origin(const Vol& v, int tile, int& x0, int
 }
 
 // ---------------------------------------------------------------- tiles
-// flags[t] = 1 if tile t holds a nonzero input voxel.
-__global__ void k_tile_flags(const float* __restrict__ x, Vol v, int32_t* __restrict__ flags) {
+// tmax[t] = the largest |x| in tile t.
+__global__ void k_tile_max(const float* __restrict__ x, Vol v, float* __restrict__ tmax) {
+  __shared__ float sh[256];
   const int tile = blockIdx.x;
   int x0, y0, z0;
   tile_origin(v, tile, x0, y0, z0);
-  int any = 0;
+  float m = 0.f;
   for (int e = threadIdx.x; e < kT * kT * kT; e += blockDim.x) {
     const int i = x0 + e % kT, j = y0 + (e / kT) % kT, k = z0 + e / (kT * kT);
-    if (i < v.nx && j < v.ny && k < v.nz && x[(size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)] != 0.f) any = 1;
+    if (i < v.nx && j < v.ny && k < v.nz) m = fmaxf(m, fabsf(x[(size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)]));
   }
-  any = __syncthreads_or(any);
-  if (threadIdx.x == 0) flags[tile] = any;
+  sh[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = fmaxf(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) tmax[tile] = sh[0];
 }
 
-// Active tiles: a flagged tile or a neighbour of one (the reach, four
-// voxels, is less than a tile), compacted in tile order.
-__global__ void k_tile_active(const int32_t* __restrict__ flags, Vol v, int32_t* __restrict__ list,
-                              int32_t* __restrict__ count) {
+// gmax = the largest tmax (one block).
+__global__ void k_volume_max(const float* __restrict__ tmax, int ntiles, float* __restrict__ gmax) {
+  __shared__ float sh[1024];
+  float m = 0.f;
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) m = fmaxf(m, tmax[t]);
+  sh[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] = fmaxf(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *gmax = sh[0];
+}
+
+// Active tiles: a flagged tile (tmax > kTileThreshold gmax, and > 0) or a
+// neighbour of one; amap[t] = 1 for them, compacted into `list`.
+__global__ void k_tile_active(const float* __restrict__ tmax, const float* __restrict__ gmax, Vol v,
+                              int32_t* __restrict__ amap, int32_t* __restrict__ list, int32_t* __restrict__ count) {
   const int ntiles = v.tx * v.ty * v.tz;
+  const float tau = kTileThreshold * *gmax;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
     const int a = t % v.tx, b = (t / v.tx) % v.ty, c = t / (v.tx * v.ty);
     int on = 0;
@@ -96,21 +122,31 @@ __global__ void k_tile_active(const int32_t* __restrict__ flags, Vol v, int32_t*
         for (int da = -1; da <= 1 && !on; ++da) {
           const int aa = a + da, bb = b + db, cc = c + dc;
           if (aa < 0 || bb < 0 || cc < 0 || aa >= v.tx || bb >= v.ty || cc >= v.tz) continue;
-          on = flags[aa + v.tx * (bb + v.ty * cc)];
+          const float m = tmax[aa + v.tx * (bb + v.ty * cc)];
+          on = m > tau && m > 0.f;
         }
+    amap[t] = on;
     if (on) list[atomicAdd(count, 1)] = t;
   }
 }
 
+// Is voxel (i, j, k) inside the volume and in an active tile?
+__device__ __forceinline__ bool live(const Vol& v, const int32_t* __restrict__ amap, int i, int j, int k) {
+  return i >= 0 && j >= 0 && k >= 0 && i < v.nx && j < v.ny && k < v.nz &&
+         amap[i / kT + v.tx * (j / kT + v.ty * (k / kT))];
+}
+
 // -------------------------------------------------------------- the conv
 // y[v][co] = sum_tap sum_ci w[tap][ci][co] * scale_in * x[v + tap - 1][ci]
-// (zero outside the volume), then y = max(y, 0) when `relu`, and y = 0 where
-// mask[v][co] <= 0 when `mask` is given (the input-gradient pass through a
-// ReLU).  Tiles not in `list` are left as they are (the caller zeroes them).
+// (zero outside the volume and outside the active tiles), then
+// y = max(y, 0) when `relu`, and y = 0 where mask[v][co] <= 0 when `mask` is
+// given (the input-gradient pass through a ReLU).  Only the tiles in `list`
+// are written; the others are never read.
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kConvThreads) k_conv(const float* __restrict__ x, const float* __restrict__ w,
                                                        float* __restrict__ y, Vol v, const int32_t* __restrict__ list,
-                                                       const int32_t* __restrict__ count, int relu,
+                                                       const int32_t* __restrict__ count,
+                                                       const int32_t* __restrict__ amap, int relu,
                                                        const float* __restrict__ mask, float scale_in) {
   constexpr int PS = pad_stride(CIN);
   extern __shared__ __align__(16) float sm[];
@@ -126,8 +162,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const float* __restrict__
       const int ci = e % CIN, hv = e / CIN;
       const int i = x0 - 1 + hv % kH, j = y0 - 1 + (hv / kH) % kH, k = z0 - 1 + hv / (kH * kH);
       float val = 0.f;
-      if (i >= 0 && j >= 0 && k >= 0 && i < v.nx && j < v.ny && k < v.nz)
-        val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
+      if (live(v, amap, i, j, k)) val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
       xs[hv * PS + ci] = val;
     }
     __syncthreads();
@@ -202,6 +237,7 @@ template <int CIN, int COUT>
 __global__ void __launch_bounds__(kConvThreads) k_conv_wgrad(const float* __restrict__ x, const float* __restrict__ g,
                                                              Vol v, const int32_t* __restrict__ list,
                                                              const int32_t* __restrict__ count,
+                                                             const int32_t* __restrict__ amap,
                                                              float* __restrict__ partial, float scale_in) {
   constexpr int PS = pad_stride(CIN);
   constexpr int NP = 27 * CIN;           // (tap, ci) pairs
@@ -223,8 +259,7 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_wgrad(const float* __rest
       const int ci = e % CIN, hv = e / CIN;
       const int i = x0 - 1 + hv % kH, j = y0 - 1 + (hv / kH) % kH, k = z0 - 1 + hv / (kH * kH);
       float val = 0.f;
-      if (i >= 0 && j >= 0 && k >= 0 && i < v.nx && j < v.ny && k < v.nz)
-        val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
+      if (live(v, amap, i, j, k)) val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
       xs[hv * PS + ci] = val;
     }
     for (int e = threadIdx.x; e < kT * kT * kT * COUT; e += kConvThreads) {
@@ -472,7 +507,9 @@ struct Denoiser {
   Vol v{};
   int device = 0;
   int nblocks = 0;              // CTAs of the conv grids (persistent over tiles)
-  int32_t* flags = nullptr;     // [tiles]
+  float* tmax = nullptr;        // [tiles] largest |input| of each tile
+  float* gmax = nullptr;        // [1] of the volume
+  int32_t* amap = nullptr;      // [tiles] 1: active
   int32_t* list = nullptr;      // [tiles]
   int32_t* count = nullptr;     // [1]
   float* act[kLayers] = {};     // output of layer l: [vox][kLayerOut[l]]
@@ -491,7 +528,7 @@ struct Denoiser {
 void dn_free(Denoiser* d) {
   if (!d) return;
   cudaSetDevice(d->device);
-  cudaFree(d->flags); cudaFree(d->list); cudaFree(d->count);
+  cudaFree(d->tmax); cudaFree(d->gmax); cudaFree(d->amap); cudaFree(d->list); cudaFree(d->count);
   for (auto& a : d->act) cudaFree(a);
   for (auto& g : d->gbuf) cudaFree(g);
   cudaFree(d->gout); cudaFree(d->lam); cudaFree(d->outflow); cudaFree(d->tsum);
@@ -507,7 +544,9 @@ Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms) {
   d->nblocks = num_sms * 2;
   auto alloc = [](void** p, size_t bytes) { VLB_CUDA(cudaMalloc(p, std::max<size_t>(bytes, 16))); };
   try {
-    alloc((void**)&d->flags, ntiles * 4);
+    alloc((void**)&d->tmax, ntiles * 4);
+    alloc((void**)&d->gmax, 4);
+    alloc((void**)&d->amap, ntiles * 4);
     alloc((void**)&d->list, ntiles * 4);
     alloc((void**)&d->count, 4);
     for (int l = 0; l < kLayers; ++l) alloc((void**)&d->act[l], nvox * kLayerOut[l] * 4);
@@ -548,13 +587,13 @@ void conv(Denoiser& d, int cin, int cout, const float* x, const float* w, float*
           float scale_in, cudaStream_t s) {
   const int g = d.nblocks;
   if (cin == 1 && cout == 16)
-    k_conv<1, 16><<<g, kConvThreads, conv_smem<1, 16>(), s>>>(x, w, y, d.v, d.list, d.count, relu, mask, scale_in);
+    k_conv<1, 16><<<g, kConvThreads, conv_smem<1, 16>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
   else if (cin == 16 && cout == 16)
-    k_conv<16, 16><<<g, kConvThreads, conv_smem<16, 16>(), s>>>(x, w, y, d.v, d.list, d.count, relu, mask, scale_in);
+    k_conv<16, 16><<<g, kConvThreads, conv_smem<16, 16>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
   else if (cin == 16 && cout == 3)
-    k_conv<16, 3><<<g, kConvThreads, conv_smem<16, 3>(), s>>>(x, w, y, d.v, d.list, d.count, relu, mask, scale_in);
+    k_conv<16, 3><<<g, kConvThreads, conv_smem<16, 3>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
   else if (cin == 3 && cout == 16)
-    k_conv<3, 16><<<g, kConvThreads, conv_smem<3, 16>(), s>>>(x, w, y, d.v, d.list, d.count, relu, mask, scale_in);
+    k_conv<3, 16><<<g, kConvThreads, conv_smem<3, 16>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
   else
     throw ArgError("unsupported conv shape");
   VLB_CUDA(cudaGetLastError());
@@ -564,13 +603,13 @@ void wgrad(Denoiser& d, int cin, int cout, const float* x, const float* g, float
            cudaStream_t s) {
   const int nb = d.nblocks, m = 27 * cin * cout;
   if (cin == 1 && cout == 16)
-    k_conv_wgrad<1, 16><<<nb, kConvThreads, wgrad_smem<1, 16>(), s>>>(x, g, d.v, d.list, d.count, d.partial,
+    k_conv_wgrad<1, 16><<<nb, kConvThreads, wgrad_smem<1, 16>(), s>>>(x, g, d.v, d.list, d.count, d.amap, d.partial,
                                                                        scale_in);
   else if (cin == 16 && cout == 16)
-    k_conv_wgrad<16, 16><<<nb, kConvThreads, wgrad_smem<16, 16>(), s>>>(x, g, d.v, d.list, d.count, d.partial,
+    k_conv_wgrad<16, 16><<<nb, kConvThreads, wgrad_smem<16, 16>(), s>>>(x, g, d.v, d.list, d.count, d.amap, d.partial,
                                                                          scale_in);
   else if (cin == 16 && cout == 3)
-    k_conv_wgrad<16, 3><<<nb, kConvThreads, wgrad_smem<16, 3>(), s>>>(x, g, d.v, d.list, d.count, d.partial,
+    k_conv_wgrad<16, 3><<<nb, kConvThreads, wgrad_smem<16, 3>(), s>>>(x, g, d.v, d.list, d.count, d.amap, d.partial,
                                                                        scale_in);
   else
     throw ArgError("unsupported conv shape");
@@ -581,22 +620,24 @@ void wgrad(Denoiser& d, int cin, int cout, const float* x, const float* g, float
 
 }  // namespace
 
-constexpr int kForwardLaunches = 4 + kLayers;  // kernels dn_forward launches
+constexpr int kForwardLaunches = 5 + kLayers;  // kernels dn_forward launches
 
 // Active tiles of input x, BF16 rounding of the weights, the forward pass
-// (act[3] = F = f(s x), three channels; act[l] zeroed outside active tiles)
-// and the flux limiter.
+// (act[3] = F = f(s x), three channels, zero outside the active tiles;
+// act[0..2] written on the active tiles only) and the flux limiter.
 void dn_forward(Denoiser& d, const float* x, float s, const float* w_master, cudaStream_t st) {
   const size_t ntiles = (size_t)d.v.tx * d.v.ty * d.v.tz, nvox = (size_t)d.v.nx * d.v.ny * d.v.nz;
-  k_tile_flags<<<(unsigned)ntiles, 256, 0, st>>>(x, d.v, d.flags);
+  k_tile_max<<<(unsigned)ntiles, 256, 0, st>>>(x, d.v, d.tmax);
+  VLB_CUDA(cudaGetLastError());
+  k_volume_max<<<1, 1024, 0, st>>>(d.tmax, (int)ntiles, d.gmax);
   VLB_CUDA(cudaGetLastError());
   VLB_CUDA(cudaMemsetAsync(d.count, 0, 4, st));
-  k_tile_active<<<(unsigned)((ntiles + 255) / 256), 256, 0, st>>>(d.flags, d.v, d.list, d.count);
+  k_tile_active<<<(unsigned)((ntiles + 255) / 256), 256, 0, st>>>(d.tmax, d.gmax, d.v, d.amap, d.list, d.count);
   VLB_CUDA(cudaGetLastError());
   k_bf16_round<<<(kDnWeights + 255) / 256, 256, 0, st>>>(w_master, d.wr, kDnWeights);
   VLB_CUDA(cudaGetLastError());
   for (int l = 0; l < kLayers; ++l) {
-    VLB_CUDA(cudaMemsetAsync(d.act[l], 0, nvox * kLayerOut[l] * 4, st));
+    if (l == kLayers - 1) VLB_CUDA(cudaMemsetAsync(d.act[l], 0, nvox * kLayerOut[l] * 4, st));  // the flux, read everywhere
     conv(d, kLayerIn[l], kLayerOut[l], l == 0 ? x : d.act[l - 1], d.wr + layer_offset(l), d.act[l], l < 3, nullptr,
          l == 0 ? s : 1.f, st);
   }
@@ -627,7 +668,6 @@ void dn_backward(Denoiser& d, const float* x, const float* t, float s, float* gw
     // gradient at the input of layer l = conv^T(g) masked by the ReLU of layer l-1
     k_flip_weights<<<(27 * cin * cout + 255) / 256, 256, 0, st>>>(d.wr + layer_offset(l), d.wt, cin, cout);
     VLB_CUDA(cudaGetLastError());
-    VLB_CUDA(cudaMemsetAsync(d.gbuf[cur ^ 1], 0, nvox * cin * 4, st));
     conv(d, cout, cin, d.gbuf[cur], d.wt, d.gbuf[cur ^ 1], false, d.act[l - 1], 1.f, st);
     cur ^= 1;
   }

@@ -25,6 +25,7 @@ it is, deposit_smoothed! at src/accelerator.jl:531).
 
     python -c 'import __graft_entry__ as g; g.load().denoiser.main()' train --out weights.npz
     python -c 'import __graft_entry__ as g; g.load().denoiser.main()' evaluate --weights weights.npz
+    python -c 'import __graft_entry__ as g; g.load().denoiser.main()' profile
 """
 from __future__ import annotations
 
@@ -295,7 +296,7 @@ def _collect_pairs(impacts, nsteps, every, low, high, device, log):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("command", choices=["train", "evaluate"])
+    ap.add_argument("command", choices=["train", "evaluate", "profile"])
     ap.add_argument("--steps", type=int, default=704, help="steps of each data run")
     ap.add_argument("--every", type=int, default=4)
     ap.add_argument("--low", type=int, default=LOW)
@@ -330,12 +331,57 @@ def main(argv=None):
             save_weights(a.out, w, scale, {"impacts": TRAIN_IMPACTS, "low": a.low, "high": a.high,
                                            "data_steps": a.steps, "every": a.every, "train_steps": a.train_steps,
                                            "batch": a.batch, "lr": a.lr})
+    elif a.command == "profile":
+        out.update(profile(a.weights, impact=a.impact, npart=a.low, device=a.device, log=log))
     else:
         out.update(evaluate(a.weights, impact=a.impact, nsteps=a.steps, every=a.every, low=a.low, high=a.high,
                             device=a.device, log=log))
     if a.json:
         Path(a.json).write_text(json.dumps(out))
     return out
+
+
+def profile(weights_path=None, *, impact: float = 45.0, npart: int = LOW, at=(100, 200, 300, 400), reps: int = 5,
+            device: int = 0, log=print):
+    """Device time of the forward pass and of the gradient (CUDA events,
+    `reps` each after two warm-ups) on the fine densities of a plain run at
+    the steps `at`, with the number of active tiles of each."""
+    import torch
+    w, scale, _ = load_weights(weights_path)
+    sim = make_run(npart, impact, -21, device=device)
+    snaps = []
+    for s in range(1, max(at) + 1):
+        if sim.step().status:
+            raise RuntimeError(f"device status at step {s}")
+        if s in at:
+            snaps.append(torch.from_numpy(sim.accelerator.grid(L.VLB_GRID_RHO_FINE)).to(f"cuda:{device}"))
+    sim.accelerator.close()
+    net = Network(snaps[0].shape, device)
+    wt = torch.from_numpy(w).to(snaps[0].device)
+    out, grad = torch.empty_like(snaps[0]), torch.empty_like(wt)
+    res = []
+    try:
+        for step, x in zip(at, snaps):
+            for _ in range(2):
+                net.forward(x, wt, scale, out)
+                net.gradient(x, x, wt, scale, grad)
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record()
+            for _ in range(reps):
+                net.forward(x, wt, scale, out)
+            e[1].record()
+            for _ in range(reps):
+                net.gradient(x, x, wt, scale, grad)
+            e[2].record()
+            e[2].synchronize()
+            r = {"step": step, "active_tiles": net.active_tiles(), "forward_ms": e[0].elapsed_time(e[1]) / reps,
+                 "gradient_ms": e[1].elapsed_time(e[2]) / reps}
+            res.append(r)
+            log(f"step {step}: {r['active_tiles']} active tiles, forward {r['forward_ms']:.3f} ms, "
+                f"gradient {r['gradient_ms']:.3f} ms")
+    finally:
+        net.close()
+    return {"profile": res}
 
 
 def evaluate(weights_path=None, *, impact: float = 45.0, nsteps: int = 704, every: int = 4, low: int = LOW,
