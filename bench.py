@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--nfine", type=int, default=64)
     ap.add_argument("--profile", default="thomas-fermi", choices=["thomas-fermi", "uniform-sphere"])
     ap.add_argument("--deposit", default="float32", choices=["float32", "fixed64"])
-    ap.add_argument("--precision", default="3xtf32", choices=["fp32", "3xtf32"],
+    ap.add_argument("--precision", default="3xtf32", choices=["fp32", "3xtf32", "bf16x3"],
                     help="mode products on the CUDA cores (fp32) or split-precision on the tensor cores")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -230,7 +230,8 @@ def main():
         return float(t.item())
 
     p, prof, proj = workload(args, vb)
-    precision = vb._lib.VLB_POISSON_3XTF32 if args.precision == "3xtf32" else vb._lib.VLB_POISSON_FP32
+    precision = {"fp32": vb._lib.VLB_POISSON_FP32, "3xtf32": vb._lib.VLB_POISSON_3XTF32,
+                 "bf16x3": vb._lib.VLB_POISSON_BF16X3}[args.precision]
     if world > 1:
         # weak scaling: npart per GPU, one cloud of world * npart particles
         # sharded over the ranks (each rank draws its own slice)

@@ -117,7 +117,7 @@ typedef struct vlb_step_params {
   int32_t advance_projectile;  /* 0 during priming (src/simulation.jl:254) */
   int32_t push;                /* 0: forces only, no Verlet (priming) */
   int32_t use_graph;           /* 1: replay the step as one captured CUDA graph */
-  int32_t poisson_precision;   /* VLB_POISSON_FP32 or VLB_POISSON_3XTF32, every mode product of the step */
+  int32_t poisson_precision;   /* VLB_POISSON_FP32, _3XTF32 or _BF16X3, every mode product of the step */
   int32_t denoise;             /* 1: the learned denoiser on the fine density (vlb_set_denoiser) */
 } vlb_step_params;
 
@@ -154,6 +154,7 @@ typedef struct vlb_step_result {
  * FP32 accumulation (even n <= 144 points per axis). */
 #define VLB_POISSON_FP32 0
 #define VLB_POISSON_3XTF32 1
+#define VLB_POISSON_BF16X3 2
 
 VLB_API const char* vlb_last_error(void);
 VLB_API const char* vlb_version(void);

@@ -32,6 +32,7 @@ VLB_GRID_CSOL_COARSE = 5
 
 VLB_POISSON_FP32 = 0
 VLB_POISSON_3XTF32 = 1
+VLB_POISSON_BF16X3 = 2
 
 # every symbol include/vlasov_b200.h declares
 EXPORTS = (

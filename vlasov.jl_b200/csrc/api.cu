@@ -147,6 +147,7 @@ void setup_level(Level& D, const vlb_level_desc& L, bool coarse) {
 void free_level(Level& D) {
   dfree(D.colloc); dfree(D.knots); dfree(D.knots_d); dfree(D.sinvT); dfree(D.MT); dfree(D.MinvT);
   dfree(D.tc_sinv.img); dfree(D.tc_M.img); dfree(D.tc_Minv.img);
+  dfree(D.tc_sinv.bimg); dfree(D.tc_M.bimg); dfree(D.tc_Minv.bimg);
   dfree(D.lap); dfree(D.invlsum); dfree(D.dual); dfree(D.dual_d); dfree(D.dlen); dfree(D.loc_cells);
   dfree(D.rho); dfree(D.phi); dfree(D.csol); dfree(D.csol_hartree);
 }
@@ -559,9 +560,10 @@ int vlb_deposit_coarse(vlb_ctx* ctx, double charge) {
 namespace {
 int check_precision(const Ctx& c, int32_t precision) {
   if (precision == VLB_POISSON_FP32) return VLB_OK;
-  if (precision != VLB_POISSON_3XTF32) return fail(VLB_ERR_ARG, "unknown mode-product precision");
+  if (precision != VLB_POISSON_3XTF32 && precision != VLB_POISSON_BF16X3)
+    return fail(VLB_ERR_ARG, "unknown mode-product precision");
   if (!c.fine.tc_sinv.img || !c.fine.tc_M.img || !c.coarse.tc_sinv.img || !c.coarse.tc_M.img)
-    return fail(VLB_ERR_ARG, "3xTF32 mode products need an even n <= 144 points per axis on both levels");
+    return fail(VLB_ERR_ARG, "tensor-core mode products need an even n <= 144 points per axis on both levels");
   return VLB_OK;
 }
 }  // namespace

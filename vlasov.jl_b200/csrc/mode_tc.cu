@@ -1,28 +1,34 @@
 // The rotating mode product on the fifth-generation tensor cores, in split
-// precision ("3xTF32"): the plain FP32 product of poisson.cu computed as
+// precision: the plain FP32 product of poisson.cu computed as
 //
 //     dest[p + m*i'] = sum_i A[i', i] * src[i + n*p]
 //                    ~ sum_i (Alo Bhi + Ahi Blo + Ahi Bhi)[p, i']
 //
-// with every operand x split into a TF32 head hi = rna(x) and a tail
-// lo = rna(x - hi), products accumulated in FP32 in tensor memory.  The
-// dropped lo*lo term and the rounding of the tails are of order 2^-22 |x|, so
-// the result carries close to FP32 accuracy (src/tensorsolver.jl:217-223
-// computes the same product with SGEMM on CUDA devices).  The accumulator
-// rounds at every MMA, so the small terms go first and the head products
-// last.
+// with every operand x split into a head and a tail, products accumulated in
+// FP32 in tensor memory (src/tensorsolver.jl:217-223 computes the same
+// product with SGEMM on CUDA devices).  Two splits:
+//   - 3xTF32 (kind::tf32): hi = rna(x) to 10 mantissa bits, lo = rna(x - hi);
+//     the dropped lo*lo term and the rounding of the tails are of order
+//     2^-22 |x|: close to FP32 accuracy;
+//   - BF16x3 (kind::f16 with BF16 operands): hi = rn(x) to 7 mantissa bits,
+//     lo = rn(x - hi); x - hi - lo and lo*lo are of order 2^-16 |x|, at twice
+//     the MMA rate of TF32.
+// The accumulator rounds at every MMA, so the small terms go first and the
+// head products last.
 //
 // As a GEMM, D[p, i'] = sum_i S[p, i] A[i', i] with both operands K-major:
 //   - the MMA's A operand is a tile of 128 consecutive p (rows of src, each
 //     n contiguous floats).  It is bulk-copied raw into shared memory, split
 //     into hi/lo by eight warps (warps w and w+4 share the rows 32(w%4).. of
-//     their tensor-memory lane quarter and take alternate 8-wide K groups)
-//     and written to tensor memory with tcgen05.st, lane r = row r;
+//     their tensor-memory lane quarter and take alternate K groups of 8 TF32
+//     or 16 BF16) and written to tensor memory with tcgen05.st, lane r =
+//     row r, one TF32 or two packed BF16 (the lower K in the low half) per
+//     column;
 //   - the MMA's B operand is the n x n matrix (eigenvectors, their inverse, or
-//     S^-1), split into hi/lo once at context creation and stored K-chunk by
-//     K-chunk in the canonical K-major no-swizzle layout of 8-row x 16-byte
-//     core matrices, so bulk copies put it in shared memory as the MMA reads
-//     it, one mbarrier per chunk;
+//     S^-1), split into hi/lo once at context creation (in both formats) and
+//     stored K-chunk by K-chunk in the canonical K-major no-swizzle layout of
+//     8-row x 16-byte core matrices, so bulk copies put it in shared memory
+//     as the MMA reads it, one mbarrier per chunk;
 //   - D is 128 lanes x N columns of FP32 in tensor memory, read back with
 //     tcgen05.ld by the eight warps (thread r: row r, half of the columns)
 //     and stored to dest[p + m*i'], 32 consecutive p per warp and column.
@@ -75,12 +81,12 @@ struct TcStage {
 struct TcArgs {
   TcStage st[kTcMaxStages];
   int nst;
-  const float* img;      // B operand image: hi then lo, each npad16 x kpad8
+  const void* img;       // B operand image: hi then lo, each npad16 x kpad (TF32 or BF16)
   const float* invl;     // epi 1
   DeviceScalars* dsc;
   unsigned* sync;        // grid-barrier counter, zero at launch
   long long m;
-  int n, npad16, kpad8, pitch;
+  int n, npad16, kpad, pitch;   // kpad: K padded to the MMA's K (8 TF32, 16 BF16)
   int colH, colL, ncols;
   unsigned raw_bytes, img_bytes;
 };
@@ -125,6 +131,16 @@ __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
+// Round to the nearest BF16 value, ties to even (finite x), as float.
+__device__ __forceinline__ float bf16_rne(float x) {
+  const unsigned u = __float_as_uint(x);
+  return __uint_as_float((u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u);
+}
+
+__device__ __forceinline__ unsigned bf16_pack(float lo_k, float hi_k) {
+  return (__float_as_uint(lo_k) >> 16) | (__float_as_uint(hi_k) & 0xFFFF0000u);
+}
+
 __device__ __forceinline__ void tmem_st8(unsigned taddr, const float (&v)[8]) {
   asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
                "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
@@ -151,14 +167,23 @@ __device__ __forceinline__ uint64_t smem_desc(unsigned addr, unsigned sbo) {
          (1ull << 46);
 }
 
-__device__ __forceinline__ void mma_tf32_ts(unsigned d_tmem, unsigned a_tmem, uint64_t b_desc, unsigned idesc,
-                                            unsigned accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
-      : "memory");
+template <bool BF>
+__device__ __forceinline__ void mma_ts(unsigned d_tmem, unsigned a_tmem, uint64_t b_desc, unsigned idesc,
+                                       unsigned accumulate) {
+  if constexpr (BF)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
 }
 
 __device__ __forceinline__ void named_arrive(int id, int count) {
@@ -192,14 +217,20 @@ __device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target) {
   return ok;
 }
 
+template <bool BF>
 __global__ void __launch_bounds__(kTcThreads, 1) k_mode_chain_tc(TcArgs a) {
+  constexpr unsigned ES = BF ? 2u : 4u;   // bytes per B element
+  constexpr int EPC = 16 / (int)ES;       // B elements per 16-byte core-matrix row
+  constexpr int KM = 2 * EPC;             // K of one MMA (two core matrices)
+  constexpr int G = KM;                   // K elements per split group (8 tensor-memory columns)
+  constexpr int CPK = BF ? 2 : 1;         // A elements per tensor-memory column
   extern __shared__ __align__(128) unsigned char smem[];
   float* raw = reinterpret_cast<float*>(smem);                                   // [128][pitch]
-  float* Bimg = reinterpret_cast<float*>(smem + a.raw_bytes);                    // hi, lo
+  unsigned char* Bimg = smem + a.raw_bytes;                                      // hi, lo
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + a.raw_bytes + 2 * a.img_bytes);
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(bars + kTcBars);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nch = (a.kpad8 + kTcChunk - 1) / kTcChunk;
+  const int nch = (a.kpad + kTcChunk - 1) / kTcChunk;
   const long long p0 = (long long)blockIdx.x * kTcRows;
   const int rows = (int)min((long long)kTcRows, a.m - p0);
   const int n = a.n;
@@ -224,13 +255,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mode_chain_tc(TcArgs a) {
     if (lane == 0)
       for (int c = 0; c < nch; ++c)
         mbar_expect_tx(smem_u32(&bars[kBarImg + c]),
-                       2u * (unsigned)a.npad16 * (unsigned)min(kTcChunk, a.kpad8 - kTcChunk * c) * 4u);
+                       2u * (unsigned)a.npad16 * (unsigned)min(kTcChunk, a.kpad - kTcChunk * c) * ES);
     __syncwarp();
     if (lane < 2 * nch) {
       // lane 2c: head of chunk c, lane 2c+1: its tail
       const int c = lane >> 1, part = lane & 1;
-      const unsigned off = (unsigned)a.npad16 * (unsigned)(kTcChunk * c) * 4u + (part ? a.img_bytes : 0u);
-      const unsigned bytes = (unsigned)a.npad16 * (unsigned)min(kTcChunk, a.kpad8 - kTcChunk * c) * 4u;
+      const unsigned off = (unsigned)a.npad16 * (unsigned)(kTcChunk * c) * ES + (part ? a.img_bytes : 0u);
+      const unsigned bytes = (unsigned)a.npad16 * (unsigned)min(kTcChunk, a.kpad - kTcChunk * c) * ES;
       bulk_g2s(smem_u32(Bimg) + off, reinterpret_cast<const char*>(a.img) + off, bytes, smem_u32(&bars[kBarImg + c]));
     }
   }
@@ -267,35 +298,35 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mode_chain_tc(TcArgs a) {
                    smem_u32(&bars[kBarRaw + 4 * s + (r >> 5)]));
       }
       // ---- MMAs: the small terms chunk by chunk, then the head products
-      const unsigned idesc = (1u << 4)                              // D: F32
-                             | (2u << 7) | (2u << 10)               // A, B: TF32
-                             | ((unsigned)(a.npad16 >> 3) << 17)    // N
-                             | ((unsigned)(kTcRows >> 4) << 24);    // M
+      const unsigned idesc = (1u << 4)                                          // D: F32
+                             | (BF ? (1u << 7) | (1u << 10) : (2u << 7) | (2u << 10))  // A, B: BF16 or TF32
+                             | ((unsigned)(a.npad16 >> 3) << 17)                // N
+                             | ((unsigned)(kTcRows >> 4) << 24);                // M
       const unsigned bh = smem_u32(Bimg), bl = bh + a.img_bytes;
       for (int c = 0; c < nch; ++c) {
         named_sync(1 + c, kTcThreads);
         if (lane == 0) {
           tc_fence_after();
           if (s == 0) ok = mbar_wait(smem_u32(&bars[kBarImg + c]), 0) && ok;
-          const int kw = min(kTcChunk, a.kpad8 - kTcChunk * c);
-          const unsigned cbase = (unsigned)a.npad16 * (unsigned)(kTcChunk * c) * 4u;
-          const unsigned sbo = (unsigned)(kw / 4) * 128u;
-          for (int q = 0; q < kw / 8; ++q) {
-            const unsigned kb = cbase + 256u * q, ka = (unsigned)(kTcChunk * c) + 8u * q;
-            mma_tf32_ts(tmem, tmem + a.colL + ka, smem_desc(bh + kb, sbo), idesc, (c > 0 || q > 0) ? 1u : 0u);
-            mma_tf32_ts(tmem, tmem + a.colH + ka, smem_desc(bl + kb, sbo), idesc, 1u);
+          const int kw = min(kTcChunk, a.kpad - kTcChunk * c);
+          const unsigned cbase = (unsigned)a.npad16 * (unsigned)(kTcChunk * c) * ES;
+          const unsigned sbo = (unsigned)(kw / EPC) * 128u;
+          for (int q = 0; q < kw / KM; ++q) {
+            const unsigned kb = cbase + 256u * q, ka = (unsigned)(kTcChunk * c + KM * q) / CPK;
+            mma_ts<BF>(tmem, tmem + a.colL + ka, smem_desc(bh + kb, sbo), idesc, (c > 0 || q > 0) ? 1u : 0u);
+            mma_ts<BF>(tmem, tmem + a.colH + ka, smem_desc(bl + kb, sbo), idesc, 1u);
           }
         }
         __syncwarp();
       }
       if (lane == 0) {
         for (int c = 0; c < nch; ++c) {
-          const int kw = min(kTcChunk, a.kpad8 - kTcChunk * c);
-          const unsigned cbase = (unsigned)a.npad16 * (unsigned)(kTcChunk * c) * 4u;
-          const unsigned sbo = (unsigned)(kw / 4) * 128u;
-          for (int q = 0; q < kw / 8; ++q)
-            mma_tf32_ts(tmem, tmem + a.colH + (unsigned)(kTcChunk * c) + 8u * q,
-                        smem_desc(bh + cbase + 256u * q, sbo), idesc, 1u);
+          const int kw = min(kTcChunk, a.kpad - kTcChunk * c);
+          const unsigned cbase = (unsigned)a.npad16 * (unsigned)(kTcChunk * c) * ES;
+          const unsigned sbo = (unsigned)(kw / EPC) * 128u;
+          for (int q = 0; q < kw / KM; ++q)
+            mma_ts<BF>(tmem, tmem + a.colH + (unsigned)(kTcChunk * c + KM * q) / CPK,
+                       smem_desc(bh + cbase + 256u * q, sbo), idesc, 1u);
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_mma)
                      : "memory");
@@ -315,32 +346,42 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mode_chain_tc(TcArgs a) {
       const bool valid = r < rows;
       const float* row = raw + (size_t)r * a.pitch;
       for (int c = 0; c < nch; ++c) {
-        const int kend = min(kTcChunk * (c + 1), a.kpad8);
-        for (int k0 = kTcChunk * c + 8 * half; k0 < kend; k0 += 16) {
-          float v[8];
+        const int kend = min(kTcChunk * (c + 1), a.kpad);
+        for (int k0 = kTcChunk * c + G * half; k0 < kend; k0 += 2 * G) {
+          float v[G];
           if (a.pitch % 4 == 0) {
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
+            for (int q = 0; q < G / 4; ++q) {
               float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
               if (valid && k0 + 4 * q < n) t = *reinterpret_cast<const float4*>(row + k0 + 4 * q);
               v[4 * q] = t.x; v[4 * q + 1] = t.y; v[4 * q + 2] = t.z; v[4 * q + 3] = t.w;
             }
           } else {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < G / 2; ++q) {
               float2 t = make_float2(0.f, 0.f);
               if (valid && k0 + 2 * q < n) t = *reinterpret_cast<const float2*>(row + k0 + 2 * q);
               v[2 * q] = t.x; v[2 * q + 1] = t.y;
             }
           }
           float hi[8], lo[8];
+          if constexpr (BF) {
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            hi[j] = tf32_rna(v[j]);
-            lo[j] = tf32_rna(__fsub_rn(v[j], hi[j]));
+            for (int j = 0; j < 8; ++j) {
+              const float h0 = bf16_rne(v[2 * j]), h1 = bf16_rne(v[2 * j + 1]);
+              const float l0 = bf16_rne(__fsub_rn(v[2 * j], h0)), l1 = bf16_rne(__fsub_rn(v[2 * j + 1], h1));
+              hi[j] = __uint_as_float(bf16_pack(h0, h1));
+              lo[j] = __uint_as_float(bf16_pack(l0, l1));
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              hi[j] = tf32_rna(v[j]);
+              lo[j] = tf32_rna(__fsub_rn(v[j], hi[j]));
+            }
           }
-          tmem_st8(lane_base + (unsigned)(a.colH + k0), hi);
-          tmem_st8(lane_base + (unsigned)(a.colL + k0), lo);
+          tmem_st8(lane_base + (unsigned)(a.colH + k0 / CPK), hi);
+          tmem_st8(lane_base + (unsigned)(a.colL + k0 / CPK), lo);
         }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
         tc_fence_before();
@@ -413,21 +454,22 @@ int raw_pitch(int n) {
 
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
-TcArgs tc_args(const TcImage& A, long long m) {
+TcArgs tc_args(const TcImage& A, long long m, bool bf) {
   TcArgs a{};
   a.n = A.n;
   a.npad16 = A.npad16;
-  a.kpad8 = A.kpad8;
+  a.kpad = bf ? A.kpad16 : A.kpad8;
   a.m = m;
   a.pitch = raw_pitch(A.n);
   a.raw_bytes = (unsigned)round_up(kTcRows * a.pitch * 4, 128);
-  a.img_bytes = (unsigned)((size_t)A.npad16 * A.kpad8 * 4);
+  a.img_bytes = (unsigned)((size_t)A.npad16 * a.kpad * (bf ? 2 : 4));
+  const int kcols = bf ? a.kpad / 2 : a.kpad;  // tensor-memory columns of one A split
   a.colH = round_up(A.npad16, 32);
-  a.colL = a.colH + round_up(A.kpad8, 32);
-  int need = a.colL + A.kpad8, cols = 32;
+  a.colL = a.colH + round_up(kcols, 32);
+  int need = a.colL + kcols, cols = 32;
   while (cols < need) cols *= 2;
   a.ncols = cols;
-  a.img = A.img;
+  a.img = bf ? static_cast<const void*>(A.bimg) : static_cast<const void*>(A.img);
   return a;
 }
 
@@ -442,9 +484,28 @@ bool tc_supported(int n) {
   t.n = n;
   t.npad16 = round_up(n, 16);
   t.kpad8 = round_up(n, 8);
-  const TcArgs a = tc_args(t, 1);
-  return a.ncols <= 512 && tc_smem(a) <= 227 * 1024;
+  t.kpad16 = round_up(n, 16);
+  for (bool bf : {false, true}) {
+    const TcArgs a = tc_args(t, 1, bf);
+    if (a.ncols > 512 || tc_smem(a) > 227 * 1024 || a.kpad > kTcChunk * kTcMaxChunks) return false;
+  }
+  return true;
 }
+
+namespace {
+float round_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;  // nearest, ties to even
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+uint16_t bits_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return (uint16_t)(u >> 16);
+}
+}  // namespace
 
 TcImage make_tc_image(const double* A, int n) {
   TcImage t;
@@ -452,7 +513,9 @@ TcImage make_tc_image(const double* A, int n) {
   t.n = n;
   t.npad16 = round_up(n, 16);
   t.kpad8 = round_up(n, 8);
-  const size_t per = (size_t)t.npad16 * t.kpad8;
+  t.kpad16 = round_up(n, 16);
+  const size_t per = (size_t)t.npad16 * t.kpad8, bper = (size_t)t.npad16 * t.kpad16;
+  std::vector<uint16_t> hb(2 * bper, 0);
   std::vector<float> h(2 * per, 0.f);
   for (int r = 0; r < n; ++r)
     for (int k = 0; k < n; ++k) {
@@ -475,16 +538,28 @@ TcImage make_tc_image(const double* A, int n) {
                        (size_t)(kc / 4) * 32 + (size_t)(r % 8) * 4 + (kc % 4);
       h[o] = hi;
       h[per + o] = lo;
+      // the BF16 image: core matrices of 8 rows x 8 halves
+      const int bwidth = std::min(kTcChunk, t.kpad16 - kTcChunk * c);
+      const size_t bo = (size_t)t.npad16 * kTcChunk * c + (size_t)(r / 8) * (bwidth / 8) * 64 +
+                        (size_t)(kc / 8) * 64 + (size_t)(r % 8) * 8 + (kc % 8);
+      const float bh = round_bf16((float)x);
+      const float bl = round_bf16((float)(x - (double)bh));
+      hb[bo] = bits_bf16(bh);
+      hb[bper + bo] = bits_bf16(bl);
     }
   void* d = nullptr;
   VLB_CUDA(cudaMalloc(&d, 2 * per * sizeof(float)));
   t.img = static_cast<float*>(d);
   VLB_CUDA(cudaMemcpy(t.img, h.data(), 2 * per * sizeof(float), cudaMemcpyHostToDevice));
+  VLB_CUDA(cudaMalloc(&d, 2 * bper * sizeof(uint16_t)));
+  t.bimg = static_cast<uint16_t*>(d);
+  VLB_CUDA(cudaMemcpy(t.bimg, hb.data(), 2 * bper * sizeof(uint16_t), cudaMemcpyHostToDevice));
   return t;
 }
 
 void tc_setup(Ctx& c) {
-  VLB_CUDA(cudaFuncSetAttribute(k_mode_chain_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  VLB_CUDA(cudaFuncSetAttribute(k_mode_chain_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  VLB_CUDA(cudaFuncSetAttribute(k_mode_chain_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
   if (!c.tc_sync) {
     void* d = nullptr;
     VLB_CUDA(cudaMalloc(&d, 64 * sizeof(unsigned)));
@@ -495,9 +570,10 @@ void tc_setup(Ctx& c) {
 
 void launch_mode_chain_tc(Ctx& c, const TcImage& A, int nst, const float* const* src, float* const* dest,
                           const int* epi, long long m, const float* invl) {
-  if (!A.img) throw ArgError("no tensor-core image for this matrix (3xTF32 products need an even n <= 144)");
+  if (!A.img || !A.bimg) throw ArgError("no tensor-core image for this matrix (the products need an even n <= 144)");
   if (nst < 1 || nst > kTcMaxStages) throw ArgError("a tensor-core chain has 1 to 3 products");
-  TcArgs a = tc_args(A, m);
+  const bool bf = c.mode_precision == VLB_POISSON_BF16X3;
+  TcArgs a = tc_args(A, m, bf);
   a.nst = nst;
   for (int s = 0; s < nst; ++s) a.st[s] = TcStage{src[s], dest[s], epi[s]};
   a.invl = invl;
@@ -516,7 +592,10 @@ void launch_mode_chain_tc(Ctx& c, const TcImage& A, int nst, const float* const*
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  VLB_CUDA(cudaLaunchKernelEx(&cfg, k_mode_chain_tc, a));
+  if (bf)
+    VLB_CUDA(cudaLaunchKernelEx(&cfg, k_mode_chain_tc<true>, a));
+  else
+    VLB_CUDA(cudaLaunchKernelEx(&cfg, k_mode_chain_tc<false>, a));
   VLB_LAUNCHED(c);
 }
 

@@ -404,7 +404,7 @@ void solve_interior(Ctx& c, Level& L) {
   k_rhs<<<dim3(1, ni, ni), std::min(1024, (ni + 31) / 32 * 32), 0, c.stream>>>(c.work[2], L.rho, L.phi, L.lap, ni);
   VLB_LAUNCHED(c);
   ProductArgs a = base_args(L, true);
-  if (c.mode_precision == VLB_POISSON_3XTF32) {
+  if (c.mode_precision != VLB_POISSON_FP32) {
     // two chains of three products on the tensor cores
     const float* s1[3] = {c.work[2], c.work[0], c.work[1]};
     float* d1[3] = {c.work[0], c.work[1], c.work[0]};
@@ -437,7 +437,7 @@ void solve_interior(Ctx& c, Level& L) {
 // three S^-1 rotations: src -> w0 -> w1 -> dst
 void coefficients(Ctx& c, Level& L, const float* src, float* w0, float* w1, float* dst) {
   ProductArgs a = base_args(L, false);
-  if (c.mode_precision == VLB_POISSON_3XTF32) {
+  if (c.mode_precision != VLB_POISSON_FP32) {
     const float* s[3] = {src, w0, w1};
     float* d[3] = {w0, w1, dst};
     const int e[3] = {EPI_PLAIN, EPI_PLAIN, EPI_PLAIN};

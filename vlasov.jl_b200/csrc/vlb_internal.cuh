@@ -22,11 +22,13 @@ constexpr int kStatusBadCell = 2;       // a particle outside the CIC domain tab
 constexpr int kStatusOverflow = 4;      // fixed-point accumulator out of range
 constexpr int kStatusMmaTimeout = 8;    // a tensor-core product gave up waiting on its copies or MMAs
 
-// A matrix split into TF32 head and tail for the tensor-core mode product:
-// [hi | lo], each npad16 x kpad8 in the canonical K-major no-swizzle layout.
+// A matrix split into head and tail for the tensor-core mode products, in
+// the canonical K-major no-swizzle layout: [hi | lo] in TF32 (img, each
+// npad16 x kpad8 floats) and in BF16 (bimg, each npad16 x kpad16 halves).
 struct TcImage {
   float* img = nullptr;
-  int n = 0, npad16 = 0, kpad8 = 0;
+  uint16_t* bimg = nullptr;
+  int n = 0, npad16 = 0, kpad8 = 0, kpad16 = 0;
 };
 
 // Device-resident scalars of one step.  One block, zeroed (partly) at the
@@ -141,7 +143,7 @@ struct Ctx {
   double* partials = nullptr;                 // [10 * n^2] reductions
   // Poisson work buffers (max n^3)
   float* work[3] = {nullptr, nullptr, nullptr};
-  int mode_precision = 0;     // VLB_POISSON_FP32 or VLB_POISSON_3XTF32
+  int mode_precision = 0;     // VLB_POISSON_FP32, VLB_POISSON_3XTF32 or VLB_POISSON_BF16X3
   // launch shapes (vlb_set_tuning): particles per work item, persistent-grid
   // CTAs per SM of the gather, the coarse deposit, the push and the record move
   int chunk = kChunk, field_cps = 3, cic_cps = 4, push_cps = 8, move_cps = 8;

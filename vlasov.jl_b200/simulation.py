@@ -331,8 +331,8 @@ class DeviceAccelerator:
         L.check(L.lib().vlb_deposit_coarse(self._h, charge))
 
     def poisson(self, precision: int = L.VLB_POISSON_FP32):
-        """poisson!(phi, rho, meshes); precision VLB_POISSON_FP32 (CUDA cores) or
-        VLB_POISSON_3XTF32 (split-precision tensor cores).  Later coefficient
+        """poisson!(phi, rho, meshes); precision VLB_POISSON_FP32 (CUDA cores),
+        VLB_POISSON_3XTF32 or VLB_POISSON_BF16X3 (split-precision tensor cores).  Later coefficient
         conversions use the same precision."""
         L.check(L.lib().vlb_poisson(self._h, precision))
 

@@ -35,7 +35,7 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
     prof = S.uniform_sphere_profile() if uniform else S.thomas_fermi_profile()
     t0 = time.time()
     from . import _lib as L
-    prec = {"fp32": L.VLB_POISSON_FP32, "3xtf32": L.VLB_POISSON_3XTF32}[precision]
+    prec = {"fp32": L.VLB_POISSON_FP32, "3xtf32": L.VLB_POISSON_3XTF32, "bf16x3": L.VLB_POISSON_BF16X3}[precision]
     sim = S.Simulation(p, prof, projectile=S.xenon_projectile(v=v, x0=x0, dt=dt), seed=seed,
                        fixed_point=fixed_point, device=device, precision=prec)
     built = time.time() - t0
@@ -81,7 +81,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--fixed-point", action="store_true")
     ap.add_argument("--uniform", action="store_true", help="uniform-sphere cloud instead of Thomas-Fermi")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "3xtf32"],
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "3xtf32", "bf16x3"],
                     help="mode products on the CUDA cores or split-precision on the tensor cores")
     ap.add_argument("--json", default=None, help="write the capture curve here")
     a = ap.parse_args(argv)
