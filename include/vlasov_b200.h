@@ -249,8 +249,8 @@ VLB_API int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* 
  *   vlb_step_advance  : projectile step (identical on every shard), push,
  *                       capture count; results are this shard's (sum the
  *                       kinetic, escaped, angular, enclosed and counts).
- * With the fixed-point deposit the summed fine density does not depend on
- * the order of the sum.  One context alone is vlb_step. */
+ * With the fixed-point deposit the summed densities do not depend on the
+ * order of the sum.  One context alone is vlb_step. */
 #define VLB_DTYPE_FLOAT32 0
 #define VLB_DTYPE_INT64 1
 
@@ -259,7 +259,9 @@ typedef struct vlb_exchange {
   int32_t rho_fine_dtype;     /* VLB_DTYPE_INT64 (fixed point) or VLB_DTYPE_FLOAT32 */
   int32_t pad0_;
   int64_t rho_fine_count;
-  float* rho_coarse;          /* n^3 float32: the coarse deposit */
+  void* rho_coarse;           /* n^3 of rho_coarse_dtype: the coarse deposit */
+  int32_t rho_coarse_dtype;   /* VLB_DTYPE_INT64 (fixed point) or VLB_DTYPE_FLOAT32 */
+  int32_t pad3_;
   int64_t rho_coarse_count;
   double* scalars;            /* float64: [0] particles outside the deposit window */
   int32_t scalars_count;

@@ -93,7 +93,8 @@ class StepResult(C.Structure):
 
 class Exchange(C.Structure):
     _fields_ = [("rho_fine", C.c_void_p), ("rho_fine_dtype", C.c_int32), ("pad0_", C.c_int32),
-                ("rho_fine_count", C.c_int64), ("rho_coarse", C.c_void_p), ("rho_coarse_count", C.c_int64),
+                ("rho_fine_count", C.c_int64), ("rho_coarse", C.c_void_p), ("rho_coarse_dtype", C.c_int32),
+                ("pad3_", C.c_int32), ("rho_coarse_count", C.c_int64),
                 ("scalars", C.c_void_p), ("scalars_count", C.c_int32), ("pad1_", C.c_int32),
                 ("reaction", C.c_void_p), ("reaction_count", C.c_int32), ("pad2_", C.c_int32),
                 ("stream", C.c_void_p)]

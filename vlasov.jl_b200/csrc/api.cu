@@ -170,6 +170,7 @@ void destroy_ctx(Ctx* c) {
   dfree(c->keys); dfree(c->keys_alt); dfree(c->skeys); dfree(c->perm); dfree(c->vals_alt);
   dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off); dfree(c->occupied); dfree(c->bounds);
   dfree(c->outlist); dfree(c->chunk_start); dfree(c->item_cell); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
+  dfree(c->rho_fixed_c); dfree(c->red_items); dfree(c->red_tail); dfree(c->diag_part);
   for (auto& w : c->work) dfree(w);
   free_denoiser(*c);
   dfree(c->tc_sync);
@@ -264,12 +265,14 @@ void enqueue_phase_deposit(Ctx& c, const vlb_step_params& p, int64_t normalize_n
     if (p.denoise) launch_denoise(c, normalize_npart);
   }
   stage_mark(c, 2);
-  launch_deposit_coarse(c, c.weight);
+  launch_deposit_coarse(c, c.weight, p.deposit_mode);
+  if (normalize_npart > 0) launch_deposit_coarse_finish(c, p.deposit_mode);
   stage_mark(c, 3);
 }
 
 void enqueue_phase_fields(Ctx& c, const vlb_step_params& p, int64_t normalize_npart) {
   if (normalize_npart > 0) {
+    launch_deposit_coarse_finish(c, p.deposit_mode);
     launch_deposit_fine_normalize(c, c.weight, p.deposit_mode, normalize_npart);
     if (p.denoise) launch_denoise(c, normalize_npart);
   }
@@ -434,6 +437,10 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     const int nf = c->fine.n, nc = c->coarse.n;
     const size_t maxg = (size_t)std::max(nf, nc) * std::max(nf, nc) * std::max(nf, nc);
     c->rho_fixed = dalloc<unsigned long long>((size_t)nf * nf * nf);
+    c->rho_fixed_c = dalloc<unsigned long long>((size_t)nc * nc * nc);
+    c->red_items = dalloc<double>(4 * (size_t)(N / kMinChunk + c->ncell + 1));
+    c->red_tail = dalloc<double>(4 * (size_t)c->num_sms);
+    c->diag_part = dalloc<double>(5 * (size_t)c->num_sms * 32);
     c->partials = dalloc<double>(10 * (size_t)std::max(nf, nc) * std::max(nf, nc));
     for (auto& w : c->work) w = dalloc<float>(maxg);
     c->dsc = dalloc<DeviceScalars>(1);
@@ -551,7 +558,7 @@ int vlb_deposit_coarse(vlb_ctx* ctx, double charge) {
   CTX_OR_FAIL;
   if (!c.sorted) return fail(VLB_ERR_STATE, "deposit before any sort of the current cloud");
   return guarded([&]() -> int {
-    launch_deposit_coarse(c, charge);
+    launch_deposit_coarse(c, charge, VLB_DEPOSIT_FLOAT32);
     VLB_CUDA(cudaStreamSynchronize(c.stream));
     return VLB_OK;
   });
@@ -1028,7 +1035,13 @@ int vlb_exchange_buffers(vlb_ctx* ctx, int32_t deposit_mode, vlb_exchange* out) 
     out->rho_fine_dtype = VLB_DTYPE_FLOAT32;
   }
   out->rho_fine_count = nf;
-  out->rho_coarse = c.coarse.rho;
+  if (deposit_mode == VLB_DEPOSIT_FIXED64) {
+    out->rho_coarse = c.rho_fixed_c;
+    out->rho_coarse_dtype = VLB_DTYPE_INT64;
+  } else {
+    out->rho_coarse = c.coarse.rho;
+    out->rho_coarse_dtype = VLB_DTYPE_FLOAT32;
+  }
   out->rho_coarse_count = nc;
   out->scalars = c.dsc->xch;
   out->scalars_count = 1;

@@ -237,6 +237,21 @@ __device__ __forceinline__ void window_axis(int l, float w0, float w1, float (&f
   for (int e = 0; e < kCicW; ++e) f[e] = e == l ? w0 : (e == l + 1 ? w1 : 0.f);
 }
 
+__device__ __forceinline__ void cic_add(float* rho, unsigned long long* fixed, size_t i, float v) {
+  if (fixed) {
+    const long long iv = llrint((double)v * kFixedScale);
+    if (iv) atomicAdd(&fixed[i], (unsigned long long)iv);
+  } else {
+    atomicAdd(&rho[i], v);
+  }
+}
+
+// The coarse density from its fixed-point accumulator.
+__global__ void k_coarse_from_fixed(float* __restrict__ rho, const unsigned long long* __restrict__ fixed, size_t tot) {
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (size_t)gridDim.x * blockDim.x)
+    rho[t] = (float)((double)(long long)fixed[t] * kFixedInv);
+}
+
 // One warp per work item of the cell sort (a run of at most `chunk` particles
 // of one fine cell).  Each lane adds its particles' eight trilinear
 // contributions into a 4^3 register window anchored at the coarse point left
@@ -247,13 +262,16 @@ __device__ __forceinline__ void window_axis(int l, float w0, float w1, float (&f
 // global atomics.  The window is summed over the warp and added to the grid
 // once per item.  Contributions carry charge / (wx wy wz)
 // (src/devicemesh.jl:104); the walk is the reference's
-// (src/kernels.jl:1083-1273) with the scatter grouped by cell.
+// (src/kernels.jl:1083-1273) with the scatter grouped by cell.  With `fixed`
+// the additions go to an int64 grid in fixed point (scale 2^40): each item's
+// window sums are fixed by the sort, so the grid does not depend on the
+// order in which items run.
 __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
     const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
     const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int nk,
     int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ gt_g, int ng,
     float lx0, float linvw, const int32_t* __restrict__ cells_g, int ncells, const float* __restrict__ dl_g,
-    float x0f, float hf, float charge, float* rho, int chunk) {
+    float x0f, float hf, float charge, float* rho, unsigned long long* fixed, int chunk) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* gt = reinterpret_cast<float*>(smem);                   // [ng]
   float* igap = gt + ng;                                        // [ng] 1 / (gt[c] - gt[c-1])
@@ -322,15 +340,15 @@ __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
             for (int ez = 0; ez < kCicW; ++ez) acc[ex + kCicW * (ey + kCicW * ez)] += fxy * fz[ez];
           }
       } else {
-        float* b = rho + (size_t)i0 + n * j0 + nn * k0;
-        atomicAdd(b, wx0 * wy0 * wz0);
-        atomicAdd(b + nn, wx0 * wy0 * wz1);
-        atomicAdd(b + n, wx0 * wy1 * wz0);
-        atomicAdd(b + n + nn, wx0 * wy1 * wz1);
-        atomicAdd(b + 1, wx1 * wy0 * wz0);
-        atomicAdd(b + 1 + nn, wx1 * wy0 * wz1);
-        atomicAdd(b + 1 + n, wx1 * wy1 * wz0);
-        atomicAdd(b + 1 + n + nn, wx1 * wy1 * wz1);
+        const size_t b = (size_t)i0 + n * j0 + nn * k0;
+        cic_add(rho, fixed, b, wx0 * wy0 * wz0);
+        cic_add(rho, fixed, b + nn, wx0 * wy0 * wz1);
+        cic_add(rho, fixed, b + n, wx0 * wy1 * wz0);
+        cic_add(rho, fixed, b + n + nn, wx0 * wy1 * wz1);
+        cic_add(rho, fixed, b + 1, wx1 * wy0 * wz0);
+        cic_add(rho, fixed, b + 1 + nn, wx1 * wy0 * wz1);
+        cic_add(rho, fixed, b + 1 + n, wx1 * wy1 * wz0);
+        cic_add(rho, fixed, b + 1 + n + nn, wx1 * wy1 * wz1);
       }
     }
     // recursive halving over the warp: after the five steps lane l holds the
@@ -382,7 +400,7 @@ __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
       if (v != 0.f) {
         const int e = e0 + r;
         const int ex = e % kCicW, ey = (e / kCicW) % kCicW, ez = e / (kCicW * kCicW);
-        atomicAdd(&rho[(size_t)(anc[0] + ex) + n * (anc[1] + ey) + nn * (anc[2] + ez)], v);
+        cic_add(rho, fixed, (size_t)(anc[0] + ex) + n * (anc[1] + ey) + nn * (anc[2] + ez), v);
       }
     }
   }
@@ -460,15 +478,31 @@ size_t cic_smem(const Ctx& c) {
   return 3 * (size_t)c.coarse.n * sizeof(float) + (size_t)c.coarse.loc_ncell * sizeof(int32_t);
 }
 
-void launch_deposit_coarse(Ctx& c, double charge) {
+// The raw coarse deposit: into rho_coarse (float32) or, in fixed point,
+// into its int64 accumulator (then launch_deposit_coarse_finish).
+void launch_deposit_coarse(Ctx& c, double charge, int mode) {
   Level& C = c.coarse;
   const size_t tot = (size_t)C.n * C.n * C.n;
   Particles& P = c.part[c.cur];
-  VLB_CUDA(cudaMemsetAsync(C.rho, 0, tot * sizeof(float), c.stream));
+  const bool fixed = mode == VLB_DEPOSIT_FIXED64;
+  if (fixed)
+    VLB_CUDA(cudaMemsetAsync(c.rho_fixed_c, 0, tot * sizeof(unsigned long long), c.stream));
+  else
+    VLB_CUDA(cudaMemsetAsync(C.rho, 0, tot * sizeof(float), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_cic, 0, sizeof(unsigned long long), c.stream));
   k_deposit_cic<<<c.num_sms * c.cic_cps, kCicThreads, cic_smem(c), c.stream>>>(
       c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.fine.nk, c.Npad, P.k, P.d, C.colloc, C.n,
-      C.loc_x0, C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho, c.chunk);
+      C.loc_x0, C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho,
+      fixed ? c.rho_fixed_c : nullptr, c.chunk);
+  VLB_LAUNCHED(c);
+}
+
+// Fixed point: the (summed) accumulator into rho_coarse.
+void launch_deposit_coarse_finish(Ctx& c, int mode) {
+  if (mode != VLB_DEPOSIT_FIXED64) return;
+  Level& C = c.coarse;
+  const size_t tot = (size_t)C.n * C.n * C.n;
+  k_coarse_from_fixed<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(C.rho, c.rho_fixed_c, tot);
   VLB_LAUNCHED(c);
 }
 

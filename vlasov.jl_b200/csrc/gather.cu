@@ -91,7 +91,13 @@ __device__ __forceinline__ void load10(const float* __restrict__ tab, int col, f
   }
 }
 
-__device__ __forceinline__ void block_add_red(float ax, float ay, float az, float ae, double* red) {
+// The projectile's reaction sums are reduced in a fixed order, so that a
+// step gives the same sums whichever CTA takes which work item: one partial
+// per work item of the gather (the warp's sum over the item's particles),
+// one per CTA of the tail, summed by k_red_total.
+
+// This CTA's sums into out[4] (no atomics).
+__device__ __forceinline__ void block_red(float ax, float ay, float az, float ae, double* out) {
   __shared__ double sh[4][kGThreads / 32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double v[4] = {ax, ay, az, ae};
@@ -104,8 +110,32 @@ __device__ __forceinline__ void block_add_red(float ax, float ay, float az, floa
   if (threadIdx.x < 4) {
     double s = 0;
     for (int ww = 0; ww < kGThreads / 32; ++ww) s += sh[threadIdx.x][ww];
-    if (s != 0.0) atomicAdd(&red[threadIdx.x], s);
+    out[threadIdx.x] = s;
   }
+}
+
+// red[c] = the item partials then the tail partials, in a fixed order.
+__global__ void __launch_bounds__(256) k_red_total(const double* __restrict__ items, DeviceScalars* dsc,
+                                                   const double* __restrict__ tail, int ntail) {
+  __shared__ double sh[4][256];
+  const int nitems = dsc->nitems, t = threadIdx.x;
+  double s[4] = {0, 0, 0, 0};
+  for (int i = t; i < nitems; i += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) s[c] += items[4 * (size_t)i + c];
+  for (int i = t; i < ntail; i += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) s[c] += tail[4 * i + c];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) sh[c][t] = s[c];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (t < o)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) sh[c][t] += sh[c][t + o];
+    __syncthreads();
+  }
+  if (t < 4) dsc->red[t] = sh[t][0];
 }
 
 // One warp per work item (at most `chunk` particles of one occupied cell),
@@ -123,14 +153,13 @@ __global__ void __launch_bounds__(kGThreads) k_field(
     const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int64_t Npad,
     const float* __restrict__ d, const float* __restrict__ csol, int n, int nk, const float* __restrict__ ov,
     const float* __restrict__ gr, int nbdt, int ncol, float spacing, float x0, float h, double w,
-    float* __restrict__ force, int chunk) {
+    float* __restrict__ force, int chunk, double* __restrict__ red_items) {
   __shared__ __align__(16) float tiles[kGThreads / 32][kTile];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   float* tile = tiles[wid];
   const int nitems = dsc->nitems;
   const ProjF P = load_proj(dsc, w);
   const float wf = (float)w;
-  float ax = 0.f, ay = 0.f, az = 0.f, ae = 0.f;
   int cached = -1;
   for (;;) {
     int item = 0;
@@ -140,7 +169,10 @@ __global__ void __launch_bounds__(kGThreads) k_field(
     const int g = item_cell[item];
     int kx, ky, kz;
     cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
-    if (!field_fits(kx, ky, kz, n)) continue;  // the tail takes these
+    if (!field_fits(kx, ky, kz, n)) {  // the tail takes these
+      if (lane < 4) red_items[4 * (size_t)item + lane] = 0.0;
+      continue;
+    }
     if (g != cached) {
       __syncwarp();
       const int bx = 2 * kx - 6, by = 2 * ky - 6, bz = 2 * kz - 6;  // 0-based stencil corner
@@ -154,6 +186,7 @@ __global__ void __launch_bounds__(kGThreads) k_field(
     }
     const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
     const int s1 = min(s0 + chunk, bounds[g + 1]);
+    float ax = 0.f, ay = 0.f, az = 0.f, ae = 0.f;
     for (int s = s0 + lane; s < s1; s += 32) {
       const float dx0 = d[s], dy0 = d[Npad + s], dz0 = d[2 * Npad + s];
       const int cx = table_column(dx0, spacing, nbdt, ncol);
@@ -230,8 +263,15 @@ __global__ void __launch_bounds__(kGThreads) k_field(
       force[Npad + s] = fy;
       force[2 * Npad + s] = fz;
     }
+    // this item's reaction sums: lane order, then a fixed butterfly
+    double v[4] = {ax, ay, az, ae};
+#pragma unroll
+    for (int cc = 0; cc < 4; ++cc) v[cc] = warp_sum(v[cc]);
+    if (lane == 0) {
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) red_items[4 * (size_t)item + cc] = v[cc];
+    }
   }
-  block_add_red(ax, ay, az, ae, dsc->red);
 }
 
 // ------------------------------------------------------------------ tail
@@ -271,7 +311,7 @@ __global__ void __launch_bounds__(kGThreads) k_tail(const int32_t* __restrict__ 
                                                     const float* __restrict__ d, const float* __restrict__ csolc,
                                                     const double* __restrict__ kc, int nkc, int nc, int nk,
                                                     float x0f, float hf, double x0, double h, double w,
-                                                    float* __restrict__ force) {
+                                                    float* __restrict__ force, double* __restrict__ red_tail) {
   const int cnt = dsc->outcount;
   const ProjF P = load_proj(dsc, w);
   const double Px = dsc->proj_pos[0], Py = dsc->proj_pos[1], Pz = dsc->proj_pos[2];
@@ -334,7 +374,7 @@ __global__ void __launch_bounds__(kGThreads) k_tail(const int32_t* __restrict__ 
     force[Npad + s] = (float)fy;
     force[2 * Npad + s] = (float)fz;
   }
-  block_add_red(ax, ay, az, ae, dsc->red);
+  block_red(ax, ay, az, ae, red_tail + 4 * blockIdx.x);
 }
 
 }  // namespace
@@ -344,14 +384,16 @@ void launch_forces(Ctx& c) {
   Level& C = c.coarse;
   Particles& P = c.part[c.cur];
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_gather, 0, sizeof(unsigned long long), c.stream));
-  VLB_CUDA(cudaMemsetAsync(c.dsc->red, 0, sizeof(c.dsc->red), c.stream));
   k_field<<<c.num_sms * c.field_cps, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc,
                                                      c.Npad, P.d, F.csol, F.n, F.nk,
                                                      c.overlap, c.gradient, c.nbdt, c.ncol, c.spacing_f, c.x0f,
-                                                     c.hf, c.weight, c.force, c.chunk);
+                                                     c.hf, c.weight, c.force, c.chunk, c.red_items);
   VLB_LAUNCHED(c);
   k_tail<<<c.num_sms, kGThreads, 0, c.stream>>>(c.outlist, c.dsc, c.Npad, P.k, P.d, C.csol, C.knots_d, C.nk,
-                                                    C.n, F.nk, c.x0f, c.hf, c.x0, c.h, c.weight, c.force);
+                                                    C.n, F.nk, c.x0f, c.hf, c.x0, c.h, c.weight, c.force,
+                                                    c.red_tail);
+  VLB_LAUNCHED(c);
+  k_red_total<<<1, 256, 0, c.stream>>>(c.red_items, c.dsc, c.red_tail, c.num_sms);
   VLB_LAUNCHED(c);
   c.have_forces = true;
 }

@@ -142,12 +142,33 @@ __global__ void __launch_bounds__(256) k_push(int64_t N, int64_t Npad, int32_t* 
   if (threadIdx.x < 5) {
     double s = 0;
     for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww) s += sh[threadIdx.x][ww];
-    atomicAdd(&diag[threadIdx.x], s);
+    diag[5 * blockIdx.x + threadIdx.x] = s;  // this CTA's partial, summed in order by k_diag_total
   } else if (threadIdx.x == 5 && r2cap > 0) {
     unsigned long long s = 0;
     for (int ww = 0; ww < (int)(blockDim.x / 32); ++ww) s += shc[ww];
     if (s) atomicAdd(&dsc->enclosed, s);
   }
+}
+
+// diag[c] = the CTA partials of k_push in CTA order (a fixed order: the
+// push's grid-stride split of the particles is static).
+__global__ void __launch_bounds__(256) k_diag_total(const double* __restrict__ part, int nb, double* diag) {
+  __shared__ double sh[5][256];
+  const int t = threadIdx.x;
+  double s[5] = {0, 0, 0, 0, 0};
+  for (int b = t; b < nb; b += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 5; ++c) s[c] += part[5 * b + c];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) sh[c][t] = s[c];
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (t < o)
+#pragma unroll
+      for (int c = 0; c < 5; ++c) sh[c][t] += sh[c][t + o];
+    __syncthreads();
+  }
+  if (t < 5) diag[t] = sh[t][0];
 }
 
 // projectile_forces!(cloud, acc, proj, jel) then step!(proj, F, dt)
@@ -239,13 +260,15 @@ double measure_fp32_peak(int device) {
 void launch_push(Ctx& c, double dt, double rcmax, double capture_radius, bool keys) {
   Particles& P = c.part[c.cur];
   const double M = c.weight;  // ELECTRON_MASS * weight
-  VLB_CUDA(cudaMemsetAsync(c.dsc->diag, 0, sizeof(c.dsc->diag), c.stream));
   if (capture_radius > 0) VLB_CUDA(cudaMemsetAsync(&c.dsc->enclosed, 0, sizeof(unsigned long long), c.stream));
-  k_push<<<grid_for(c, (c.N + 3) / 4, 256, c.push_cps), 256, 0, c.stream>>>(
+  const int grid = grid_for(c, (c.N + 3) / 4, 256, c.push_cps);
+  k_push<<<grid, 256, 0, c.stream>>>(
       c.N, c.Npad, P.k, P.d, P.pk, P.pd, c.force, (float)(dt * dt / M), c.hf, c.x0f, (float)(M / (2 * dt)),
-      (float)(rcmax * rcmax), (float)(1 / (2 * M)), c.dsc->diag,
+      (float)(rcmax * rcmax), (float)(1 / (2 * M)), c.diag_part,
       capture_radius > 0 ? capture_radius * capture_radius : 0.0, c.x0, c.h, c.dsc, keys ? c.keys : nullptr,
       c.counts, c.fine.nk);
+  VLB_LAUNCHED(c);
+  k_diag_total<<<1, 256, 0, c.stream>>>(c.diag_part, grid, c.dsc->diag);
   VLB_LAUNCHED(c);
   c.keys_ready = keys;
 }

@@ -140,6 +140,12 @@ struct Ctx {
   int64_t scan_status_size = 0;
   // deposit
   unsigned long long* rho_fixed = nullptr;    // [n^3] int64 accumulator
+  unsigned long long* rho_fixed_c = nullptr;  // [nc^3] the coarse deposit's, in fixed point
+  // order-fixed reductions: the projectile's reaction sums per work item of
+  // the gather and per CTA of the tail, the push's diagnostics per CTA
+  double* red_items = nullptr;                // [max items][4]
+  double* red_tail = nullptr;                 // [num_sms][4]
+  double* diag_part = nullptr;                // [num_sms * 32][5]
   double* partials = nullptr;                 // [10 * n^2] reductions
   // Poisson work buffers (max n^3)
   float* work[3] = {nullptr, nullptr, nullptr};
@@ -188,7 +194,8 @@ void launch_sort(Ctx& c);
 void launch_deposit_fine(Ctx& c, double charge, int mode);
 void launch_deposit_fine_raw(Ctx& c, int mode);
 void launch_deposit_fine_normalize(Ctx& c, double charge, int mode, int64_t npart_global);
-void launch_deposit_coarse(Ctx& c, double charge);
+void launch_deposit_coarse(Ctx& c, double charge, int mode);
+void launch_deposit_coarse_finish(Ctx& c, int mode);
 // poisson.cu
 void launch_poisson(Ctx& c);
 void launch_grid_charge(Ctx& c, Level& L, const float* rho, double* out);

@@ -6,7 +6,7 @@ make.  Each rank holds a slice of the cloud and runs the step's three phases
 ranks sum, in place:
 
   after the deposit : the raw fine density (int64 fixed point, or float32),
-                      the coarse density and the count of particles outside
+                      the coarse density (the same) and the count of particles outside
                       the fine deposit window;
   after the forces  : the projectile's four reaction sums.
 
@@ -89,8 +89,9 @@ class LibraryShard:
         self.acc, self.device = acc, device
         x = acc.exchange(deposit_mode)
         fine_dtype = torch.int64 if x.rho_fine_dtype == L.VLB_DTYPE_INT64 else torch.float32
+        coarse_dtype = torch.int64 if x.rho_coarse_dtype == L.VLB_DTYPE_INT64 else torch.float32
         self._deposit = [device_tensor(x.rho_fine, x.rho_fine_count, fine_dtype, device),
-                         device_tensor(x.rho_coarse, x.rho_coarse_count, torch.float32, device),
+                         device_tensor(x.rho_coarse, x.rho_coarse_count, coarse_dtype, device),
                          device_tensor(x.scalars, x.scalars_count, torch.float64, device)]
         self._reaction = device_tensor(x.reaction, x.reaction_count, torch.float64, device)
         self._stream = torch.cuda.ExternalStream(x.stream, device=torch.device("cuda", device))
