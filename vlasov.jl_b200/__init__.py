@@ -18,5 +18,6 @@ from . import sharded
 from . import autotune
 from . import sweep
 from . import denoiser
+from . import precision_run
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -158,15 +158,16 @@ def detach(sim):
 
 # ------------------------------------------------------------ the data
 def make_run(npart: int, impact: float, seed: int, *, nfine: int = 64, device: int = 0,
-             precision: int = L.VLB_POISSON_3XTF32):
+             precision: int = L.VLB_POISSON_3XTF32, fixed_point: bool = False):
     """A primed run of the Xe25+ 500 keV collision (the headline workload's
-    grids and projectile, impact parameter `impact`)."""
+    grids and projectile, impact parameter `impact`); the priming step uses
+    the run's own deposit."""
     ninner, nouter = T.grids(nfine)
     p = S.SimulationParameters(nfine=nfine, ninner=ninner, nouter=nouter, rcluster=78.0, rbox=235.0, nions=196.0,
                                nelectrons=196.0, nparticles=int(npart), nsteps=0, dt=0.5)
     proj = S.xenon_projectile(v=0.40, impact=impact, x0=-70.0, dt=0.5)
     return S.Simulation(p, S.thomas_fermi_profile(), projectile=proj, seed=seed, device=device,
-                        precision=precision)
+                        precision=precision, fixed_point=fixed_point)
 
 
 def collect(sim, nsteps: int, every: int = 4):
