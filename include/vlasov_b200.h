@@ -121,6 +121,12 @@ typedef struct vlb_step_params {
   int32_t denoise;             /* 1: the learned denoiser on the fine density (vlb_set_denoiser) */
 } vlb_step_params;
 
+/* Device-side error flags (vlb_step_result.status, vlb_dn_status). */
+#define VLB_STATUS_SCAN_TIMEOUT 1  /* a look-back scan gave up waiting */
+#define VLB_STATUS_BAD_CELL 2      /* a particle outside the coarse deposit's cell table */
+#define VLB_STATUS_OVERFLOW 4      /* a fixed-point accumulator out of range */
+#define VLB_STATUS_MMA_TIMEOUT 8   /* a tensor-core kernel gave up waiting on its copies or MMAs */
+
 #define VLB_DEPOSIT_FLOAT32 0
 #define VLB_DEPOSIT_FIXED64 1   /* int64 fixed point, charge scaled by 2^40 */
 
@@ -136,7 +142,7 @@ typedef struct vlb_step_result {
   int32_t nout;                /* outside the fine deposit window */
   int32_t outcount;            /* 10^3 stencil leaves the fine grid */
   int32_t noccupied;           /* occupied fine cells */
-  int32_t status;              /* device-side error flags, 0 when clean */
+  int32_t status;              /* device-side error flags (VLB_STATUS_*), 0 when clean */
   int32_t denoised;            /* 1: the step used the denoiser's density, 0: the deposit's */
   int32_t pad_;
 } vlb_step_result;
@@ -307,6 +313,9 @@ VLB_API int vlb_dn_gradient(vlb_denoiser* dn, const float* x, const float* targe
                     const float* weights, float* grad, double* loss, void* stream);
 VLB_API int vlb_dn_adam(vlb_denoiser* dn, float* weights, const float* grad, float* m, float* v, float lr,
                 int32_t step, void* stream);
+/* device flags raised by the denoiser's kernels since the last call (a
+ * tensor-core wait that gave up: VLB_STATUS_MMA_TIMEOUT); synchronises */
+VLB_API int vlb_dn_status(vlb_denoiser* dn, int32_t* flags);
 /* tiles of 8^3 voxels the last pass computed: those within one tile of a
  * tile whose largest |x| exceeds 1e-3 of the volume's (the others pass
  * through unchanged) */

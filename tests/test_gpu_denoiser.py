@@ -1,12 +1,15 @@
-"""The learned denoiser on the GPU: its forward pass, loss, weight gradient
-and Adam step against the float64 oracle (oracle/denoiser.py); the tile
+"""The learned denoiser on the GPU: its forward pass (the 16 -> 16 layers on
+the tensor cores, the others on the CUDA cores), loss, weight gradient and
+Adam step against the float64 oracle (oracle/denoiser.py); the tile
 skip; the network in the step, with its charge check and fallback; training
 on the GPU beating the plain deposit on held-out data; the committed
 network's gain at 8e6 against 8e7 particles.
 
-Tolerances: the kernels compute in float32 against the oracle's float64,
-with the same BF16 weights: outputs to 2e-5 of their largest value,
-gradients to 1e-4 (relative L2 per layer)."""
+Tolerances: the kernels compute in float32 (on the tensor cores: exact
+products of the BF16 weights with BF16 heads and tails of the activations,
+summed in float32) against the oracle's float64, with the same BF16
+weights: outputs to 2e-5 of their largest value, gradients to 1e-4
+(relative L2 per layer)."""
 import numpy as np
 import pytest
 
@@ -59,6 +62,7 @@ def test_forward_matches_oracle(cuda_device):
         assert abs(out.astype(np.float64).sum() - x.astype(np.float64).sum()) <= 1e-5 * x.sum()
         assert net.active_tiles() == D.active_tiles(x)
         assert net.active_tiles() < np.prod([-(-n // 8) for n in x.shape])  # some tiles skipped
+        assert net.status() == 0
     finally:
         net.close()
 

@@ -40,7 +40,7 @@ EXPORTS = (
     "vlb_download_particles", "vlb_sort", "vlb_get_sort", "vlb_deposit_fine", "vlb_deposit_coarse",
     "vlb_poisson", "vlb_set_precision", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
     "vlb_push", "vlb_step", "vlb_dn_weight_count", "vlb_set_denoiser", "vlb_clear_denoiser", "vlb_dn_create",
-    "vlb_dn_destroy", "vlb_dn_forward", "vlb_dn_gradient", "vlb_dn_adam", "vlb_dn_active_tiles", "vlb_set_tuning", "vlb_get_tuning", "vlb_batch_create", "vlb_batch_step",
+    "vlb_dn_destroy", "vlb_dn_forward", "vlb_dn_gradient", "vlb_dn_adam", "vlb_dn_status", "vlb_dn_active_tiles", "vlb_set_tuning", "vlb_get_tuning", "vlb_batch_create", "vlb_batch_step",
     "vlb_batch_destroy", "vlb_exchange_buffers", "vlb_step_deposit", "vlb_step_fields", "vlb_step_advance",
     "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
     "vlb_enclosed_charge", "vlb_profile", "vlb_stage_count", "vlb_stage_name", "vlb_stage_times",
@@ -159,6 +159,7 @@ def lib():
             "vlb_dn_forward": (C.c_int, [vp, vp, C.c_float, vp, vp, vp]),
             "vlb_dn_gradient": (C.c_int, [vp, vp, vp, C.c_float, vp, vp, C.POINTER(C.c_double), vp]),
             "vlb_dn_adam": (C.c_int, [vp, vp, vp, vp, vp, C.c_float, C.c_int32, vp]),
+            "vlb_dn_status": (C.c_int, [vp, P_I]),
             "vlb_dn_active_tiles": (C.c_int, [vp, P_I]),
             "vlb_set_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),
             "vlb_get_tuning": (C.c_int, [vp, C.POINTER(Tuning)]),

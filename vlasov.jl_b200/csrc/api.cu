@@ -170,7 +170,7 @@ void destroy_ctx(Ctx* c) {
   dfree(c->keys); dfree(c->keys_alt); dfree(c->skeys); dfree(c->perm); dfree(c->vals_alt);
   dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off); dfree(c->occupied); dfree(c->bounds);
   dfree(c->outlist); dfree(c->chunk_start); dfree(c->item_cell); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
-  dfree(c->rho_fixed_c); dfree(c->red_items); dfree(c->red_tail); dfree(c->diag_part);
+  dfree(c->rho_fixed_c); dfree(c->red_items); dfree(c->red_tail); dfree(c->red_blocks); dfree(c->diag_part);
   for (auto& w : c->work) dfree(w);
   free_denoiser(*c);
   dfree(c->tc_sync);
@@ -440,6 +440,7 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->rho_fixed_c = dalloc<unsigned long long>((size_t)nc * nc * nc);
     c->red_items = dalloc<double>(4 * (size_t)(N / kMinChunk + c->ncell + 1));
     c->red_tail = dalloc<double>(4 * (size_t)c->num_sms);
+    c->red_blocks = dalloc<double>(4 * (size_t)c->num_sms);
     c->diag_part = dalloc<double>(5 * (size_t)c->num_sms * 32);
     c->partials = dalloc<double>(10 * (size_t)std::max(nf, nc) * std::max(nf, nc));
     for (auto& w : c->work) w = dalloc<float>(maxg);
@@ -766,6 +767,7 @@ int vlb_set_denoiser(vlb_ctx* ctx, const float* weights, int32_t count, double i
     ++c.config_epoch;
     const int n = c.fine.n;
     c.dn = dn_create(n, n, n, c.device, c.num_sms);
+    dn_route_status(c.dn, &c.dsc->status);  // a timed-out wait shows in the step's status
     std::vector<float> w(weights, weights + count);
     for (float& f : w) {  // round to BF16, ties to even
       uint32_t u;

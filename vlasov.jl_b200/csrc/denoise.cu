@@ -29,9 +29,14 @@
 // few escaped electrons (a pseudo-particle deposits ~1e-8 against a peak of
 // ~4e-3) passes through unchanged instead of filling the grid with tiles.
 //
-//   k_conv<CIN, COUT>     one layer (also the input-gradient pass, with the
-//                         weights flipped and transposed), 256 threads per
-//                         tile, two voxels per thread sharing the weight reads
+//   k_conv16_tc           the 16 -> 16 layers (and their input-gradient
+//                         passes) on the tensor cores: implicit GEMM, BF16
+//                         weights and BF16 head + tail activations, FP32
+//                         accumulation in tensor memory
+//   k_conv<CIN, COUT>     the other layers on the CUDA cores (also the
+//                         input-gradient pass, with the weights flipped and
+//                         transposed), 256 threads per tile, two voxels per
+//                         thread sharing the weight reads
 //   k_conv_wgrad<..>      weight gradient, per-CTA partial sums over tiles,
 //                         reduced in a fixed order by k_reduce_partials
 //   k_flux_limit          the positivity limiter of the flux
@@ -46,6 +51,7 @@
 #include <cstring>
 #include <vector>
 
+#include "tc_util.cuh"
 #include "vlb_internal.cuh"
 
 namespace vlb {
@@ -136,6 +142,25 @@ __device__ __forceinline__ bool live(const Vol& v, const int32_t* __restrict__ a
          amap[i / kT + v.tx * (j / kT + v.ty * (k / kT))];
 }
 
+// Threads 0..26: nb[d] = 1 when the tile next to `tile` in direction d
+// (d = dx + 3 dy + 9 dz, each in 0..2 for -1..+1) is inside and active.
+__device__ __forceinline__ void tile_neighbours(const Vol& v, const int32_t* __restrict__ amap, int tile, int* nb) {
+  const int d = threadIdx.x;
+  if (d >= 27) return;
+  const int a = tile % v.tx + d % 3 - 1, b = (tile / v.tx) % v.ty + (d / 3) % 3 - 1, c = tile / (v.tx * v.ty) + d / 9 - 1;
+  nb[d] = a >= 0 && b >= 0 && c >= 0 && a < v.tx && b < v.ty && c < v.tz ? amap[a + v.tx * (b + v.ty * c)] : 0;
+}
+
+// Halo coordinate h (0..kH-1) -> which of the three tiles along the axis.
+__device__ __forceinline__ int halo_side(int h) { return h == 0 ? 0 : (h == kH - 1 ? 2 : 1); }
+
+// Voxel (i, j, k) of halo position (xx, yy, zz) inside the volume and in an
+// active tile, by the tile's neighbour flags.
+__device__ __forceinline__ bool live_nb(const Vol& v, const int* nb, int i, int j, int k, int xx, int yy, int zz) {
+  return i >= 0 && j >= 0 && k >= 0 && i < v.nx && j < v.ny && k < v.nz &&
+         nb[halo_side(xx) + 3 * halo_side(yy) + 9 * halo_side(zz)];
+}
+
 // -------------------------------------------------------------- the conv
 // y[v][co] = sum_tap sum_ci w[tap][ci][co] * scale_in * x[v + tap - 1][ci]
 // (zero outside the volume and outside the active tiles), then
@@ -153,16 +178,22 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const float* __restrict__
   float* ws = sm;                                   // [27][CIN][COUT]
   float* xs = sm + 27 * CIN * COUT;                 // [kH^3][PS]
   for (int e = threadIdx.x; e < 27 * CIN * COUT; e += kConvThreads) ws[e] = w[e];
+  __shared__ int nb[27];
   const int n = *count;
   for (int li = blockIdx.x; li < n; li += gridDim.x) {
     int x0, y0, z0;
     tile_origin(v, list[li], x0, y0, z0);
     __syncthreads();
+    tile_neighbours(v, amap, list[li], nb);
+    __syncthreads();
+#pragma unroll 4
     for (int e = threadIdx.x; e < kH * kH * kH * CIN; e += kConvThreads) {
       const int ci = e % CIN, hv = e / CIN;
-      const int i = x0 - 1 + hv % kH, j = y0 - 1 + (hv / kH) % kH, k = z0 - 1 + hv / (kH * kH);
+      const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
+      const int i = x0 - 1 + xx, j = y0 - 1 + yy, k = z0 - 1 + zz;
       float val = 0.f;
-      if (live(v, amap, i, j, k)) val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
+      if (live_nb(v, nb, i, j, k, xx, yy, zz))
+        val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
       xs[hv * PS + ci] = val;
     }
     __syncthreads();
@@ -230,6 +261,200 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const float* __restrict__
   }
 }
 
+// ------------------------------------------- the 16 -> 16 layers, tcgen05
+// y[v][co] = sum_tap sum_ci w[tap][ci][co] x[v + tap - 1][ci] as an implicit
+// GEMM on the tensor cores: M = 128 voxels (two z planes of the tile), N = 16
+// output channels, K = 16 input channels per tap (one kind::f16 MMA), 27
+// taps.  The weights are BF16 (exact); each activation is split into a BF16
+// head and tail (x - head - tail ~ 2^-17 |x|), so two MMAs per tap give
+// exact products summed in FP32 in tensor memory, the tails first.
+//
+// A shared-memory descriptor walks its 128 rows as 16 core matrices of 8
+// rows at one stride.  A row is 16 bytes (8 channels) of one voxel, 8
+// consecutive x make a core matrix, and the next core matrix is the next y
+// -- and after eight of them the next z plane.  The halo is therefore kept
+// three times, shifted in y by db = 0, 1, 2 (copy db holds halo rows
+// y = b + db, b = 0..7, as [z 10][b 8][x 10]): in a copy a plane is 80 rows
+// and eight y steps of 10 rows make exactly one plane, so tap (da, db, dc)
+// of M block m is copy db from plane 2m + dc, column da, at stride 10 rows.
+// Channel blocks of 8 are the K core matrices (LBO = one block).
+constexpr int kTcConvWarps = 8;                         // staging and epilogue warps
+constexpr int kTcConvThreads = 32 * kTcConvWarps + 32;  // + the MMA warp
+constexpr unsigned kHaloRows = kH * kT * kH;            // rows of one shifted copy: 800
+constexpr unsigned kChBlockBytes = kHaloRows * 16;      // 8 channels: 12,800 B
+constexpr unsigned kCopyBytes = 2 * kChBlockBytes;      // 16 channels: 25,600 B
+constexpr unsigned kConvABytes = 6 * kCopyBytes;        // 3 shifts x (head, tail): 153,600 B
+constexpr unsigned kConvBBytes = 27 * 512;              // the BF16 weight image: 13,824 B
+constexpr size_t kConvTcSmem = kConvABytes + kConvBBytes + 64;
+constexpr int kStageItems = (kH * kH * kH * 4 + 32 * kTcConvWarps - 1) / (32 * kTcConvWarps);  // 16
+
+// The B image of one 16 -> 16 layer from its (BF16-valued) weights
+// w[tap][ci][co]: per tap, [co group 2][ci block 2][co 8][ci 8] halves.
+__global__ void k_conv16_image(const float* __restrict__ w, uint16_t* __restrict__ img) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 27 * 256; e += gridDim.x * blockDim.x) {
+    const int tap = e >> 8, ci = (e >> 4) & 15, co = e & 15;
+    img[tap * 256 + (co >> 3) * 128 + (ci >> 3) * 64 + (co & 7) * 8 + (ci & 7)] =
+        (uint16_t)(__float_as_uint(w[e]) >> 16);
+  }
+}
+
+__global__ void __launch_bounds__(kTcConvThreads, 1) k_conv16_tc(
+    const float* __restrict__ x, const uint16_t* __restrict__ wimg, float* __restrict__ y, Vol v,
+    const int32_t* __restrict__ list, const int32_t* __restrict__ count, const int32_t* __restrict__ amap, int relu,
+    const float* __restrict__ mask, int32_t* status) {
+  using namespace tc;
+  extern __shared__ __align__(128) float smf[];
+  unsigned char* tsm = reinterpret_cast<unsigned char*>(smf);
+  unsigned char* A = tsm;                                           // [db][part][ch block][z][b][x] x 16 B
+  unsigned char* B = tsm + kConvABytes;                             // the weight image
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + kConvABytes + kConvBBytes);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == kTcConvWarps) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(64)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (unsigned e = tid; e < kConvBBytes / 16; e += blockDim.x)
+    reinterpret_cast<uint4*>(B)[e] = reinterpret_cast<const uint4*>(wimg)[e];
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const unsigned tmem = *tmem_slot;
+  const int n = *count;
+  __shared__ int nb[27];
+  bool ok = true;
+  unsigned phase = 0;
+  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+    int x0, y0, z0;
+    tile_origin(v, list[li], x0, y0, z0);
+    tile_neighbours(v, amap, list[li], nb);
+    __syncthreads();
+    if (warp < kTcConvWarps) {
+      // ---- stage the halo: 4 channels per item; every load of the thread
+      // in flight before the first use, then head and tail into each
+      // shifted copy that holds the voxel's row
+      float4 tv[kStageItems];
+#pragma unroll
+      for (int it = 0; it < kStageItems; ++it) {
+        const int e = tid + 32 * kTcConvWarps * it;
+        tv[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (e >= kH * kH * kH * 4) continue;
+        const int q4 = e & 3, hv = e >> 2;
+        const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
+        const int i = x0 - 1 + xx, j = y0 - 1 + yy, k = z0 - 1 + zz;
+        if (live_nb(v, nb, i, j, k, xx, yy, zz))
+          tv[it] = *reinterpret_cast<const float4*>(x + ((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * 16 + 4 * q4);
+      }
+#pragma unroll
+      for (int it = 0; it < kStageItems; ++it) {
+        const int e = tid + 32 * kTcConvWarps * it;
+        if (e >= kH * kH * kH * 4) continue;
+        const int q4 = e & 3, hv = e >> 2;
+        const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
+        const float4 t = tv[it];
+        const float h0 = bf16_rne(t.x), h1 = bf16_rne(t.y), h2 = bf16_rne(t.z), h3 = bf16_rne(t.w);
+        const uint2 H = make_uint2(bf16_pack(h0, h1), bf16_pack(h2, h3));
+        const uint2 Lo = make_uint2(bf16_pack(bf16_rne(t.x - h0), bf16_rne(t.y - h1)),
+                                    bf16_pack(bf16_rne(t.z - h2), bf16_rne(t.w - h3)));
+        const unsigned inrow = (unsigned)(q4 >> 1) * kChBlockBytes + (unsigned)(q4 & 1) * 8u;
+#pragma unroll
+        for (int db = 0; db < 3; ++db) {
+          const int b = yy - db;
+          if (b < 0 || b >= kT) continue;
+          const unsigned off = inrow + (unsigned)((zz * kT + b) * kH + xx) * 16u;
+          *reinterpret_cast<uint2*>(A + (2 * db) * kCopyBytes + off) = H;
+          *reinterpret_cast<uint2*>(A + (2 * db + 1) * kCopyBytes + off) = Lo;
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == kTcConvWarps) {
+      // ---- the MMAs: four M blocks of 16 accumulator columns
+      if (lane == 0) {
+        const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+        const unsigned a0 = smem_u32(A), b0 = smem_u32(B);
+        for (int m = 0; m < 4; ++m) {
+          unsigned acc = 0;
+          for (int part = 1; part >= 0; --part)  // the tails first
+            for (int tap = 0; tap < 27; ++tap) {
+              const int da = tap % 3, db = (tap / 3) % 3, dc = tap / 9;
+              const unsigned aa = a0 + (unsigned)(2 * db + part) * kCopyBytes +
+                                  (unsigned)((2 * m + dc) * kT * kH + da) * 16u;
+              mma_ss_bf16(tmem + 16u * m, smem_desc(aa, kChBlockBytes, 16u * kH),
+                          smem_desc(b0 + 512u * tap, 128u, 256u), idesc, acc);
+              acc = 1;
+            }
+        }
+        commit(smem_u32(bar));
+      }
+      __syncwarp();
+    } else {
+      // ---- epilogue: warp w reads lanes 32 (w % 4).. of M blocks 2 (w / 4)
+      // and 2 (w / 4) + 1; row r = a + 8 b + 64 z'
+      ok = mbar_wait(smem_u32(bar), phase) && ok;
+      fence_after();
+      const int quarter = warp & 3, half = warp >> 2;
+      const int r = 32 * quarter + lane;
+      const int a = r & 7, b = (r >> 3) & 7, zq = r >> 6;
+      for (int mm = 0; mm < 2; ++mm) {
+        const int m = 2 * half + mm;
+        unsigned u[16];
+        tmem_ld16(tmem + ((unsigned)(32 * quarter) << 16) + 16u * m, u);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int i = x0 + a, j = y0 + b, k = z0 + 2 * m + zq;
+        if (!ok || i >= v.nx || j >= v.ny || k >= v.nz) continue;
+        const size_t vox = (size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k);
+        float o[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) {
+          float t = __uint_as_float(u[c]);
+          if (relu) t = fmaxf(t, 0.f);
+          o[c] = t;
+        }
+        if (mask) {
+          const float4* mk = reinterpret_cast<const float4*>(mask + vox * 16);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const float4 mv = mk[q];
+            if (!(mv.x > 0.f)) o[4 * q] = 0.f;
+            if (!(mv.y > 0.f)) o[4 * q + 1] = 0.f;
+            if (!(mv.z > 0.f)) o[4 * q + 2] = 0.f;
+            if (!(mv.w > 0.f)) o[4 * q + 3] = 0.f;
+          }
+        }
+        float4* dst = reinterpret_cast<float4*>(y + vox * 16);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dst[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+      }
+    }
+    phase ^= 1u;
+    fence_before();
+    const int bad = __syncthreads_or(!ok);
+    fence_after();
+    if (bad) break;
+  }
+  if (!ok) atomicOr(status, kStatusMmaTimeout);
+  // no MMA may still be in flight when the tensor memory is freed
+  if (__syncthreads_or(!ok) && warp == kTcConvWarps && lane == 0) mbar_wait(smem_u32(bar), phase ^ 1u);
+  fence_before();
+  __syncthreads();
+  if (warp == kTcConvWarps) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64) : "memory");
+  }
+}
+
 // gw[tap][ci][co] = sum_v x[v + tap - 1][ci] * g[v][co] over the active
 // tiles; each CTA sums its tiles into partial[blockIdx.x][27 * CIN * COUT].
 // Thread t owns (tap, ci) pairs t and t + 256 (432 pairs at CIN = 16).
@@ -250,16 +475,22 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_wgrad(const float* __rest
   for (int p = 0; p < PER; ++p)
 #pragma unroll
     for (int co = 0; co < COUT; ++co) acc[p][co] = 0.f;
+  __shared__ int nb[27];
   const int n = *count;
   for (int li = blockIdx.x; li < n; li += gridDim.x) {
     int x0, y0, z0;
     tile_origin(v, list[li], x0, y0, z0);
     __syncthreads();
+    tile_neighbours(v, amap, list[li], nb);
+    __syncthreads();
+#pragma unroll 4
     for (int e = threadIdx.x; e < kH * kH * kH * CIN; e += kConvThreads) {
       const int ci = e % CIN, hv = e / CIN;
-      const int i = x0 - 1 + hv % kH, j = y0 - 1 + (hv / kH) % kH, k = z0 - 1 + hv / (kH * kH);
+      const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
+      const int i = x0 - 1 + xx, j = y0 - 1 + yy, k = z0 - 1 + zz;
       float val = 0.f;
-      if (live(v, amap, i, j, k)) val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
+      if (live_nb(v, nb, i, j, k, xx, yy, zz))
+        val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
       xs[hv * PS + ci] = val;
     }
     for (int e = threadIdx.x; e < kT * kT * kT * COUT; e += kConvThreads) {
@@ -507,6 +738,10 @@ struct Denoiser {
   Vol v{};
   int device = 0;
   int nblocks = 0;              // CTAs of the conv grids (persistent over tiles)
+  int sms = 0;                  // CTAs of the tensor-core conv grid (one per SM)
+  uint16_t* wimg = nullptr;     // BF16 weight image of the 16 -> 16 layer being run
+  int32_t* status_own = nullptr;  // device flags of a stand-alone denoiser
+  int32_t* status = nullptr;      // where its kernels raise flags (status_own, or a step's)
   float* tmax = nullptr;        // [tiles] largest |input| of each tile
   float* gmax = nullptr;        // [1] of the volume
   int32_t* amap = nullptr;      // [tiles] 1: active
@@ -525,6 +760,8 @@ struct Denoiser {
   double* loss = nullptr;       // [1]
 };
 
+void dn_route_status(Denoiser* d, int32_t* status) { d->status = status; }
+
 void dn_free(Denoiser* d) {
   if (!d) return;
   cudaSetDevice(d->device);
@@ -532,6 +769,7 @@ void dn_free(Denoiser* d) {
   for (auto& a : d->act) cudaFree(a);
   for (auto& g : d->gbuf) cudaFree(g);
   cudaFree(d->gout); cudaFree(d->lam); cudaFree(d->outflow); cudaFree(d->tsum);
+  cudaFree(d->wimg); cudaFree(d->status_own);
   cudaFree(d->wr); cudaFree(d->wt); cudaFree(d->partial); cudaFree(d->lpart); cudaFree(d->loss);
   delete d;
 }
@@ -542,6 +780,7 @@ Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms) {
   d->v = Vol{nx, ny, nz, (nx + kT - 1) / kT, (ny + kT - 1) / kT, (nz + kT - 1) / kT};
   const size_t ntiles = (size_t)d->v.tx * d->v.ty * d->v.tz, nvox = (size_t)nx * ny * nz;
   d->nblocks = num_sms * 2;
+  d->sms = num_sms;
   auto alloc = [](void** p, size_t bytes) { VLB_CUDA(cudaMalloc(p, std::max<size_t>(bytes, 16))); };
   try {
     alloc((void**)&d->tmax, ntiles * 4);
@@ -552,6 +791,10 @@ Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms) {
     for (int l = 0; l < kLayers; ++l) alloc((void**)&d->act[l], nvox * kLayerOut[l] * 4);
     for (auto& g : d->gbuf) alloc((void**)&g, nvox * 16 * 4);
     alloc((void**)&d->gout, nvox * 4);
+    alloc((void**)&d->wimg, 27 * 256 * 2);
+    alloc((void**)&d->status_own, 4);
+    VLB_CUDA(cudaMemset(d->status_own, 0, 4));
+    d->status = d->status_own;
     alloc((void**)&d->lam, nvox * 4);
     alloc((void**)&d->outflow, nvox * 4);
     alloc((void**)&d->tsum, nvox * 4);
@@ -566,6 +809,7 @@ Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms) {
   }
   static bool attrs = false;
   if (!attrs) {
+    VLB_CUDA(cudaFuncSetAttribute(k_conv16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConvTcSmem));
     VLB_CUDA(cudaFuncSetAttribute(k_conv<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<1, 16>()));
     VLB_CUDA(cudaFuncSetAttribute(k_conv<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<16, 16>()));
     VLB_CUDA(cudaFuncSetAttribute(k_conv<16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<16, 3>()));
@@ -588,8 +832,13 @@ void conv(Denoiser& d, int cin, int cout, const float* x, const float* w, float*
   const int g = d.nblocks;
   if (cin == 1 && cout == 16)
     k_conv<1, 16><<<g, kConvThreads, conv_smem<1, 16>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
-  else if (cin == 16 && cout == 16)
-    k_conv<16, 16><<<g, kConvThreads, conv_smem<16, 16>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
+  else if (cin == 16 && cout == 16) {
+    // on the tensor cores (scale_in is 1 for these layers)
+    k_conv16_image<<<27, 256, 0, s>>>(w, d.wimg);
+    VLB_CUDA(cudaGetLastError());
+    k_conv16_tc<<<d.sms, kTcConvThreads, kConvTcSmem, s>>>(x, d.wimg, y, d.v, d.list, d.count, d.amap, relu, mask,
+                                                         d.status);
+  }
   else if (cin == 16 && cout == 3)
     k_conv<16, 3><<<g, kConvThreads, conv_smem<16, 3>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
   else if (cin == 3 && cout == 16)
@@ -832,6 +1081,18 @@ int vlb_dn_adam(vlb_denoiser* h, float* weights, const float* grad, float* m, fl
   return dn_guard([&]() -> int {
     VLB_CUDA(cudaSetDevice(h->d->device));
     dn_adam(*h->d, weights, grad, m, v, lr, step, static_cast<cudaStream_t>(stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_dn_status(vlb_denoiser* h, int32_t* flags) {
+  if (!h || !flags) return dn_fail(VLB_ERR_ARG, "vlb_dn_status: bad arguments");
+  return dn_guard([&]() -> int {
+    Denoiser& d = *h->d;
+    VLB_CUDA(cudaSetDevice(d.device));
+    VLB_CUDA(cudaDeviceSynchronize());
+    VLB_CUDA(cudaMemcpy(flags, d.status_own, 4, cudaMemcpyDeviceToHost));
+    VLB_CUDA(cudaMemset(d.status_own, 0, 4));
     return VLB_OK;
   });
 }

@@ -114,18 +114,16 @@ __device__ __forceinline__ void block_red(float ax, float ay, float az, float ae
   }
 }
 
-// red[c] = the item partials then the tail partials, in a fixed order.
-__global__ void __launch_bounds__(256) k_red_total(const double* __restrict__ items, DeviceScalars* dsc,
-                                                   const double* __restrict__ tail, int ntail) {
+// Sum of the four components over [begin, end) of a partials array, by
+// one block in a fixed order (strided by thread, then a tree); thread c < 4
+// returns component c.
+__device__ __forceinline__ double block_sum4(const double* __restrict__ p, int begin, int end) {
   __shared__ double sh[4][256];
-  const int nitems = dsc->nitems, t = threadIdx.x;
+  const int t = threadIdx.x;
   double s[4] = {0, 0, 0, 0};
-  for (int i = t; i < nitems; i += blockDim.x)
+  for (int i = begin + t; i < end; i += blockDim.x)
 #pragma unroll
-    for (int c = 0; c < 4; ++c) s[c] += items[4 * (size_t)i + c];
-  for (int i = t; i < ntail; i += blockDim.x)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) s[c] += tail[4 * i + c];
+    for (int c = 0; c < 4; ++c) s[c] += p[4 * (size_t)i + c];
 #pragma unroll
   for (int c = 0; c < 4; ++c) sh[c][t] = s[c];
   __syncthreads();
@@ -135,7 +133,28 @@ __global__ void __launch_bounds__(256) k_red_total(const double* __restrict__ it
       for (int c = 0; c < 4; ++c) sh[c][t] += sh[c][t + o];
     __syncthreads();
   }
-  if (t < 4) dsc->red[t] = sh[t][0];
+  const double r = t < 4 ? sh[t][0] : 0.0;
+  __syncthreads();
+  return r;
+}
+
+// First level: block b sums the work items of its contiguous share (the
+// shares depend only on the item count and the grid).
+__global__ void __launch_bounds__(256) k_red_blocks(const double* __restrict__ items, const DeviceScalars* dsc,
+                                                    double* __restrict__ block_out) {
+  const int nitems = dsc->nitems;
+  const int per = (nitems + gridDim.x - 1) / gridDim.x;
+  const int b0 = min(nitems, (int)blockIdx.x * per), b1 = min(nitems, b0 + per);
+  const double r = block_sum4(items, b0, b1);
+  if (threadIdx.x < 4) block_out[4 * blockIdx.x + threadIdx.x] = r;
+}
+
+// red[c] = the block partials, then the tail's, in a fixed order.
+__global__ void __launch_bounds__(256) k_red_total(const double* __restrict__ blocks, int nblocks,
+                                                   const double* __restrict__ tail, int ntail, DeviceScalars* dsc) {
+  const double a = block_sum4(blocks, 0, nblocks);
+  const double b = block_sum4(tail, 0, ntail);
+  if (threadIdx.x < 4) dsc->red[threadIdx.x] = a + b;
 }
 
 // One warp per work item (at most `chunk` particles of one occupied cell),
@@ -393,7 +412,9 @@ void launch_forces(Ctx& c) {
                                                     C.n, F.nk, c.x0f, c.hf, c.x0, c.h, c.weight, c.force,
                                                     c.red_tail);
   VLB_LAUNCHED(c);
-  k_red_total<<<1, 256, 0, c.stream>>>(c.red_items, c.dsc, c.red_tail, c.num_sms);
+  k_red_blocks<<<c.num_sms, 256, 0, c.stream>>>(c.red_items, c.dsc, c.red_blocks);
+  VLB_LAUNCHED(c);
+  k_red_total<<<1, 256, 0, c.stream>>>(c.red_blocks, c.num_sms, c.red_tail, c.num_sms, c.dsc);
   VLB_LAUNCHED(c);
   c.have_forces = true;
 }

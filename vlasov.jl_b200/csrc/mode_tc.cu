@@ -52,6 +52,7 @@
 #include <cstring>
 #include <vector>
 
+#include "tc_util.cuh"
 #include "vlb_internal.cuh"
 
 namespace vlb {
@@ -70,7 +71,6 @@ constexpr int kTcMaxStages = 3;    // products per launch
 constexpr int kBarRaw = 0, kBarMma = 4 * kTcMaxStages, kBarImg = kBarMma + kTcMaxStages;
 constexpr int kTcBars = kBarImg + kTcMaxChunks;
 constexpr int kDoneBarrier = 8;    // named barrier: the MMAs of a product are done
-constexpr long long kTcSpinLimit = 1ll << 22;
 
 struct TcStage {
   const float* src;
@@ -91,100 +91,13 @@ struct TcArgs {
   unsigned raw_bytes, img_bytes;
 };
 
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+using namespace tc;
 
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
+__device__ __forceinline__ void tc_fence_before() { fence_before(); }
+__device__ __forceinline__ void tc_fence_after() { fence_after(); }
 
-__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-  for (long long it = 0; it < kTcSpinLimit; ++it) {
-    unsigned ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// Round the magnitude to 10 explicit mantissa bits, ties away from zero (the
-// TF32 rounding of cvt.rna, done on the integer pipe).
-__device__ __forceinline__ float tf32_rna(float x) {
-  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
-}
-
-// Round to the nearest BF16 value, ties to even (finite x), as float.
-__device__ __forceinline__ float bf16_rne(float x) {
-  const unsigned u = __float_as_uint(x);
-  return __uint_as_float((u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u);
-}
-
-__device__ __forceinline__ unsigned bf16_pack(float lo_k, float hi_k) {
-  return (__float_as_uint(lo_k) >> 16) | (__float_as_uint(hi_k) & 0xFFFF0000u);
-}
-
-__device__ __forceinline__ void tmem_st8(unsigned taddr, const float (&v)[8]) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-               "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-               "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-               "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned* v) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-        "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-      : "r"(taddr)
-      : "memory");
-}
-
-// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8
-// rows x 16 bytes; LBO = 128 B between the two K halves of one MMA step,
-// SBO between 8-row groups; version 1 (bits 46-47).
-__device__ __forceinline__ uint64_t smem_desc(unsigned addr, unsigned sbo) {
-  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) |
-         (1ull << 46);
-}
-
-template <bool BF>
-__device__ __forceinline__ void mma_ts(unsigned d_tmem, unsigned a_tmem, uint64_t b_desc, unsigned idesc,
-                                       unsigned accumulate) {
-  if constexpr (BF)
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
-        : "memory");
-  else
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
+// The chains' B images: LBO = 128 B between the two K halves of one MMA step.
+__device__ __forceinline__ uint64_t smem_desc(unsigned addr, unsigned sbo) { return tc::smem_desc(addr, 128u, sbo); }
 
 __device__ __forceinline__ void named_arrive(int id, int count) {
   asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
@@ -204,7 +117,7 @@ __device__ __forceinline__ bool grid_sync(unsigned* ctr, unsigned target) {
     __threadfence();
     atomicAdd(ctr, 1u);
     unsigned v = 0;
-    for (long long it = 0; it < kTcSpinLimit; ++it) {
+    for (long long it = 0; it < kSpinLimit; ++it) {
       asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
       if (v >= target) break;
       __nanosleep(64);

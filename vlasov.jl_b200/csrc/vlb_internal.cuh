@@ -17,10 +17,10 @@ constexpr int kChunk = 128;       // default particles per work item of the gath
 constexpr int kMinChunk = 32;     // smallest chunk a tuning may set (sizes the item list)
 
 // Error flags raised by kernels into DeviceScalars::status.
-constexpr int kStatusScanTimeout = 1;   // decoupled look-back gave up
-constexpr int kStatusBadCell = 2;       // a particle outside the CIC domain table
-constexpr int kStatusOverflow = 4;      // fixed-point accumulator out of range
-constexpr int kStatusMmaTimeout = 8;    // a tensor-core product gave up waiting on its copies or MMAs
+constexpr int kStatusScanTimeout = VLB_STATUS_SCAN_TIMEOUT;  // decoupled look-back gave up
+constexpr int kStatusBadCell = VLB_STATUS_BAD_CELL;          // a particle outside the CIC domain table
+constexpr int kStatusOverflow = VLB_STATUS_OVERFLOW;         // fixed-point accumulator out of range
+constexpr int kStatusMmaTimeout = VLB_STATUS_MMA_TIMEOUT;    // a tensor-core kernel gave up waiting
 
 // A matrix split into head and tail for the tensor-core mode products, in
 // the canonical K-major no-swizzle layout: [hi | lo] in TF32 (img, each
@@ -145,6 +145,7 @@ struct Ctx {
   // the gather and per CTA of the tail, the push's diagnostics per CTA
   double* red_items = nullptr;                // [max items][4]
   double* red_tail = nullptr;                 // [num_sms][4]
+  double* red_blocks = nullptr;               // [num_sms][4] first level of their sum
   double* diag_part = nullptr;                // [num_sms * 32][5]
   double* partials = nullptr;                 // [10 * n^2] reductions
   // Poisson work buffers (max n^3)
@@ -202,6 +203,7 @@ void launch_grid_charge(Ctx& c, Level& L, const float* rho, double* out);
 // denoise.cu
 Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms);
 void dn_free(Denoiser* d);
+void dn_route_status(Denoiser* d, int32_t* status);
 void launch_denoise(Ctx& c, int64_t npart_global);
 void free_denoiser(Ctx& c);
 // mode_tc.cu

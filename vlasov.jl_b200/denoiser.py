@@ -124,6 +124,12 @@ class Network:
         L.check(L.lib().vlb_dn_adam(self._h, _ptr(weights), _ptr(grad), _ptr(m), _ptr(v), float(lr), int(step),
                                     self._stream()))
 
+    def status(self) -> int:
+        """Device flags raised since the last call (VLB_STATUS_*); synchronises."""
+        f = C.c_int32()
+        L.check(L.lib().vlb_dn_status(self._h, C.byref(f)))
+        return f.value
+
     def active_tiles(self) -> int:
         n = C.c_int32()
         L.check(L.lib().vlb_dn_active_tiles(self._h, C.byref(n)))
