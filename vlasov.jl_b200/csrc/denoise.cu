@@ -136,29 +136,67 @@ __global__ void k_tile_active(const float* __restrict__ tmax, const float* __res
   }
 }
 
-// Is voxel (i, j, k) inside the volume and in an active tile?
-__device__ __forceinline__ bool live(const Vol& v, const int32_t* __restrict__ amap, int i, int j, int k) {
-  return i >= 0 && j >= 0 && k >= 0 && i < v.nx && j < v.ny && k < v.nz &&
-         amap[i / kT + v.tx * (j / kT + v.ty * (k / kT))];
-}
-
-// Threads 0..26: nb[d] = 1 when the tile next to `tile` in direction d
-// (d = dx + 3 dy + 9 dz, each in 0..2 for -1..+1) is inside and active.
-__device__ __forceinline__ void tile_neighbours(const Vol& v, const int32_t* __restrict__ amap, int tile, int* nb) {
-  const int d = threadIdx.x;
-  if (d >= 27) return;
-  const int a = tile % v.tx + d % 3 - 1, b = (tile / v.tx) % v.ty + (d / 3) % 3 - 1, c = tile / (v.tx * v.ty) + d / 9 - 1;
-  nb[d] = a >= 0 && b >= 0 && c >= 0 && a < v.tx && b < v.ty && c < v.tz ? amap[a + v.tx * (b + v.ty * c)] : 0;
+// The active neighbours of each active tile as a 27-bit mask: bit d set when
+// the tile next to it in direction d (d = dx + 3 dy + 9 dz, each in 0..2 for
+// -1..+1) is inside and active.  The conv kernels read one word per tile.
+__global__ void k_tile_nbmask(const int32_t* __restrict__ amap, const int32_t* __restrict__ list,
+                              const int32_t* __restrict__ count, Vol v, uint32_t* __restrict__ nbmask) {
+  const int n = *count;
+  for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < n; li += gridDim.x * blockDim.x) {
+    const int t = list[li];
+    const int a = t % v.tx, b = (t / v.tx) % v.ty, c = t / (v.tx * v.ty);
+    uint32_t m = 0;
+    for (int d = 0; d < 27; ++d) {
+      const int aa = a + d % 3 - 1, bb = b + (d / 3) % 3 - 1, cc = c + d / 9 - 1;
+      if (aa >= 0 && bb >= 0 && cc >= 0 && aa < v.tx && bb < v.ty && cc < v.tz && amap[aa + v.tx * (bb + v.ty * cc)])
+        m |= 1u << d;
+    }
+    nbmask[t] = m;
+  }
 }
 
 // Halo coordinate h (0..kH-1) -> which of the three tiles along the axis.
 __device__ __forceinline__ int halo_side(int h) { return h == 0 ? 0 : (h == kH - 1 ? 2 : 1); }
 
 // Voxel (i, j, k) of halo position (xx, yy, zz) inside the volume and in an
-// active tile, by the tile's neighbour flags.
-__device__ __forceinline__ bool live_nb(const Vol& v, const int* nb, int i, int j, int k, int xx, int yy, int zz) {
+// active tile, by the tile's neighbour mask.
+__device__ __forceinline__ bool live_m(const Vol& v, uint32_t m, int i, int j, int k, int xx, int yy, int zz) {
   return i >= 0 && j >= 0 && k >= 0 && i < v.nx && j < v.ny && k < v.nz &&
-         nb[halo_side(xx) + 3 * halo_side(yy) + 9 * halo_side(zz)];
+         ((m >> (halo_side(xx) + 3 * halo_side(yy) + 9 * halo_side(zz))) & 1u);
+}
+
+// The 10^3 halo of a tile, CIN channels per voxel, into shared memory rows of
+// pad_stride(CIN) floats (zero outside the volume and the active tiles),
+// times scale_in; 16-byte loads and stores when CIN is a multiple of 4.
+template <int CIN>
+__device__ __forceinline__ void stage_halo(const float* __restrict__ x, const Vol& v, uint32_t nbm, int x0, int y0,
+                                           int z0, float* xs, float scale_in) {
+  constexpr int PS = pad_stride(CIN);
+  if constexpr (CIN % 4 == 0) {
+#pragma unroll 4
+    for (int e = threadIdx.x; e < kH * kH * kH * (CIN / 4); e += kConvThreads) {
+      const int q = e % (CIN / 4), hv = e / (CIN / 4);
+      const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
+      const int i = x0 - 1 + xx, j = y0 - 1 + yy, k = z0 - 1 + zz;
+      float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (live_m(v, nbm, i, j, k, xx, yy, zz)) {
+        val = *reinterpret_cast<const float4*>(x + ((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + 4 * q);
+        val.x *= scale_in; val.y *= scale_in; val.z *= scale_in; val.w *= scale_in;
+      }
+      *reinterpret_cast<float4*>(xs + hv * PS + 4 * q) = val;
+    }
+  } else {
+#pragma unroll 4
+    for (int e = threadIdx.x; e < kH * kH * kH * CIN; e += kConvThreads) {
+      const int ci = e % CIN, hv = e / CIN;
+      const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
+      const int i = x0 - 1 + xx, j = y0 - 1 + yy, k = z0 - 1 + zz;
+      float val = 0.f;
+      if (live_m(v, nbm, i, j, k, xx, yy, zz))
+        val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
+      xs[hv * PS + ci] = val;
+    }
+  }
 }
 
 // -------------------------------------------------------------- the conv
@@ -171,31 +209,20 @@ template <int CIN, int COUT>
 __global__ void __launch_bounds__(kConvThreads) k_conv(const float* __restrict__ x, const float* __restrict__ w,
                                                        float* __restrict__ y, Vol v, const int32_t* __restrict__ list,
                                                        const int32_t* __restrict__ count,
-                                                       const int32_t* __restrict__ amap, int relu,
+                                                       const uint32_t* __restrict__ nbmask, int relu,
                                                        const float* __restrict__ mask, float scale_in) {
   constexpr int PS = pad_stride(CIN);
   extern __shared__ __align__(16) float sm[];
   float* ws = sm;                                   // [27][CIN][COUT]
   float* xs = sm + 27 * CIN * COUT;                 // [kH^3][PS]
   for (int e = threadIdx.x; e < 27 * CIN * COUT; e += kConvThreads) ws[e] = w[e];
-  __shared__ int nb[27];
   const int n = *count;
   for (int li = blockIdx.x; li < n; li += gridDim.x) {
     int x0, y0, z0;
     tile_origin(v, list[li], x0, y0, z0);
+    const uint32_t nbm = nbmask[list[li]];
     __syncthreads();
-    tile_neighbours(v, amap, list[li], nb);
-    __syncthreads();
-#pragma unroll 4
-    for (int e = threadIdx.x; e < kH * kH * kH * CIN; e += kConvThreads) {
-      const int ci = e % CIN, hv = e / CIN;
-      const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
-      const int i = x0 - 1 + xx, j = y0 - 1 + yy, k = z0 - 1 + zz;
-      float val = 0.f;
-      if (live_nb(v, nb, i, j, k, xx, yy, zz))
-        val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
-      xs[hv * PS + ci] = val;
-    }
+    stage_halo<CIN>(x, v, nbm, x0, y0, z0, xs, scale_in);
     __syncthreads();
     // thread: voxel (a, b, c) and (a, b, c + 4)
     const int a = threadIdx.x % kT, b = (threadIdx.x / kT) % kT, c = threadIdx.x / (kT * kT);
@@ -278,15 +305,16 @@ __global__ void __launch_bounds__(kConvThreads) k_conv(const float* __restrict__
 // and eight y steps of 10 rows make exactly one plane, so tap (da, db, dc)
 // of M block m is copy db from plane 2m + dc, column da, at stride 10 rows.
 // Channel blocks of 8 are the K core matrices (LBO = one block).
-constexpr int kTcConvWarps = 8;                         // staging and epilogue warps
-constexpr int kTcConvThreads = 32 * kTcConvWarps + 32;  // + the MMA warp
+constexpr int kTcConvWarps = 11;                        // staging warps (the first 8 also the epilogue)
+constexpr int kTcEpiWarps = 8;
+constexpr int kTcConvThreads = 32 * kTcConvWarps + 32;  // + the MMA warp: 12 warps
 constexpr unsigned kHaloRows = kH * kT * kH;            // rows of one shifted copy: 800
 constexpr unsigned kChBlockBytes = kHaloRows * 16;      // 8 channels: 12,800 B
 constexpr unsigned kCopyBytes = 2 * kChBlockBytes;      // 16 channels: 25,600 B
 constexpr unsigned kConvABytes = 6 * kCopyBytes;        // 3 shifts x (head, tail): 153,600 B
 constexpr unsigned kConvBBytes = 27 * 512;              // the BF16 weight image: 13,824 B
 constexpr size_t kConvTcSmem = kConvABytes + kConvBBytes + 64;
-constexpr int kStageItems = (kH * kH * kH * 4 + 32 * kTcConvWarps - 1) / (32 * kTcConvWarps);  // 16
+constexpr int kStageItems = (kH * kH * kH * 4 + 32 * kTcConvWarps - 1) / (32 * kTcConvWarps);  // 12
 
 // The B image of one 16 -> 16 layer from its (BF16-valued) weights
 // w[tap][ci][co]: per tap, [co group 2][ci block 2][co 8][ci 8] halves.
@@ -298,10 +326,53 @@ __global__ void k_conv16_image(const float* __restrict__ w, uint16_t* __restrict
   }
 }
 
+// The staging warps' share of one tile's halo: 4 channels per item, every
+// load in flight before the first use.
+__device__ __forceinline__ void halo_load(const float* __restrict__ x, const Vol& v, uint32_t nbm, int x0, int y0,
+                                          int z0, int tid, float4 (&tv)[kStageItems]) {
+#pragma unroll
+  for (int it = 0; it < kStageItems; ++it) {
+    const int e = tid + 32 * kTcConvWarps * it;
+    tv[it] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (e >= kH * kH * kH * 4) continue;
+    const int q4 = e & 3, hv = e >> 2;
+    const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
+    const int i = x0 - 1 + xx, j = y0 - 1 + yy, k = z0 - 1 + zz;
+    if (live_m(v, nbm, i, j, k, xx, yy, zz))
+      tv[it] = *reinterpret_cast<const float4*>(x + ((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * 16 + 4 * q4);
+  }
+}
+
+// Head and tail of the items into each shifted copy that holds the voxel's row.
+__device__ __forceinline__ void halo_store(unsigned char* A, const float4 (&tv)[kStageItems], int tid) {
+  using namespace tc;
+#pragma unroll
+  for (int it = 0; it < kStageItems; ++it) {
+    const int e = tid + 32 * kTcConvWarps * it;
+    if (e >= kH * kH * kH * 4) continue;
+    const int q4 = e & 3, hv = e >> 2;
+    const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
+    const float4 t = tv[it];
+    const float h0 = bf16_rne(t.x), h1 = bf16_rne(t.y), h2 = bf16_rne(t.z), h3 = bf16_rne(t.w);
+    const uint2 H = make_uint2(bf16_pack(h0, h1), bf16_pack(h2, h3));
+    const uint2 Lo = make_uint2(bf16_pack(bf16_rne(t.x - h0), bf16_rne(t.y - h1)),
+                                bf16_pack(bf16_rne(t.z - h2), bf16_rne(t.w - h3)));
+    const unsigned inrow = (unsigned)(q4 >> 1) * kChBlockBytes + (unsigned)(q4 & 1) * 8u;
+#pragma unroll
+    for (int db = 0; db < 3; ++db) {
+      const int b = yy - db;
+      if (b < 0 || b >= kT) continue;
+      const unsigned off = inrow + (unsigned)((zz * kT + b) * kH + xx) * 16u;
+      *reinterpret_cast<uint2*>(A + (2 * db) * kCopyBytes + off) = H;
+      *reinterpret_cast<uint2*>(A + (2 * db + 1) * kCopyBytes + off) = Lo;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kTcConvThreads, 1) k_conv16_tc(
     const float* __restrict__ x, const uint16_t* __restrict__ wimg, float* __restrict__ y, Vol v,
-    const int32_t* __restrict__ list, const int32_t* __restrict__ count, const int32_t* __restrict__ amap, int relu,
-    const float* __restrict__ mask, int32_t* status) {
+    const int32_t* __restrict__ list, const int32_t* __restrict__ count, const uint32_t* __restrict__ nbmask,
+    int relu, const float* __restrict__ mask, int32_t* status) {
   using namespace tc;
   extern __shared__ __align__(128) float smf[];
   unsigned char* tsm = reinterpret_cast<unsigned char*>(smf);
@@ -329,85 +400,64 @@ __global__ void __launch_bounds__(kTcConvThreads, 1) k_conv16_tc(
   fence_after();
   const unsigned tmem = *tmem_slot;
   const int n = *count;
-  __shared__ int nb[27];
   bool ok = true;
   unsigned phase = 0;
-  for (int li = blockIdx.x; li < n; li += gridDim.x) {
+  // a software pipeline over the tiles: the staging warps hold the next
+  // tile's halo in registers, its loads in flight while this tile's MMAs run
+  float4 tv[kStageItems];
+  int li = blockIdx.x;
+  if (li < n && warp < kTcConvWarps) {
     int x0, y0, z0;
     tile_origin(v, list[li], x0, y0, z0);
-    tile_neighbours(v, amap, list[li], nb);
-    __syncthreads();
+    halo_load(x, v, nbmask[list[li]], x0, y0, z0, tid, tv);
+  }
+  for (; li < n; li += gridDim.x) {
+    int x0, y0, z0;
+    tile_origin(v, list[li], x0, y0, z0);
+    const int next = li + gridDim.x;
     if (warp < kTcConvWarps) {
-      // ---- stage the halo: 4 channels per item; every load of the thread
-      // in flight before the first use, then head and tail into each
-      // shifted copy that holds the voxel's row
-      float4 tv[kStageItems];
-#pragma unroll
-      for (int it = 0; it < kStageItems; ++it) {
-        const int e = tid + 32 * kTcConvWarps * it;
-        tv[it] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (e >= kH * kH * kH * 4) continue;
-        const int q4 = e & 3, hv = e >> 2;
-        const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
-        const int i = x0 - 1 + xx, j = y0 - 1 + yy, k = z0 - 1 + zz;
-        if (live_nb(v, nb, i, j, k, xx, yy, zz))
-          tv[it] = *reinterpret_cast<const float4*>(x + ((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * 16 + 4 * q4);
-      }
-#pragma unroll
-      for (int it = 0; it < kStageItems; ++it) {
-        const int e = tid + 32 * kTcConvWarps * it;
-        if (e >= kH * kH * kH * 4) continue;
-        const int q4 = e & 3, hv = e >> 2;
-        const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
-        const float4 t = tv[it];
-        const float h0 = bf16_rne(t.x), h1 = bf16_rne(t.y), h2 = bf16_rne(t.z), h3 = bf16_rne(t.w);
-        const uint2 H = make_uint2(bf16_pack(h0, h1), bf16_pack(h2, h3));
-        const uint2 Lo = make_uint2(bf16_pack(bf16_rne(t.x - h0), bf16_rne(t.y - h1)),
-                                    bf16_pack(bf16_rne(t.z - h2), bf16_rne(t.w - h3)));
-        const unsigned inrow = (unsigned)(q4 >> 1) * kChBlockBytes + (unsigned)(q4 & 1) * 8u;
-#pragma unroll
-        for (int db = 0; db < 3; ++db) {
-          const int b = yy - db;
-          if (b < 0 || b >= kT) continue;
-          const unsigned off = inrow + (unsigned)((zz * kT + b) * kH + xx) * 16u;
-          *reinterpret_cast<uint2*>(A + (2 * db) * kCopyBytes + off) = H;
-          *reinterpret_cast<uint2*>(A + (2 * db + 1) * kCopyBytes + off) = Lo;
-        }
-      }
+      halo_store(A, tv, tid);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     fence_before();
     __syncthreads();
     fence_after();
     if (warp == kTcConvWarps) {
-      // ---- the MMAs: four M blocks of 16 accumulator columns
+      // ---- the MMAs: four M blocks of 16 accumulator columns; the
+      // descriptors differ only in their start address
       if (lane == 0) {
         const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
-        const unsigned a0 = smem_u32(A), b0 = smem_u32(B);
+        const uint64_t ad0 = smem_desc(smem_u32(A), kChBlockBytes, 16u * kH);
+        const uint64_t bd0 = smem_desc(smem_u32(B), 128u, 256u);
         for (int m = 0; m < 4; ++m) {
-          unsigned acc = 0;
-          for (int part = 1; part >= 0; --part)  // the tails first
+          for (int part = 1; part >= 0; --part) {  // the tails first
+#pragma unroll
             for (int tap = 0; tap < 27; ++tap) {
               const int da = tap % 3, db = (tap / 3) % 3, dc = tap / 9;
-              const unsigned aa = a0 + (unsigned)(2 * db + part) * kCopyBytes +
-                                  (unsigned)((2 * m + dc) * kT * kH + da) * 16u;
-              mma_ss_bf16(tmem + 16u * m, smem_desc(aa, kChBlockBytes, 16u * kH),
-                          smem_desc(b0 + 512u * tap, 128u, 256u), idesc, acc);
-              acc = 1;
+              const unsigned off = (unsigned)(2 * db + part) * kCopyBytes + (unsigned)((2 * m + dc) * kT * kH + da) * 16u;
+              mma_ss_bf16(tmem + 16u * m, ad0 + (off >> 4), bd0 + (uint64_t)(512u * tap >> 4), idesc,
+                          (part == 1 && tap == 0) ? 0u : 1u);
             }
+          }
         }
         commit(smem_u32(bar));
       }
       __syncwarp();
     } else {
-      // ---- epilogue: warp w reads lanes 32 (w % 4).. of M blocks 2 (w / 4)
-      // and 2 (w / 4) + 1; row r = a + 8 b + 64 z'
+      // the next tile's halo loads go out now
+      if (next < n) {
+        int nx0, ny0, nz0;
+        tile_origin(v, list[next], nx0, ny0, nz0);
+        halo_load(x, v, nbmask[list[next]], nx0, ny0, nz0, tid, tv);
+      }
+      // ---- epilogue: warp w < 8 reads lanes 32 (w % 4).. of M blocks
+      // 2 (w / 4) and 2 (w / 4) + 1; row r = a + 8 b + 64 z'
       ok = mbar_wait(smem_u32(bar), phase) && ok;
       fence_after();
       const int quarter = warp & 3, half = warp >> 2;
       const int r = 32 * quarter + lane;
       const int a = r & 7, b = (r >> 3) & 7, zq = r >> 6;
-      for (int mm = 0; mm < 2; ++mm) {
+      for (int mm = 0; mm < (warp < kTcEpiWarps ? 2 : 0); ++mm) {
         const int m = 2 * half + mm;
         unsigned u[16];
         tmem_ld16(tmem + ((unsigned)(32 * quarter) << 16) + 16u * m, u);
@@ -462,7 +512,7 @@ template <int CIN, int COUT>
 __global__ void __launch_bounds__(kConvThreads) k_conv_wgrad(const float* __restrict__ x, const float* __restrict__ g,
                                                              Vol v, const int32_t* __restrict__ list,
                                                              const int32_t* __restrict__ count,
-                                                             const int32_t* __restrict__ amap,
+                                                             const uint32_t* __restrict__ nbmask,
                                                              float* __restrict__ partial, float scale_in) {
   constexpr int PS = pad_stride(CIN);
   constexpr int NP = 27 * CIN;           // (tap, ci) pairs
@@ -475,30 +525,30 @@ __global__ void __launch_bounds__(kConvThreads) k_conv_wgrad(const float* __rest
   for (int p = 0; p < PER; ++p)
 #pragma unroll
     for (int co = 0; co < COUT; ++co) acc[p][co] = 0.f;
-  __shared__ int nb[27];
   const int n = *count;
   for (int li = blockIdx.x; li < n; li += gridDim.x) {
     int x0, y0, z0;
     tile_origin(v, list[li], x0, y0, z0);
+    const uint32_t nbm = nbmask[list[li]];
     __syncthreads();
-    tile_neighbours(v, amap, list[li], nb);
-    __syncthreads();
-#pragma unroll 4
-    for (int e = threadIdx.x; e < kH * kH * kH * CIN; e += kConvThreads) {
-      const int ci = e % CIN, hv = e / CIN;
-      const int xx = hv % kH, yy = (hv / kH) % kH, zz = hv / (kH * kH);
-      const int i = x0 - 1 + xx, j = y0 - 1 + yy, k = z0 - 1 + zz;
-      float val = 0.f;
-      if (live_nb(v, nb, i, j, k, xx, yy, zz))
-        val = x[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * CIN + ci] * scale_in;
-      xs[hv * PS + ci] = val;
-    }
-    for (int e = threadIdx.x; e < kT * kT * kT * COUT; e += kConvThreads) {
-      const int co = e % COUT, tv = e / COUT;
-      const int i = x0 + tv % kT, j = y0 + (tv / kT) % kT, k = z0 + tv / (kT * kT);
-      float val = 0.f;
-      if (i < v.nx && j < v.ny && k < v.nz) val = g[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * COUT + co];
-      gs[tv * COUT + co] = val;
+    stage_halo<CIN>(x, v, nbm, x0, y0, z0, xs, scale_in);
+    if constexpr (COUT % 4 == 0) {
+      for (int e = threadIdx.x; e < kT * kT * kT * (COUT / 4); e += kConvThreads) {
+        const int q = e % (COUT / 4), tv = e / (COUT / 4);
+        const int i = x0 + tv % kT, j = y0 + (tv / kT) % kT, k = z0 + tv / (kT * kT);
+        float4 val = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (i < v.nx && j < v.ny && k < v.nz)
+          val = *reinterpret_cast<const float4*>(g + ((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * COUT + 4 * q);
+        *reinterpret_cast<float4*>(gs + tv * COUT + 4 * q) = val;
+      }
+    } else {
+      for (int e = threadIdx.x; e < kT * kT * kT * COUT; e += kConvThreads) {
+        const int co = e % COUT, tv = e / COUT;
+        const int i = x0 + tv % kT, j = y0 + (tv / kT) % kT, k = z0 + tv / (kT * kT);
+        float val = 0.f;
+        if (i < v.nx && j < v.ny && k < v.nz) val = g[((size_t)i + (size_t)v.nx * (j + (size_t)v.ny * k)) * COUT + co];
+        gs[tv * COUT + co] = val;
+      }
     }
     __syncthreads();
 #pragma unroll
@@ -745,6 +795,7 @@ struct Denoiser {
   float* tmax = nullptr;        // [tiles] largest |input| of each tile
   float* gmax = nullptr;        // [1] of the volume
   int32_t* amap = nullptr;      // [tiles] 1: active
+  uint32_t* nbmask = nullptr;   // [tiles] active neighbours of each active tile (27 bits)
   int32_t* list = nullptr;      // [tiles]
   int32_t* count = nullptr;     // [1]
   float* act[kLayers] = {};     // output of layer l: [vox][kLayerOut[l]]
@@ -765,7 +816,7 @@ void dn_route_status(Denoiser* d, int32_t* status) { d->status = status; }
 void dn_free(Denoiser* d) {
   if (!d) return;
   cudaSetDevice(d->device);
-  cudaFree(d->tmax); cudaFree(d->gmax); cudaFree(d->amap); cudaFree(d->list); cudaFree(d->count);
+  cudaFree(d->tmax); cudaFree(d->gmax); cudaFree(d->amap); cudaFree(d->nbmask); cudaFree(d->list); cudaFree(d->count);
   for (auto& a : d->act) cudaFree(a);
   for (auto& g : d->gbuf) cudaFree(g);
   cudaFree(d->gout); cudaFree(d->lam); cudaFree(d->outflow); cudaFree(d->tsum);
@@ -786,6 +837,7 @@ Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms) {
     alloc((void**)&d->tmax, ntiles * 4);
     alloc((void**)&d->gmax, 4);
     alloc((void**)&d->amap, ntiles * 4);
+    alloc((void**)&d->nbmask, ntiles * 4);
     alloc((void**)&d->list, ntiles * 4);
     alloc((void**)&d->count, 4);
     for (int l = 0; l < kLayers; ++l) alloc((void**)&d->act[l], nvox * kLayerOut[l] * 4);
@@ -831,18 +883,18 @@ void conv(Denoiser& d, int cin, int cout, const float* x, const float* w, float*
           float scale_in, cudaStream_t s) {
   const int g = d.nblocks;
   if (cin == 1 && cout == 16)
-    k_conv<1, 16><<<g, kConvThreads, conv_smem<1, 16>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
+    k_conv<1, 16><<<g, kConvThreads, conv_smem<1, 16>(), s>>>(x, w, y, d.v, d.list, d.count, d.nbmask, relu, mask, scale_in);
   else if (cin == 16 && cout == 16) {
     // on the tensor cores (scale_in is 1 for these layers)
     k_conv16_image<<<27, 256, 0, s>>>(w, d.wimg);
     VLB_CUDA(cudaGetLastError());
-    k_conv16_tc<<<d.sms, kTcConvThreads, kConvTcSmem, s>>>(x, d.wimg, y, d.v, d.list, d.count, d.amap, relu, mask,
+    k_conv16_tc<<<d.sms, kTcConvThreads, kConvTcSmem, s>>>(x, d.wimg, y, d.v, d.list, d.count, d.nbmask, relu, mask,
                                                          d.status);
   }
   else if (cin == 16 && cout == 3)
-    k_conv<16, 3><<<g, kConvThreads, conv_smem<16, 3>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
+    k_conv<16, 3><<<g, kConvThreads, conv_smem<16, 3>(), s>>>(x, w, y, d.v, d.list, d.count, d.nbmask, relu, mask, scale_in);
   else if (cin == 3 && cout == 16)
-    k_conv<3, 16><<<g, kConvThreads, conv_smem<3, 16>(), s>>>(x, w, y, d.v, d.list, d.count, d.amap, relu, mask, scale_in);
+    k_conv<3, 16><<<g, kConvThreads, conv_smem<3, 16>(), s>>>(x, w, y, d.v, d.list, d.count, d.nbmask, relu, mask, scale_in);
   else
     throw ArgError("unsupported conv shape");
   VLB_CUDA(cudaGetLastError());
@@ -852,13 +904,13 @@ void wgrad(Denoiser& d, int cin, int cout, const float* x, const float* g, float
            cudaStream_t s) {
   const int nb = d.nblocks, m = 27 * cin * cout;
   if (cin == 1 && cout == 16)
-    k_conv_wgrad<1, 16><<<nb, kConvThreads, wgrad_smem<1, 16>(), s>>>(x, g, d.v, d.list, d.count, d.amap, d.partial,
+    k_conv_wgrad<1, 16><<<nb, kConvThreads, wgrad_smem<1, 16>(), s>>>(x, g, d.v, d.list, d.count, d.nbmask, d.partial,
                                                                        scale_in);
   else if (cin == 16 && cout == 16)
-    k_conv_wgrad<16, 16><<<nb, kConvThreads, wgrad_smem<16, 16>(), s>>>(x, g, d.v, d.list, d.count, d.amap, d.partial,
+    k_conv_wgrad<16, 16><<<nb, kConvThreads, wgrad_smem<16, 16>(), s>>>(x, g, d.v, d.list, d.count, d.nbmask, d.partial,
                                                                          scale_in);
   else if (cin == 16 && cout == 3)
-    k_conv_wgrad<16, 3><<<nb, kConvThreads, wgrad_smem<16, 3>(), s>>>(x, g, d.v, d.list, d.count, d.amap, d.partial,
+    k_conv_wgrad<16, 3><<<nb, kConvThreads, wgrad_smem<16, 3>(), s>>>(x, g, d.v, d.list, d.count, d.nbmask, d.partial,
                                                                        scale_in);
   else
     throw ArgError("unsupported conv shape");
@@ -869,7 +921,7 @@ void wgrad(Denoiser& d, int cin, int cout, const float* x, const float* g, float
 
 }  // namespace
 
-constexpr int kForwardLaunches = 5 + kLayers;  // kernels dn_forward launches
+constexpr int kForwardLaunches = 6 + kLayers;  // kernels dn_forward launches
 
 // Active tiles of input x, BF16 rounding of the weights, the forward pass
 // (act[3] = F = f(s x), three channels, zero outside the active tiles;
@@ -882,6 +934,8 @@ void dn_forward(Denoiser& d, const float* x, float s, const float* w_master, cud
   VLB_CUDA(cudaGetLastError());
   VLB_CUDA(cudaMemsetAsync(d.count, 0, 4, st));
   k_tile_active<<<(unsigned)((ntiles + 255) / 256), 256, 0, st>>>(d.tmax, d.gmax, d.v, d.amap, d.list, d.count);
+  VLB_CUDA(cudaGetLastError());
+  k_tile_nbmask<<<(unsigned)((ntiles + 255) / 256), 256, 0, st>>>(d.amap, d.list, d.count, d.v, d.nbmask);
   VLB_CUDA(cudaGetLastError());
   k_bf16_round<<<(kDnWeights + 255) / 256, 256, 0, st>>>(w_master, d.wr, kDnWeights);
   VLB_CUDA(cudaGetLastError());

@@ -230,6 +230,46 @@ __device__ __forceinline__ int locate_cell(const float* __restrict__ gt, const f
   return c;
 }
 
+// The locate of one axis for the particles of one work item.  They share a
+// fine cell, so their coarse left points lie in the item's window: the
+// points anc .. anc + 2 after the anchor.  The item keeps the window's four
+// coordinates in registers, and a particle inside (gt[anc], gt[anc + 3]]
+// finds its point with two comparisons -- the point locate_cell finds --
+// then reads its inverse gap and dual lengths in one round of independent
+// loads instead of a chain; the weight takes the same arithmetic.  Any
+// other particle takes locate_cell.
+struct CicAxis {
+  bool fast;
+  float g0, g1, g2, g3;        // gt[anc .. anc + 3]
+};
+
+__device__ __forceinline__ void cic_axis(CicAxis& A, int anc, int ng, const float* gt) {
+  A.fast = anc >= 0 && anc + 3 <= ng - 1;
+  if (!A.fast) return;
+  A.g0 = gt[anc]; A.g1 = gt[anc + 1]; A.g2 = gt[anc + 2]; A.g3 = gt[anc + 3];
+}
+
+// c = the first grid index with gt[c] >= x (0: outside), its weight w, and
+// the inverse dual lengths of the points c - 1 and c.
+__device__ __forceinline__ int cic_locate(const CicAxis& A, int anc, float x, float& w, float& il0, float& il1,
+                                          const float* gt, const float* igap, const float* idl, int ng, float lx0,
+                                          float linvw, const int32_t* cells, int ncells) {
+  int c;
+  if (A.fast && x > A.g0 && x <= A.g3) {
+    const int o = (A.g1 < x) + (A.g2 < x);
+    c = anc + 1 + o;
+    const float gc = o == 0 ? A.g1 : (o == 1 ? A.g2 : A.g3);
+    w = fsub(gc, x) * igap[c];
+  } else {
+    c = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, x, w);
+  }
+  if (c > 0) {
+    il0 = idl[c - 1];
+    il1 = idl[c];
+  }
+  return c;
+}
+
 // The two weights of one axis spread over the window's four points: the left
 // point sits at offset l in [0, 2].
 __device__ __forceinline__ void window_axis(int l, float w0, float w1, float (&f)[kCicW]) {
@@ -309,6 +349,10 @@ __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
         anc[ax] = c > 0 ? c - 1 : -1000;
       }
     }
+    CicAxis AX, AY, AZ;
+    cic_axis(AX, anc[0], ng, gt);
+    cic_axis(AY, anc[1], ng, gt);
+    cic_axis(AZ, anc[2], ng, gt);
     float acc[kCicW3];
 #pragma unroll
     for (int e = 0; e < kCicW3; ++e) acc[e] = 0.f;
@@ -316,15 +360,15 @@ __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
       const float px = fadd(fadd(x0f, fmul((float)(k[s] - 1), hf)), d[s]);
       const float py = fadd(fadd(x0f, fmul((float)(k[Npad + s] - 1), hf)), d[Npad + s]);
       const float pz = fadd(fadd(x0f, fmul((float)(k[2 * Npad + s] - 1), hf)), d[2 * Npad + s]);
-      float ax, ay, az;
-      const int ix = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, px, ax);
-      const int iy = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, py, ay);
-      const int iz = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, pz, az);
+      float ax, ay, az, ix0, ix1, iy0, iy1, iz0, iz1;
+      const int ix = cic_locate(AX, anc[0], px, ax, ix0, ix1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
+      const int iy = cic_locate(AY, anc[1], py, ay, iy0, iy1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
+      const int iz = cic_locate(AZ, anc[2], pz, az, iz0, iz1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
       if (!(ix > 0 && iy > 0 && iz > 0)) continue;
       const int i0 = ix - 1, j0 = iy - 1, k0 = iz - 1;  // 0-based left points
-      const float wx0 = ax * idl[i0], wx1 = (1.f - ax) * idl[i0 + 1];
-      const float wy0 = ay * idl[j0], wy1 = (1.f - ay) * idl[j0 + 1];
-      const float wz0 = charge * az * idl[k0], wz1 = charge * (1.f - az) * idl[k0 + 1];
+      const float wx0 = ax * ix0, wx1 = (1.f - ax) * ix1;
+      const float wy0 = ay * iy0, wy1 = (1.f - ay) * iy1;
+      const float wz0 = charge * az * iz0, wz1 = charge * (1.f - az) * iz1;
       const int lx = i0 - anc[0], ly = j0 - anc[1], lz = k0 - anc[2];
       if ((unsigned)lx <= kCicW - 2 && (unsigned)ly <= kCicW - 2 && (unsigned)lz <= kCicW - 2) {
         float fx[kCicW], fy[kCicW], fz[kCicW];
