@@ -119,6 +119,8 @@ typedef struct vlb_step_params {
   int32_t use_graph;           /* 1: replay the step as one captured CUDA graph */
   int32_t poisson_precision;   /* VLB_POISSON_FP32, _3XTF32 or _BF16X3, every mode product of the step */
   int32_t denoise;             /* 1: the learned denoiser on the fine density (vlb_set_denoiser) */
+  int32_t energy;              /* 1: the energy budget's two sums (step!(sim; energy=true)) */
+  int32_t pad_;
 } vlb_step_params;
 
 /* Device-side error flags (vlb_step_result.status, vlb_dn_status). */
@@ -145,6 +147,8 @@ typedef struct vlb_step_result {
   int32_t status;              /* device-side error flags (VLB_STATUS_*), 0 when clean */
   int32_t denoised;            /* 1: the step used the denoiser's density, 0: the deposit's */
   int32_t pad_;
+  double hartree;              /* energy steps: 1/2 sum w phi_H at the step's positions (src/simulation.jl:511) */
+  double interaction;          /* energy steps: sum w phi at the advanced positions (src/simulation.jl:393) */
 } vlb_step_result;
 
 /* Grid selectors for vlb_get_grid / vlb_set_grid. */
@@ -154,6 +158,8 @@ typedef struct vlb_step_result {
 #define VLB_GRID_PHI_COARSE 3
 #define VLB_GRID_CSOL_FINE 4
 #define VLB_GRID_CSOL_COARSE 5
+#define VLB_GRID_CSOL_HARTREE_FINE 6    /* S^-1 phi_H of the last step run with params.energy */
+#define VLB_GRID_CSOL_HARTREE_COARSE 7  /* S^-1 phi_H of the last solve */
 
 /* Precision of the mode products (the tensor solves and the S^-1 conversions):
  * FP32 on the CUDA cores, or split-precision 3xTF32 on the tensor cores with
@@ -320,6 +326,17 @@ VLB_API int vlb_dn_status(vlb_denoiser* dn, int32_t* flags);
  * tile whose largest |x| exceeds 1e-3 of the volume's (the others pass
  * through unchanged) */
 VLB_API int vlb_dn_active_tiles(vlb_denoiser* dn, int32_t* n);
+
+/* ---- the energy budget's sums (interaction_energy, src/energy.jl:19-43):
+ * sum over the cloud of w phi(p), phi the smoothed fine potential inside the
+ * host margin knots[3] < p < knots[end-2], the coarse spline outside it, 0
+ * outside both, for the total coefficients (csol, as after a step) or the
+ * Hartree ones (S^-1 phi before the mean field; the fine level's are those
+ * of the last step run with params.energy).  The cloud may have moved since
+ * its last sort (as after a push).  Synchronises. */
+#define VLB_ENERGY_TOTAL 0
+#define VLB_ENERGY_HARTREE 1
+VLB_API int vlb_interaction_energy(vlb_ctx* ctx, int32_t coefficients, double* out);
 
 /* ---- launch shapes.  No counterpart in the reference (whose kernels take
  * fixed workgroup sizes, src/accelerator.jl:253-259).  chunk: particles per

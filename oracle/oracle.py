@@ -85,6 +85,7 @@ def lib():
             "orc_deposit_smoothed_host": (ll, [pl, ps, ll, P_D, dbl, P_D]),
             "orc_deposit_cic_host": (ll, [pl, ll, P_D, dbl, P_D]),
             "orc_forces_host": (ll, [pl, pl, ps, ll, P_D, P_D, P_D, dbl, ll, P_D]),
+            "orc_interaction_energy": (dbl, [pl, pl, ps, ll, P_D, P_D, P_D, dbl, dbl]),
             "orc_projectile_forces_host": (None, [ll, P_D, P_D, pp, dbl, dbl, dbl, P_D, P_D, P_D]),
             "orc_verlet_host": (None, [ll, P_D, P_D, P_D, dbl, dbl, dbl, P_D]),
             "orc_enclosed_charge_host": (dbl, [ll, P_D, dbl, P_D, dbl]),

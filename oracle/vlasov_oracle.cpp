@@ -953,6 +953,64 @@ long long orc_forces_host(const orc_level* F, const orc_level* C, const orc_smoo
   return nout;
 }
 
+// smoothed_potential (src/fields.jl:405-429): the 10^3 overlap-weighted sum
+// of csol around p's nearest knots.
+double smoothed_potential(const orc_level* F, const orc_smoothing* sm, const double* csolf, const double* p) {
+  const double* g = F->knots;
+  const int n = F->n, nk = F->nk;
+  int b[3], col[3];
+  for (int d = 0; d < 3; ++d) {
+    const int ci = nearest_knot(g, nk, p[d]);
+    b[d] = 2 * ci - 5;
+    col[d] = (int)std::floor((p[d] - g[ci - 1] + sm->spacing / 2) / sm->spacing * sm->nbdt + 0.5) + 1;
+  }
+  const double* ox = sm->overlap + 10 * (size_t)(col[0] - 1);
+  const double* oy = sm->overlap + 10 * (size_t)(col[1] - 1);
+  const double* oz = sm->overlap + 10 * (size_t)(col[2] - 1);
+  double phi = 0;
+  for (int kk = 0; kk < 10; ++kk) {
+    const int k = b[2] + kk - 1;
+    for (int jj = 0; jj < 10; ++jj) {
+      const int j = b[1] + jj - 1;
+      const double wyz = oy[jj] * oz[kk];
+      const double* row = csolf + (size_t)(b[0] - 1) + (size_t)n * (j + (size_t)n * k);
+      double s = 0;
+      for (int ii = 0; ii < 10; ++ii) s += row[ii] * ox[ii];
+      phi += s * wyz;
+    }
+  }
+  return phi;
+}
+
+extern "C" {
+
+// interaction_energy (src/energy.jl:19-43): sum of w phi(p) over the
+// particles, phi the smoothed fine potential inside the host margin, the
+// coarse spline outside it, enclosed / r outside both.  pos AoS [3N].
+double orc_interaction_energy(const orc_level* F, const orc_level* C, const orc_smoothing* sm, long long N,
+                              const double* pos, const double* csolf, const double* csolc, double w,
+                              double enclosed) {
+  const double* g = F->knots;
+  const double lo = g[2], hi = g[F->nk - 3];
+  double total = 0;
+#pragma omp parallel for schedule(static) reduction(+ : total)
+  for (long long i = 0; i < N; ++i) {
+    const double* p = pos + 3 * i;
+    bool in = true;
+    for (int d = 0; d < 3; ++d) in = in && lo < p[d] && p[d] < hi;
+    double phi;
+    if (in) {
+      phi = smoothed_potential(F, sm, csolf, p);
+    } else if (!spline_potential(C->knots, C->nk, csolc, C->n, p[0], p[1], p[2], &phi)) {
+      phi = enclosed / std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    }
+    total += w * phi;
+  }
+  return total;
+}
+
+}  // extern "C"
+
 // projectile_forces! host (src/projectile.jl:203-232), ball softening, serial.
 void orc_projectile_forces_host(long long N, const double* pos, double* force, const orc_projectile* pr,
                                 double w, double nions, double jel_radius, double F[3], double* e_el, double* e_jel) {

@@ -29,17 +29,21 @@ VLB_GRID_PHI_FINE = 2
 VLB_GRID_PHI_COARSE = 3
 VLB_GRID_CSOL_FINE = 4
 VLB_GRID_CSOL_COARSE = 5
+VLB_GRID_CSOL_HARTREE_FINE = 6
+VLB_GRID_CSOL_HARTREE_COARSE = 7
 
 VLB_POISSON_FP32 = 0
 VLB_POISSON_3XTF32 = 1
 VLB_POISSON_BF16X3 = 2
+VLB_ENERGY_TOTAL = 0
+VLB_ENERGY_HARTREE = 1
 
 # every symbol include/vlasov_b200.h declares
 EXPORTS = (
     "vlb_last_error", "vlb_version", "vlb_create", "vlb_destroy", "vlb_upload_particles",
     "vlb_download_particles", "vlb_sort", "vlb_get_sort", "vlb_deposit_fine", "vlb_deposit_coarse",
     "vlb_poisson", "vlb_set_precision", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
-    "vlb_push", "vlb_step", "vlb_dn_weight_count", "vlb_set_denoiser", "vlb_clear_denoiser", "vlb_dn_create",
+    "vlb_push", "vlb_step", "vlb_interaction_energy", "vlb_dn_weight_count", "vlb_set_denoiser", "vlb_clear_denoiser", "vlb_dn_create",
     "vlb_dn_destroy", "vlb_dn_forward", "vlb_dn_gradient", "vlb_dn_adam", "vlb_dn_status", "vlb_dn_active_tiles", "vlb_set_tuning", "vlb_get_tuning", "vlb_batch_create", "vlb_batch_step",
     "vlb_batch_destroy", "vlb_exchange_buffers", "vlb_step_deposit", "vlb_step_fields", "vlb_step_advance",
     "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
@@ -80,7 +84,8 @@ class StepParams(C.Structure):
     _fields_ = [("dt", C.c_double), ("rcmax", C.c_double), ("jellium_nions", C.c_double),
                 ("jellium_radius", C.c_double), ("capture_radius", C.c_double), ("deposit_mode", C.c_int32),
                 ("advance_projectile", C.c_int32), ("push", C.c_int32), ("use_graph", C.c_int32),
-                ("poisson_precision", C.c_int32), ("denoise", C.c_int32)]
+                ("poisson_precision", C.c_int32), ("denoise", C.c_int32), ("energy", C.c_int32),
+                ("pad_", C.c_int32)]
 
 
 class StepResult(C.Structure):
@@ -88,7 +93,8 @@ class StepResult(C.Structure):
                 ("projectile_force", C.c_double * 3), ("e_electrons", C.c_double), ("e_jellium", C.c_double),
                 ("enclosed_charge", C.c_double), ("total_charge", C.c_double), ("nout", C.c_int32),
                 ("outcount", C.c_int32), ("noccupied", C.c_int32), ("status", C.c_int32),
-                ("denoised", C.c_int32), ("pad_", C.c_int32)]
+                ("denoised", C.c_int32), ("pad_", C.c_int32), ("hartree", C.c_double),
+                ("interaction", C.c_double)]
 
 
 class Exchange(C.Structure):
@@ -151,6 +157,7 @@ def lib():
             "vlb_push": (C.c_int, [vp, C.c_double, C.c_double, P_D]),
             "vlb_step": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams), C.POINTER(StepResult)]),
             "vlb_exchange_buffers": (C.c_int, [vp, C.c_int32, C.POINTER(Exchange)]),
+            "vlb_interaction_energy": (C.c_int, [vp, C.c_int32, P_D]),
             "vlb_dn_weight_count": (C.c_int, []),
             "vlb_set_denoiser": (C.c_int, [vp, P_F, C.c_int32, C.c_double, C.c_double]),
             "vlb_clear_denoiser": (C.c_int, [vp]),

@@ -138,10 +138,8 @@ void setup_level(Level& D, const vlb_level_desc& L, bool coarse) {
   VLB_CUDA(cudaMemset(D.rho, 0, tot * sizeof(float)));
   VLB_CUDA(cudaMemset(D.phi, 0, tot * sizeof(float)));
   VLB_CUDA(cudaMemset(D.csol, 0, tot * sizeof(float)));
-  if (coarse) {
-    D.csol_hartree = dalloc<float>(tot);
-    VLB_CUDA(cudaMemset(D.csol_hartree, 0, tot * sizeof(float)));
-  }
+  D.csol_hartree = dalloc<float>(tot);
+  VLB_CUDA(cudaMemset(D.csol_hartree, 0, tot * sizeof(float)));
 }
 
 void free_level(Level& D) {
@@ -171,6 +169,7 @@ void destroy_ctx(Ctx* c) {
   dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off); dfree(c->occupied); dfree(c->bounds);
   dfree(c->outlist); dfree(c->chunk_start); dfree(c->item_cell); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
   dfree(c->rho_fixed_c); dfree(c->red_items); dfree(c->red_tail); dfree(c->red_blocks); dfree(c->diag_part);
+  dfree(c->e_items); dfree(c->e_blocks);
   for (auto& w : c->work) dfree(w);
   free_denoiser(*c);
   dfree(c->tc_sync);
@@ -197,6 +196,8 @@ float* grid_ptr(Ctx& c, int which) {
     case VLB_GRID_PHI_COARSE: return c.coarse.phi;
     case VLB_GRID_CSOL_FINE: return c.fine.csol;
     case VLB_GRID_CSOL_COARSE: return c.coarse.csol;
+    case VLB_GRID_CSOL_HARTREE_FINE: return c.fine.csol_hartree;
+    case VLB_GRID_CSOL_HARTREE_COARSE: return c.coarse.csol_hartree;
     default: throw ArgError("unknown grid selector");
   }
 }
@@ -278,6 +279,11 @@ void enqueue_phase_fields(Ctx& c, const vlb_step_params& p, int64_t normalize_np
   }
   launch_poisson(c);
   stage_mark(c, 4);
+  if (p.energy) {
+    // the Hartree energy, on the Hartree potential alone (src/simulation.jl:505-513)
+    launch_coefficients(c, c.fine, c.fine.phi, c.fine.csol_hartree);
+    launch_energy(c, c.fine.csol_hartree, c.coarse.csol_hartree, &c.dsc->energy[0]);
+  }
   launch_mean_field_coefficients(c, c.fine, c.fine.phi, c.fine.csol, p.jellium_nions, p.jellium_radius);
   launch_mean_field_coefficients(c, c.coarse, c.coarse.phi, c.coarse.csol, p.jellium_nions, p.jellium_radius);
   stage_mark(c, 5);
@@ -291,6 +297,9 @@ void enqueue_phase_advance(Ctx& c, const vlb_step_params& p) {
   if (p.push) launch_push(c, p.dt, p.rcmax, p.capture_radius, true);
   stage_mark(c, 8);
   if (!p.push && p.capture_radius > 0) launch_enclosed(c, p.capture_radius);
+  // the interaction with the total potential at the advanced positions
+  // (src/simulation.jl:393-394)
+  if (p.energy) launch_energy(c, c.fine.csol, c.coarse.csol, &c.dsc->energy[1]);
   stage_mark(c, 9);
 }
 
@@ -304,7 +313,7 @@ bool same_params(const vlb_step_params& a, const vlb_step_params& b) {
   return a.dt == b.dt && a.rcmax == b.rcmax && a.jellium_nions == b.jellium_nions &&
          a.jellium_radius == b.jellium_radius && a.capture_radius == b.capture_radius &&
          a.deposit_mode == b.deposit_mode && a.advance_projectile == b.advance_projectile && a.push == b.push &&
-         a.poisson_precision == b.poisson_precision && a.denoise == b.denoise;
+         a.poisson_precision == b.poisson_precision && a.denoise == b.denoise && a.energy == b.energy;
 }
 
 // Two graphs, one per parity of the sort's double buffer: the step moves
@@ -441,6 +450,8 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->red_items = dalloc<double>(4 * (size_t)(N / kMinChunk + c->ncell + 1));
     c->red_tail = dalloc<double>(4 * (size_t)c->num_sms);
     c->red_blocks = dalloc<double>(4 * (size_t)c->num_sms);
+    c->e_items = dalloc<double>((size_t)(N / kMinChunk + c->ncell + 1));
+    c->e_blocks = dalloc<double>((size_t)c->num_sms);
     c->diag_part = dalloc<double>(5 * (size_t)c->num_sms * 32);
     c->partials = dalloc<double>(10 * (size_t)std::max(nf, nc) * std::max(nf, nc));
     for (auto& w : c->work) w = dalloc<float>(maxg);
@@ -493,6 +504,7 @@ int vlb_upload_particles(vlb_ctx* ctx, const int32_t* knode, const float* delta,
     }
     VLB_CUDA(cudaStreamSynchronize(c.stream));
     c.sorted = false;
+    c.items_valid = false;
     c.keys_ready = false;
     return VLB_OK;
   });
@@ -719,6 +731,8 @@ void collect_step(Ctx& c, vlb_projectile* proj, const vlb_step_params* params, v
     result->noccupied = h.noccupied;
     result->status = h.status;
     result->denoised = h.denoised;
+    result->hartree = params->energy ? 0.5 * h.energy[0] : 0.0;
+    result->interaction = params->energy ? h.energy[1] : 0.0;
   }
   if (!params->push) c.sorted = true;  // forces-only: the cloud did not move
 }
@@ -796,6 +810,22 @@ int vlb_clear_denoiser(vlb_ctx* ctx) {
   });
 }
 
+// ------------------------------------------------------------ energy
+int vlb_interaction_energy(vlb_ctx* ctx, int32_t coefficients, double* out) {
+  CTX_OR_FAIL;
+  if (!out || (coefficients != VLB_ENERGY_TOTAL && coefficients != VLB_ENERGY_HARTREE))
+    return fail(VLB_ERR_ARG, "vlb_interaction_energy: bad arguments");
+  if (!c.items_valid) return fail(VLB_ERR_STATE, "interaction energy before any sort of the cloud");
+  return guarded([&]() -> int {
+    const int which = coefficients == VLB_ENERGY_HARTREE ? 0 : 1;
+    launch_energy(c, which ? c.fine.csol : c.fine.csol_hartree, which ? c.coarse.csol : c.coarse.csol_hartree,
+                  &c.dsc->energy[which]);
+    fetch_scalars(c);
+    *out = c.hsc->energy[which];
+    return status_code(c);
+  });
+}
+
 // ------------------------------------------------------------ tuning
 int vlb_set_tuning(vlb_ctx* ctx, const vlb_tuning* t) {
   CTX_OR_FAIL;
@@ -813,6 +843,7 @@ int vlb_set_tuning(vlb_ctx* ctx, const vlb_tuning* t) {
   c.graph_valid = false;  // the captured step has the old launch shapes
   ++c.config_epoch;
   c.sorted = false;       // the work items follow the chunk
+  c.items_valid = false;
   return VLB_OK;
 }
 

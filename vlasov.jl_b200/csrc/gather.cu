@@ -396,6 +396,167 @@ __global__ void __launch_bounds__(kGThreads) k_tail(const int32_t* __restrict__ 
   block_red(ax, ay, az, ae, red_tail + 4 * blockIdx.x);
 }
 
+// ---------------------------------------------------------------- energy
+// The interaction energy sum_p w phi(p) of interaction_energy
+// (src/energy.jl:19-43) with phi the potential of the coefficients `csolf`
+// (fine) and `csolc` (coarse): inside the host margin knots[3] < p <
+// knots[end-2] (every axis) the smoothed potential of smoothed_potential
+// (src/fields.jl:405-429, the 10^3 overlap-weighted sum at the nearest
+// knots), else the coarse spline's value, else 0 (the reference's call
+// passes no enclosed charge).
+//
+// One warp per work item of the last sort.  Between that sort and this
+// call the cloud may have moved (the energy of the total potential is taken
+// after the push), so the warp stages the 14^3 coefficients around its cell:
+// the stencils of the cell and of its neighbours one knot away.  A particle
+// further away, or inside the margin from a cell whose stencil does not fit
+// the grid, reads its stencil from global memory.  Positions are rebuilt in
+// float64 as the host does; the 10^3 sum is FP32, the sums over particles
+// float64, one per work item, reduced in a fixed order.
+constexpr int kEW = 14;
+constexpr int kEThreads = 128;
+
+__device__ __forceinline__ float smoothed_sum(const float* __restrict__ c, int sy, int sz, const float (&ox)[10],
+                                              const float (&oy)[10], const float (&oz)[10]) {
+  float phi = 0.f;
+#pragma unroll 2
+  for (int kk = 0; kk < 10; ++kk) {
+#pragma unroll
+    for (int jj = 0; jj < 10; ++jj) {
+      const float* row = c + jj * sy + kk * sz;
+      float sx = 0.f;
+#pragma unroll
+      for (int ii = 0; ii < 10; ++ii) sx = fmaf(row[ii], ox[ii], sx);
+      phi = fmaf(sx, oy[jj] * oz[kk], phi);
+    }
+  }
+  return phi;
+}
+
+__global__ void __launch_bounds__(kEThreads) k_energy(
+    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
+    const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int64_t Npad,
+    const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ csolf, int n, int nk,
+    const float* __restrict__ ov, int nbdt, int ncol, float spacing, double x0, double h, double lo, double hi,
+    const float* __restrict__ csolc, const double* __restrict__ kc, int nkc, int nc, double w, int chunk,
+    double* __restrict__ e_items) {
+  __shared__ float tiles[kEThreads / 32][kEW * kEW * kEW];
+  const int lane = threadIdx.x & 31;
+  float* tile = tiles[threadIdx.x >> 5];
+  const int nitems = dsc->nitems;
+  int cached = -1;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = (int)atomicAdd(&dsc->work_energy, 1ull);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nitems) break;
+    const int g = item_cell[item];
+    int kx, ky, kz;
+    cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
+    // 0-based corner of the 14^3 block: the cell's stencil corner 2k - 6, less two
+    const int cx0 = 2 * kx - 8, cy0 = 2 * ky - 8, cz0 = 2 * kz - 8;
+    if (g != cached) {
+      __syncwarp();
+      for (int e = lane; e < kEW * kEW * kEW; e += 32) {
+        const int i = cx0 + e % kEW, j = cy0 + (e / kEW) % kEW, kk = cz0 + e / (kEW * kEW);
+        tile[e] = (i >= 0 && j >= 0 && kk >= 0 && i < n && j < n && kk < n)
+                      ? csolf[(size_t)i + (size_t)n * (j + (size_t)n * kk)]
+                      : 0.f;
+      }
+      cached = g;
+      __syncwarp();
+    }
+    const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
+    const int s1 = min(s0 + chunk, bounds[g + 1]);
+    double e = 0.0;
+    for (int s = s0 + lane; s < s1; s += 32) {
+      const int kp[3] = {k[s], k[Npad + s], k[2 * Npad + s]};
+      const float dp[3] = {d[s], d[Npad + s], d[2 * Npad + s]};
+      double p[3];
+      bool inside = true;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        p[a] = x0 + (double)(kp[a] - 1) * h + (double)dp[a];
+        inside = inside && lo < p[a] && p[a] < hi;
+      }
+      double phi = 0.0;
+      if (inside) {
+        float ox[10], oy[10], oz[10];
+        {
+          const float* t0 = ov + (size_t)(table_column(dp[0], spacing, nbdt, ncol) - 1) * 10;
+          const float* t1 = ov + (size_t)(table_column(dp[1], spacing, nbdt, ncol) - 1) * 10;
+          const float* t2 = ov + (size_t)(table_column(dp[2], spacing, nbdt, ncol) - 1) * 10;
+#pragma unroll
+          for (int a = 0; a < 10; ++a) {
+            ox[a] = __ldg(t0 + a);
+            oy[a] = __ldg(t1 + a);
+            oz[a] = __ldg(t2 + a);
+          }
+        }
+        // stencil corner of the particle's own nearest knots, in the block
+        const int bx = 2 * kp[0] - 6 - cx0, by = 2 * kp[1] - 6 - cy0, bz = 2 * kp[2] - 6 - cz0;
+        if (bx >= 0 && by >= 0 && bz >= 0 && bx <= kEW - 10 && by <= kEW - 10 && bz <= kEW - 10)
+          phi = smoothed_sum(tile + bx + kEW * (by + kEW * bz), kEW, kEW * kEW, ox, oy, oz);
+        else
+          phi = smoothed_sum(csolf + (size_t)(2 * kp[0] - 6) + (size_t)n * ((2 * kp[1] - 6) + (size_t)n * (2 * kp[2] - 6)),
+                             n, n * n, ox, oy, oz);
+      } else {
+        const int ix = cell_index_d(kc, nkc, p[0]), iy = cell_index_d(kc, nkc, p[1]), iz = cell_index_d(kc, nkc, p[2]);
+        if (ix && iy && iz) {
+          double vx[4], vy[4], vz[4], dd;
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            basis_vd(kc, nkc, 2 * (ix - 1) + a + 1, p[0], vx[a], dd);
+            basis_vd(kc, nkc, 2 * (iy - 1) + a + 1, p[1], vy[a], dd);
+            basis_vd(kc, nkc, 2 * (iz - 1) + a + 1, p[2], vz[a], dd);
+          }
+          for (int ak = 0; ak < 4; ++ak)
+            for (int aj = 0; aj < 4; ++aj) {
+              const float* row =
+                  csolc + (size_t)2 * (ix - 1) + (size_t)nc * ((2 * (iy - 1) + aj) + (size_t)nc * (2 * (iz - 1) + ak));
+              const double wyz = vy[aj] * vz[ak];
+#pragma unroll
+              for (int ai = 0; ai < 4; ++ai) phi += (double)row[ai] * vx[ai] * wyz;
+            }
+        }
+      }
+      e += w * phi;
+    }
+    e = warp_sum(e);
+    if (lane == 0) e_items[item] = e;
+  }
+}
+
+// Two levels of an order-fixed sum of one component: block b sums its
+// contiguous share of the items, then one block the block sums.
+__device__ __forceinline__ double block_sum1(const double* __restrict__ p, int begin, int end) {
+  __shared__ double sh[256];
+  const int t = threadIdx.x;
+  double s = 0;
+  for (int i = begin + t; i < end; i += blockDim.x) s += p[i];
+  sh[t] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (t < o) sh[t] += sh[t + o];
+    __syncthreads();
+  }
+  return sh[0];
+}
+
+__global__ void __launch_bounds__(256) k_energy_blocks(const double* __restrict__ items, const DeviceScalars* dsc,
+                                                       double* __restrict__ block_out) {
+  const int nitems = dsc->nitems;
+  const int per = (nitems + gridDim.x - 1) / gridDim.x;
+  const int b0 = min(nitems, (int)blockIdx.x * per), b1 = min(nitems, b0 + per);
+  const double r = block_sum1(items, b0, b1);
+  if (threadIdx.x == 0) block_out[blockIdx.x] = r;
+}
+
+__global__ void __launch_bounds__(256) k_energy_total(const double* __restrict__ blocks, int nblocks, double* out) {
+  const double r = block_sum1(blocks, 0, nblocks);
+  if (threadIdx.x == 0) *out = r;
+}
+
 }  // namespace
 
 void launch_forces(Ctx& c) {
@@ -417,6 +578,24 @@ void launch_forces(Ctx& c) {
   k_red_total<<<1, 256, 0, c.stream>>>(c.red_blocks, c.num_sms, c.red_tail, c.num_sms, c.dsc);
   VLB_LAUNCHED(c);
   c.have_forces = true;
+}
+
+// The interaction energy of the coefficients (csolf, csolc) over the cloud
+// as it is, into *out; the work items of the last sort.
+void launch_energy(Ctx& c, const float* csolf, const float* csolc, double* out) {
+  Level& F = c.fine;
+  Level& C = c.coarse;
+  Particles& P = c.part[c.cur];
+  VLB_CUDA(cudaMemsetAsync(&c.dsc->work_energy, 0, sizeof(unsigned long long), c.stream));
+  k_energy<<<c.num_sms * 4, kEThreads, 0, c.stream>>>(
+      c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.k, P.d, csolf, F.n, F.nk, c.overlap, c.nbdt,
+      c.ncol, c.spacing_f, c.x0, c.h, F.h_knots[2], F.h_knots[F.nk - 3], csolc, C.knots_d, C.nk, C.n, c.weight,
+      c.chunk, c.e_items);
+  VLB_LAUNCHED(c);
+  k_energy_blocks<<<c.num_sms, 256, 0, c.stream>>>(c.e_items, c.dsc, c.e_blocks);
+  VLB_LAUNCHED(c);
+  k_energy_total<<<1, 256, 0, c.stream>>>(c.e_blocks, c.num_sms, out);
+  VLB_LAUNCHED(c);
 }
 
 }  // namespace vlb

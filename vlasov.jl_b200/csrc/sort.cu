@@ -479,6 +479,7 @@ void launch_sort(Ctx& c) {
   VLB_LAUNCHED(c);
   c.cur ^= 1;
   c.sorted = true;
+  c.items_valid = true;
 }
 
 }  // namespace vlb

@@ -54,6 +54,8 @@ struct DeviceScalars {
                                      // [1] charge of the denoiser's prediction (not exchanged)
   int32_t denoised;                  // 1: the step used the denoiser's density
   int32_t pad_dn;
+  unsigned long long work_energy;    // work counter of the energy kernel
+  double energy[2];                  // sum w phi: [0] on the Hartree coefficients, [1] on the total
   int32_t reset_end;
   int32_t pad0;
   // --- persistent ---
@@ -88,7 +90,7 @@ struct Level {
   float* rho = nullptr;
   float* phi = nullptr;
   float* csol = nullptr;
-  float* csol_hartree = nullptr;    // coarse only: S^-1 phi before the mean field
+  float* csol_hartree = nullptr;    // S^-1 phi before the mean field (coarse: every step; fine: energy steps)
   // host copies kept for reference
   std::vector<double> h_knots, h_colloc;
 };
@@ -146,6 +148,9 @@ struct Ctx {
   double* red_items = nullptr;                // [max items][4]
   double* red_tail = nullptr;                 // [num_sms][4]
   double* red_blocks = nullptr;               // [num_sms][4] first level of their sum
+  double* e_items = nullptr;                  // [max items] interaction energy per work item
+  double* e_blocks = nullptr;                 // [num_sms] first level of their sum
+  bool items_valid = false;                   // the work items describe the cloud (its last sort)
   double* diag_part = nullptr;                // [num_sms * 32][5]
   double* partials = nullptr;                 // [10 * n^2] reductions
   // Poisson work buffers (max n^3)
@@ -218,6 +223,7 @@ void launch_mean_field_coefficients(Ctx& c, Level& L, const float* phi, float* c
 void launch_mean_field_add(Ctx& c, Level& L, double nions, double radius);
 // gather.cu
 void launch_forces(Ctx& c);
+void launch_energy(Ctx& c, const float* csolf, const float* csolc, double* out);
 // push.cu
 void launch_projectile_update(Ctx& c, double dt, double nions, double jradius, int advance);
 void launch_projectile_force_only(Ctx& c, double nions, double jradius);

@@ -134,6 +134,8 @@ class ShardedDiagnostics:
     outcount: int
     projectile_force: tuple
     status: int
+    hartree: float = 0.0        # energy steps: the energy budget's sums over the ranks
+    interaction: float = 0.0
 
 
 class ShardedStepper:
@@ -176,16 +178,16 @@ class ShardedStepper:
             b.step_fields(params, self.npart_global)
         self._sum([[b.reaction_buffer()] for b in bs])
         rs = [b.step_advance(p, params) for b, p in zip(bs, projs)]
-        local = [0.0] * 9
+        local = [0.0] * 11
         for r in rs:
             vals = [r.kinetic, r.escaped, *r.angular, r.enclosed_charge, float(r.nout), float(r.outcount),
-                    float(r.status != 0)]
+                    float(r.status != 0), getattr(r, "hartree", 0.0), getattr(r, "interaction", 0.0)]
             local = [x + y for x, y in zip(local, vals)]
         t = bs[0].tensor(local)
         self.comm.all_reduce_sum(t)
         g = [float(v) for v in t.tolist()]
         return ShardedDiagnostics(g[0], g[1], tuple(g[2:5]), g[5], int(round(g[6])), int(round(g[7])),
-                                  tuple(rs[0].projectile_force), int(g[8] != 0))
+                                  tuple(rs[0].projectile_force), int(g[8] != 0), g[9], g[10])
 
 
 def _synchronize_all(backends):
@@ -250,7 +252,7 @@ class ShardedSimulation:
     def _deposit_mode(self):
         return L.VLB_DEPOSIT_FIXED64 if self.fixed_point else L.VLB_DEPOSIT_FLOAT32
 
-    def _params(self, *, advance: bool, push: bool, capture: float) -> L.StepParams:
+    def _params(self, *, advance: bool, push: bool, capture: float, energy: bool = False) -> L.StepParams:
         sp = L.StepParams()
         sp.dt = self.params.dt
         sp.rcmax = self.params.rcmax
@@ -262,6 +264,7 @@ class ShardedSimulation:
         sp.push = int(push)
         sp.use_graph = 0
         sp.poisson_precision = self.precision
+        sp.energy = int(energy and push)
         return sp
 
     def prime_leapfrog(self, positions, momenta):
@@ -283,9 +286,11 @@ class ShardedSimulation:
         pk, pd = S.pack_positions(back, self.x0, self.h)
         acc.upload(k, d, pk, pd)
 
-    def step(self) -> ShardedDiagnostics:
+    def step(self, energy: bool = False) -> ShardedDiagnostics:
+        """With energy, the diagnostics carry the budget's two sums over the
+        whole cloud (S.EnergyBudget.of(sim.jellium, d))."""
         return self.stepper.step(self.projectile,
-                                 self._params(advance=True, push=True, capture=self.capture_radius))
+                                 self._params(advance=True, push=True, capture=self.capture_radius, energy=energy))
 
     def close(self):
         self.accelerator.close()

@@ -451,6 +451,12 @@ class DeviceAccelerator:
     def profile(self, on: bool):
         L.check(L.lib().vlb_profile(self._h, int(on)))
 
+    def interaction_energy(self, coefficients: int = L.VLB_ENERGY_TOTAL) -> float:
+        """sum w phi over the cloud as it is (interaction_energy, src/energy.jl:19-43)."""
+        out = C.c_double()
+        L.check(L.lib().vlb_interaction_energy(self._h, int(coefficients), C.byref(out)))
+        return out.value
+
     def stage_times(self) -> dict:
         n = L.lib().vlb_stage_count()
         ms = np.zeros(12)
@@ -477,6 +483,29 @@ class StepDiagnostics:
     total_charge: float
     status: int = 0
     denoised: int = 0            # 1: the step's fine density came from the learned denoiser
+    hartree: float = 0.0         # energy steps: 1/2 sum w phi_H at the step's positions
+    interaction: float = 0.0     # energy steps: sum w phi at the advanced positions
+
+
+@dataclass
+class EnergyBudget:
+    """The energy of the system after a step (EnergyBudget,
+    src/energy.jl:69-79): total = ions + kinetic + hartree + meanfield, the
+    mean field by difference, meanfield = interaction - 2 hartree
+    (energy_budget, src/energy.jl:111-117)."""
+    total: float
+    kinetic: float
+    hartree: float
+    meanfield: float
+    ions: float
+    escaped: float
+
+    @staticmethod
+    def of(jellium: "Jellium", d: "StepDiagnostics") -> "EnergyBudget":
+        meanfield = d.interaction - 2 * d.hartree
+        ions = 3 * jellium.nions ** 2 / (5 * jellium.radius)   # ion_self_energy, src/energy.jl:51
+        return EnergyBudget(ions + d.kinetic + d.hartree + meanfield, d.kinetic, d.hartree, meanfield, ions,
+                            d.escaped)
 
 
 class Simulation:
@@ -509,7 +538,7 @@ class Simulation:
     def mass(self):
         return ELECTRON_MASS * self.weight
 
-    def _params(self, *, advance: bool, push: bool, capture: float) -> L.StepParams:
+    def _params(self, *, advance: bool, push: bool, capture: float, energy: bool = False) -> L.StepParams:
         sp = L.StepParams()
         sp.dt = self.params.dt
         sp.rcmax = self.params.rcmax
@@ -522,6 +551,7 @@ class Simulation:
         sp.use_graph = int(self.use_graph and push)
         sp.poisson_precision = self.precision
         sp.denoise = int(self.denoise and push)
+        sp.energy = int(energy and push)
         return sp
 
     def prime_leapfrog(self, positions, momenta, consistent: bool = False):
@@ -544,13 +574,20 @@ class Simulation:
         pk, pd = pack_positions(back, self.x0, self.h)
         acc.upload(k, d, pk, pd)
 
-    def step(self) -> StepDiagnostics:
-        """step!(sim; energy=false) on the device."""
+    def step(self, energy: bool = False) -> StepDiagnostics:
+        """step!(sim; energy) on the device.  With energy, the diagnostics
+        carry the budget's two sums (EnergyBudget.of(sim.jellium, d) is the
+        reference's return value)."""
         r = self.accelerator.fused_step(self.projectile, self._params(advance=True, push=True,
-                                                                      capture=self.capture_radius))
+                                                                      capture=self.capture_radius, energy=energy))
         self.steps_done += 1
         return StepDiagnostics(r.kinetic, r.escaped, tuple(r.angular), r.enclosed_charge, r.nout, r.outcount,
-                               r.noccupied, tuple(r.projectile_force), r.total_charge, r.status, r.denoised)
+                               r.noccupied, tuple(r.projectile_force), r.total_charge, r.status, r.denoised,
+                               r.hartree, r.interaction)
+
+    def energy_budget(self, d: StepDiagnostics) -> EnergyBudget:
+        """The EnergyBudget of a step run with energy=True."""
+        return EnergyBudget.of(self.jellium, d)
 
     def run(self, nsteps: int | None = None, callback=None):
         nsteps = self.params.nsteps if nsteps is None else nsteps
