@@ -301,6 +301,23 @@ def main():
     step_h2d = 112  # vlb_projectile in
     step_d2h = 480  # the step's scalar block out
 
+    # the same steps with the energy budget's two sums (step!(sim; energy=true))
+    energy = None
+    if world == 1:
+        for _ in range(max(args.warmup, 3)):
+            sim.step(energy=True)
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record(ext)
+        for _ in range(args.steps):
+            de = sim.step(energy=True)
+        h1.record(ext)
+        h1.synchronize()
+        energy_ms = h0.elapsed_time(h1) / args.steps
+        b = sim.energy_budget(de)
+        energy = {"ms_per_step": energy_ms, "vs_plain": energy_ms / ms, "steps": args.steps,
+                  "last_budget": {"total": b.total, "kinetic": b.kinetic, "hartree": b.hartree,
+                                  "meanfield": b.meanfield, "ions": b.ions}}
+
     # the same steps with the learned denoiser after the fine deposit
     learned = None
     if world == 1 and not args.no_learned and args.nfine == 64:
@@ -366,6 +383,8 @@ def main():
     }
     if learned:
         line["learned"] = learned
+    if energy:
+        line["energy_step"] = energy
     if cpu:
         line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)

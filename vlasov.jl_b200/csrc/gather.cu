@@ -416,19 +416,31 @@ __global__ void __launch_bounds__(kGThreads) k_tail(const int32_t* __restrict__ 
 constexpr int kEW = 14;
 constexpr int kEThreads = 128;
 
+// sum_{ii,jj,kk} c[ii + sy jj + sz kk] ox[ii] oy[jj] oz[kk] (c 8-byte aligned,
+// sy and sz even): y first into five packed accumulators per plane, then x,
+// then z, as the gather contracts.
 __device__ __forceinline__ float smoothed_sum(const float* __restrict__ c, int sy, int sz, const float (&ox)[10],
                                               const float (&oy)[10], const float (&oz)[10]) {
+  float2 ox2[5];
+#pragma unroll
+  for (int a = 0; a < 5; ++a) ox2[a] = make_float2(ox[2 * a], ox[2 * a + 1]);
   float phi = 0.f;
 #pragma unroll 2
   for (int kk = 0; kk < 10; ++kk) {
+    float2 y2[5];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) y2[a] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int jj = 0; jj < 10; ++jj) {
-      const float* row = c + jj * sy + kk * sz;
-      float sx = 0.f;
+      const float2* row = reinterpret_cast<const float2*>(c + jj * sy + kk * sz);
+      const float2 w = make_float2(oy[jj], oy[jj]);
 #pragma unroll
-      for (int ii = 0; ii < 10; ++ii) sx = fmaf(row[ii], ox[ii], sx);
-      phi = fmaf(sx, oy[jj] * oz[kk], phi);
+      for (int a = 0; a < 5; ++a) y2[a] = __ffma2_rn(row[a], w, y2[a]);
     }
+    float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) t = __ffma2_rn(ox2[a], y2[a], t);
+    phi = fmaf(oz[kk], t.x + t.y, phi);
   }
   return phi;
 }

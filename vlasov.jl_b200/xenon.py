@@ -22,9 +22,11 @@ import time
 
 def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point: bool = False,
         uniform: bool = False, nsteps: int | None = None, device: int = 0, seed: int = -1, quiet: bool = False,
-        precision: str = "fp32"):
+        precision: str = "fp32", energy_every: int = 0):
     """Runs the crossing; returns a dict with the capture curve (q(<8) and
-    outcount after every step), the final charge and the timing."""
+    outcount after every step), the final charge and the timing, and with
+    energy_every > 0 the energy budget of every energy_every-th step
+    (run!(sim; energy_every), src/simulation.jl:419-440)."""
     import numpy as np
     from . import simulation as S
 
@@ -46,11 +48,18 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
         sys.stdout.flush()
     fs = 41.341373335  # atomic units of time per femtosecond
     q, out, xs = np.zeros(nsteps), np.zeros(nsteps, dtype=np.int64), np.zeros(nsteps)
+    budgets = []
     acc = sim.accelerator
     t_run = time.time()
     tprev = t_run
     for s in range(1, nsteps + 1):
-        d = sim.step()
+        energy = energy_every > 0 and (s - 1) % energy_every == 0
+        d = sim.step(energy=energy)
+        if energy:
+            b = sim.energy_budget(d)
+            budgets.append({"step": s, "total": b.total, "kinetic": b.kinetic, "hartree": b.hartree,
+                            "meanfield": b.meanfield, "ions": b.ions, "escaped": b.escaped,
+                            "ion_energy_loss": sim.projectile.energy_loss()})
         q[s - 1] = d.enclosed_charge
         out[s - 1] = d.outcount
         xs[s - 1] = sim.projectile.position[0]
@@ -71,7 +80,7 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
     return {"npart": npart, "nfine": nfine, "nsteps": nsteps, "q8": q.tolist(), "outcount": out.tolist(),
             "x_ion": xs.tolist(), "final_q8": float(q[-1]), "final_outcount": int(out[-1]),
             "wall_s": elapsed, "built_s": built, "fixed_point": fixed_point, "uniform": uniform,
-            "precision": precision}
+            "precision": precision, "energy": budgets}
 
 
 def main(argv=None):
@@ -83,12 +92,13 @@ def main(argv=None):
     ap.add_argument("--uniform", action="store_true", help="uniform-sphere cloud instead of Thomas-Fermi")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "3xtf32", "bf16x3"],
                     help="mode products on the CUDA cores or split-precision on the tensor cores")
+    ap.add_argument("--energy-every", type=int, default=0, help="energy budget every N steps (0: none)")
     ap.add_argument("--json", default=None, help="write the capture curve here")
     a = ap.parse_args(argv)
     if a.nfine % 2:
         ap.error("--nfine must be even")
     r = run(a.particules, a.nfine, fixed_point=a.fixed_point, uniform=a.uniform, nsteps=a.steps,
-            precision=a.precision)
+            precision=a.precision, energy_every=a.energy_every)
     if a.json:
         with open(a.json, "w") as f:
             json.dump(r, f)
