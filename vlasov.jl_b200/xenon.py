@@ -22,11 +22,12 @@ import time
 
 def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point: bool = False,
         uniform: bool = False, nsteps: int | None = None, device: int = 0, seed: int = -1, quiet: bool = False,
-        precision: str = "fp32", energy_every: int = 0):
+        precision: str = "fp32", energy_every: int = 0, isolated: bool = False):
     """Runs the crossing; returns a dict with the capture curve (q(<8) and
     outcount after every step), the final charge and the timing, and with
     energy_every > 0 the energy budget of every energy_every-th step
-    (run!(sim; energy_every), src/simulation.jl:419-440)."""
+    (run!(sim; energy_every), src/simulation.jl:419-440).  isolated: the
+    cluster alone, no projectile (the budget's conservation test)."""
     import numpy as np
     from . import simulation as S
 
@@ -38,8 +39,9 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
     t0 = time.time()
     from . import _lib as L
     prec = {"fp32": L.VLB_POISSON_FP32, "3xtf32": L.VLB_POISSON_3XTF32, "bf16x3": L.VLB_POISSON_BF16X3}[precision]
-    sim = S.Simulation(p, prof, projectile=S.xenon_projectile(v=v, x0=x0, dt=dt), seed=seed,
-                       fixed_point=fixed_point, device=device, precision=prec)
+    proj = None if isolated else S.xenon_projectile(v=v, x0=x0, dt=dt)
+    sim = S.Simulation(p, prof, projectile=proj, seed=seed, fixed_point=fixed_point, device=device,
+                       precision=prec)
     built = time.time() - t0
     if not quiet:
         print(f"Na196 + Xe25+, 500 keV, b = 45 a0 | {npart:.1e} particles, grid {2 * nfine + 2}^3")
@@ -59,13 +61,13 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
             b = sim.energy_budget(d)
             budgets.append({"step": s, "total": b.total, "kinetic": b.kinetic, "hartree": b.hartree,
                             "meanfield": b.meanfield, "ions": b.ions, "escaped": b.escaped,
-                            "ion_energy_loss": sim.projectile.energy_loss()})
+                            "ion_energy_loss": sim.projectile.energy_loss() if sim.projectile else 0.0})
         q[s - 1] = d.enclosed_charge
         out[s - 1] = d.outcount
-        xs[s - 1] = sim.projectile.position[0]
+        xs[s - 1] = sim.projectile.position[0] if sim.projectile else 0.0
         if not quiet and (s % every == 0 or s == nsteps):
             now = time.time()
-            print(f"{s:7d} {s * dt / fs:10.2f} {sim.projectile.position[0]:12.1f} {d.enclosed_charge:10.3f} "
+            print(f"{s:7d} {s * dt / fs:10.2f} {xs[s - 1]:12.1f} {d.enclosed_charge:10.3f} "
                   f"{d.outcount:10d} {1000 * (now - tprev) / every:10.1f}")
             sys.stdout.flush()
             tprev = now
@@ -93,12 +95,13 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp32", choices=["fp32", "3xtf32", "bf16x3"],
                     help="mode products on the CUDA cores or split-precision on the tensor cores")
     ap.add_argument("--energy-every", type=int, default=0, help="energy budget every N steps (0: none)")
+    ap.add_argument("--isolated", action="store_true", help="the cluster alone, without the projectile")
     ap.add_argument("--json", default=None, help="write the capture curve here")
     a = ap.parse_args(argv)
     if a.nfine % 2:
         ap.error("--nfine must be even")
     r = run(a.particules, a.nfine, fixed_point=a.fixed_point, uniform=a.uniform, nsteps=a.steps,
-            precision=a.precision, energy_every=a.energy_every)
+            precision=a.precision, energy_every=a.energy_every, isolated=a.isolated)
     if a.json:
         with open(a.json, "w") as f:
             json.dump(r, f)
