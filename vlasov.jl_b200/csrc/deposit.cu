@@ -356,10 +356,29 @@ __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
     float acc[kCicW3];
 #pragma unroll
     for (int e = 0; e < kCicW3; ++e) acc[e] = 0.f;
+    // the next particle's loads are in flight while this one is added
+    int nk3[3] = {0, 0, 0};
+    float nd3[3] = {0.f, 0.f, 0.f};
+    if (s0 + lane < s1) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        nk3[a] = k[a * Npad + s0 + lane];
+        nd3[a] = d[a * Npad + s0 + lane];
+      }
+    }
     for (int s = s0 + lane; s < s1; s += 32) {
-      const float px = fadd(fadd(x0f, fmul((float)(k[s] - 1), hf)), d[s]);
-      const float py = fadd(fadd(x0f, fmul((float)(k[Npad + s] - 1), hf)), d[Npad + s]);
-      const float pz = fadd(fadd(x0f, fmul((float)(k[2 * Npad + s] - 1), hf)), d[2 * Npad + s]);
+      const int ck[3] = {nk3[0], nk3[1], nk3[2]};
+      const float cd[3] = {nd3[0], nd3[1], nd3[2]};
+      if (s + 32 < s1) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          nk3[a] = k[a * Npad + s + 32];
+          nd3[a] = d[a * Npad + s + 32];
+        }
+      }
+      const float px = fadd(fadd(x0f, fmul((float)(ck[0] - 1), hf)), cd[0]);
+      const float py = fadd(fadd(x0f, fmul((float)(ck[1] - 1), hf)), cd[1]);
+      const float pz = fadd(fadd(x0f, fmul((float)(ck[2] - 1), hf)), cd[2]);
       float ax, ay, az, ix0, ix1, iy0, iy1, iz0, iz1;
       const int ix = cic_locate(AX, anc[0], px, ax, ix0, ix1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
       const int iy = cic_locate(AY, anc[1], py, ay, iy0, iy1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
