@@ -295,12 +295,20 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_upsweep(const uint32_t*
   for (int b = tid; b <= (int)mask; b += kRadixThreads) hist[b] = 0;
   __syncthreads();
   const int64_t tile = blockIdx.x;
-  for (int r = 0; r < kRadixPerWarp / 32; ++r) {
+  constexpr int R = kRadixPerWarp / 32;
+  uint32_t kv[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t e = tile * kRadixTile + (int64_t)w * kRadixPerWarp + r * 32 + lane;
+    kv[r] = e < N ? keys[e] : 0u;
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
     int64_t e = tile * kRadixTile + (int64_t)w * kRadixPerWarp + r * 32 + lane;
     bool valid = e < N;
     unsigned m = __ballot_sync(0xffffffffu, valid);
     if (valid) {
-      uint32_t d = (keys[e] >> shift) & mask;
+      uint32_t d = (kv[r] >> shift) & mask;
       unsigned peers = __match_any_sync(m, d);
       if (lane == __ffs(peers) - 1) atomicAdd(&hist[d], (uint32_t)__popc(peers));
     }
@@ -309,26 +317,38 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_upsweep(const uint32_t*
   for (int b = tid; b <= (int)mask; b += kRadixThreads) table[(int64_t)b * ntiles + tile] = hist[b];
 }
 
+// The tile's scatter.  Its digit bases (one column of the scanned table,
+// strided by the tile count) are staged in shared memory first, their loads
+// in flight with the keys', so that no element waits on a global load for
+// its address.
 __global__ void __launch_bounds__(kRadixThreads) k_radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, int64_t N, int shift, uint32_t mask, const uint32_t* __restrict__ table,
     int64_t ntiles) {
   __shared__ uint32_t whist[kRadixWarps][1 << kMaxDigitBits];
+  __shared__ uint32_t sbase[1 << kMaxDigitBits];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int nb = (int)mask + 1;
+  for (int b = tid; b < nb; b += kRadixThreads) sbase[b] = table[(int64_t)b * ntiles + blockIdx.x];
   for (int b = lane; b < nb; b += 32) whist[w][b] = 0;
   __syncwarp();
   const int64_t tile = blockIdx.x;
   constexpr int R = kRadixPerWarp / 32;
   uint32_t key[R], val[R], local[R];
   unsigned valid_bits = 0;
+  // every load of the thread in flight before the ranking uses them
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t e = tile * kRadixTile + (int64_t)w * kRadixPerWarp + r * 32 + lane;
+    const bool valid = e < N;
+    key[r] = valid ? keys_in[e] : 0u;
+    val[r] = valid ? (vals_in ? vals_in[e] : (uint32_t)e) : 0u;
+  }
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     int64_t e = tile * kRadixTile + (int64_t)w * kRadixPerWarp + r * 32 + lane;
     bool valid = e < N;
     unsigned m = __ballot_sync(0xffffffffu, valid);
-    key[r] = valid ? keys_in[e] : 0u;
-    val[r] = valid ? (vals_in ? vals_in[e] : (uint32_t)e) : 0u;
     local[r] = 0;
     if (valid) {
       valid_bits |= 1u << r;
@@ -361,7 +381,7 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_downsweep(
   for (int r = 0; r < R; ++r) {
     if (!(valid_bits & (1u << r))) continue;
     uint32_t d = (key[r] >> shift) & mask;
-    uint32_t pos = table[(int64_t)d * ntiles + tile] + whist[w][d] + local[r];
+    uint32_t pos = sbase[d] + whist[w][d] + local[r];
     if (keys_out) keys_out[pos] = key[r];
     vals_out[pos] = val[r];
   }
