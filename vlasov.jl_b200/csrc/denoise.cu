@@ -863,7 +863,6 @@ Denoiser* dn_create(int nx, int ny, int nz, int device, int num_sms) {
   if (!attrs) {
     VLB_CUDA(cudaFuncSetAttribute(k_conv16_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConvTcSmem));
     VLB_CUDA(cudaFuncSetAttribute(k_conv<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<1, 16>()));
-    VLB_CUDA(cudaFuncSetAttribute(k_conv<16, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<16, 16>()));
     VLB_CUDA(cudaFuncSetAttribute(k_conv<16, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<16, 3>()));
     VLB_CUDA(cudaFuncSetAttribute(k_conv<3, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)conv_smem<3, 16>()));
     VLB_CUDA(cudaFuncSetAttribute(k_conv_wgrad<1, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
