@@ -407,9 +407,9 @@ VLB_API int vlb_fp32_peak(int32_t device, double* tflops);
 VLB_API int vlb_stream(vlb_ctx* ctx, void** stream);
 
 /* Total charge sum_ijk rho[i,j,k] m0[i] m0[j] m0[k] of a density the caller
- * holds on the device, for callers that cannot allocate device memory: a host
- * capturing a CUDA graph, where an allocation is an unsafe call that fails; an
- * embedding runtime whose pool has already claimed the GPU's memory; a loop
+ * holds on the device, for callers that cannot allocate device memory: an
+ * embedding runtime whose caching pool has already claimed the GPU's memory;
+ * a plugin whose host forbids allocation outside its set-up phase; a loop
  * that must not stall on cudaMalloc's synchronisation.  It allocates nothing:
  * the scratch (one float64 per (j,k) column) is a fixed 512 KiB of static
  * device memory that every GPU loading the library keeps until exit, so n is

@@ -2,10 +2,10 @@
 //
 // Some callers of this library cannot call cudaMalloc when they need a
 // result:
-//   - a host that is capturing a CUDA graph: in the global and thread-local
-//     capture modes an allocation is an unsafe call and fails;
-//   - an embedding runtime whose own pool has already claimed the GPU's
-//     memory, so a fresh cudaMalloc fails or fragments it;
+//   - an embedding runtime (a Julia or Python host with its own caching
+//     allocator) whose pool has already claimed the GPU's memory, so a fresh
+//     cudaMalloc fails or fragments it;
+//   - a plugin whose host forbids allocation outside its set-up phase;
 //   - a loop that must not stall, since cudaMalloc can synchronise the device.
 //
 // vlb_total_charge_noalloc serves them.  It computes sum rho m0x m0y m0z over
