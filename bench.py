@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--deposit", default="float32", choices=["float32", "fixed64"])
     ap.add_argument("--precision", default="3xtf32", choices=["fp32", "3xtf32", "bf16x3"],
                     help="mode products on the CUDA cores (fp32) or split-precision on the tensor cores")
+    ap.add_argument("--gather", default="fp32", choices=["fp32", "tcgen05"],
+                    help="the gather's sums over y as 3xTF32 MMAs on the tensor cores, or FP32 FMAs")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
@@ -71,7 +73,7 @@ def workload(args, vb):
 def config_dict(args, n):
     return {"workload": "Na196 + Xe25+ 500 keV b=45 a0 collision, one fused step",
             "npart_per_gpu": args.npart, "fine_grid": f"{2 * args.nfine + 2}^3", "coarse_grid": f"{2 * args.nfine + 2}^3",
-            "profile": args.profile, "deposit": args.deposit, "mode_products": args.precision, "dt": 0.5, "projectile": "Xe25+ v=0.40 x0=-70 b=45",
+            "profile": args.profile, "deposit": args.deposit, "mode_products": args.precision, "gather": args.gather, "dt": 0.5, "projectile": "Xe25+ v=0.40 x0=-70 b=45",
             "cuda_graph": (not args.no_graph) if n == 1 else "per-phase eager (collectives between phases)",
             "l2": "inputs larger than L2 (2 x 384 MB particle state)",
             "parallelism": (f"{n} particle shards, NCCL all-reduce of the deposited grids and the projectile's "
@@ -243,6 +245,7 @@ def main():
         sim = vb.Simulation(p, prof, projectile=proj, device=local, fixed_point=args.deposit == "fixed64",
                             precision=precision, use_graph=not args.no_graph, seed=-1)
     acc = sim.accelerator
+    acc.set_tuning(field_tensor_cores=1 if args.gather == "tcgen05" else 0)
     ext = torch.cuda.ExternalStream(acc.stream_handle(), device=torch.device("cuda", local))
     for _ in range(max(args.warmup, 3)):
         sim.step()

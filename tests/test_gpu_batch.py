@@ -76,8 +76,8 @@ def test_launch_shapes_change_no_result(cuda_device):
     try:
         for s in b:
             s.accelerator.set_tuning(chunk=64, field_ctas_per_sm=2, cic_ctas_per_sm=8, push_ctas_per_sm=16,
-                                     move_ctas_per_sm=4)
-            assert s.accelerator.tuning()["chunk"] == 64
+                                     move_ctas_per_sm=4, field_tensor_cores=1)
+            assert s.accelerator.tuning()["chunk"] == 64 and s.accelerator.tuning()["field_tensor_cores"] == 1
         for _ in range(3):
             for sa, sb in zip(a, b):
                 x, y = sa.step(), sb.step()

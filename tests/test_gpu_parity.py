@@ -202,10 +202,14 @@ def test_coefficients_and_mean_field(case, acc):
         assert rel_l2(acc.grid(wcs), c) < 2e-5
 
 
-def test_forces_with_projectile(case, acc):
+@pytest.mark.parametrize("tensor_cores", [1, 0], ids=["tcgen05-3xtf32", "fp32-fma"])
+def test_forces_with_projectile(case, acc, tensor_cores):
+    """Both forms of the gather (sums over y as 3xTF32 MMAs, or FP32 FMAs)
+    against the float64 oracle, same bars."""
     O = case.O
     k, d, pk, pdl = oracle_sorted(case)
     O.forces(k, d)
+    acc.set_tuning(field_tensor_cores=tensor_cores)
     acc.upload(case.k, case.d, case.pk, case.pd)
     acc.sort()
     acc.set_grid(L.VLB_GRID_CSOL_FINE, O.csolf.astype(np.float32))
@@ -227,7 +231,10 @@ def test_forces_with_projectile(case, acc):
     out = case.orc.outside(k, case.meshes.fine.n)
     inside = np.ones(N, bool)
     inside[out] = False
-    assert rel_l2(f[:, inside], force[:, inside]) < 2e-5
+    acc.set_tuning(field_tensor_cores=0)
+    e_in = rel_l2(f[:, inside], force[:, inside])
+    print(f"\n[gather, tensor cores {tensor_cores}] rel L2 vs the oracle: {e_in:.2e}")
+    assert e_in < 2e-5
     assert rel_l2(f[:, out], force[:, out]) < 1e-5
     assert np.all(np.isfinite(f))
     assert rel_l2(gred[:3], red[:3]) < 1e-4 and abs(gred[3] - red[3]) < 1e-4 * abs(red[3])

@@ -112,7 +112,8 @@ VLB_DTYPE_INT64 = 1
 
 class Tuning(C.Structure):
     _fields_ = [("chunk", C.c_int32), ("field_ctas_per_sm", C.c_int32), ("cic_ctas_per_sm", C.c_int32),
-                ("push_ctas_per_sm", C.c_int32), ("move_ctas_per_sm", C.c_int32), ("reserved", C.c_int32 * 3)]
+                ("push_ctas_per_sm", C.c_int32), ("move_ctas_per_sm", C.c_int32),
+                ("field_tensor_cores", C.c_int32), ("reserved", C.c_int32 * 2)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}

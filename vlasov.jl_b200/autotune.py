@@ -1,6 +1,7 @@
 """Autotuner of the launch shapes of one run (vlb_set_tuning).
 
-The shapes are the particles per work item of the gather and the coarse
+The shapes are the gather's form (its sums over y on the tensor cores or
+on the FP32 pipes), the particles per work item of the gather and the coarse
 deposit (`chunk`) and the CTAs per SM of the persistent grids of the gather,
 the coarse deposit, the push and the record move of the sort.  They change
 no result beyond the order of float32 atomic sums, only the time.
@@ -21,6 +22,7 @@ from pathlib import Path
 
 # candidate values, and the stages each shape is judged by
 SEARCH = {
+    "field_tensor_cores": ((0, 1), ("forces",)),
     "chunk": ((64, 128, 256), ("deposit_coarse", "forces", "sort")),
     "field_ctas_per_sm": ((2, 3, 4), ("forces",)),
     "cic_ctas_per_sm": ((2, 4, 8), ("deposit_coarse",)),

@@ -12,6 +12,7 @@
 namespace vlb {
 
 void deposit_setup(Ctx& c);
+void field_setup(Ctx& c);
 double measure_fp32_peak(int device);
 int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
 
@@ -464,6 +465,7 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     for (auto& e : c->ev) VLB_CUDA(cudaEventCreate(&e));
     c->evs_made = true;
     deposit_setup(*c);
+    field_setup(*c);
     tc_setup(*c);
     VLB_CUDA(cudaDeviceSynchronize());
     return VLB_OK;
@@ -835,7 +837,10 @@ int vlb_set_tuning(vlb_ctx* ctx, const vlb_tuning* t) {
   const int32_t cps[4] = {t->field_ctas_per_sm, t->cic_ctas_per_sm, t->push_ctas_per_sm, t->move_ctas_per_sm};
   for (int32_t v : cps)
     if (v < 1 || v > 32) return fail(VLB_ERR_ARG, "CTAs per SM must be in [1, 32]");
+  if (t->field_tensor_cores != 0 && t->field_tensor_cores != 1)
+    return fail(VLB_ERR_ARG, "field_tensor_cores must be 0 or 1");
   c.chunk = t->chunk;
+  c.field_tc = t->field_tensor_cores != 0;
   c.field_cps = t->field_ctas_per_sm;
   c.cic_cps = t->cic_ctas_per_sm;
   c.push_cps = t->push_ctas_per_sm;
@@ -856,6 +861,7 @@ int vlb_get_tuning(vlb_ctx* ctx, vlb_tuning* t) {
   t->cic_ctas_per_sm = c.cic_cps;
   t->push_ctas_per_sm = c.push_cps;
   t->move_ctas_per_sm = c.move_cps;
+  t->field_tensor_cores = c.field_tc ? 1 : 0;
   return VLB_OK;
 }
 

@@ -23,6 +23,7 @@
 // projectile like everyone else's.  The reference runs this part on the host
 // after a device-to-host copy; here it stays on the device.
 
+#include "tc_util.cuh"
 #include "vlb_internal.cuh"
 
 namespace vlb {
@@ -30,6 +31,8 @@ namespace vlb {
 int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
 
 namespace {
+
+using namespace tc;
 
 constexpr int kGThreads = 256;
 
@@ -290,6 +293,428 @@ __global__ void __launch_bounds__(kGThreads) k_field(
 #pragma unroll
       for (int cc = 0; cc < 4; ++cc) red_items[4 * (size_t)item + cc] = v[cc];
     }
+  }
+}
+
+// ------------------------------------------------ gather on the tensor cores
+// The same gather with its sums over y on the tensor cores.  For the
+// particles p of one work item (at most 128: one per tensor-memory lane) and
+// the cell's stencil c[kk][jj][ii] (z, y, x),
+//
+//     Yo[p, 10 kk + ii] = sum_jj oy_p[jj] c[kk][jj][ii],   Yg: gy_p likewise,
+//
+// are two GEMMs with M = 128 particles, N = 100 stencil columns (padded to
+// 112) and K = 10, sharing B[n, jj] = c[kk][jj][ii].  Both run in 3xTF32 in
+// one accumulation each: along K, A = [a_hi | a_lo | a_hi] and
+// B = [c_hi | c_hi | c_lo] (K = 30, padded to 32), so that
+// D = a_hi c_hi + a_lo c_hi + a_hi c_lo with hi = rna_tf32(x) and
+// lo = rna_tf32(x - hi): the dropped a_lo c_lo and the tails' rounding are of
+// order 2^-22 of the terms, FP32 accuracy.  The threads then read their
+// particle's rows of Yo and Yg from tensor memory and finish on the CUDA
+// cores: x, then z (330 FMA a particle in place of the 2,330 of k_field).
+//
+// A CTA is two halves of 128 threads over the same 128 tensor-memory lanes
+// (warps w and w + 4 share lanes 32 (w % 4) ..): thread r of each half owns
+// particle row r.  Half 0 writes the oy operand and sums the z planes 0-4,
+// half 1 writes the gy operand, stages the stencil and sums the planes 5-9;
+// half 0 adds half 1's partial sums (in that order), the projectile term and
+// stores the force.  Two CTAs per SM, 256 tensor-memory columns each (Yo in
+// [0, 112), Yg in [128, 240)).
+//
+// Pipeline: while the MMAs of item t run, the threads load item t's x and
+// z tables and split item t+1's y tables into the other shared-memory A
+// buffers (and its stencil into the other B buffer when the cell changes);
+// then they wait for item t's MMAs, read D and finish item t.  Items go
+// round-robin to the CTAs (item = blockIdx.x + t gridDim.x); a thread's
+// delta is loaded two items ahead, the items' cell data one and two ahead.
+// The reaction sums of an item: each of half 0's warps' butterfly, then the
+// four warps in order.  Every wait is bounded.
+constexpr int kFtThreads = 256;
+constexpr int kFtRows = 128;                       // the MMA's M: particles per item at most
+constexpr int kFtN = 112;                          // the MMA's N: 100 stencil columns, padded
+constexpr unsigned kFtA = 128u * 128u;             // one A operand: 128 rows x 32 TF32
+constexpr unsigned kFtB = (unsigned)kFtN * 128u;   // the B operand: 112 rows x 32 TF32
+constexpr unsigned kFtBars = 4u * kFtA + 2u * kFtB;
+constexpr unsigned kFtSmem = kFtBars + 32u;        // + two mbarriers and the tensor-memory slot
+constexpr unsigned kFtCols = 256;
+constexpr unsigned kFtColG = 128;                  // first column of Yg
+constexpr int kFtHalfBarrier = 1;                  // named barrier: half 1's partial sums are written
+
+// Byte offset of K group kg (4 TF32) of row r in a K-major operand of 32
+// TF32 per row, no swizzle: 8 x 16-byte core matrices, the 8 K groups of a
+// row group contiguous (LBO 128 bytes between K neighbours, SBO 1024 bytes
+// between row groups).
+__device__ __forceinline__ unsigned ft_off(int r, int kg) {
+  return (unsigned)((r >> 3) * 1024 + kg * 128 + (r & 7) * 16);
+}
+
+struct FtItem {
+  int item;       // -1: none
+  int code;       // occupied cell code
+  int s0, s1;     // particle slots
+  bool has;       // the stencil fits: MMAs and forces
+};
+
+struct FtPart {
+  float dx, dy, dz;
+  int cx, cz;           // table columns of x and z
+  int s;
+  bool valid;
+};
+
+struct FtTab {
+  float ox[10], gx[10];
+  float oz[5], gz[5];   // this half's five z planes
+};
+
+__device__ __forceinline__ FtItem ft_resolve(int item, int g, int nitems, const int32_t* __restrict__ occupied,
+                                             const int32_t* __restrict__ bounds,
+                                             const int32_t* __restrict__ chunk_start, int chunk, int n, int nk) {
+  FtItem it{-1, 0, 0, 0, false};
+  if (item >= nitems) return it;
+  it.item = item;
+  it.code = occupied[g];
+  int kx, ky, kz;
+  cell_knots((uint32_t)it.code, nk, kx, ky, kz);
+  it.has = field_fits(kx, ky, kz, n);
+  it.s0 = bounds[g] + (item - chunk_start[g]) * chunk;
+  it.s1 = min(it.s0 + chunk, bounds[g + 1]);
+  return it;
+}
+
+// Row r of an A operand from the ten values v: [hi | lo | hi | 0 0].
+__device__ __forceinline__ void ft_store_a(unsigned char* A, int r, const float (&v)[10]) {
+  float hi[10], lo[10];
+#pragma unroll
+  for (int j = 0; j < 10; ++j) {
+    hi[j] = tf32_rna(v[j]);
+    lo[j] = tf32_rna(__fsub_rn(v[j], hi[j]));
+  }
+  auto at = [&](int kg) { return reinterpret_cast<float4*>(A + ft_off(r, kg)); };
+  *at(0) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+  *at(1) = make_float4(hi[4], hi[5], hi[6], hi[7]);
+  *at(2) = make_float4(hi[8], hi[9], lo[0], lo[1]);
+  *at(3) = make_float4(lo[2], lo[3], lo[4], lo[5]);
+  *at(4) = make_float4(lo[6], lo[7], lo[8], lo[9]);
+  *at(5) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+  *at(6) = make_float4(hi[4], hi[5], hi[6], hi[7]);
+  *at(7) = make_float4(hi[8], hi[9], 0.f, 0.f);
+}
+
+// Row t < 100 (t = 10 kk + ii) of a cell's B operand: [hi | hi | lo | 0 0]
+// of c[kk][0..9][ii].  Rows 100..111 are never written: they only feed the D
+// columns that nothing reads.
+__device__ __forceinline__ void ft_stage_b(unsigned char* B, int t, const float* __restrict__ csol, int n, int code,
+                                           int nk) {
+  if (t >= 100) return;
+  int kx, ky, kz;
+  cell_knots((uint32_t)code, nk, kx, ky, kz);
+  const int kk = t / 10, ii = t - 10 * kk;
+  const float* src =
+      csol + (size_t)(2 * kx - 6 + ii) + (size_t)n * ((size_t)(2 * ky - 6) + (size_t)n * (size_t)(2 * kz - 6 + kk));
+  float H[10], Lo[10];
+#pragma unroll
+  for (int jj = 0; jj < 10; ++jj) {
+    const float v = __ldg(src + (size_t)n * jj);
+    H[jj] = tf32_rna(v);
+    Lo[jj] = tf32_rna(__fsub_rn(v, H[jj]));
+  }
+  auto at = [&](int kg) { return reinterpret_cast<float4*>(B + ft_off(t, kg)); };
+  *at(0) = make_float4(H[0], H[1], H[2], H[3]);
+  *at(1) = make_float4(H[4], H[5], H[6], H[7]);
+  *at(2) = make_float4(H[8], H[9], H[0], H[1]);
+  *at(3) = make_float4(H[2], H[3], H[4], H[5]);
+  *at(4) = make_float4(H[6], H[7], H[8], H[9]);
+  *at(5) = make_float4(Lo[0], Lo[1], Lo[2], Lo[3]);
+  *at(6) = make_float4(Lo[4], Lo[5], Lo[6], Lo[7]);
+  *at(7) = make_float4(Lo[8], Lo[9], 0.f, 0.f);
+}
+
+// The x and z sums of half H over its z planes kk = 5H .. 5H+4 (D columns
+// 50H .. 50H+49, read in 16-column groups from column 48H), from the rows
+// of Yo and Yg at lane_base.
+template <int H>
+__device__ __forceinline__ void ft_finish(unsigned lane_base, const FtTab& p, float& sx, float& sy, float& sz) {
+  sx = sy = sz = 0.f;
+  float u0 = 0.f, u1 = 0.f, v0 = 0.f, v1 = 0.f, w0 = 0.f, w1 = 0.f;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int c0 = 48 * H + 16 * q;
+    unsigned yo[16], yg[16];
+    tmem_ld16(lane_base + (unsigned)c0, yo);
+    tmem_ld16(lane_base + kFtColG + (unsigned)c0, yg);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int nn = c0 + j;
+      if (nn >= 50 * H && nn < 50 * H + 50) {
+        const int kl = nn / 10 - 5 * H, ii = nn % 10;
+        const float Yo = __uint_as_float(yo[j]), Yg = __uint_as_float(yg[j]);
+        if (ii & 1) {
+          u1 = fmaf(p.gx[ii], Yo, u1);
+          v1 = fmaf(p.ox[ii], Yg, v1);
+          w1 = fmaf(p.ox[ii], Yo, w1);
+        } else {
+          u0 = fmaf(p.gx[ii], Yo, u0);
+          v0 = fmaf(p.ox[ii], Yg, v0);
+          w0 = fmaf(p.ox[ii], Yo, w0);
+        }
+        if (ii == 9) {
+          sx = fmaf(p.oz[kl], u0 + u1, sx);
+          sy = fmaf(p.oz[kl], v0 + v1, sy);
+          sz = fmaf(p.gz[kl], w0 + w1, sz);
+          u0 = u1 = v0 = v1 = w0 = w1 = 0.f;
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void ft_named_arrive(int id, int count) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+__device__ __forceinline__ void ft_named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+__global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
+    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
+    const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int64_t Npad,
+    const float* __restrict__ d, const float* __restrict__ csol, int n, int nk, const float* __restrict__ ov,
+    const float* __restrict__ gr, int nbdt, int ncol, float spacing, float x0, float h, double w,
+    float* __restrict__ force, int chunk, double* __restrict__ red_items) {
+  extern __shared__ __align__(1024) unsigned char ftsm[];
+  __shared__ double red[2][4][4];
+  __shared__ float part[3][kFtRows];  // half 1's partial sums
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ftsm + kFtBars);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(ftsm + kFtBars + 16);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int half = tid >> 7, r = tid & (kFtRows - 1);
+  const int nitems = dsc->nitems;
+  const ProjF P = load_proj(dsc, w);
+  const float wf = (float)w;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kFtCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(&bars[0]), 1);
+    mbar_init(smem_u32(&bars[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const unsigned tmem = *tmem_slot;
+  const unsigned lane_base = tmem + ((unsigned)(32 * (warp & 3)) << 16);
+  const unsigned sbase = smem_u32(ftsm);
+  const unsigned idesc = (1u << 4)                          // D: F32
+                         | (2u << 7) | (2u << 10)            // A, B: TF32, both K-major
+                         | ((unsigned)(kFtN >> 3) << 17)     // N
+                         | ((unsigned)(kFtRows >> 4) << 24); // M
+
+  auto load_delta = [&](const FtItem& it, float (&dd)[3]) {
+    if (!it.has) return;
+    const int s = it.s0 + r;
+    if (s < it.s1) {
+      dd[0] = d[s];
+      dd[1] = d[Npad + s];
+      dd[2] = d[2 * Npad + s];
+    }
+  };
+
+  // the thread's share of a prepared item: its half's y table split into
+  // the A buffer of `buf`; delta and the x and z table columns kept
+  auto prep = [&](const FtItem& it, int buf, const float (&dd)[3], FtPart& p) {
+    p.valid = false;
+    p.s = 0;
+    if (!it.has) return;
+    const int s = it.s0 + r;
+    p.s = s;
+    p.valid = s < it.s1;
+    if (!p.valid) return;
+    p.dx = dd[0];
+    p.dy = dd[1];
+    p.dz = dd[2];
+    p.cx = table_column(p.dx, spacing, nbdt, ncol);
+    const int cy = table_column(p.dy, spacing, nbdt, ncol);
+    p.cz = table_column(p.dz, spacing, nbdt, ncol);
+    float yv[10];
+    load10(half ? gr : ov, cy, yv);
+    ft_store_a(ftsm + (unsigned)(2 * buf + half) * kFtA, r, yv);
+  };
+
+  // the x tables and this half's z values of a prepared particle
+  auto tables = [&](const FtPart& p, FtTab& tb) {
+    if (!p.valid) return;
+    load10(ov, p.cx, tb.ox);
+    load10(gr, p.cx, tb.gx);
+    const float* zo = ov + (size_t)(p.cz - 1) * 10 + 5 * half;
+    const float* zg = gr + (size_t)(p.cz - 1) * 10 + 5 * half;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      tb.oz[k] = __ldg(zo + k);
+      tb.gz[k] = __ldg(zg + k);
+    }
+  };
+
+  auto issue = [&](int buf) {
+    fence_after();
+    const unsigned ao = sbase + (unsigned)(2 * buf) * kFtA, ag = ao + kFtA;
+    const unsigned bb = sbase + 4u * kFtA + (unsigned)buf * kFtB;
+    // the K steps holding the small terms first
+#pragma unroll
+    for (int q = 3; q >= 0; --q) {
+      const uint64_t bd = tc::smem_desc(bb + 256u * q, 128u, 1024u);
+      mma_ss_tf32(tmem, tc::smem_desc(ao + 256u * q, 128u, 1024u), bd, idesc, q != 3 ? 1u : 0u);
+      mma_ss_tf32(tmem + kFtColG, tc::smem_desc(ag + 256u * q, 128u, 1024u), bd, idesc, q != 3 ? 1u : 0u);
+    }
+    commit(smem_u32(&bars[buf]));
+  };
+
+  const int G = gridDim.x;
+  auto item_at = [&](int t) { return (int)blockIdx.x + t * G; };
+  auto cell_of = [&](int item) { return item < nitems ? item_cell[item] : 0; };
+  auto resolve = [&](int item, int g) {
+    return ft_resolve(item, g, nitems, occupied, bounds, chunk_start, chunk, n, nk);
+  };
+
+  // items t (cur), t+1 (nxt, delta in dn), t+2 (after), item_cell of t+3
+  FtItem cur = resolve(item_at(0), cell_of(item_at(0)));
+  FtItem nxt = resolve(item_at(1), cell_of(item_at(1)));
+  FtItem after = resolve(item_at(2), cell_of(item_at(2)));
+  int g3 = cell_of(item_at(3));
+  float dc[3] = {0.f, 0.f, 0.f}, dn[3] = {0.f, 0.f, 0.f};
+  load_delta(cur, dc);
+  load_delta(nxt, dn);
+  int staged0 = -1, staged1 = -1;  // cell code in each B buffer
+  unsigned phase = 0;        // bit b: parity of the next completion of bars[b]
+  bool ok = true;            // the same in every thread after each barrier
+  unsigned pending = 0;      // bit b: a commit on bars[b] not yet seen complete
+
+  FtPart pc;
+  if (cur.has) {
+    if (half == 1) ft_stage_b(ftsm + 4u * kFtA, r, csol, n, cur.code, nk);
+    staged0 = cur.code;
+  }
+  prep(cur, 0, dc, pc);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  fence_before();
+  __syncthreads();
+  if (tid == 0 && cur.has) issue(0);
+  if (cur.has) pending |= 1u;
+
+  int b = 0;
+  for (int t = 0; cur.item >= 0; ++t) {
+    // item t's tables; delta two items ahead; cell data three ahead;
+    // item_cell four ahead
+    FtTab tb;
+    tables(pc, tb);
+    float d2[3] = {0.f, 0.f, 0.f};
+    load_delta(after, d2);
+    const FtItem after2 = resolve(item_at(t + 3), g3);
+    g3 = cell_of(item_at(t + 4));
+
+    // item t+1 into the other buffers while item t's MMAs run
+    const int nb = b ^ 1;
+    FtPart pn;
+    if (nxt.has && (nb ? staged1 : staged0) != nxt.code) {
+      if (half == 1) ft_stage_b(ftsm + 4u * kFtA + (unsigned)nb * kFtB, r, csol, n, nxt.code, nk);
+      if (nb)
+        staged1 = nxt.code;
+      else
+        staged0 = nxt.code;
+    }
+    prep(nxt, nb, dn, pn);
+
+    // item t
+    bool got = false;
+    if (cur.has && ok && ((pending >> b) & 1u)) {
+      got = mbar_wait(smem_u32(&bars[b]), (phase >> b) & 1u);
+      ok = got;
+      if (got) {
+        pending &= ~(1u << b);
+        phase ^= 1u << b;
+      }
+    }
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    if (got) {
+      fence_after();
+      if (half == 0)
+        ft_finish<0>(lane_base, tb, sx, sy, sz);
+      else
+        ft_finish<1>(lane_base, tb, sx, sy, sz);
+    }
+    if (half == 1) {
+      part[0][r] = sx;
+      part[1][r] = sy;
+      part[2][r] = sz;
+      ft_named_arrive(kFtHalfBarrier, kFtThreads);
+    } else {
+      ft_named_sync(kFtHalfBarrier, kFtThreads);
+      float ax = 0.f, ay = 0.f, az = 0.f, ae = 0.f;
+      if (got && pc.valid) {
+        sx += part[0][r];
+        sy += part[1][r];
+        sz += part[2][r];
+        float fx = -wf * sx, fy = -wf * sy, fz = -wf * sz;
+        if (P.on) {
+          int kx, ky, kz;
+          cell_knots((uint32_t)cur.code, nk, kx, ky, kz);
+          float fx2, fy2, fz2, e;
+          proj_term(P, kx, ky, kz, pc.dx, pc.dy, pc.dz, x0, h, fx2, fy2, fz2, e);
+          fx -= fx2;
+          fy -= fy2;
+          fz -= fz2;
+          ax = fx2;
+          ay = fy2;
+          az = fz2;
+          ae = e;
+        }
+        force[pc.s] = fx;
+        force[Npad + pc.s] = fy;
+        force[2 * Npad + pc.s] = fz;
+      }
+      double v[4] = {ax, ay, az, ae};
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) v[cc] = warp_sum(v[cc]);
+      if (lane == 0) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) red[b][warp][cc] = v[cc];
+      }
+    }
+    // D read, item t+1's operands written: hand them to the MMA
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    fence_before();
+    ok = __syncthreads_and(ok) != 0;  // after a wait that gave up, no more MMAs
+    if (nxt.has && ok) {
+      if (tid == 0) issue(nb);
+      pending |= 1u << nb;
+    }
+    if (tid < 4)
+      red_items[4 * (size_t)cur.item + tid] = ((red[b][0][tid] + red[b][1][tid]) + red[b][2][tid]) + red[b][3][tid];
+    cur = nxt;
+    nxt = after;
+    after = after2;
+    pc = pn;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) dn[k] = d2[k];
+    b = nb;
+  }
+
+  if (!ok && tid == 0) atomicOr(&dsc->status, kStatusMmaTimeout);
+  // nothing may still be in flight when the tensor memory is freed (after a
+  // wait that gave up, at most one commit per barrier is outstanding)
+  for (int bb = 0; bb < 2; ++bb)
+    if (pending & (1u << bb)) mbar_wait(smem_u32(&bars[bb]), (phase >> bb) & 1u);
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kFtCols) : "memory");
   }
 }
 
@@ -571,15 +996,26 @@ __global__ void __launch_bounds__(256) k_energy_total(const double* __restrict__
 
 }  // namespace
 
+void field_setup(Ctx& c) {
+  (void)c;
+  VLB_CUDA(cudaFuncSetAttribute(k_field_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFtSmem));
+}
+
 void launch_forces(Ctx& c) {
   Level& F = c.fine;
   Level& C = c.coarse;
   Particles& P = c.part[c.cur];
-  VLB_CUDA(cudaMemsetAsync(&c.dsc->work_gather, 0, sizeof(unsigned long long), c.stream));
-  k_field<<<c.num_sms * c.field_cps, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc,
-                                                     c.Npad, P.d, F.csol, F.n, F.nk,
-                                                     c.overlap, c.gradient, c.nbdt, c.ncol, c.spacing_f, c.x0f,
-                                                     c.hf, c.weight, c.force, c.chunk, c.red_items);
+  if (c.field_tc && c.chunk <= kFtRows) {
+    k_field_tc<<<2 * c.num_sms, kFtThreads, kFtSmem, c.stream>>>(
+        c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.d, F.csol, F.n, F.nk, c.overlap,
+        c.gradient, c.nbdt, c.ncol, c.spacing_f, c.x0f, c.hf, c.weight, c.force, c.chunk, c.red_items);
+  } else {
+    VLB_CUDA(cudaMemsetAsync(&c.dsc->work_gather, 0, sizeof(unsigned long long), c.stream));
+    k_field<<<c.num_sms * c.field_cps, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.chunk_start, c.item_cell,
+                                                                 c.dsc, c.Npad, P.d, F.csol, F.n, F.nk, c.overlap,
+                                                                 c.gradient, c.nbdt, c.ncol, c.spacing_f, c.x0f,
+                                                                 c.hf, c.weight, c.force, c.chunk, c.red_items);
+  }
   VLB_LAUNCHED(c);
   k_tail<<<c.num_sms, kGThreads, 0, c.stream>>>(c.outlist, c.dsc, c.Npad, P.k, P.d, C.csol, C.knots_d, C.nk,
                                                     C.n, F.nk, c.x0f, c.hf, c.x0, c.h, c.weight, c.force,

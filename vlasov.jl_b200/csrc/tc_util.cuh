@@ -1,5 +1,5 @@
-// Device helpers of the tcgen05 kernels (the mode-product chains and the
-// denoiser's convolutions): shared-memory addresses, mbarriers with bounded
+// Device helpers of the tcgen05 kernels (the mode-product chains, the
+// gather's y sums and the denoiser's convolutions): shared-memory addresses, mbarriers with bounded
 // waits, bulk copies, tensor-memory fences, loads and stores, shared-memory
 // matrix descriptors, the MMA issue forms, and the head/tail roundings.
 #pragma once
@@ -117,6 +117,17 @@ __device__ __forceinline__ void mma_ss_bf16(unsigned d_tmem, uint64_t a_desc, ui
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// D (tensor memory) += A (shared memory) B (shared memory), TF32 operands.
+__device__ __forceinline__ void mma_ss_tf32(unsigned d_tmem, uint64_t a_desc, uint64_t b_desc, unsigned idesc,
+                                            unsigned accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
       "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
       : "memory");
 }

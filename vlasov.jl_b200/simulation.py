@@ -433,8 +433,9 @@ class DeviceAccelerator:
         return t.as_dict()
 
     def set_tuning(self, **kw):
-        """Changes some launch shapes (chunk, field_ctas_per_sm,
-        cic_ctas_per_sm, push_ctas_per_sm, move_ctas_per_sm)."""
+        """Changes some launch shapes (field_tensor_cores, chunk,
+        field_ctas_per_sm, cic_ctas_per_sm, push_ctas_per_sm,
+        move_ctas_per_sm)."""
         cur = self.tuning()
         unknown = set(kw) - set(cur)
         if unknown:
