@@ -32,6 +32,7 @@ import numpy as np  # noqa: E402
 
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 GATHER_FLOP_PER_PARTICLE = 4600.0       # 2000 FMA + 300 mul/FMA per 10^3 contraction
+GATHER_TC_FLOP_PER_PARTICLE = 12000.0   # 3 split products x (oy, gy) x 100 columns x 10 y x 2
 PUSH_BYTES_PER_PARTICLE = 48 + 12 + 48 + 4  # read (k, d, pk, pd) + force; write the record + the next sort's cell key
 
 
@@ -47,7 +48,7 @@ def parse():
     ap.add_argument("--deposit", default="float32", choices=["float32", "fixed64"])
     ap.add_argument("--precision", default="3xtf32", choices=["fp32", "3xtf32", "bf16x3"],
                     help="mode products on the CUDA cores (fp32) or split-precision on the tensor cores")
-    ap.add_argument("--gather", default="fp32", choices=["fp32", "tcgen05"],
+    ap.add_argument("--gather", default="tcgen05", choices=["tcgen05", "fp32"],
                     help="the gather's sums over y as 3xTF32 MMAs on the tensor cores, or FP32 FMAs")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -345,6 +346,8 @@ def main():
     fp32_peak = vb._lib.C.c_double()
     L.check(L.lib().vlb_fp32_peak(local, vb._lib.C.byref(fp32_peak)))
     t_forces = stages.get("forces", float("nan"))
+    gather_kernel = ("k_field_tc (smoothed gather + projectile, sums over y as 3xTF32 tcgen05 MMAs), forces stage"
+                     if args.gather == "tcgen05" else "k_field (smoothed gather + projectile, FP32 FMAs), forces stage")
     achieved = GATHER_FLOP_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e12
     t_push = stages.get("push", float("nan"))
     push_gbs = PUSH_BYTES_PER_PARTICLE * args.npart / (t_push * 1e-3) / 1e9
@@ -373,9 +376,12 @@ def main():
                 "h2d_bytes_per_step": step_h2d + cloud_bytes / args.steps,
                 "d2h_bytes_per_step": step_d2h + cloud_bytes / args.steps},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": "k_field (smoothed gather + projectile), forces stage", "bound": "fp32",
+        "roofline": {"kernel": gather_kernel, "bound": "fp32",
                      "achieved": achieved, "peak": fp32_peak.value, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak.value, "traffic": None,
+                     "flop_per_particle": GATHER_FLOP_PER_PARTICLE,
+                     "note": "FP32-equivalent FLOP of the smoothed gather (the reference's operation count) over "
+                             "the forces stage's event time",
                      "peak_source": "measured FP32 FMA kernel (vlb_fp32_peak), this GPU, this run"},
         "roofline_hbm": {"kernel": "k_push (packed Verlet)", "bound": "hbm", "achieved": push_gbs,
                          "peak": pk_.get("hbm_gbs"), "unit": "GB/s", "frac": push_gbs / pk_.get("hbm_gbs", 1),
@@ -384,6 +390,14 @@ def main():
         "clocks": clk,
         "last_step": {"q8": d.enclosed_charge, "outcount": d.outcount, "noccupied": d.noccupied},
     }
+    if args.gather == "tcgen05":
+        tf32_peak = pk_.get("bf16_tflops", 1590.0) / 2
+        tens = GATHER_TC_FLOP_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e12
+        line["roofline"]["tensor"] = {
+            "achieved": tens, "peak": tf32_peak, "unit": "TFLOP/s", "frac": tens / tf32_peak,
+            "flop_per_particle": GATHER_TC_FLOP_PER_PARTICLE,
+            "note": "3xTF32 products of the sums over y (3 x 2 x 100 x 10 x 2 FLOP a particle, no padding)",
+            "peak_source": f"dense TF32 taken as half the bf16 figure of MEASURED_PEAKS.json ({how})"}
     if learned:
         line["learned"] = learned
     if energy:

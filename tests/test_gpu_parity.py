@@ -231,7 +231,7 @@ def test_forces_with_projectile(case, acc, tensor_cores):
     out = case.orc.outside(k, case.meshes.fine.n)
     inside = np.ones(N, bool)
     inside[out] = False
-    acc.set_tuning(field_tensor_cores=0)
+    acc.set_tuning(field_tensor_cores=1)
     e_in = rel_l2(f[:, inside], force[:, inside])
     print(f"\n[gather, tensor cores {tensor_cores}] rel L2 vs the oracle: {e_in:.2e}")
     assert e_in < 2e-5

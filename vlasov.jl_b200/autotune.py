@@ -22,7 +22,7 @@ from pathlib import Path
 
 # candidate values, and the stages each shape is judged by
 SEARCH = {
-    "field_tensor_cores": ((0, 1), ("forces",)),
+    "field_tensor_cores": ((1, 0), ("forces",)),
     "chunk": ((64, 128, 256), ("deposit_coarse", "forces", "sort")),
     "field_ctas_per_sm": ((2, 3, 4), ("forces",)),
     "cic_ctas_per_sm": ((2, 4, 8), ("deposit_coarse",)),

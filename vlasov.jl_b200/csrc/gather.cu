@@ -298,8 +298,8 @@ __global__ void __launch_bounds__(kGThreads) k_field(
 
 // ------------------------------------------------ gather on the tensor cores
 // The same gather with its sums over y on the tensor cores.  For the
-// particles p of one work item (at most 128: one per tensor-memory lane) and
-// the cell's stencil c[kk][jj][ii] (z, y, x),
+// particles p of one work item (at most 128: one per thread and per
+// tensor-memory lane) and the cell's stencil c[kk][jj][ii] (z, y, x),
 //
 //     Yo[p, 10 kk + ii] = sum_jj oy_p[jj] c[kk][jj][ii],   Yg: gy_p likewise,
 //
@@ -309,27 +309,24 @@ __global__ void __launch_bounds__(kGThreads) k_field(
 // B = [c_hi | c_hi | c_lo] (K = 30, padded to 32), so that
 // D = a_hi c_hi + a_lo c_hi + a_hi c_lo with hi = rna_tf32(x) and
 // lo = rna_tf32(x - hi): the dropped a_lo c_lo and the tails' rounding are of
-// order 2^-22 of the terms, FP32 accuracy.  The threads then read their
-// particle's rows of Yo and Yg from tensor memory and finish on the CUDA
-// cores: x, then z (330 FMA a particle in place of the 2,330 of k_field).
+// order 2^-22 of the terms, FP32 accuracy.  Each thread then reads its
+// particle's rows of Yo and Yg from tensor memory and finishes on the CUDA
+// cores with packed FMAs: x, then z (165 FFMA2 + 30 FMA a particle in place
+// of the 1,150 FFMA2 of k_field).  Two CTAs per SM, 256 tensor-memory columns
+// each (Yo in [0, 112), Yg in [128, 240)).
 //
-// A CTA is two halves of 128 threads over the same 128 tensor-memory lanes
-// (warps w and w + 4 share lanes 32 (w % 4) ..): thread r of each half owns
-// particle row r.  Half 0 writes the oy operand and sums the z planes 0-4,
-// half 1 writes the gy operand, stages the stencil and sums the planes 5-9;
-// half 0 adds half 1's partial sums (in that order), the projectile term and
-// stores the force.  Two CTAs per SM, 256 tensor-memory columns each (Yo in
-// [0, 112), Yg in [128, 240)).
-//
-// Pipeline: while the MMAs of item t run, the threads load item t's x and
-// z tables and split item t+1's y tables into the other shared-memory A
-// buffers (and its stencil into the other B buffer when the cell changes);
-// then they wait for item t's MMAs, read D and finish item t.  Items go
-// round-robin to the CTAs (item = blockIdx.x + t gridDim.x); a thread's
-// delta is loaded two items ahead, the items' cell data one and two ahead.
-// The reaction sums of an item: each of half 0's warps' butterfly, then the
-// four warps in order.  Every wait is bounded.
-constexpr int kFtThreads = 256;
+// Pipeline, one iteration per item t: the loads go out first (delta of item
+// t+2, cell data of t+3 (used at the end of the iteration), item_cell of
+// t+4, the six tables of item t+1 and,
+// when its cell differs from the buffer's, its stencil); then the threads
+// wait for item t's MMAs (issued at the end of the previous iteration),
+// read D, finish item t with the tables loaded one iteration earlier, and
+// only then split item t+1's y tables and stencil into the other
+// shared-memory buffers and hand them to the MMA.  Items go round-robin to
+// the CTAs (item = blockIdx.x + t gridDim.x).  The reaction sums of an item:
+// each warp's float butterfly, then the four warps in order, in float64.
+// Every wait is bounded.
+constexpr int kFtThreads = 128;
 constexpr int kFtRows = 128;                       // the MMA's M: particles per item at most
 constexpr int kFtN = 112;                          // the MMA's N: 100 stencil columns, padded
 constexpr unsigned kFtA = 128u * 128u;             // one A operand: 128 rows x 32 TF32
@@ -338,7 +335,6 @@ constexpr unsigned kFtBars = 4u * kFtA + 2u * kFtB;
 constexpr unsigned kFtSmem = kFtBars + 32u;        // + two mbarriers and the tensor-memory slot
 constexpr unsigned kFtCols = 256;
 constexpr unsigned kFtColG = 128;                  // first column of Yg
-constexpr int kFtHalfBarrier = 1;                  // named barrier: half 1's partial sums are written
 
 // Byte offset of K group kg (4 TF32) of row r in a K-major operand of 32
 // TF32 per row, no swizzle: 8 x 16-byte core matrices, the 8 K groups of a
@@ -349,46 +345,68 @@ __device__ __forceinline__ unsigned ft_off(int r, int kg) {
 }
 
 struct FtItem {
-  int item;       // -1: none
-  int code;       // occupied cell code
-  int s0, s1;     // particle slots
-  bool has;       // the stencil fits: MMAs and forces
+  int item;         // -1: none
+  int code;         // occupied cell code
+  int kx, ky, kz;   // its knots
+  int s0, s1;       // particle slots
+  bool has;         // the stencil fits: MMAs and forces
 };
 
+// One particle of an item: delta, slot, and the six table columns as
+// neighbour pairs (ten values each).
 struct FtPart {
   float dx, dy, dz;
-  int cx, cz;           // table columns of x and z
   int s;
   bool valid;
+  float2 oy[5], gy[5], ox[5], gx[5], oz[5], gz[5];
 };
 
-struct FtTab {
-  float ox[10], gx[10];
-  float oz[5], gz[5];   // this half's five z planes
+// An item's cell data as loaded (used an iteration later, so that no
+// thread waits on the loads).
+struct FtRaw {
+  int item, code, b0, b1, cs;
 };
 
-__device__ __forceinline__ FtItem ft_resolve(int item, int g, int nitems, const int32_t* __restrict__ occupied,
-                                             const int32_t* __restrict__ bounds,
-                                             const int32_t* __restrict__ chunk_start, int chunk, int n, int nk) {
-  FtItem it{-1, 0, 0, 0, false};
-  if (item >= nitems) return it;
-  it.item = item;
-  it.code = occupied[g];
-  int kx, ky, kz;
-  cell_knots((uint32_t)it.code, nk, kx, ky, kz);
-  it.has = field_fits(kx, ky, kz, n);
-  it.s0 = bounds[g] + (item - chunk_start[g]) * chunk;
-  it.s1 = min(it.s0 + chunk, bounds[g + 1]);
+__device__ __forceinline__ FtRaw ft_load_item(int item, int g, int nitems, const int32_t* __restrict__ occupied,
+                                              const int32_t* __restrict__ bounds,
+                                              const int32_t* __restrict__ chunk_start) {
+  FtRaw r{-1, 0, 0, 0, 0};
+  if (item >= nitems) return r;
+  r.item = item;
+  r.code = occupied[g];
+  r.b0 = bounds[g];
+  r.b1 = bounds[g + 1];
+  r.cs = chunk_start[g];
+  return r;
+}
+
+__device__ __forceinline__ FtItem ft_derive(const FtRaw& r, int chunk, int n, int nk) {
+  FtItem it{-1, 0, 0, 0, 0, 0, 0, false};
+  if (r.item < 0) return it;
+  it.item = r.item;
+  it.code = r.code;
+  cell_knots((uint32_t)it.code, nk, it.kx, it.ky, it.kz);
+  it.has = field_fits(it.kx, it.ky, it.kz, n);
+  it.s0 = r.b0 + (r.item - r.cs) * chunk;
+  it.s1 = min(it.s0 + chunk, r.b1);
   return it;
 }
 
+__device__ __forceinline__ void ft_load_pairs(const float* __restrict__ tab, int col, float2 (&v)[5]) {
+  const float2* p = reinterpret_cast<const float2*>(tab + (size_t)(col - 1) * 10);
+#pragma unroll
+  for (int a = 0; a < 5; ++a) v[a] = __ldg(p + a);
+}
+
 // Row r of an A operand from the ten values v: [hi | lo | hi | 0 0].
-__device__ __forceinline__ void ft_store_a(unsigned char* A, int r, const float (&v)[10]) {
+__device__ __forceinline__ void ft_store_a(unsigned char* A, int r, const float2 (&v2)[5]) {
   float hi[10], lo[10];
 #pragma unroll
-  for (int j = 0; j < 10; ++j) {
-    hi[j] = tf32_rna(v[j]);
-    lo[j] = tf32_rna(__fsub_rn(v[j], hi[j]));
+  for (int j = 0; j < 5; ++j) {
+    hi[2 * j] = tf32_rna(v2[j].x);
+    hi[2 * j + 1] = tf32_rna(v2[j].y);
+    lo[2 * j] = tf32_rna(__fsub_rn(v2[j].x, hi[2 * j]));
+    lo[2 * j + 1] = tf32_rna(__fsub_rn(v2[j].y, hi[2 * j + 1]));
   }
   auto at = [&](int kg) { return reinterpret_cast<float4*>(A + ft_off(r, kg)); };
   *at(0) = make_float4(hi[0], hi[1], hi[2], hi[3]);
@@ -401,23 +419,24 @@ __device__ __forceinline__ void ft_store_a(unsigned char* A, int r, const float 
   *at(7) = make_float4(hi[8], hi[9], 0.f, 0.f);
 }
 
-// Row t < 100 (t = 10 kk + ii) of a cell's B operand: [hi | hi | lo | 0 0]
-// of c[kk][0..9][ii].  Rows 100..111 are never written: they only feed the D
-// columns that nothing reads.
-__device__ __forceinline__ void ft_stage_b(unsigned char* B, int t, const float* __restrict__ csol, int n, int code,
-                                           int nk) {
-  if (t >= 100) return;
-  int kx, ky, kz;
-  cell_knots((uint32_t)code, nk, kx, ky, kz);
+// Row t < 100 (t = 10 kk + ii) of a cell's stencil: c[kk][0..9][ii].
+__device__ __forceinline__ void ft_load_b(const FtItem& it, int t, const float* __restrict__ csol, int n,
+                                          float (&c)[10]) {
   const int kk = t / 10, ii = t - 10 * kk;
-  const float* src =
-      csol + (size_t)(2 * kx - 6 + ii) + (size_t)n * ((size_t)(2 * ky - 6) + (size_t)n * (size_t)(2 * kz - 6 + kk));
+  const float* src = csol + (size_t)(2 * it.kx - 6 + ii) +
+                     (size_t)n * ((size_t)(2 * it.ky - 6) + (size_t)n * (size_t)(2 * it.kz - 6 + kk));
+#pragma unroll
+  for (int jj = 0; jj < 10; ++jj) c[jj] = __ldg(src + (size_t)n * jj);
+}
+
+// That row of the B operand: [hi | hi | lo | 0 0].  Rows 100..111 are never
+// written: they only feed the D columns that nothing reads.
+__device__ __forceinline__ void ft_store_b(unsigned char* B, int t, const float (&c)[10]) {
   float H[10], Lo[10];
 #pragma unroll
   for (int jj = 0; jj < 10; ++jj) {
-    const float v = __ldg(src + (size_t)n * jj);
-    H[jj] = tf32_rna(v);
-    Lo[jj] = tf32_rna(__fsub_rn(v, H[jj]));
+    H[jj] = tf32_rna(c[jj]);
+    Lo[jj] = tf32_rna(__fsub_rn(c[jj], H[jj]));
   }
   auto at = [&](int kg) { return reinterpret_cast<float4*>(B + ft_off(t, kg)); };
   *at(0) = make_float4(H[0], H[1], H[2], H[3]);
@@ -430,51 +449,46 @@ __device__ __forceinline__ void ft_stage_b(unsigned char* B, int t, const float*
   *at(7) = make_float4(Lo[8], Lo[9], 0.f, 0.f);
 }
 
-// The x and z sums of half H over its z planes kk = 5H .. 5H+4 (D columns
-// 50H .. 50H+49, read in 16-column groups from column 48H), from the rows
-// of Yo and Yg at lane_base.
-template <int H>
-__device__ __forceinline__ void ft_finish(unsigned lane_base, const FtTab& p, float& sx, float& sy, float& sz) {
+// The x and z sums of one particle from its rows of Yo and Yg at lane_base:
+// for each z plane kk, packed FMAs over the x pairs (ii, ii+1) (a pair never
+// straddles a plane or a 16-column group), then the plane's z weight.
+__device__ __forceinline__ void ft_finish(unsigned lane_base, const FtPart& p, float& sx, float& sy, float& sz) {
   sx = sy = sz = 0.f;
-  float u0 = 0.f, u1 = 0.f, v0 = 0.f, v1 = 0.f, w0 = 0.f, w1 = 0.f;
+  // two chains per sum: the pairs a = 0, 2, 4 and a = 1, 3
+  float2 U0 = make_float2(0.f, 0.f), V0 = U0, W0 = U0, U1 = U0, V1 = U0, W1 = U0;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int c0 = 48 * H + 16 * q;
+  for (int q = 0; q < 7; ++q) {
     unsigned yo[16], yg[16];
-    tmem_ld16(lane_base + (unsigned)c0, yo);
-    tmem_ld16(lane_base + kFtColG + (unsigned)c0, yg);
+    tmem_ld16(lane_base + 16u * q, yo);
+    tmem_ld16(lane_base + kFtColG + 16u * q, yg);
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int nn = c0 + j;
-      if (nn >= 50 * H && nn < 50 * H + 50) {
-        const int kl = nn / 10 - 5 * H, ii = nn % 10;
-        const float Yo = __uint_as_float(yo[j]), Yg = __uint_as_float(yg[j]);
-        if (ii & 1) {
-          u1 = fmaf(p.gx[ii], Yo, u1);
-          v1 = fmaf(p.ox[ii], Yg, v1);
-          w1 = fmaf(p.ox[ii], Yo, w1);
+    for (int j = 0; j < 16; j += 2) {
+      const int nn = 16 * q + j;
+      if (nn < 100) {
+        const int kk = nn / 10, a = (nn % 10) / 2;
+        const float2 Yo = make_float2(__uint_as_float(yo[j]), __uint_as_float(yo[j + 1]));
+        const float2 Yg = make_float2(__uint_as_float(yg[j]), __uint_as_float(yg[j + 1]));
+        if (a & 1) {
+          U1 = __ffma2_rn(p.gx[a], Yo, U1);
+          V1 = __ffma2_rn(p.ox[a], Yg, V1);
+          W1 = __ffma2_rn(p.ox[a], Yo, W1);
         } else {
-          u0 = fmaf(p.gx[ii], Yo, u0);
-          v0 = fmaf(p.ox[ii], Yg, v0);
-          w0 = fmaf(p.ox[ii], Yo, w0);
+          U0 = __ffma2_rn(p.gx[a], Yo, U0);
+          V0 = __ffma2_rn(p.ox[a], Yg, V0);
+          W0 = __ffma2_rn(p.ox[a], Yo, W0);
         }
-        if (ii == 9) {
-          sx = fmaf(p.oz[kl], u0 + u1, sx);
-          sy = fmaf(p.oz[kl], v0 + v1, sy);
-          sz = fmaf(p.gz[kl], w0 + w1, sz);
-          u0 = u1 = v0 = v1 = w0 = w1 = 0.f;
+        if (a == 4) {
+          const float oz = (kk & 1) ? p.oz[kk >> 1].y : p.oz[kk >> 1].x;
+          const float gz = (kk & 1) ? p.gz[kk >> 1].y : p.gz[kk >> 1].x;
+          sx = fmaf(oz, (U0.x + U0.y) + (U1.x + U1.y), sx);
+          sy = fmaf(oz, (V0.x + V0.y) + (V1.x + V1.y), sy);
+          sz = fmaf(gz, (W0.x + W0.y) + (W1.x + W1.y), sz);
+          U0 = V0 = W0 = U1 = V1 = W1 = make_float2(0.f, 0.f);
         }
       }
     }
   }
-}
-
-__device__ __forceinline__ void ft_named_arrive(int id, int count) {
-  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
-}
-__device__ __forceinline__ void ft_named_sync(int id, int count) {
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
 }
 
 __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
@@ -485,11 +499,9 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     float* __restrict__ force, int chunk, double* __restrict__ red_items) {
   extern __shared__ __align__(1024) unsigned char ftsm[];
   __shared__ double red[2][4][4];
-  __shared__ float part[3][kFtRows];  // half 1's partial sums
   uint64_t* bars = reinterpret_cast<uint64_t*>(ftsm + kFtBars);
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(ftsm + kFtBars + 16);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int half = tid >> 7, r = tid & (kFtRows - 1);
   const int nitems = dsc->nitems;
   const ProjF P = load_proj(dsc, w);
   const float wf = (float)w;
@@ -509,7 +521,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   __syncthreads();
   fence_after();
   const unsigned tmem = *tmem_slot;
-  const unsigned lane_base = tmem + ((unsigned)(32 * (warp & 3)) << 16);
+  const unsigned lane_base = tmem + ((unsigned)(32 * warp) << 16);
   const unsigned sbase = smem_u32(ftsm);
   const unsigned idesc = (1u << 4)                          // D: F32
                          | (2u << 7) | (2u << 10)            // A, B: TF32, both K-major
@@ -518,7 +530,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
 
   auto load_delta = [&](const FtItem& it, float (&dd)[3]) {
     if (!it.has) return;
-    const int s = it.s0 + r;
+    const int s = it.s0 + tid;
     if (s < it.s1) {
       dd[0] = d[s];
       dd[1] = d[Npad + s];
@@ -526,39 +538,27 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     }
   };
 
-  // the thread's share of a prepared item: its half's y table split into
-  // the A buffer of `buf`; delta and the x and z table columns kept
-  auto prep = [&](const FtItem& it, int buf, const float (&dd)[3], FtPart& p) {
+  // the loads of a particle of item `it` whose delta is dd: its six tables
+  auto load_part = [&](const FtItem& it, const float (&dd)[3], FtPart& p) {
     p.valid = false;
     p.s = 0;
     if (!it.has) return;
-    const int s = it.s0 + r;
+    const int s = it.s0 + tid;
     p.s = s;
     p.valid = s < it.s1;
     if (!p.valid) return;
     p.dx = dd[0];
     p.dy = dd[1];
     p.dz = dd[2];
-    p.cx = table_column(p.dx, spacing, nbdt, ncol);
+    const int cx = table_column(p.dx, spacing, nbdt, ncol);
     const int cy = table_column(p.dy, spacing, nbdt, ncol);
-    p.cz = table_column(p.dz, spacing, nbdt, ncol);
-    float yv[10];
-    load10(half ? gr : ov, cy, yv);
-    ft_store_a(ftsm + (unsigned)(2 * buf + half) * kFtA, r, yv);
-  };
-
-  // the x tables and this half's z values of a prepared particle
-  auto tables = [&](const FtPart& p, FtTab& tb) {
-    if (!p.valid) return;
-    load10(ov, p.cx, tb.ox);
-    load10(gr, p.cx, tb.gx);
-    const float* zo = ov + (size_t)(p.cz - 1) * 10 + 5 * half;
-    const float* zg = gr + (size_t)(p.cz - 1) * 10 + 5 * half;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      tb.oz[k] = __ldg(zo + k);
-      tb.gz[k] = __ldg(zg + k);
-    }
+    const int cz = table_column(p.dz, spacing, nbdt, ncol);
+    ft_load_pairs(ov, cy, p.oy);
+    ft_load_pairs(gr, cy, p.gy);
+    ft_load_pairs(ov, cx, p.ox);
+    ft_load_pairs(gr, cx, p.gx);
+    ft_load_pairs(ov, cz, p.oz);
+    ft_load_pairs(gr, cz, p.gz);
   };
 
   auto issue = [&](int buf) {
@@ -578,11 +578,10 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   const int G = gridDim.x;
   auto item_at = [&](int t) { return (int)blockIdx.x + t * G; };
   auto cell_of = [&](int item) { return item < nitems ? item_cell[item] : 0; };
-  auto resolve = [&](int item, int g) {
-    return ft_resolve(item, g, nitems, occupied, bounds, chunk_start, chunk, n, nk);
-  };
+  auto load_item = [&](int item, int g) { return ft_load_item(item, g, nitems, occupied, bounds, chunk_start); };
+  auto resolve = [&](int item, int g) { return ft_derive(load_item(item, g), chunk, n, nk); };
 
-  // items t (cur), t+1 (nxt, delta in dn), t+2 (after), item_cell of t+3
+  // items t (cur), t+1 (nxt, delta in dn), t+2 (after); item_cell of t+3
   FtItem cur = resolve(item_at(0), cell_of(item_at(0)));
   FtItem nxt = resolve(item_at(1), cell_of(item_at(1)));
   FtItem after = resolve(item_at(2), cell_of(item_at(2)));
@@ -591,16 +590,24 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   load_delta(cur, dc);
   load_delta(nxt, dn);
   int staged0 = -1, staged1 = -1;  // cell code in each B buffer
-  unsigned phase = 0;        // bit b: parity of the next completion of bars[b]
-  bool ok = true;            // the same in every thread after each barrier
-  unsigned pending = 0;      // bit b: a commit on bars[b] not yet seen complete
+  unsigned phase = 0;              // bit b: parity of the next completion of bars[b]
+  bool ok = true;                  // the same in every thread after each barrier
+  unsigned pending = 0;            // bit b: a commit on bars[b] not yet seen complete
 
   FtPart pc;
+  load_part(cur, dc, pc);
   if (cur.has) {
-    if (half == 1) ft_stage_b(ftsm + 4u * kFtA, r, csol, n, cur.code, nk);
+    if (tid < 100) {
+      float c[10];
+      ft_load_b(cur, tid, csol, n, c);
+      ft_store_b(ftsm + 4u * kFtA, tid, c);
+    }
     staged0 = cur.code;
+    if (pc.valid) {
+      ft_store_a(ftsm, tid, pc.oy);
+      ft_store_a(ftsm + kFtA, tid, pc.gy);
+    }
   }
-  prep(cur, 0, dc, pc);
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   fence_before();
   __syncthreads();
@@ -609,28 +616,20 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
 
   int b = 0;
   for (int t = 0; cur.item >= 0; ++t) {
-    // item t's tables; delta two items ahead; cell data three ahead;
-    // item_cell four ahead
-    FtTab tb;
-    tables(pc, tb);
+    const int nb = b ^ 1;
+    // ---- loads: delta of t+2, cell data of t+3, item_cell of t+4, the
+    // tables of t+1 and, when needed, its stencil
     float d2[3] = {0.f, 0.f, 0.f};
     load_delta(after, d2);
-    const FtItem after2 = resolve(item_at(t + 3), g3);
+    const FtRaw raw3 = load_item(item_at(t + 3), g3);
     g3 = cell_of(item_at(t + 4));
-
-    // item t+1 into the other buffers while item t's MMAs run
-    const int nb = b ^ 1;
     FtPart pn;
-    if (nxt.has && (nb ? staged1 : staged0) != nxt.code) {
-      if (half == 1) ft_stage_b(ftsm + 4u * kFtA + (unsigned)nb * kFtB, r, csol, n, nxt.code, nk);
-      if (nb)
-        staged1 = nxt.code;
-      else
-        staged0 = nxt.code;
-    }
-    prep(nxt, nb, dn, pn);
+    load_part(nxt, dn, pn);
+    const bool restage = nxt.has && (nb ? staged1 : staged0) != nxt.code;
+    float cb[10];
+    if (restage && tid < 100) ft_load_b(nxt, tid, csol, n, cb);
 
-    // item t
+    // ---- item t
     bool got = false;
     if (cur.has && ok && ((pending >> b) & 1u)) {
       got = mbar_wait(smem_u32(&bars[b]), (phase >> b) & 1u);
@@ -640,32 +639,16 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
         phase ^= 1u << b;
       }
     }
-    float sx = 0.f, sy = 0.f, sz = 0.f;
+    float ax = 0.f, ay = 0.f, az = 0.f, ae = 0.f;
     if (got) {
       fence_after();
-      if (half == 0)
-        ft_finish<0>(lane_base, tb, sx, sy, sz);
-      else
-        ft_finish<1>(lane_base, tb, sx, sy, sz);
-    }
-    if (half == 1) {
-      part[0][r] = sx;
-      part[1][r] = sy;
-      part[2][r] = sz;
-      ft_named_arrive(kFtHalfBarrier, kFtThreads);
-    } else {
-      ft_named_sync(kFtHalfBarrier, kFtThreads);
-      float ax = 0.f, ay = 0.f, az = 0.f, ae = 0.f;
-      if (got && pc.valid) {
-        sx += part[0][r];
-        sy += part[1][r];
-        sz += part[2][r];
+      float sx, sy, sz;
+      ft_finish(lane_base, pc, sx, sy, sz);
+      if (pc.valid) {
         float fx = -wf * sx, fy = -wf * sy, fz = -wf * sz;
         if (P.on) {
-          int kx, ky, kz;
-          cell_knots((uint32_t)cur.code, nk, kx, ky, kz);
           float fx2, fy2, fz2, e;
-          proj_term(P, kx, ky, kz, pc.dx, pc.dy, pc.dz, x0, h, fx2, fy2, fz2, e);
+          proj_term(P, cur.kx, cur.ky, cur.kz, pc.dx, pc.dy, pc.dz, x0, h, fx2, fy2, fz2, e);
           fx -= fx2;
           fy -= fy2;
           fz -= fz2;
@@ -678,15 +661,32 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
         force[Npad + pc.s] = fy;
         force[2 * Npad + pc.s] = fz;
       }
-      double v[4] = {ax, ay, az, ae};
-#pragma unroll
-      for (int cc = 0; cc < 4; ++cc) v[cc] = warp_sum(v[cc]);
-      if (lane == 0) {
-#pragma unroll
-        for (int cc = 0; cc < 4; ++cc) red[b][warp][cc] = v[cc];
-      }
     }
-    // D read, item t+1's operands written: hand them to the MMA
+    ax = warp_sumf(ax);
+    ay = warp_sumf(ay);
+    az = warp_sumf(az);
+    ae = warp_sumf(ae);
+    if (lane == 0) {
+      red[b][warp][0] = ax;
+      red[b][warp][1] = ay;
+      red[b][warp][2] = az;
+      red[b][warp][3] = ae;
+    }
+
+    // ---- item t+1's operands into the other buffers (their last reader,
+    // the MMAs of item t-1, completed in the previous iteration)
+    if (restage) {
+      if (tid < 100) ft_store_b(ftsm + 4u * kFtA + (unsigned)nb * kFtB, tid, cb);
+      if (nb)
+        staged1 = nxt.code;
+      else
+        staged0 = nxt.code;
+    }
+    if (pn.valid) {
+      unsigned char* Ao = ftsm + (unsigned)(2 * nb) * kFtA;
+      ft_store_a(Ao, tid, pn.oy);
+      ft_store_a(Ao + kFtA, tid, pn.gy);
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     fence_before();
     ok = __syncthreads_and(ok) != 0;  // after a wait that gave up, no more MMAs
@@ -698,7 +698,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
       red_items[4 * (size_t)cur.item + tid] = ((red[b][0][tid] + red[b][1][tid]) + red[b][2][tid]) + red[b][3][tid];
     cur = nxt;
     nxt = after;
-    after = after2;
+    after = ft_derive(raw3, chunk, n, nk);
     pc = pn;
 #pragma unroll
     for (int k = 0; k < 3; ++k) dn[k] = d2[k];

@@ -159,7 +159,7 @@ struct Ctx {
   // launch shapes (vlb_set_tuning): particles per work item, persistent-grid
   // CTAs per SM of the gather, the coarse deposit, the push and the record move
   int chunk = kChunk, field_cps = 3, cic_cps = 4, push_cps = 8, move_cps = 8;
-  bool field_tc = false;  // the gather's y sums on the tensor cores (chunk <= 128)
+  bool field_tc = true;  // the gather's y sums on the tensor cores (chunk <= 128)
   unsigned* tc_sync = nullptr;  // grid-barrier counter of the tensor-core chains
   // the learned denoiser of the fine density (vlb_set_denoiser)
   Denoiser* dn = nullptr;
