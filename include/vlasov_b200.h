@@ -120,7 +120,7 @@ typedef struct vlb_step_params {
   int32_t poisson_precision;   /* VLB_POISSON_FP32, _3XTF32 or _BF16X3, every mode product of the step */
   int32_t denoise;             /* 1: the learned denoiser on the fine density (vlb_set_denoiser) */
   int32_t energy;              /* 1: the energy budget's two sums (step!(sim; energy=true)) */
-  int32_t pad_;
+  int32_t film;                /* 1: append a film frame after the step (vlb_film_reserve) */
 } vlb_step_params;
 
 /* Device-side error flags (vlb_step_result.status, vlb_dn_status). */
@@ -334,6 +334,34 @@ VLB_API int vlb_dn_active_tiles(vlb_denoiser* dn, int32_t* n);
  * Hartree ones (S^-1 phi before the mean field; the fine level's are those
  * of the last step run with params.energy).  The cloud may have moved since
  * its last sort (as after a push).  Synchronises. */
+/* ---- the film: the density slices and capture scalars of the reference's
+ * movie (scripts/xenon.jl:370-410, which reads sim.rho and the cloud back to
+ * the host for every frame and renders them with GLMakie/Cairo), kept on the
+ * device as headless buffers.  Rendering is out of scope; the frames go to
+ * the caller as arrays.
+ *
+ * vlb_film_reserve allocates `capacity` frames (and frees any earlier film).
+ * A vlb_step with params.film = 1 then appends one frame after its push:
+ *   frame f: n*n float32, i fastest, the fine density's plane average
+ *            (rho[:, :, iz1] + rho[:, :, iz2]) / 2 in float32 (0-based planes;
+ *            the script's reaction plane is iz1 = nfine - 1, iz2 = nfine);
+ *   scalars[4 f .. 4 f + 3]: the projectile's x and y after the step, the
+ *            particles within params.capture_radius of it (0 when that radius
+ *            is <= 0) and the particles within `radius` of the origin (the
+ *            script's net charge is nions - weight * that count, radius 35).
+ * Frames past the capacity are counted, not stored.  Steps with film = 0 run
+ * the film's kernels as no-ops (the captured step keeps them); batch and
+ * sharded steps take no frames.  Reserving or clearing drops the captured
+ * step.  No counterpart entry point in the reference. */
+VLB_API int vlb_film_reserve(vlb_ctx* ctx, int32_t capacity, int32_t iz1, int32_t iz2, double radius);
+/* Frames asked for since the reservation (taken) and held (stored = min(taken,
+ * capacity)).  Synchronises. */
+VLB_API int vlb_film_frames(vlb_ctx* ctx, int32_t* taken, int32_t* stored);
+/* Frames [first, first + count) to host arrays: frames [count*n*n] float32,
+ * scalars [4*count] float64 (either may be NULL).  Synchronises. */
+VLB_API int vlb_film_download(vlb_ctx* ctx, int32_t first, int32_t count, float* frames, double* scalars);
+VLB_API int vlb_film_clear(vlb_ctx* ctx);
+
 #define VLB_ENERGY_TOTAL 0
 #define VLB_ENERGY_HARTREE 1
 VLB_API int vlb_interaction_energy(vlb_ctx* ctx, int32_t coefficients, double* out);

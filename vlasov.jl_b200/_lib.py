@@ -43,7 +43,8 @@ EXPORTS = (
     "vlb_last_error", "vlb_version", "vlb_create", "vlb_destroy", "vlb_upload_particles",
     "vlb_download_particles", "vlb_sort", "vlb_get_sort", "vlb_deposit_fine", "vlb_deposit_coarse",
     "vlb_poisson", "vlb_set_precision", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
-    "vlb_push", "vlb_step", "vlb_interaction_energy", "vlb_dn_weight_count", "vlb_set_denoiser", "vlb_clear_denoiser", "vlb_dn_create",
+    "vlb_push", "vlb_step", "vlb_interaction_energy", "vlb_film_reserve", "vlb_film_frames", "vlb_film_download",
+    "vlb_film_clear", "vlb_dn_weight_count", "vlb_set_denoiser", "vlb_clear_denoiser", "vlb_dn_create",
     "vlb_dn_destroy", "vlb_dn_forward", "vlb_dn_gradient", "vlb_dn_adam", "vlb_dn_status", "vlb_dn_active_tiles", "vlb_set_tuning", "vlb_get_tuning", "vlb_batch_create", "vlb_batch_step",
     "vlb_batch_destroy", "vlb_exchange_buffers", "vlb_step_deposit", "vlb_step_fields", "vlb_step_advance",
     "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
@@ -85,7 +86,7 @@ class StepParams(C.Structure):
                 ("jellium_radius", C.c_double), ("capture_radius", C.c_double), ("deposit_mode", C.c_int32),
                 ("advance_projectile", C.c_int32), ("push", C.c_int32), ("use_graph", C.c_int32),
                 ("poisson_precision", C.c_int32), ("denoise", C.c_int32), ("energy", C.c_int32),
-                ("pad_", C.c_int32)]
+                ("film", C.c_int32)]
 
 
 class StepResult(C.Structure):
@@ -159,6 +160,10 @@ def lib():
             "vlb_step": (C.c_int, [vp, C.POINTER(ProjectileDesc), C.POINTER(StepParams), C.POINTER(StepResult)]),
             "vlb_exchange_buffers": (C.c_int, [vp, C.c_int32, C.POINTER(Exchange)]),
             "vlb_interaction_energy": (C.c_int, [vp, C.c_int32, P_D]),
+            "vlb_film_reserve": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, C.c_double]),
+            "vlb_film_frames": (C.c_int, [vp, P_I, P_I]),
+            "vlb_film_download": (C.c_int, [vp, C.c_int32, C.c_int32, P_F, P_D]),
+            "vlb_film_clear": (C.c_int, [vp]),
             "vlb_dn_weight_count": (C.c_int, []),
             "vlb_set_denoiser": (C.c_int, [vp, P_F, C.c_int32, C.c_double, C.c_double]),
             "vlb_clear_denoiser": (C.c_int, [vp]),

@@ -173,6 +173,8 @@ void destroy_ctx(Ctx* c) {
   dfree(c->e_items); dfree(c->e_blocks);
   for (auto& w : c->work) dfree(w);
   free_denoiser(*c);
+  dfree(c->film_frames);
+  dfree(c->film_scalars);
   dfree(c->tc_sync);
   dfree(c->dsc);
   if (c->hsc) cudaFreeHost(c->hsc);
@@ -209,8 +211,9 @@ size_t grid_size(Ctx& c, int which) {
 }
 
 // projectile -> device scalars (persistent part)
-void upload_projectile(Ctx& c, const vlb_projectile* p) {
+void upload_projectile(Ctx& c, const vlb_projectile* p, int32_t film_due = 0) {
   DeviceScalars& h = *c.hin;
+  h.film_due = film_due;
   for (int d = 0; d < 3; ++d) {
     h.proj_pos[d] = p ? p->position[d] : 0.0;
     h.proj_prev[d] = p ? p->previous[d] : 0.0;
@@ -223,7 +226,7 @@ void upload_projectile(Ctx& c, const vlb_projectile* p) {
   h.proj_ball = p ? p->ball_radius : 1.0;
   h.proj_active = p ? p->active : 0;
   const size_t off = offsetof(DeviceScalars, proj_pos);
-  const size_t len = offsetof(DeviceScalars, pad1) - off;
+  const size_t len = offsetof(DeviceScalars, film_due) + sizeof(int32_t) - off;
   VLB_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(c.dsc) + off, reinterpret_cast<char*>(c.hin) + off, len,
                            cudaMemcpyHostToDevice, c.stream));
 }
@@ -301,6 +304,9 @@ void enqueue_phase_advance(Ctx& c, const vlb_step_params& p) {
   // the interaction with the total potential at the advanced positions
   // (src/simulation.jl:393-394)
   if (p.energy) launch_energy(c, c.fine.csol, c.coarse.csol, &c.dsc->energy[1]);
+  // a film frame when the step asked for one (the kernels return at once
+  // otherwise, so a captured step keeps them)
+  if (c.film_cap > 0) launch_film(c, p.capture_radius);
   stage_mark(c, 9);
 }
 
@@ -685,6 +691,7 @@ int check_step_params(Ctx& c, const vlb_step_params* params) {
   if (params->deposit_mode != VLB_DEPOSIT_FLOAT32 && params->deposit_mode != VLB_DEPOSIT_FIXED64)
     return fail(VLB_ERR_ARG, "unknown deposit mode");
   if (params->denoise && !c.dn) return fail(VLB_ERR_STATE, "denoise asked for, and no denoiser is set");
+  if (params->film && c.film_cap <= 0) return fail(VLB_ERR_STATE, "a film frame asked for, and no film is reserved");
   return check_precision(c, params->poisson_precision);
 }
 
@@ -746,7 +753,7 @@ int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, 
   c.mode_precision = params->poisson_precision;
   return guarded([&]() -> int {
     c.shard_phase = 0;
-    upload_projectile(c, proj);
+    upload_projectile(c, proj, params->film ? 1 : 0);
     const bool graph = params->use_graph && !c.profile;
     // the captured step starts from keys written by the previous push
     if (graph && c.graph_valid && c.keys_ready && same_params(c.graph_params, *params)) {
@@ -808,6 +815,79 @@ int vlb_clear_denoiser(vlb_ctx* ctx) {
     free_denoiser(c);
     ++c.config_epoch;
     c.graph_valid = false;
+    return VLB_OK;
+  });
+}
+
+// ------------------------------------------------------------ film
+int vlb_film_reserve(vlb_ctx* ctx, int32_t capacity, int32_t iz1, int32_t iz2, double radius) {
+  CTX_OR_FAIL;
+  const int n = c.fine.n;
+  if (capacity < 1 || iz1 < 0 || iz1 >= n || iz2 < 0 || iz2 >= n || !(radius >= 0))
+    return fail(VLB_ERR_ARG, "vlb_film_reserve: capacity >= 1, planes in [0, n) and radius >= 0 are required");
+  if ((size_t)capacity * n * n > ((size_t)1 << 34))
+    return fail(VLB_ERR_ARG, "vlb_film_reserve: more than 64 GB of frames");
+  return guarded([&]() -> int {
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    dfree(c.film_frames);
+    dfree(c.film_scalars);
+    c.film_cap = 0;
+    c.film_frames = dalloc<float>((size_t)capacity * n * n);
+    c.film_scalars = dalloc<double>(4 * (size_t)capacity);
+    VLB_CUDA(cudaMemset(&c.dsc->film_next, 0, sizeof(int32_t)));
+    VLB_CUDA(cudaMemset(&c.dsc->film_inside, 0, sizeof(unsigned long long)));
+    c.film_cap = capacity;
+    c.film_iz1 = iz1;
+    c.film_iz2 = iz2;
+    c.film_r2 = radius * radius;
+    c.graph_valid = false;  // the captured step gains the film's kernels
+    ++c.config_epoch;
+    return VLB_OK;
+  });
+}
+
+int vlb_film_frames(vlb_ctx* ctx, int32_t* taken, int32_t* stored) {
+  CTX_OR_FAIL;
+  if (c.film_cap <= 0) return fail(VLB_ERR_STATE, "vlb_film_frames: no film is reserved");
+  return guarded([&]() -> int {
+    int32_t next = 0;
+    VLB_CUDA(cudaMemcpyAsync(&next, &c.dsc->film_next, sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    if (taken) *taken = next;
+    if (stored) *stored = next < c.film_cap ? next : c.film_cap;
+    return VLB_OK;
+  });
+}
+
+int vlb_film_download(vlb_ctx* ctx, int32_t first, int32_t count, float* frames, double* scalars) {
+  CTX_OR_FAIL;
+  if (c.film_cap <= 0) return fail(VLB_ERR_STATE, "vlb_film_download: no film is reserved");
+  if (first < 0 || count < 0 || first + count > c.film_cap)
+    return fail(VLB_ERR_ARG, "vlb_film_download: frames out of the reserved range");
+  const size_t nn = (size_t)c.fine.n * c.fine.n;
+  return guarded([&]() -> int {
+    if (frames && count)
+      VLB_CUDA(cudaMemcpyAsync(frames, c.film_frames + (size_t)first * nn, (size_t)count * nn * sizeof(float),
+                               cudaMemcpyDeviceToHost, c.stream));
+    if (scalars && count)
+      VLB_CUDA(cudaMemcpyAsync(scalars, c.film_scalars + 4 * (size_t)first, 4 * (size_t)count * sizeof(double),
+                               cudaMemcpyDeviceToHost, c.stream));
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_film_clear(vlb_ctx* ctx) {
+  CTX_OR_FAIL;
+  return guarded([&]() -> int {
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    dfree(c.film_frames);
+    dfree(c.film_scalars);
+    c.film_frames = nullptr;
+    c.film_scalars = nullptr;
+    c.film_cap = 0;
+    c.graph_valid = false;
+    ++c.config_epoch;
     return VLB_OK;
   });
 }

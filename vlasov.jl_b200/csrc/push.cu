@@ -213,6 +213,56 @@ __global__ void __launch_bounds__(256) k_enclosed(int64_t N, int64_t Npad, const
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&dsc->enclosed, cnt);
 }
 
+// ---- the film: what scripts/xenon.jl:396-410 reads back for a frame of its
+// movie, kept on the device.  Each kernel returns at once unless the step
+// asked for a frame (film_due, uploaded with the projectile), so the three
+// stay in a captured step.  Frame f = film_next: the fine density's plane
+// average Float32.((rho[:, :, iz1] + rho[:, :, iz2]) ./ 2), then four
+// float64 scalars: the projectile's x and y after its step, the step's count
+// within the capture radius of it (enclosed_charge, src/projectile.jl:243),
+// and the count within the film radius of the origin (the script's net
+// charge, 196 - w #{|r| < 35}).  Frames past the capacity are counted, not
+// stored.
+__global__ void __launch_bounds__(256) k_film_slice(const float* __restrict__ rho, int n, int iz1, int iz2,
+                                                    float* __restrict__ frames, int cap,
+                                                    const DeviceScalars* __restrict__ dsc) {
+  if (!dsc->film_due) return;
+  const int f = dsc->film_next;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= cap || t >= n * n) return;
+  const size_t nn = (size_t)n * n;
+  frames[(size_t)f * nn + t] = __fmul_rn(__fadd_rn(rho[(size_t)iz1 * nn + t], rho[(size_t)iz2 * nn + t]), 0.5f);
+}
+
+// Particles within sqrt(r2) of the origin, float64 positions as k_enclosed.
+__global__ void __launch_bounds__(256) k_film_count(int64_t N, int64_t Npad, const int32_t* __restrict__ k,
+                                                    const float* __restrict__ d, double x0, double h, double r2,
+                                                    DeviceScalars* dsc) {
+  if (!dsc->film_due) return;
+  unsigned long long cnt = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    const double px = x0 + (double)(k[i] - 1) * h + (double)d[i];
+    const double py = x0 + (double)(k[Npad + i] - 1) * h + (double)d[Npad + i];
+    const double pz = x0 + (double)(k[2 * Npad + i] - 1) * h + (double)d[2 * Npad + i];
+    if (px * px + py * py + pz * pz < r2) ++cnt;
+  }
+  cnt = __reduce_add_sync(0xffffffffu, (unsigned)cnt);
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&dsc->film_inside, cnt);
+}
+
+__global__ void k_film_finish(double* __restrict__ scalars, int cap, int have_capture, DeviceScalars* dsc) {
+  if (!dsc->film_due) return;
+  const int f = dsc->film_next;
+  if (f < cap) {
+    scalars[4 * (size_t)f + 0] = dsc->proj_pos[0];
+    scalars[4 * (size_t)f + 1] = dsc->proj_pos[1];
+    scalars[4 * (size_t)f + 2] = have_capture ? (double)dsc->enclosed : 0.0;
+    scalars[4 * (size_t)f + 3] = (double)dsc->film_inside;
+  }
+  dsc->film_next = f + 1;
+  dsc->film_inside = 0;
+}
+
 // Long chains of independent FMAs: the FP32 pipe's ceiling at the current
 // clocks, the denominator of the gather's and deposit's roofline.
 __global__ void __launch_bounds__(256) k_fma_peak(float* out, int iters, float a, float b) {
@@ -280,6 +330,18 @@ void launch_projectile_update(Ctx& c, double dt, double nions, double jradius, i
 
 void launch_projectile_force_only(Ctx& c, double nions, double jradius) {
   k_projectile<<<1, 32, 0, c.stream>>>(c.dsc, c.weight, 0.0, nions, jradius, 0);
+  VLB_LAUNCHED(c);
+}
+
+void launch_film(Ctx& c, double capture_radius) {
+  Particles& P = c.part[c.cur];
+  const int n = c.fine.n;
+  k_film_slice<<<(n * n + 255) / 256, 256, 0, c.stream>>>(c.fine.rho, n, c.film_iz1, c.film_iz2, c.film_frames,
+                                                         c.film_cap, c.dsc);
+  VLB_LAUNCHED(c);
+  k_film_count<<<grid_for(c, c.N, 256, 8), 256, 0, c.stream>>>(c.N, c.Npad, P.k, P.d, c.x0, c.h, c.film_r2, c.dsc);
+  VLB_LAUNCHED(c);
+  k_film_finish<<<1, 1, 0, c.stream>>>(c.film_scalars, c.film_cap, capture_radius > 0 ? 1 : 0, c.dsc);
   VLB_LAUNCHED(c);
 }
 

@@ -63,8 +63,11 @@ struct DeviceScalars {
   double proj_pos[3], proj_prev[3], proj_vel[3], proj_force[3];
   double proj_charge, proj_mass, proj_sigma, proj_ball;
   int32_t proj_active;
-  int32_t pad1;
+  int32_t film_due;                  // 1: this step appends a film frame (uploaded with the projectile)
   double e_el, e_jel;
+  unsigned long long film_inside;    // particles within the film radius of the origin (a frame's count)
+  int32_t film_next;                 // frames taken since vlb_film_reserve
+  int32_t film_pad;
 };
 
 struct Level {
@@ -166,6 +169,11 @@ struct Ctx {
   float* dn_weights = nullptr;  // BF16-rounded weights on the device
   float* dn_pred = nullptr;     // [n^3] its prediction
   double dn_scale = 1, dn_tol = 1e-3;
+  // the film (vlb_film_reserve): density slices and their scalars
+  int film_cap = 0, film_iz1 = 0, film_iz2 = 0;
+  double film_r2 = 0;
+  float* film_frames = nullptr;    // [film_cap][n_fine^2]
+  double* film_scalars = nullptr;  // [film_cap][4]
   // scalars
   DeviceScalars* dsc = nullptr;
   DeviceScalars* hsc = nullptr;  // pinned, results
@@ -230,6 +238,7 @@ void launch_projectile_update(Ctx& c, double dt, double nions, double jradius, i
 void launch_projectile_force_only(Ctx& c, double nions, double jradius);
 void launch_push(Ctx& c, double dt, double rcmax, double capture_radius, bool keys);
 void launch_enclosed(Ctx& c, double radius);
+void launch_film(Ctx& c, double capture_radius);
 
 
 }  // namespace vlb

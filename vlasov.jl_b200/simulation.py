@@ -452,6 +452,28 @@ class DeviceAccelerator:
     def profile(self, on: bool):
         L.check(L.lib().vlb_profile(self._h, int(on)))
 
+    # -- the film (vlb_film_*): density slices and capture scalars on the device
+    def film_reserve(self, capacity: int, iz1: int, iz2: int, radius: float):
+        L.check(L.lib().vlb_film_reserve(self._h, int(capacity), int(iz1), int(iz2), float(radius)))
+
+    def film_frames(self) -> tuple[int, int]:
+        """(taken, stored) frames since the reservation."""
+        taken, stored = C.c_int32(), C.c_int32()
+        L.check(L.lib().vlb_film_frames(self._h, C.byref(taken), C.byref(stored)))
+        return taken.value, stored.value
+
+    def film_download(self, first: int = 0, count: int | None = None):
+        """(frames (count, n, n) float32 [j][i], scalars (count, 4) float64)."""
+        if count is None:
+            count = self.film_frames()[1] - first
+        frames = np.empty((count, self.nf, self.nf), np.float32)
+        scalars = np.empty((count, 4), np.float64)
+        L.check(L.lib().vlb_film_download(self._h, int(first), int(count), L.pf(frames), L.pd(scalars)))
+        return frames, scalars
+
+    def film_clear(self):
+        L.check(L.lib().vlb_film_clear(self._h))
+
     def interaction_energy(self, coefficients: int = L.VLB_ENERGY_TOTAL) -> float:
         """sum w phi over the cloud as it is (interaction_energy, src/energy.jl:19-43)."""
         out = C.c_double()
@@ -509,6 +531,20 @@ class EnergyBudget:
                             d.escaped)
 
 
+@dataclass
+class Film:
+    """Frames of the reference's movie (scripts/xenon.jl:370-410), as arrays:
+    frames (count, n, n) float32 [j][i], the projectile's x and y, q(<capture
+    radius) around it and the net charge nions - w #{|r| < radius}; `taken`
+    counts the frames asked for (more than stored when the film was full)."""
+    frames: np.ndarray
+    proj_x: np.ndarray
+    proj_y: np.ndarray
+    q_capture: np.ndarray
+    q_net: np.ndarray
+    taken: int
+
+
 class Simulation:
     """The reference's resident device simulation (src/simulation.jl:171-216,
     472-531): meshes and tables built once on the host in float64, the packed
@@ -539,7 +575,8 @@ class Simulation:
     def mass(self):
         return ELECTRON_MASS * self.weight
 
-    def _params(self, *, advance: bool, push: bool, capture: float, energy: bool = False) -> L.StepParams:
+    def _params(self, *, advance: bool, push: bool, capture: float, energy: bool = False,
+                film: bool = False) -> L.StepParams:
         sp = L.StepParams()
         sp.dt = self.params.dt
         sp.rcmax = self.params.rcmax
@@ -553,6 +590,7 @@ class Simulation:
         sp.poisson_precision = self.precision
         sp.denoise = int(self.denoise and push)
         sp.energy = int(energy and push)
+        sp.film = int(film and push)
         return sp
 
     def prime_leapfrog(self, positions, momenta, consistent: bool = False):
@@ -575,16 +613,33 @@ class Simulation:
         pk, pd = pack_positions(back, self.x0, self.h)
         acc.upload(k, d, pk, pd)
 
-    def step(self, energy: bool = False) -> StepDiagnostics:
+    def step(self, energy: bool = False, film: bool = False) -> StepDiagnostics:
         """step!(sim; energy) on the device.  With energy, the diagnostics
         carry the budget's two sums (EnergyBudget.of(sim.jellium, d) is the
-        reference's return value)."""
+        reference's return value).  With film, the step appends a frame to
+        the film reserved by film()."""
         r = self.accelerator.fused_step(self.projectile, self._params(advance=True, push=True,
-                                                                      capture=self.capture_radius, energy=energy))
+                                                                      capture=self.capture_radius, energy=energy,
+                                                                      film=film))
         self.steps_done += 1
         return StepDiagnostics(r.kinetic, r.escaped, tuple(r.angular), r.enclosed_charge, r.nout, r.outcount,
                                r.noccupied, tuple(r.projectile_force), r.total_charge, r.status, r.denoised,
                                r.hartree, r.interaction)
+
+    def film(self, capacity: int, radius: float = 35.0):
+        """Reserves `capacity` frames of the reference's movie
+        (scripts/xenon.jl:370-410): the fine density averaged over the two
+        planes around z = 0 and the capture scalars, taken on the device by
+        the steps run with film=True."""
+        n = self.params.nfine
+        self.accelerator.film_reserve(capacity, n - 1, n, radius)
+
+    def film_frames(self) -> "Film":
+        """The frames taken so far (a download; the film stays reserved)."""
+        frames, sc = self.accelerator.film_download()
+        taken, _ = self.accelerator.film_frames()
+        return Film(frames, sc[:, 0].copy(), sc[:, 1].copy(), self.weight * sc[:, 2],
+                    self.jellium.nions - self.weight * sc[:, 3], taken)
 
     def energy_budget(self, d: StepDiagnostics) -> EnergyBudget:
         """The EnergyBudget of a step run with energy=True."""

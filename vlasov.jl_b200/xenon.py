@@ -5,7 +5,10 @@ sampled from the Thomas-Fermi profile with Ran2(-1), rcluster = 78, rbox = 235,
 dt = 0.5, Xe25+ of mass 131.3*1836.154 at v = 0.40 from x = -70 with b = 45
 and a ball softening of radius 5, ceil(140 / (v dt)) = 700 steps.  It prints
 the reference's table -- q(<8 a0) and the out-of-stencil count every 50 steps
--- and the charge carried away.  The film (GLMakie/Cairo) is not produced.
+-- and the charge carried away.  With --film N the movie's frames (the
+density slice at z = 0 and the capture scalars, scripts/xenon.jl:370-410) are
+taken on the device and written as arrays; rendering them (GLMakie/Cairo in
+the reference) is not done here.
 
     python -c 'import __graft_entry__ as g; g.load().xenon.main()' --particules 8000000 --nfine 64
 
@@ -22,12 +25,16 @@ import time
 
 def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point: bool = False,
         uniform: bool = False, nsteps: int | None = None, device: int = 0, seed: int = -1, quiet: bool = False,
-        precision: str = "fp32", energy_every: int = 0, isolated: bool = False):
+        precision: str = "fp32", energy_every: int = 0, isolated: bool = False, film_stride: int = 0,
+        film_out: str | None = None):
     """Runs the crossing; returns a dict with the capture curve (q(<8) and
     outcount after every step), the final charge and the timing, and with
     energy_every > 0 the energy budget of every energy_every-th step
     (run!(sim; energy_every), src/simulation.jl:419-440).  isolated: the
-    cluster alone, no projectile (the budget's conservation test)."""
+    cluster alone, no projectile (the budget's conservation test).
+    film_stride > 0: the movie's frames (scripts/xenon.jl:370-410) at step 1
+    and every film_stride-th step, taken on the device and written to
+    film_out (.npz: frames, times_fs, proj_x, proj_y, q_capture, q_net)."""
     import numpy as np
     from . import simulation as S
 
@@ -52,11 +59,17 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
     q, out, xs = np.zeros(nsteps), np.zeros(nsteps, dtype=np.int64), np.zeros(nsteps)
     budgets = []
     acc = sim.accelerator
+    film_steps = []
+    if film_stride > 0:
+        sim.film(1 + nsteps // film_stride)
     t_run = time.time()
     tprev = t_run
     for s in range(1, nsteps + 1):
         energy = energy_every > 0 and (s - 1) % energy_every == 0
-        d = sim.step(energy=energy)
+        frame = film_stride > 0 and (s % film_stride == 0 or s == 1)
+        d = sim.step(energy=energy, film=frame)
+        if frame:
+            film_steps.append(s)
         if energy:
             b = sim.energy_budget(d)
             budgets.append({"step": s, "total": b.total, "kinetic": b.kinetic, "hartree": b.hartree,
@@ -74,6 +87,13 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
         if d.status != 0:
             raise RuntimeError(f"device status {d.status} at step {s}")
     elapsed = time.time() - t_run
+    film = None
+    if film_stride > 0:
+        f = sim.film_frames()
+        film = {"frames": len(f.frames), "q_net_final": float(f.q_net[-1]) if len(f.q_net) else None}
+        if film_out:
+            np.savez(film_out, frames=f.frames, times_fs=np.array(film_steps) * dt / fs, proj_x=f.proj_x,
+                     proj_y=f.proj_y, q_capture=f.q_capture, q_net=f.q_net)
     acc.close()
     if not quiet:
         print(f"\n{nsteps} steps in {elapsed:.1f} s -- {1000 * elapsed / nsteps:.2f} ms/step (wall clock, "
@@ -82,7 +102,7 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
     return {"npart": npart, "nfine": nfine, "nsteps": nsteps, "q8": q.tolist(), "outcount": out.tolist(),
             "x_ion": xs.tolist(), "final_q8": float(q[-1]), "final_outcount": int(out[-1]),
             "wall_s": elapsed, "built_s": built, "fixed_point": fixed_point, "uniform": uniform,
-            "precision": precision, "energy": budgets}
+            "precision": precision, "energy": budgets, "film": film}
 
 
 def main(argv=None):
@@ -97,11 +117,15 @@ def main(argv=None):
     ap.add_argument("--energy-every", type=int, default=0, help="energy budget every N steps (0: none)")
     ap.add_argument("--isolated", action="store_true", help="the cluster alone, without the projectile")
     ap.add_argument("--json", default=None, help="write the capture curve here")
+    ap.add_argument("--film", type=int, default=0,
+                    help="take the movie's frames at step 1 and every N steps on the device (the script's N is 4)")
+    ap.add_argument("--film-out", default="film.npz", help="where --film writes its frames")
     a = ap.parse_args(argv)
     if a.nfine % 2:
         ap.error("--nfine must be even")
     r = run(a.particules, a.nfine, fixed_point=a.fixed_point, uniform=a.uniform, nsteps=a.steps,
-            precision=a.precision, energy_every=a.energy_every, isolated=a.isolated)
+            precision=a.precision, energy_every=a.energy_every, isolated=a.isolated, film_stride=a.film,
+            film_out=a.film_out if a.film else None)
     if a.json:
         with open(a.json, "w") as f:
             json.dump(r, f)
