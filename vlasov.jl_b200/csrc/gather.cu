@@ -2,16 +2,17 @@
 // projectile fused in, and the out-of-stencil tail.
 //
 // Gather (src/kernels.jl:339-470, host reference src/fields.jl:305-347):
-// one CTA per occupied cell, taken from a dynamic work counter.  The cell's
-// 10^3 stencil of csol is staged once in shared memory; each thread takes a
-// particle, builds its three table columns from delta with the reference's
-// Float32 arithmetic, and contracts
+// the particles of one work item (at most `chunk` of one occupied cell)
+// share the cell's 10^3 stencil of csol; each particle's three table
+// columns come from delta with the reference's Float32 arithmetic, and
 //
-//     F = -w ( sum c gx oy oz, sum c ox gy oz, sum c ox oy gz )
+//     F = -w ( sum c gx oy oz, sum c ox gy oz, sum c ox oy gz ).
 //
-// with all sixty smoothing values in registers.  The sum over the stencil is
-// reassociated (y first, then x, then z) against the reference's order,
-// which changes rounding only.  The projectile's Gaussian force
+// The sum over the stencil is reassociated (y first, then x, then z)
+// against the reference's order, which changes rounding only.  Two forms:
+// k_field_tc (the default) computes the sums over y of a whole item as
+// 3xTF32 GEMMs on the tensor cores and finishes each particle on the CUDA
+// cores; k_field computes everything with FP32 FMAs, one warp per item.  The projectile's Gaussian force
 // (src/projectile.jl:95-108) is evaluated per particle at the position
 // rebuilt from the *cell's* (clamped) knots, as the reference does, its
 // reaction subtracted, and the four reaction sums reduced per CTA in float64.
