@@ -33,6 +33,9 @@ import numpy as np  # noqa: E402
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 GATHER_FLOP_PER_PARTICLE = 4600.0       # 2000 FMA + 300 mul/FMA per 10^3 contraction
 GATHER_TC_FLOP_PER_PARTICLE = 12000.0   # 3 split products x (oy, gy) x 100 columns x 10 y x 2
+# DRAM bytes (read + write) of one gather launch per particle, from the ncu
+# captures of 4e6 particles (profiles/k_field_tc_4M.md, profiles/k_field_4M.md)
+GATHER_TRAFFIC_PER_PARTICLE = {"tcgen05": (49486336 + 6479616) / 4e6, "fp32": (49494784 + 7127296) / 4e6}
 PUSH_BYTES_PER_PARTICLE = 48 + 12 + 48 + 4  # read (k, d, pk, pd) + force; write the record + the next sort's cell key
 
 
@@ -378,7 +381,11 @@ def main():
         "gpu_launches": int(launches),
         "roofline": {"kernel": gather_kernel, "bound": "fp32",
                      "achieved": achieved, "peak": fp32_peak.value, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak.value, "traffic": None,
+                     "frac": achieved / fp32_peak.value,
+                     "traffic": GATHER_TRAFFIC_PER_PARTICLE[args.gather] * args.npart,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 4e6-particle launch, "
+                                       "scaled by the particle count (bytes per launch; the forces written "
+                                       "mostly stay in L2 past the kernel's end)",
                      "flop_per_particle": GATHER_FLOP_PER_PARTICLE,
                      "note": "FP32-equivalent FLOP of the smoothed gather (the reference's operation count) over "
                              "the forces stage's event time",
