@@ -633,7 +633,9 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     // ---- item t
     bool got = false;
     if (cur.has && ok && ((pending >> b) & 1u)) {
-      got = mbar_wait(smem_u32(&bars[b]), (phase >> b) & 1u);
+      // the same outcome in the whole warp: the tensor-memory loads of the
+      // finish are warp-collective
+      got = __all_sync(0xffffffffu, mbar_wait(smem_u32(&bars[b]), (phase >> b) & 1u));
       ok = got;
       if (got) {
         pending &= ~(1u << b);
