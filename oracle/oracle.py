@@ -7,7 +7,8 @@ two semantics the reference has:
 * ``DeviceSemanticsStep``: the resident device path (src/simulation.jl:472-531)
   on the packed float32 cloud, continuous arithmetic in float64;
 * ``HostStep``: the CPU path (src/simulation.jl:309-352) on float64 positions,
-  the config-1 reference run and the CPU baseline.
+  the reference's CPU run of the small crossing (nfine = 28, 1e5 particles)
+  and the CPU baseline.
 
 Only tests/, __graft_entry__.smoke() and bench.py (its CPU-baseline and
 reference arms) import this module.
