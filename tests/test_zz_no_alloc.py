@@ -1,11 +1,11 @@
 """The allocation-free total charge, for callers that cannot allocate device
 memory: an embedding runtime whose caching pool holds the GPU's memory, a
 plugin whose host forbids allocation after set-up, a loop that must not stall
-on cudaMalloc.  The entry point
-keeps its scratch in static device memory; here the caller (the test) owns
-the device inputs and the output, and the result is checked against the
-charge the existing fine-deposit entry point reports for the same density,
-on two calls in a row.  The file is collected last on purpose."""
+on cudaMalloc.  The entry point keeps its scratch in static device memory;
+here the caller (the test) owns the device inputs and the output, and the
+result is checked against the charge the existing fine-deposit entry point
+reports for the same density, on two calls in a row.  The file is collected
+last on purpose."""
 import ctypes as C
 
 import numpy as np
