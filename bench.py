@@ -33,6 +33,7 @@ import numpy as np  # noqa: E402
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 GATHER_FLOP_PER_PARTICLE = 4600.0       # 2000 FMA + 300 mul/FMA per 10^3 contraction
 GATHER_TC_FLOP_PER_PARTICLE = 12000.0   # 3 split products x (oy, gy) x 100 columns x 10 y x 2
+GATHER_BYTES_PER_PARTICLE = 24.0        # delta in, force out
 # DRAM bytes (read + write) of one gather launch per particle, from the ncu
 # captures of 4e6 particles (profiles/k_field_tc_4M.md, profiles/k_field_4M.md)
 GATHER_TRAFFIC_PER_PARTICLE = {"tcgen05": (49486336 + 6479616) / 4e6, "fp32": (49494784 + 7127296) / 4e6}
@@ -389,7 +390,12 @@ def main():
                      "flop_per_particle": GATHER_FLOP_PER_PARTICLE,
                      "note": "FP32-equivalent FLOP of the smoothed gather (the reference's operation count) over "
                              "the forces stage's event time",
-                     "peak_source": "measured FP32 FMA kernel (vlb_fp32_peak), this GPU, this run"},
+                     "peak_source": "measured FP32 FMA kernel (vlb_fp32_peak), this GPU, this run",
+                     "hbm_beside": {"achieved": GATHER_BYTES_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e9,
+                                    "peak": pk_.get("hbm_gbs"), "unit": "GB/s",
+                                    "frac": GATHER_BYTES_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e9
+                                    / pk_.get("hbm_gbs", 1),
+                                    "note": "12 B of delta read + 12 B of force written a particle"}},
         "roofline_hbm": {"kernel": "k_push (packed Verlet)", "bound": "hbm", "achieved": push_gbs,
                          "peak": pk_.get("hbm_gbs"), "unit": "GB/s", "frac": push_gbs / pk_.get("hbm_gbs", 1),
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({how})"},
