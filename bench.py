@@ -56,7 +56,7 @@ def parse():
                     help="the gather's sums over y as 3xTF32 MMAs on the tensor cores, or FP32 FMAs")
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--cpu-steps", type=int, default=6, help="timed steps of the CPU baseline (primed, 1 warm-up)")
     ap.add_argument("--no-learned", action="store_true", help="skip the step with the learned denoiser")
     return ap.parse_args()
 
@@ -147,61 +147,54 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def cpu_baseline(args, vb, nthreads=None):
-    """The oracle's restatement of the reference CPU step, timed on the host
-    cores.  Sample: `cpu_steps` full steps of the same workload."""
+def host_reference(args, nsteps, warmup):
+    """The reference's CPU step path (update_forces! + step!, src/simulation.jl:
+    309-352, 382-396) as the oracle restates it (oracle.HostStep, float64,
+    OpenMP over the host cores), on this workload: the oracle's own seeded
+    draw of the cloud (no product library is loaded), prime_leapfrog!
+    (src/simulation.jl:233-277), `warmup` untimed steps, then `nsteps` timed
+    steps.  The set-up tables come from the package's pure-Python table
+    builders, as the reference's host hands its own tables over.  Returns
+    (ms per step, threads)."""
     from oracle import oracle as orc
+    vb = load()
     p, prof, proj = workload(args, vb)
     meshes = vb.build_meshes(p.nfine, p.ninner, p.nouter, p.rcluster, p.rbox)
     sm = vb.gaussian_smoothing(meshes.fine.axis)
     w = p.nelectrons / p.nparticles
-    pos, mom = vb.sample_thomas_fermi(prof, p.nparticles, w)
+    pos, mom = orc.sample_thomas_fermi(prof, p.nparticles, w, seed=-1)
     jel = vb.Jellium.of(p.nions)
-    if nthreads:
-        orc.lib().orc_set_threads(nthreads)
     cores = orc.lib().orc_num_threads()
+    proj.softening_mode = 1  # the CPU path's ball softening (src/projectile.jl:203-232)
     st = orc.HostStep(meshes, sm, w, jel, p.dt, p.rcmax, proj)
-    prev = pos - p.dt * mom / w  # a step back at constant velocity (timing sample only)
-    st.step(pos, prev)           # untimed warm-up of the buffers
-    t0 = time.perf_counter()
-    for _ in range(args.cpu_steps):
+    pos, prev = st.prime(pos, mom)
+    for _ in range(warmup):
         pos, prev, _ = st.step(pos, prev)
-    dt = (time.perf_counter() - t0) / args.cpu_steps
-    return dt * 1e3, cores
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        pos, prev, _ = st.step(pos, prev)
+    return (time.perf_counter() - t0) / nsteps * 1e3, cores
+
+
+REFERENCE_MAX_TIMED = 60  # timed CPU steps at most: about 75 s of the 16-thread host at 8e6
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    vb = load()
-    ms, cores = None, None
-    from oracle import oracle as orc
-    p, prof, proj = workload(args, vb)
-    meshes = vb.build_meshes(p.nfine, p.ninner, p.nouter, p.rcluster, p.rbox)
-    sm = vb.gaussian_smoothing(meshes.fine.axis)
-    w = p.nelectrons / p.nparticles
-    pos, mom = vb.sample_thomas_fermi(prof, p.nparticles, w)
-    jel = vb.Jellium.of(p.nions)
-    cores = orc.lib().orc_num_threads()
-    st = orc.HostStep(meshes, sm, w, jel, p.dt, p.rcmax, proj)
-    # priming as the reference CPU path does it (src/simulation.jl:233-277)
-    half = pos - (p.dt / (2 * w)) * mom
-    force, _ = st.update_forces(half, advance=False)
-    prev = -pos + 2 * half + (p.dt / w) * force
-    for _ in range(args.warmup):
-        pos, prev, _ = st.step(pos, prev)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        pos, prev, _ = st.step(pos, prev)
-    ms = (time.perf_counter() - t0) / args.steps * 1e3
+    timed = max(1, min(args.steps, REFERENCE_MAX_TIMED))
+    warm = max(1, min(args.warmup, 3))
+    ms, cores = host_reference(args, timed, warm)
     line = {"metric": "ms/step at 8M particles, 130^3 grid; learned vs plain at equal capture error", "value": ms, "unit": "ms/step", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ran2 Thomas-Fermi cloud)",
             "config": config_dict(args, 1), "impl": "reference",
             "cpu_baseline": {"value": ms, "unit": "ms/step", "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} full CPU steps of the workload (float64 restatement of the "
-                                       "reference CPU path, OpenMP contiguous chunks)"},
+                             "sample": f"{timed} primed full CPU steps of the workload after {warm} untimed ones "
+                                       "(float64 restatement of the reference CPU path, OpenMP contiguous chunks, "
+                                       "ball softening; at most "
+                                       f"{REFERENCE_MAX_TIMED} timed steps whatever --steps asks)"},
             "e2e": {"value": ms, "unit": "ms/step", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -346,12 +339,33 @@ def main():
                    "steps": args.steps, "network": "vlasov.jl_b200/data/denoiser_xe25_130.npz",
                    "trained_on": meta_dn}
 
+    # the strict FP32 drop-in: mode products and the gather's sums on the
+    # CUDA cores in FP32, the same steps timed the same way
+    fp32 = None
+    if world == 1:
+        saved_prec = sim.precision
+        sim.precision = vb._lib.VLB_POISSON_FP32
+        acc.set_tuning(field_tensor_cores=0)
+        for _ in range(max(args.warmup, 3)):
+            sim.step()
+        j0, j1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        j0.record(ext)
+        for _ in range(args.steps):
+            sim.step()
+        j1.record(ext)
+        j1.synchronize()
+        fp32 = {"ms_per_step": j0.elapsed_time(j1) / args.steps, "steps": args.steps,
+                "mode_products": "fp32 (CUDA cores)", "gather": "fp32 (CUDA cores)",
+                "note": "the plain FP32 drop-in, timed like value (graph replays, CUDA events)"}
+        sim.precision = saved_prec
+        acc.set_tuning(field_tensor_cores=1 if args.gather == "tcgen05" else 0)
+
     pk_, how = peaks()
     fp32_peak = vb._lib.C.c_double()
     L.check(L.lib().vlb_fp32_peak(local, vb._lib.C.byref(fp32_peak)))
-    t_forces = stages.get("forces", float("nan"))
-    gather_kernel = ("k_field_tc (smoothed gather + projectile, sums over y as 3xTF32 tcgen05 MMAs), forces stage"
-                     if args.gather == "tcgen05" else "k_field (smoothed gather + projectile, FP32 FMAs), forces stage")
+    t_forces = stages.get("forces_kernel", float("nan"))
+    gather_kernel = ("k_field_tc (smoothed gather + projectile, sums over y as 3xTF32 tcgen05 MMAs)"
+                     if args.gather == "tcgen05" else "k_field (smoothed gather + projectile, FP32 FMAs)")
     achieved = GATHER_FLOP_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e12
     t_push = stages.get("push", float("nan"))
     push_gbs = PUSH_BYTES_PER_PARTICLE * args.npart / (t_push * 1e-3) / 1e9
@@ -363,10 +377,10 @@ def main():
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         try:
-            cms, cores = cpu_baseline(args, vb)
+            cms, cores = host_reference(args, args.cpu_steps, 1)
             cpu = {"value": cms, "unit": "ms/step", "cores": cores, "kind": "port",
-                   "sample": f"{args.cpu_steps} full CPU steps of the same workload (float64 restatement of the "
-                             "reference CPU path, OpenMP)"}
+                   "sample": f"{args.cpu_steps} primed full CPU steps of the same workload after 1 untimed one "
+                             "(float64 restatement of the reference CPU path, OpenMP, ball softening)"}
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "ms/step", "cores": None, "kind": "port", "sample": f"failed: {ex}"}
     line = {
@@ -389,7 +403,8 @@ def main():
                                        "mostly stay in L2 past the kernel's end)",
                      "flop_per_particle": GATHER_FLOP_PER_PARTICLE,
                      "note": "FP32-equivalent FLOP of the smoothed gather (the reference's operation count) over "
-                             "the forces stage's event time",
+                             "the gather kernel's own event time (events around its launch in profiled eager steps)",
+                     "kernel_ms": t_forces, "forces_stage_ms": stages.get("forces"),
                      "peak_source": "measured FP32 FMA kernel (vlb_fp32_peak), this GPU, this run",
                      "hbm_beside": {"achieved": GATHER_BYTES_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e9,
                                     "peak": pk_.get("hbm_gbs"), "unit": "GB/s",
@@ -411,6 +426,8 @@ def main():
             "flop_per_particle": GATHER_TC_FLOP_PER_PARTICLE,
             "note": "3xTF32 products of the sums over y (3 x 2 x 100 x 10 x 2 FLOP a particle, no padding)",
             "peak_source": f"dense TF32 taken as half the bf16 figure of MEASURED_PEAKS.json ({how})"}
+    if fp32:
+        line["fp32_dropin"] = fp32
     if learned:
         line["learned"] = learned
     if energy:

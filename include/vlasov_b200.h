@@ -90,10 +90,28 @@ typedef struct vlb_config {
   int32_t flags;               /* reserved, 0 */
 } vlb_config;
 
+/* How the projectile's Coulomb force is softened (vlb_projectile.softening).
+ * The reference's two paths differ here:
+ *   VLB_SOFTENING_DEVICE: its resident device path.  Particles whose 10^3
+ *     stencil fits take a Gaussian of width `sigma` (gaussian_force_kernel,
+ *     src/accelerator.jl:632, src/kernels.jl:425-443) at the position rebuilt
+ *     from their cell's clamped knots, and the projectile sums that Gaussian
+ *     reaction over every particle; out-of-stencil particles take the ball of
+ *     radius `ball_radius` on their own force (src/accelerator.jl:719-723).
+ *     e_electrons = w q sum erf(r / sqrt(2) sigma) / r.
+ *   VLB_SOFTENING_BALL: its CPU path, projectile_forces! with BallSoftening
+ *     (src/projectile.jl:79-80, 203-232): the uniform ball of radius
+ *     `ball_radius` for every particle, both ways, at the particle's own
+ *     position.  e_electrons = w sum uniform_sphere_potential(q, R, r)
+ *     (src/meanfield.jl:52-54). */
+#define VLB_SOFTENING_DEVICE 0
+#define VLB_SOFTENING_BALL 1
+
 /* Projectile state (src/projectile.jl:141-150).  `sigma` is the width of
  * the Gaussian kernel the fused force path uses, scale(softening)
- * (src/accelerator.jl:632); `ball_radius` the ball softening applied to
- * out-of-stencil particles (src/accelerator.jl:719-723). */
+ * (src/accelerator.jl:632); `ball_radius` the radius of the ball softening
+ * (the out-of-stencil particles' in VLB_SOFTENING_DEVICE, everyone's in
+ * VLB_SOFTENING_BALL). */
 typedef struct vlb_projectile {
   double position[3];
   double previous[3];
@@ -103,7 +121,7 @@ typedef struct vlb_projectile {
   double sigma;
   double ball_radius;
   int32_t active;              /* 0: isolated cluster, no projectile */
-  int32_t pad_;
+  int32_t softening;           /* VLB_SOFTENING_DEVICE (0) or VLB_SOFTENING_BALL */
 } vlb_projectile;
 
 /* Parameters of one fused step (step!(sim; energy=false), src/simulation.jl:382-416). */
@@ -351,7 +369,8 @@ VLB_API int vlb_dn_active_tiles(vlb_denoiser* dn, int32_t* n);
  *            script's net charge is nions - weight * that count, radius 35).
  * Frames past the capacity are counted, not stored.  Steps with film = 0 run
  * the film's kernels as no-ops (the captured step keeps them); batch and
- * sharded steps take no frames.  Reserving or clearing drops the captured
+ * sharded steps take no frames (they return VLB_ERR_ARG when params.film is
+ * set).  Reserving or clearing drops the captured
  * step.  No counterpart entry point in the reference. */
 VLB_API int vlb_film_reserve(vlb_ctx* ctx, int32_t capacity, int32_t iz1, int32_t iz2, double radius);
 /* Frames asked for since the reservation (taken) and held (stored = min(taken,
@@ -381,7 +400,14 @@ typedef struct vlb_tuning {
   int32_t field_tensor_cores; /* 1: the gather's sums over y as 3xTF32 MMAs
                                  (tcgen05, two CTAs per SM, field_ctas_per_sm
                                  unused; needs chunk <= 128); 0: FP32 FMAs */
-  int32_t reserved[2];
+  int32_t scan_wait_polls;    /* 0: the sort's look-back waits give up after
+                                 4,194,304 polls; n > 0: after n; -1: at once
+                                 (a test of the bounded waits).  A wait that
+                                 gives up sets VLB_STATUS_SCAN_TIMEOUT (the step
+                                 returns VLB_ERR_TIMEOUT) and its tile sums its
+                                 predecessors' inputs itself: the sort stays
+                                 exact. */
+  int32_t reserved[1];
 } vlb_tuning;
 
 VLB_API int vlb_set_tuning(vlb_ctx* ctx, const vlb_tuning* tuning);
@@ -448,7 +474,10 @@ VLB_API int vlb_stream(vlb_ctx* ctx, void** stream);
  * rho: device float32 [n*n*n], i fastest; m0: device float64 [n] (order-0 dual
  * moments); q: device float64 [1], written; stream: a cudaStream_t, or NULL.
  * Runs on the current device.  The first call on a device resolves the
- * scratch's device address; make it before any stream capture.  Calls share
+ * scratch's device address and caches it for the rest of the process; make
+ * it before any stream capture.  The cache assumes the device's context lives
+ * until exit: resetting the device (cudaDeviceReset) or tearing down and
+ * recreating its primary context between calls is not supported.  Calls share
  * the scratch: calls that overlap on the GPU race, so keep them on one stream.
  * No counterpart in the reference (its total_charge allocates through its
  * backend); the reduction is the one vlb_deposit_fine applies. */

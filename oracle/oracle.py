@@ -44,7 +44,7 @@ class OrcSmoothing(C.Structure):
 class OrcProjectile(C.Structure):
     _fields_ = [("pos", C.c_double * 3), ("prev", C.c_double * 3), ("vel", C.c_double * 3),
                 ("charge", C.c_double), ("mass", C.c_double), ("gauss_sigma", C.c_double),
-                ("ball_radius", C.c_double), ("active", C.c_int32)]
+                ("ball_radius", C.c_double), ("active", C.c_int32), ("softening", C.c_int32)]
 
 
 _lib = None
@@ -90,6 +90,7 @@ def lib():
             "orc_projectile_forces_host": (None, [ll, P_D, P_D, pp, dbl, dbl, dbl, P_D, P_D, P_D]),
             "orc_verlet_host": (None, [ll, P_D, P_D, P_D, dbl, dbl, dbl, P_D]),
             "orc_enclosed_charge_host": (dbl, [ll, P_D, dbl, P_D, dbl]),
+            "orc_sample_thomas_fermi": (None, [P_D, i32, P_D, i32, dbl, ll, dbl, i32, i32, P_D, P_D]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -157,8 +158,13 @@ class Smoothing:
         return C.byref(self.s)
 
 
-def projectile_struct(proj, active=True) -> OrcProjectile:
+SOFTENING_DEVICE = 0  # the reference's device path: Gaussian in the stencil, ball in the tail
+SOFTENING_BALL = 1    # its CPU path: the ball everywhere (src/projectile.jl:203-232)
+
+
+def projectile_struct(proj, active=True, softening=SOFTENING_DEVICE) -> OrcProjectile:
     p = OrcProjectile()
+    p.softening = softening
     if proj is None:
         p.active = 0
         p.gauss_sigma = p.ball_radius = 1.0
@@ -173,6 +179,17 @@ def projectile_struct(proj, active=True) -> OrcProjectile:
 
 
 # -------------------------------------------------------------- functions
+def sample_thomas_fermi(profile, npart: int, weight: float, seed: int = -1, consistent: bool = False):
+    """(positions, momenta) float64 (npart, 3) of the seeded ran2 stream
+    (src/initial.jl:94-113), drawn by the oracle alone."""
+    q = np.ascontiguousarray(profile.quantiles, dtype=np.float64)
+    r = np.ascontiguousarray(profile.density, dtype=np.float64)
+    pos, mom = np.empty((npart, 3)), np.empty((npart, 3))
+    lib().orc_sample_thomas_fermi(pd(q), len(q), pd(r), len(r), float(profile.rmax), int(npart), float(weight),
+                                  int(seed), int(consistent), pd(pos), pd(mom))
+    return pos, mom
+
+
 def cellsort(k: np.ndarray, nk: int):
     """Stable counting sort of a (3, N) knot array: perm, occupied, bounds, keys."""
     N = k.shape[1]
@@ -227,12 +244,13 @@ class DeviceSemanticsStep:
     discrete choices as its Float32 kernels, every continuous quantity in
     float64.  State: k, d, pk, pd as (3, N) int32/float32 arrays."""
 
-    def __init__(self, meshes, sm, weight, jellium, dt, rcmax, projectile=None):
+    def __init__(self, meshes, sm, weight, jellium, dt, rcmax, projectile=None, softening=SOFTENING_DEVICE):
         self.F, self.Cl = Level(meshes.fine), Level(meshes.coarse)
         self.S = Smoothing(sm)
         self.meshes, self.sm = meshes, sm
         self.w, self.jel, self.dt, self.rcmax = weight, jellium, dt, rcmax
         self.proj = projectile
+        self.softening = softening
         self.c = fixed_fine_constants(meshes.fine, sm)
         nf, nc = self.F.n, self.Cl.n
         self.rhof = np.zeros(nf ** 3)
@@ -270,7 +288,7 @@ class DeviceSemanticsStep:
                                       self.jel.radius)
         force = np.empty((3, N))
         red = np.zeros(4)
-        pr = projectile_struct(self.proj)
+        pr = projectile_struct(self.proj, softening=self.softening)
         self.outcount = lib().orc_forces_device(self.F.ref(), self.Cl.ref(), self.S.ref(), N, pi(ki), pf(df),
                                                 pi(self.occ), pi(self.bnd), len(self.occ), pd(self.csolf),
                                                 pd(self.csolc), self.w, c["x0"], c["h"], C.byref(pr), pd(force),
@@ -281,14 +299,14 @@ class DeviceSemanticsStep:
     def projectile_force(self):
         F = np.zeros(3)
         ee, ej = np.zeros(1), np.zeros(1)
-        pr = projectile_struct(self.proj)
+        pr = projectile_struct(self.proj, softening=self.softening)
         lib().orc_projectile_force_device(C.byref(pr), self.w, self.jel.nions, self.jel.radius, pd(self.red),
                                           pd(F), pd(ee), pd(ej))
         return F
 
     def advance_projectile(self):
         F = self.projectile_force()
-        pr = projectile_struct(self.proj)
+        pr = projectile_struct(self.proj, softening=self.softening)
         lib().orc_projectile_step(C.byref(pr), pd(F), self.dt)
         self.proj.position = np.array(pr.pos[:])
         self.proj.previous = np.array(pr.prev[:])
@@ -365,7 +383,23 @@ class HostStep:
             self.proj.velocity = np.array(pr.vel[:])
         return force, F
 
+    def prime(self, pos, mom, consistent=False):
+        """prime_leapfrog! (src/simulation.jl:233-277): the forces at the half
+        step back q(-dt/2) = q0 - dt/(2M) p, without the projectile (it is
+        neither advanced nor felt while priming, src/simulation.jl:242-246,
+        343), then q(-dt) = -q0 + 2 q(-dt/2) + c F with the Fortran's c = dt/M
+        (src/particles.jl:441-469), or dt^2/4M when `consistent`.  Returns
+        (pos, prev)."""
+        M, dt = self.w, self.dt
+        pos = np.array(pos, dtype=np.float64)  # a copy: step() advances its arrays in place
+        half = pos - (dt / (2 * M)) * mom
+        force, _ = self.update_forces(half, advance=False)
+        coef = dt * dt / (4 * M) if consistent else dt / M
+        return pos, -pos + 2 * half + coef * force
+
     def step(self, pos, prev):
+        """One step; pos and prev are advanced in place (float64 C-contiguous
+        arrays) and returned."""
         force, _ = self.update_forces(pos)
         diag = np.zeros(5)
         pos, prev = np.ascontiguousarray(pos), np.ascontiguousarray(prev)

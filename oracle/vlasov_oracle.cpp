@@ -65,6 +65,7 @@ struct orc_projectile {
   double pos[3], prev[3], vel[3];
   double charge, mass, gauss_sigma, ball_radius;
   int32_t active;
+  int32_t softening;  // 0: the device path's (Gaussian in the stencil, ball in the tail); 1: the ball everywhere
 };
 
 }  // extern "C"
@@ -647,6 +648,9 @@ long long orc_forces_device(const orc_level* F, const orc_level* C, const orc_sm
   const double *ov = sm->overlap, *gr = sm->gradient;
   double coef = pr && pr->active ? -w * pr->charge : 0.0;
   double sig = pr ? pr->gauss_sigma : 1.0;
+  // the CPU path's softening, projectile_forces! with BallSoftening
+  // (src/projectile.jl:203-232): the ball for every particle, both ways
+  const bool ball = pr && pr->softening == 1;
   double rx = 0, ry = 0, rz = 0, re = 0;
   long long nouts = 0;
 #pragma omp parallel for schedule(dynamic, 4) reduction(+ : rx, ry, rz, re, nouts)
@@ -690,7 +694,18 @@ long long orc_forces_device(const orc_level* F, const orc_level* C, const orc_sm
           fx -= m * dx; fy -= m * dy; fz -= m * dz;
         }
       }
-      if (coef != 0) {
+      if (coef != 0 && ball) {
+        // the particle's own position (the cell's, when the stencil fits)
+        double px = x0 + (double)(knode[s] - 1) * h + (double)d0;
+        double py = x0 + (double)(knode[N + s] - 1) * h + (double)d1;
+        double pz = x0 + (double)(knode[2 * N + s] - 1) * h + (double)d2;
+        double dx = pr->pos[0] - px, dy = pr->pos[1] - py, dz = pr->pos[2] - pz;
+        double d2s = dx * dx + dy * dy + dz * dz;
+        double mm = coef * ball_force_kernel(d2s, pr->ball_radius);
+        if (ok) { fx -= mm * dx; fy -= mm * dy; fz -= mm * dz; }  // the tail took its own above
+        rx += mm * dx; ry += mm * dy; rz += mm * dz;
+        re += sphere_potential(1.0, pr->ball_radius, std::sqrt(d2s));
+      } else if (coef != 0) {
         // fused projectile, position rebuilt from the (clamped) cell
         double px = x0 + (double)(kx - 1) * h + (double)d0;
         double py = x0 + (double)(ky - 1) * h + (double)d1;
@@ -1079,6 +1094,90 @@ double orc_enclosed_charge_host(long long N, const double* pos, double w, const 
     if (dx * dx + dy * dy + dz * dz < r2) ++cnt;
   }
   return w * (double)cnt;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- sampling
+// The seeded initial cloud, so that the CPU baseline needs nothing of the
+// product.  ran2 as the thesis has it (src/random.jl:31-90): L'Ecuyer's
+// two multiplicative congruential generators combined through a 32-entry
+// Bays-Durham table; IQ1 = 3668 (53668 when `consistent`), so that the
+// Schrage product k*IR1 wraps round 32 bits as the Fortran's does.
+namespace {
+
+struct OrcRan2 {
+  static constexpr int32_t M1 = 2147483563, M2 = 2147483399;
+  int32_t q1, s1, s2, last, table[32];
+
+  static int32_t wrap(int64_t v) { return (int32_t)(uint32_t)(uint64_t)v; }
+  // a*x mod m by Schrage's factorisation, in wrapping 32-bit arithmetic
+  static int32_t lcg(int32_t x, int32_t a, int32_t q, int32_t r, int32_t m) {
+    const int32_t k = x / q;
+    int32_t y = wrap((int64_t)wrap((int64_t)a * wrap((int64_t)x - (int64_t)k * q)) - (int64_t)wrap((int64_t)k * r));
+    return y < 0 ? wrap((int64_t)y + m) : y;
+  }
+  OrcRan2(int32_t seed, bool consistent) {
+    q1 = consistent ? 53668 : 3668;
+    s1 = seed < 0 ? -seed : 1;
+    if (s1 < 1) s1 = 1;
+    s2 = s1;
+    for (int j = 40; j >= 1; --j) {  // 8 warm-up draws, then the table from the top
+      s1 = lcg(s1, 40014, q1, 12211, M1);
+      if (j <= 32) table[j - 1] = s1;
+    }
+    last = table[0];
+  }
+  float uniform() {
+    s1 = lcg(s1, 40014, q1, 12211, M1);
+    s2 = lcg(s2, 40692, 52774, 3791, M2);
+    const int32_t slot = last / (1 + (M1 - 2) / 32);
+    last = wrap((int64_t)table[slot] - s2);
+    table[slot] = s1;
+    if (last < 1) last = wrap((int64_t)last + (M1 - 1));
+    const float v = (1.0f / (float)M1) * (float)last;
+    const float top = 1.0f - 1.2e-7f;
+    return v < top ? v : top;
+  }
+};
+
+// linear interpolation on [0, 1] sampled at n regular points (src/initial.jl:161-168)
+double regular_interp(const double* v, int n, double u) {
+  const int j = std::min((int)std::floor(u * (n - 1)) + 1, n - 1);
+  const double a = (double)(j - 1) / (n - 1), b = (double)j / (n - 1);
+  return v[j - 1] + (v[j] - v[j - 1]) * (u - a) / (b - a);
+}
+
+// a vector of length r in the direction (phi = 2 pi u1, cos theta = 2 u2 - 1) (src/initial.jl:323-328)
+void sphere_point(double r, double u1, double u2, double* out) {
+  const double c = 2 * u2 - 1, s = std::sqrt(1 - c * c), ph = 2 * PI * u1;
+  out[0] = r * std::cos(ph) * s;
+  out[1] = r * std::sin(ph) * s;
+  out[2] = r * c;
+}
+
+}  // namespace
+
+extern "C" {
+
+// sample_thomas_fermi (src/initial.jl:94-113, 184-203): per particle six
+// uniforms -- the radius from the quantile table, its direction, the Fermi
+// momentum p_F(r) = (3 pi^2 rho(r))^(1/3) times cbrt(u) (uniform in the
+// Fermi ball), its direction -- momenta times the weight.  AoS 3*npart.
+void orc_sample_thomas_fermi(const double* quantiles, int32_t nq, const double* density, int32_t nr, double rmax,
+                             long long npart, double weight, int32_t seed, int32_t consistent, double* pos,
+                             double* mom) {
+  OrcRan2 g(seed, consistent != 0);
+  const double kf = std::cbrt(3 * (PI * PI));
+  for (long long i = 0; i < npart; ++i) {
+    double u[6];
+    for (int j = 0; j < 6; ++j) u[j] = (double)g.uniform();
+    const double r = regular_interp(quantiles, nq, u[0]);
+    sphere_point(r, u[1], u[2], pos + 3 * i);
+    const double rho = regular_interp(density, nr, r / rmax);
+    const double p = std::cbrt(u[3]) * kf * std::cbrt(rho);
+    sphere_point(p * weight, u[4], u[5], mom + 3 * i);
+  }
 }
 
 }  // extern "C"

@@ -1,8 +1,8 @@
 """The ctypes mirrors of the C ABI's structs (vlasov.jl_b200/_lib.py) against
 the header itself: a small C program built with gcc from
 include/vlasov_b200.h prints sizeof and the offset of every field, and each
-must equal the mirror's.  A binding in another host language (the Julia
-sketch of INTEGRATION.md) has to match the same numbers."""
+must equal the mirror's.  A binding in another host language (a Julia
+ccall binding, for one) has to match the same numbers."""
 import ctypes as C
 import shutil
 import subprocess

@@ -71,6 +71,28 @@ def test_batches_refuse_bad_contexts(cuda_device):
         _close(sims)
 
 
+def test_batch_and_sharded_steps_refuse_film_frames(cuda_device):
+    import ctypes as C
+    sims = _build(cuda_device)[:2]
+    batch = SW.Batch(sims)
+    try:
+        for s in sims:
+            s.film(4)
+        params = sims[0]._params(advance=True, push=True, capture=8.0, film=True)
+        projs = (L.ProjectileDesc * 2)(*[s.projectile.to_desc() for s in sims])
+        res = (L.StepResult * 2)()
+        assert L.lib().vlb_batch_step(batch._h, projs, C.byref(params), res) == L.VLB_ERR_ARG
+        assert b"film" in L.lib().vlb_last_error()
+        p0 = sims[0].projectile.to_desc()
+        assert L.lib().vlb_step_deposit(sims[0].accelerator.handle, C.byref(p0), C.byref(params)) == L.VLB_ERR_ARG
+        # the refusals left the runs as they were: a plain batch step runs
+        assert all(d.status == 0 for d in batch.step())
+        assert sims[0].accelerator.film_frames() == (0, 0)
+    finally:
+        batch.close()
+        _close(sims)
+
+
 def test_launch_shapes_change_no_result(cuda_device):
     a, b = _build(cuda_device)[:2], _build(cuda_device)[:2]
     try:

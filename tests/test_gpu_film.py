@@ -96,6 +96,10 @@ def test_film_arguments_are_checked(cuda_device):
         sim.film(2)
         with pytest.raises(L.VlbError):
             acc.film_download(1, 2)
+        # first + count beyond int32: refused, not wrapped round
+        big = 2 ** 31 - 1
+        assert L.lib().vlb_film_download(acc.handle, big, big, None, None) == L.VLB_ERR_ARG
+        assert L.lib().vlb_film_download(acc.handle, 1, big, None, None) == L.VLB_ERR_ARG
         acc.film_clear()
         with pytest.raises(L.VlbError):
             acc.film_frames()

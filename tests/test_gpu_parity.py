@@ -202,42 +202,52 @@ def test_coefficients_and_mean_field(case, acc):
         assert rel_l2(acc.grid(wcs), c) < 2e-5
 
 
+@pytest.mark.parametrize("softening", [L.VLB_SOFTENING_DEVICE, L.VLB_SOFTENING_BALL], ids=["device-gauss", "cpu-ball"])
 @pytest.mark.parametrize("tensor_cores", [1, 0], ids=["tcgen05-3xtf32", "fp32-fma"])
-def test_forces_with_projectile(case, acc, tensor_cores):
+def test_forces_with_projectile(case, acc, tensor_cores, softening):
     """Both forms of the gather (sums over y as 3xTF32 MMAs, or FP32 FMAs)
-    against the float64 oracle, same bars."""
+    against the float64 oracle, same bars, with the projectile softened as
+    the reference's device path does (Gaussian in the stencil, ball in the
+    tail) and as its CPU path does (the ball everywhere)."""
     O = case.O
-    k, d, pk, pdl = oracle_sorted(case)
-    O.forces(k, d)
-    acc.set_tuning(field_tensor_cores=tensor_cores)
-    acc.upload(case.k, case.d, case.pk, case.pd)
-    acc.sort()
-    acc.set_grid(L.VLB_GRID_CSOL_FINE, O.csolf.astype(np.float32))
-    acc.set_grid(L.VLB_GRID_CSOL_COARSE, O.csolc.astype(np.float32))
-    # the oracle reads the same float32-rounded coefficients
-    O.csolf = acc.grid(L.VLB_GRID_CSOL_FINE).astype(np.float64).ravel()
-    O.csolc = acc.grid(L.VLB_GRID_CSOL_COARSE).astype(np.float64).ravel()
-    N = k.shape[1]
-    force = np.empty((3, N))
-    red = np.zeros(4)
-    pr = case.orc.projectile_struct(O.proj)
-    outc = case.orc.lib().orc_forces_device(O.F.ref(), O.Cl.ref(), O.S.ref(), N, case.orc.pi(k), case.orc.pf(d),
-                                            case.orc.pi(O.occ), case.orc.pi(O.bnd), len(O.occ), case.orc.pd(O.csolf),
-                                            case.orc.pd(O.csolc), case.w, O.c["x0"], O.c["h"],
-                                            __import__("ctypes").byref(pr), case.orc.pd(force), case.orc.pd(red))
-    gred, goutc = acc.forces(O.proj)
-    f = acc.force()
-    assert goutc == outc
-    out = case.orc.outside(k, case.meshes.fine.n)
-    inside = np.ones(N, bool)
-    inside[out] = False
-    acc.set_tuning(field_tensor_cores=1)
-    e_in = rel_l2(f[:, inside], force[:, inside])
-    print(f"\n[gather, tensor cores {tensor_cores}] rel L2 vs the oracle: {e_in:.2e}")
-    assert e_in < 2e-5
-    assert rel_l2(f[:, out], force[:, out]) < 1e-5
-    assert np.all(np.isfinite(f))
-    assert rel_l2(gred[:3], red[:3]) < 1e-4 and abs(gred[3] - red[3]) < 1e-4 * abs(red[3])
+    O.proj.softening_mode = softening
+    O.softening = softening
+    try:
+        k, d, pk, pdl = oracle_sorted(case)
+        O.forces(k, d)
+        acc.set_tuning(field_tensor_cores=tensor_cores)
+        acc.upload(case.k, case.d, case.pk, case.pd)
+        acc.sort()
+        acc.set_grid(L.VLB_GRID_CSOL_FINE, O.csolf.astype(np.float32))
+        acc.set_grid(L.VLB_GRID_CSOL_COARSE, O.csolc.astype(np.float32))
+        # the oracle reads the same float32-rounded coefficients
+        O.csolf = acc.grid(L.VLB_GRID_CSOL_FINE).astype(np.float64).ravel()
+        O.csolc = acc.grid(L.VLB_GRID_CSOL_COARSE).astype(np.float64).ravel()
+        N = k.shape[1]
+        force = np.empty((3, N))
+        red = np.zeros(4)
+        pr = case.orc.projectile_struct(O.proj, softening=softening)
+        outc = case.orc.lib().orc_forces_device(O.F.ref(), O.Cl.ref(), O.S.ref(), N, case.orc.pi(k), case.orc.pf(d),
+                                                case.orc.pi(O.occ), case.orc.pi(O.bnd), len(O.occ), case.orc.pd(O.csolf),
+                                                case.orc.pd(O.csolc), case.w, O.c["x0"], O.c["h"],
+                                                __import__("ctypes").byref(pr), case.orc.pd(force), case.orc.pd(red))
+        gred, goutc = acc.forces(O.proj)
+        f = acc.force()
+        assert goutc == outc
+        out = case.orc.outside(k, case.meshes.fine.n)
+        inside = np.ones(N, bool)
+        inside[out] = False
+        acc.set_tuning(field_tensor_cores=1)
+        e_in = rel_l2(f[:, inside], force[:, inside])
+        print(f"\n[gather, tensor cores {tensor_cores}, softening {softening}] rel L2 vs the oracle: {e_in:.2e}")
+        assert e_in < 2e-5
+        assert rel_l2(f[:, out], force[:, out]) < 1e-5
+        assert np.all(np.isfinite(f))
+        assert rel_l2(gred[:3], red[:3]) < 1e-4 and abs(gred[3] - red[3]) < 1e-4 * abs(red[3])
+    finally:
+        O.proj.softening_mode = L.VLB_SOFTENING_DEVICE
+        O.softening = L.VLB_SOFTENING_DEVICE
+        acc.set_tuning(field_tensor_cores=1)
 
 
 def test_verlet_push_is_bit_exact(case, acc):

@@ -1,0 +1,156 @@
+"""The reference's CPU path as the oracle restates it (oracle.HostStep:
+update_forces! and step!, src/simulation.jl:309-352, 382-396, with the
+priming of prime_leapfrog!, src/simulation.jl:233-277).  It is the CPU
+baseline and the reference arm of the benchmark, and its capture curve is
+the golden fixture the GPU's CPU-path mode is held to; these tests pin it.
+
+* its ball-softened projectile, the CPU path's projectile_forces!
+  (src/projectile.jl:203-232), equals the device-semantics oracle run with the
+  ball everywhere, particle by particle, on the same positions;
+* the priming is the reference's, with the Fortran's dt/M coefficient;
+* a few whole steps agree with the device-semantics step in the ball
+  softening (the two paths differ only in their discrete choices: float32
+  packed positions, the stencil-fit versus margin tests);
+* the first steps of the committed golden run (tests/golden/capture_host_1e5.npz,
+  made by tests/golden/make_capture_host.py) are reproduced.
+"""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import load_package
+
+vb = load_package()
+GOLDEN = Path(__file__).resolve().parent / "golden" / "capture_host_1e5.npz"
+
+
+def _setup(orc, npart, nfine=28, seed=-1):
+    p = vb.SimulationParameters.for_grid(nfine, rcluster=78.0, rbox=235.0, nparticles=npart, dt=0.5)
+    meshes = vb.build_meshes(p.nfine, p.ninner, p.nouter, p.rcluster, p.rbox)
+    sm = vb.gaussian_smoothing(meshes.fine.axis)
+    w = p.nelectrons / p.nparticles
+    pos, mom = vb.sample_thomas_fermi(vb.thomas_fermi_profile(), p.nparticles, w, seed=seed)
+    kn = meshes.fine.axis.knots
+    x0, h = float(kn[0]), float((kn[-1] - kn[0]) / (len(kn) - 1))
+    return p, meshes, sm, w, pos, mom, x0, h
+
+
+def test_ball_softening_of_the_device_oracle_is_the_cpu_projectile_forces(orc):
+    """orc_forces_device with the ball everywhere against the CPU path's
+    projectile_forces!, on zero coefficients (so that the forces are the
+    reaction alone) and positions that the packed form holds exactly."""
+    p, meshes, sm, w, pos, mom, x0, h = _setup(orc, 20_000)
+    rng = np.random.default_rng(3)
+    far = rng.random(len(pos)) < 0.1
+    pos[far] *= rng.uniform(2.5, 4.0, (far.sum(), 1))       # some outside the fine grid
+    k, d = vb.pack_positions(pos, x0, h)
+    pos = vb.unpack_positions(k, d, x0, h)                   # exactly what (k, d) holds
+    jel = vb.Jellium.of(p.nions)
+    proj = vb.xenon_projectile(x0=-6.0, impact=3.0)          # inside the cluster, ball radius 5
+    O = orc.DeviceSemanticsStep(meshes, sm, w, jel, p.dt, p.rcmax, proj, softening=orc.SOFTENING_BALL)
+    ks, ds, _, _ = O.sort(k, d, k, d)
+    N = ks.shape[1]
+    zf, zc = np.zeros(O.F.n ** 3), np.zeros(O.Cl.n ** 3)
+    force, red = np.empty((3, N)), np.zeros(4)
+    pr = orc.projectile_struct(proj, softening=orc.SOFTENING_BALL)
+    orc.lib().orc_forces_device(O.F.ref(), O.Cl.ref(), O.S.ref(), N, orc.pi(ks), orc.pf(ds), orc.pi(O.occ),
+                                orc.pi(O.bnd), len(O.occ), orc.pd(zf), orc.pd(zc), w, O.c["x0"], O.c["h"],
+                                C.byref(pr), orc.pd(force), orc.pd(red))
+    Fd, eed, ejd = np.zeros(3), np.zeros(1), np.zeros(1)
+    orc.lib().orc_projectile_force_device(C.byref(pr), w, jel.nions, jel.radius, orc.pd(red), orc.pd(Fd),
+                                          orc.pd(eed), orc.pd(ejd))
+    # the CPU path on the same positions, in the sorted order
+    ps = np.ascontiguousarray(pos[O.perm])
+    hforce = np.zeros((N, 3))
+    Fh, eeh, ejh = np.zeros(3), np.zeros(1), np.zeros(1)
+    orc.lib().orc_projectile_forces_host(N, orc.pd(ps), orc.pd(hforce), C.byref(pr), w, jel.nions, jel.radius,
+                                         orc.pd(Fh), orc.pd(eeh), orc.pd(ejh))
+    scale = np.max(np.abs(hforce))
+    assert np.max(np.abs(force.T - hforce)) < 1e-12 * scale
+    assert np.allclose(Fd, Fh, rtol=1e-11, atol=1e-13 * np.max(np.abs(Fh)))
+    assert abs(eed[0] - eeh[0]) < 1e-11 * abs(eeh[0]) and abs(ejd[0] - ejh[0]) < 1e-12 * abs(ejh[0])
+    # the Gaussian of the device path is a different softening: not the same
+    O2 = orc.projectile_struct(proj)
+    force2, red2 = np.empty((3, N)), np.zeros(4)
+    orc.lib().orc_forces_device(O.F.ref(), O.Cl.ref(), O.S.ref(), N, orc.pi(ks), orc.pf(ds), orc.pi(O.occ),
+                                orc.pi(O.bnd), len(O.occ), orc.pd(zf), orc.pd(zc), w, O.c["x0"], O.c["h"],
+                                C.byref(O2), orc.pd(force2), orc.pd(red2))
+    assert np.max(np.abs(force2.T - hforce)) > 1e-3 * scale
+
+
+def test_priming_is_prime_leapfrog_with_the_fortran_coefficient(orc):
+    p, meshes, sm, w, pos, mom, x0, h = _setup(orc, 5_000)
+    jel = vb.Jellium.of(p.nions)
+    proj = vb.xenon_projectile(x0=-10.0, impact=5.0)
+    P0 = proj.position.copy()
+    st = orc.HostStep(meshes, sm, w, jel, p.dt, p.rcmax, proj)
+    q0, prev = st.prime(pos, mom)
+    assert np.array_equal(proj.position, P0)                 # the projectile did not move
+    # the forces at q(-dt/2), without the projectile, from a fresh host step
+    ref = orc.HostStep(meshes, sm, w, jel, p.dt, p.rcmax, None)
+    half = pos - (p.dt / (2 * w)) * mom
+    F, _ = ref.update_forces(half, advance=False)
+    assert np.array_equal(q0, pos)
+    assert np.allclose(prev, pos - (p.dt / w) * mom + (p.dt / w) * F, rtol=0, atol=1e-12)
+    _, prev_c = st.prime(pos, mom, consistent=True)
+    assert np.allclose(prev_c, -pos + 2 * half + p.dt ** 2 / (4 * w) * F, rtol=0, atol=1e-12)
+
+
+def test_host_steps_follow_the_device_semantics_in_the_ball_softening(orc):
+    """Three primed steps of the CPU path against the device-semantics step
+    with the ball everywhere, from the same packed cloud."""
+    p, meshes, sm, w, pos, mom, x0, h = _setup(orc, 20_000)
+    k, d = vb.pack_positions(pos, x0, h)
+    pos = vb.unpack_positions(k, d, x0, h)
+    jel = vb.Jellium.of(p.nions)
+    mk = lambda: vb.xenon_projectile(x0=-12.0, impact=4.0)  # noqa: E731
+    H = orc.HostStep(meshes, sm, w, jel, p.dt, p.rcmax, mk())
+    q, prev = H.prime(pos, mom)
+    D = orc.DeviceSemanticsStep(meshes, sm, w, jel, p.dt, p.rcmax, mk(), softening=orc.SOFTENING_BALL)
+    # the device-semantics priming: forces at the half step, no projectile
+    proj_d = D.proj
+    D.proj = None
+    kh, dh = vb.pack_positions(pos - (p.dt / (2 * w)) * mom, x0, h)
+    kh, dh, pk, pd, _, _ = D.step(kh, dh, k.copy(), d.copy(), advance=False, push=False)
+    q0 = vb.unpack_positions(pk, pd, x0, h)
+    hp = vb.unpack_positions(kh, dh, x0, h)
+    back = -q0 + 2 * hp + (p.dt / w) * D.force.T
+    D.proj = proj_d
+    kd, dd = vb.pack_positions(q0, x0, h)
+    pkd, pdd = vb.pack_positions(back, x0, h)
+    # the host arrays follow the device-semantics sorts
+    q, prev = q[D.perm], prev[D.perm]
+    for _ in range(3):
+        q, prev, hd = H.step(q, prev)
+        kd, dd, pkd, pdd, dd_diag, _ = D.step(kd, dd, pkd, pdd)
+        q, prev = q[D.perm], prev[D.perm]
+        pos_d = vb.unpack_positions(kd, dd, x0, h)
+        err = np.abs(pos_d - q)
+        # float32 packed state against float64, and a handful of particles
+        # between the two paths' outside tests
+        assert np.median(err) < 1e-5
+        assert np.mean(err.max(axis=1) < 1e-4) > 0.999
+        assert abs(dd_diag[0] - hd[0]) < 1e-4 * hd[0]
+    assert np.allclose(H.proj.position, D.proj.position, rtol=0, atol=1e-8)
+
+
+@pytest.mark.skipif(not GOLDEN.exists(), reason="golden capture fixture not generated")
+def test_host_step_reproduces_the_golden_run_start(orc):
+    """The first 200 steps of the committed 700-step run, recomputed (the
+    projectile reaches the cluster's edge, q(<8) is non-zero from about step
+    150)."""
+    g = np.load(GOLDEN)
+    orc.lib().orc_set_threads(8)
+    p, meshes, sm, w, pos, mom, x0, h = _setup(orc, int(round(196.0 / float(g["weight"]))))
+    jel = vb.Jellium.of(p.nions)
+    proj = vb.xenon_projectile(v=0.40, impact=45.0, x0=-70.0, dt=0.5)
+    st = orc.HostStep(meshes, sm, w, jel, p.dt, p.rcmax, proj)
+    pos, prev = st.prime(pos, mom)
+    for s in range(200):
+        pos, prev, _ = st.step(pos, prev)
+        assert abs(st.enclosed_charge(pos, 8.0) - g["q8"][s]) < 0.5 * w
+        assert abs(proj.position[0] - g["x_ion"][s]) < 1e-9
+        assert st.noutf == g["margin_out"][s]
+    assert g["q8"][199] > 0.05

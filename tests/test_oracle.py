@@ -54,6 +54,21 @@ def test_sampling_python_restatement_matches_library(vb):
     assert np.array_equal(pos, p2) and np.array_equal(mom, m2)
 
 
+def test_oracle_sampler_matches_the_python_restatement_and_the_library(O, vb):
+    """The oracle's own C++ draw (the CPU baseline's, which loads nothing of
+    the product) against the pure-Python ran2 restatement and the library's
+    sampler, bit for bit."""
+    from oracle.ran2 import sample_thomas_fermi
+    prof = vb.thomas_fermi_profile()
+    pos, mom = O.sample_thomas_fermi(prof, 300, 196 / 300)
+    p2, m2 = sample_thomas_fermi(prof.quantiles, prof.density, prof.rmax, 300, 196 / 300)
+    assert np.array_equal(pos, p2) and np.array_equal(mom, m2)
+    for seed, cons in ((-1, False), (-5, True)):
+        a = O.sample_thomas_fermi(prof, 50_000, 196 / 50_000, seed=seed, consistent=cons)
+        b = vb.sample_thomas_fermi(prof, 50_000, 196 / 50_000, seed=seed, consistent=cons)
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
 def test_uniform_sphere_sampling():
     # test/runtests.jl:979-1026 on the cluster-size ball
     prof = vb.uniform_sphere_profile()

@@ -37,6 +37,12 @@ VLB_POISSON_3XTF32 = 1
 VLB_POISSON_BF16X3 = 2
 VLB_ENERGY_TOTAL = 0
 VLB_ENERGY_HARTREE = 1
+VLB_SOFTENING_DEVICE = 0
+VLB_SOFTENING_BALL = 1
+VLB_STATUS_SCAN_TIMEOUT = 1
+VLB_STATUS_BAD_CELL = 2
+VLB_STATUS_OVERFLOW = 4
+VLB_STATUS_MMA_TIMEOUT = 8
 
 # every symbol include/vlasov_b200.h declares
 EXPORTS = (
@@ -78,7 +84,7 @@ class Config(C.Structure):
 class ProjectileDesc(C.Structure):
     _fields_ = [("position", C.c_double * 3), ("previous", C.c_double * 3), ("velocity", C.c_double * 3),
                 ("charge", C.c_double), ("mass", C.c_double), ("sigma", C.c_double),
-                ("ball_radius", C.c_double), ("active", C.c_int32), ("pad_", C.c_int32)]
+                ("ball_radius", C.c_double), ("active", C.c_int32), ("softening", C.c_int32)]
 
 
 class StepParams(C.Structure):
@@ -114,7 +120,7 @@ VLB_DTYPE_INT64 = 1
 class Tuning(C.Structure):
     _fields_ = [("chunk", C.c_int32), ("field_ctas_per_sm", C.c_int32), ("cic_ctas_per_sm", C.c_int32),
                 ("push_ctas_per_sm", C.c_int32), ("move_ctas_per_sm", C.c_int32),
-                ("field_tensor_cores", C.c_int32), ("reserved", C.c_int32 * 2)]
+                ("field_tensor_cores", C.c_int32), ("scan_wait_polls", C.c_int32), ("reserved", C.c_int32 * 1)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}

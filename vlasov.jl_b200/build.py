@@ -13,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -47,15 +48,34 @@ def _stale(target: Path, deps) -> bool:
 
 
 def build_library(force: bool = False, verbose: bool = False) -> Path:
-    deps = _sources() + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "vlasov_b200.h"]
+    """One object per source, compiled in parallel, then one link."""
+    headers = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "vlasov_b200.h"]
+    deps = _sources() + headers
     if not force and not _stale(LIB, deps):
         return LIB
-    LIBDIR.mkdir(exist_ok=True)
-    cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(ROOT / "include"),
-           *map(str, _sources()), "-o", str(LIB), "-lcudart"]
+    objdir = LIBDIR / "obj"
+    objdir.mkdir(parents=True, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "--shared"]
+    jobs = []
+    for src in _sources():
+        obj = objdir / (src.name + ".o")
+        if force or _stale(obj, [src, *headers]):
+            jobs.append([_nvcc(), *ARCH, *compile_flags, "-I", str(ROOT / "include"), "-c", str(src),
+                         "-o", str(obj)])
     if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
+        for cmd in jobs:
+            print(" ".join(cmd), file=sys.stderr)
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4) or 1) as pool:
+        done = list(pool.map(lambda cmd: subprocess.run(cmd, capture_output=True, text=True), jobs))
+    for cmd, r in zip(jobs, done):
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise subprocess.CalledProcessError(r.returncode, cmd)
+    link = [_nvcc(), *ARCH, "--shared", "-Xcompiler", "-fPIC",
+            *[str(objdir / (src.name + ".o")) for src in _sources()], "-o", str(LIB), "-lcudart"]
+    if verbose:
+        print(" ".join(link), file=sys.stderr)
+    subprocess.run(link, check=True)
     return LIB
 
 

@@ -22,7 +22,7 @@ thread_local std::string g_err;
 
 const char* kStageNames[kNumStages] = {"sort",          "deposit_fine", "deposit_coarse", "poisson",
                                         "coefficients",  "forces",       "projectile",     "push",
-                                        "capture",       "transfer",     "reserved10",     "reserved11"};
+                                        "capture",       "transfer",     "forces_kernel",  "reserved11"};
 
 int fail(int code, const std::string& msg) {
   g_err = msg;
@@ -225,6 +225,9 @@ void upload_projectile(Ctx& c, const vlb_projectile* p, int32_t film_due = 0) {
   h.proj_sigma = p ? p->sigma : 1.0;
   h.proj_ball = p ? p->ball_radius : 1.0;
   h.proj_active = p ? p->active : 0;
+  if (p && p->softening != VLB_SOFTENING_DEVICE && p->softening != VLB_SOFTENING_BALL)
+    throw ArgError("projectile softening must be VLB_SOFTENING_DEVICE or VLB_SOFTENING_BALL");
+  h.proj_soft = p ? p->softening : VLB_SOFTENING_DEVICE;
   const size_t off = offsetof(DeviceScalars, proj_pos);
   const size_t len = offsetof(DeviceScalars, film_due) + sizeof(int32_t) - off;
   VLB_CUDA(cudaMemcpyAsync(reinterpret_cast<char*>(c.dsc) + off, reinterpret_cast<char*>(c.hin) + off, len,
@@ -713,6 +716,10 @@ void collect_step(Ctx& c, vlb_projectile* proj, const vlb_step_params* params, v
       VLB_CUDA(cudaEventElapsedTime(&ms, c.ev[i], c.ev[i + 1]));
       c.stage_ms[i] += ms;
     }
+    // the gather kernel alone (its pair of events is recorded by launch_forces)
+    float ms = 0;
+    VLB_CUDA(cudaEventElapsedTime(&ms, c.ev[kEvGatherBegin], c.ev[kEvGatherEnd]));
+    c.stage_ms[kEvGatherBegin] += ms;
   }
   c.sorted = false;  // after the push the lists describe the previous positions
   c.have_forces = true;
@@ -862,7 +869,7 @@ int vlb_film_frames(vlb_ctx* ctx, int32_t* taken, int32_t* stored) {
 int vlb_film_download(vlb_ctx* ctx, int32_t first, int32_t count, float* frames, double* scalars) {
   CTX_OR_FAIL;
   if (c.film_cap <= 0) return fail(VLB_ERR_STATE, "vlb_film_download: no film is reserved");
-  if (first < 0 || count < 0 || first + count > c.film_cap)
+  if (first < 0 || count < 0 || (int64_t)first + (int64_t)count > (int64_t)c.film_cap)
     return fail(VLB_ERR_ARG, "vlb_film_download: frames out of the reserved range");
   const size_t nn = (size_t)c.fine.n * c.fine.n;
   return guarded([&]() -> int {
@@ -919,12 +926,14 @@ int vlb_set_tuning(vlb_ctx* ctx, const vlb_tuning* t) {
     if (v < 1 || v > 32) return fail(VLB_ERR_ARG, "CTAs per SM must be in [1, 32]");
   if (t->field_tensor_cores != 0 && t->field_tensor_cores != 1)
     return fail(VLB_ERR_ARG, "field_tensor_cores must be 0 or 1");
+  if (t->scan_wait_polls < -1) return fail(VLB_ERR_ARG, "scan_wait_polls must be -1, 0 or positive");
   c.chunk = t->chunk;
   c.field_tc = t->field_tensor_cores != 0;
   c.field_cps = t->field_ctas_per_sm;
   c.cic_cps = t->cic_ctas_per_sm;
   c.push_cps = t->push_ctas_per_sm;
   c.move_cps = t->move_ctas_per_sm;
+  c.scan_wait_polls = t->scan_wait_polls;
   c.graph_valid = false;  // the captured step has the old launch shapes
   ++c.config_epoch;
   c.sorted = false;       // the work items follow the chunk
@@ -942,6 +951,7 @@ int vlb_get_tuning(vlb_ctx* ctx, vlb_tuning* t) {
   t->push_ctas_per_sm = c.push_cps;
   t->move_ctas_per_sm = c.move_cps;
   t->field_tensor_cores = c.field_tc ? 1 : 0;
+  t->scan_wait_polls = c.scan_wait_polls;
   return VLB_OK;
 }
 
@@ -1080,6 +1090,7 @@ int vlb_batch_step(vlb_batch* b, vlb_projectile* projs, const vlb_step_params* p
     if (c->profile) return fail(VLB_ERR_STATE, "a batch step cannot be profiled");
   }
   if (!params->push) return fail(VLB_ERR_ARG, "a batch step pushes the clouds");
+  if (params->film) return fail(VLB_ERR_ARG, "a batch step takes no film frames (params.film must be 0)");
   return guarded([&]() -> int {
     const size_t n = b->ctx.size();
     for (size_t i = 0; i < n; ++i) {
@@ -1173,6 +1184,7 @@ int vlb_exchange_buffers(vlb_ctx* ctx, int32_t deposit_mode, vlb_exchange* out) 
 int vlb_step_deposit(vlb_ctx* ctx, const vlb_projectile* proj, const vlb_step_params* params) {
   CTX_OR_FAIL;
   if (int rc = check_step_params(c, params)) return rc;
+  if (params->film) return fail(VLB_ERR_ARG, "a sharded step takes no film frames (params.film must be 0)");
   c.mode_precision = params->poisson_precision;
   return guarded([&]() -> int {
     upload_projectile(c, proj);

@@ -21,8 +21,13 @@
 // the fine grid take the coarse spline gradient (src/fields.jl:358-393) in
 // float64, or nothing outside both grids, plus the ball-softened projectile
 // reaction (src/projectile.jl:79-80).  Their Gaussian reaction sums go to the
-// projectile like everyone else's.  The reference runs this part on the host
-// after a device-to-host copy; here it stays on the device.
+// projectile like everyone else's (the ball's, in the CPU path's softening).
+// The reference runs this part on the host after a device-to-host copy; here
+// it stays on the device.
+//
+// The softening (DeviceScalars::proj_soft) is the reference device path's
+// (Gaussian for stencil particles, ball for the tail) or its CPU path's
+// (the ball everywhere, src/projectile.jl:203-232).
 
 #include "tc_util.cuh"
 #include "vlb_internal.cuh"
@@ -53,8 +58,8 @@ __device__ __forceinline__ float gaussian_force_kernel(float r2, float sigma) {
 }
 
 struct ProjF {
-  float px, py, pz, coef, sigma;
-  bool on;
+  float px, py, pz, coef, sigma, R;
+  bool on, ball;
 };
 
 __device__ __forceinline__ ProjF load_proj(const DeviceScalars* dsc, double w) {
@@ -65,11 +70,23 @@ __device__ __forceinline__ ProjF load_proj(const DeviceScalars* dsc, double w) {
   p.pz = (float)dsc->proj_pos[2];
   p.coef = p.on ? (float)(-w * dsc->proj_charge) : 0.f;
   p.sigma = p.on ? (float)dsc->proj_sigma : 1.f;
+  p.R = p.on ? (float)dsc->proj_ball : 1.f;
+  p.ball = dsc->proj_soft == VLB_SOFTENING_BALL;
   p.on = p.on && p.coef != 0.f;
   return p;
 }
 
-// Gaussian projectile term at the position rebuilt from a cell's knots.
+// force_kernel(BallSoftening(R), r2) (src/projectile.jl:79-80)
+__device__ __forceinline__ float ball_force_kernel(float r2, float R) {
+  return r2 > R * R ? 1.f / (r2 * sqrtf(r2)) : 1.f / (R * R * R);
+}
+
+// The projectile's term at the position rebuilt from a cell's knots: the
+// Gaussian of the reference's device path, or with P.ball the ball of its CPU
+// path (src/projectile.jl:203-232).  (fx2, fy2, fz2) is the reaction the
+// particle's force loses and the projectile gains; e its share of the
+// electrons' energy sum: erf(r / sqrt(2) sigma) / r (Gaussian), or
+// uniform_sphere_potential(1, R, r) (ball, src/meanfield.jl:52-54).
 __device__ __forceinline__ void proj_term(const ProjF& P, int kx, int ky, int kz, float dx0, float dy0, float dz0,
                                           float x0, float h, float& fx2, float& fy2, float& fz2, float& e) {
   const float px = fadd(fadd(x0, fmul((float)(kx - 1), h)), dx0);
@@ -77,12 +94,18 @@ __device__ __forceinline__ void proj_term(const ProjF& P, int kx, int ky, int kz
   const float pz = fadd(fadd(x0, fmul((float)(kz - 1), h)), dz0);
   const float dx = P.px - px, dy = P.py - py, dz = P.pz - pz;
   const float d2 = dx * dx + dy * dy + dz * dz;
-  const float mm = P.coef * gaussian_force_kernel(d2, P.sigma);
+  const float r = sqrtf(d2);
+  float mm;
+  if (P.ball) {
+    mm = P.coef * ball_force_kernel(d2, P.R);
+    e = r < P.R ? -(3.f - (r / P.R) * (r / P.R)) / (2.f * P.R) : -1.f / r;
+  } else {
+    mm = P.coef * gaussian_force_kernel(d2, P.sigma);
+    e = r < 1.0e-4f * P.sigma ? 0.7978845608f / P.sigma : erff(r / 1.4142135624f / P.sigma) / r;
+  }
   fx2 = mm * dx;
   fy2 = mm * dy;
   fz2 = mm * dz;
-  const float r = sqrtf(d2);
-  e = r < 1.0e-4f * P.sigma ? 0.7978845608f / P.sigma : erff(r / 1.4142135624f / P.sigma) / r;
 }
 
 __device__ __forceinline__ void load10(const float* __restrict__ tab, int col, float* v) {
@@ -806,16 +829,26 @@ __global__ void __launch_bounds__(kGThreads) k_tail(const int32_t* __restrict__ 
       fx -= m * dx;
       fy -= m * dy;
       fz -= m * dz;
-      // the Gaussian reaction on the projectile, at the clamped cell's position
-      const uint32_t cell = cell_key(kxp, kyp, kzp, nk);
-      int kx, ky, kz;
-      cell_knots(cell, nk, kx, ky, kz);
-      float fx2, fy2, fz2, e;
-      proj_term(P, kx, ky, kz, dx0, dy0, dz0, x0f, hf, fx2, fy2, fz2, e);
-      ax += fx2;
-      ay += fy2;
-      az += fz2;
-      ae += e;
+      if (P.ball) {
+        // the CPU path: the same ball reaction on the projectile
+        const double r = sqrt(r2);
+        ax += (float)(m * dx);
+        ay += (float)(m * dy);
+        az += (float)(m * dz);
+        ae += (float)(r < R ? -(3.0 - (r / R) * (r / R)) / (2.0 * R) : -1.0 / r);
+      } else {
+        // the device path: the Gaussian reaction on the projectile, at the
+        // clamped cell's position
+        const uint32_t cell = cell_key(kxp, kyp, kzp, nk);
+        int kx, ky, kz;
+        cell_knots(cell, nk, kx, ky, kz);
+        float fx2, fy2, fz2, e;
+        proj_term(P, kx, ky, kz, dx0, dy0, dz0, x0f, hf, fx2, fy2, fz2, e);
+        ax += fx2;
+        ay += fy2;
+        az += fz2;
+        ae += e;
+      }
     }
     force[s] = (float)fx;
     force[Npad + s] = (float)fy;
@@ -1008,6 +1041,7 @@ void launch_forces(Ctx& c) {
   Level& F = c.fine;
   Level& C = c.coarse;
   Particles& P = c.part[c.cur];
+  if (c.profile) VLB_CUDA(cudaEventRecord(c.ev[kEvGatherBegin], c.stream));
   if (c.field_tc && c.chunk <= kFtRows) {
     k_field_tc<<<2 * c.num_sms, kFtThreads, kFtSmem, c.stream>>>(
         c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.d, F.csol, F.n, F.nk, c.overlap,
@@ -1020,6 +1054,7 @@ void launch_forces(Ctx& c) {
                                                                  c.hf, c.weight, c.force, c.chunk, c.red_items);
   }
   VLB_LAUNCHED(c);
+  if (c.profile) VLB_CUDA(cudaEventRecord(c.ev[kEvGatherEnd], c.stream));
   k_tail<<<c.num_sms, kGThreads, 0, c.stream>>>(c.outlist, c.dsc, c.Npad, P.k, P.d, C.csol, C.knots_d, C.nk,
                                                     C.n, F.nk, c.x0f, c.hf, c.x0, c.h, c.weight, c.force,
                                                     c.red_tail);

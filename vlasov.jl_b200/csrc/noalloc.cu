@@ -21,7 +21,9 @@
 // where the GPU can reach host memory.  So the first call on each device,
 // with that device current, asks the runtime for the array's device address
 // (cudaGetSymbolAddress) and caches it; the kernels receive that address.
-// Make that first call before any stream capture.
+// Make that first call before any stream capture.  The cached address is
+// only good while the device's context lives: a device reset, or a primary
+// context torn down and recreated between calls, is not supported.
 //
 // All calls share the one array, which keeps the last call's contents.
 // Nothing in it must start at zero: every call writes all the n*n partials

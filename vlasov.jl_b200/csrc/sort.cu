@@ -17,8 +17,11 @@
 //      pass stable (warp multi-split ranks + a scanned digit table);
 //   5. one gather of the 48-byte records into the other buffer (swap).
 //
-// Every spin of the look-back is bounded: after kSpinLimit polls the tile
-// records kStatusScanTimeout in the step's status word and gives up.
+// Every spin of the look-back is bounded: after kSpinLimit polls (or the
+// context's scan_wait_polls) the tile records kStatusScanTimeout in the
+// step's status word and stops waiting; it then sums its predecessors'
+// inputs itself, so the scan's result stays exact and every index it hands
+// on stays in range.
 
 #include "vlb_internal.cuh"
 
@@ -202,12 +205,18 @@ __global__ void __launch_bounds__(256) k_expand_lists(const int32_t* __restrict_
 template <class In, class Out>
 __global__ void __launch_bounds__(kScanThreads) k_scan(In in, Out out, int64_t n, unsigned long long* status,
                                                        unsigned long long* ticket, int32_t* total,
-                                                       int32_t* err) {
+                                                       int32_t* err, long long spin_limit) {
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ unsigned long long s_prefix;
+  __shared__ unsigned long long s_part[kScanThreads / 32];
+  __shared__ unsigned long long s_agg;
   __shared__ int64_t s_tile;
+  __shared__ int s_fallback;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  if (tid == 0) s_tile = (int64_t)atomicAdd(ticket, 1ull);
+  if (tid == 0) {
+    s_tile = (int64_t)atomicAdd(ticket, 1ull);
+    s_fallback = 0;
+  }
   __syncthreads();
   const int64_t tile = s_tile;
   const int64_t base = tile * kScanTile + (int64_t)tid * kScanItems;
@@ -240,17 +249,20 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(In in, Out out, int64_t n
     if (lane == kScanThreads / 32 - 1) {
       unsigned long long agg = wi;  // tile aggregate
       unsigned long long prefix = 0;
+      s_agg = agg;
       if (tile == 0) {
         st_relaxed(&status[0], kFlagIncl | agg);
       } else {
         st_relaxed(&status[tile], kFlagAgg | agg);
+        // spin_limit < 0: give up before the first poll (a test of the fallback)
+        bool gave_up = spin_limit < 0;
         int64_t j = tile - 1;
         long long spins = 0;
-        while (j >= 0) {
+        while (!gave_up && j >= 0) {
           unsigned long long s = ld_relaxed(&status[j]);
           unsigned long long flag = s & ~kValMask;
           if (flag == 0) {
-            if (++spins > kSpinLimit) { atomicOr(err, kStatusScanTimeout); break; }
+            if (++spins > spin_limit) { gave_up = true; break; }
             __nanosleep(32);
             continue;
           }
@@ -258,13 +270,39 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(In in, Out out, int64_t n
           if (flag == kFlagIncl) break;
           --j;
         }
-        st_relaxed(&status[tile], kFlagIncl | (prefix + agg));
+        if (gave_up) {
+          atomicOr(err, kStatusScanTimeout);
+          s_fallback = 1;  // the CTA sums the predecessors' inputs itself, below
+        } else {
+          st_relaxed(&status[tile], kFlagIncl | (prefix + agg));
+        }
       }
       s_prefix = prefix;
-      if (total && (tile + 1) * (int64_t)kScanTile >= n) *total = (int32_t)(prefix + agg);
+      if (total && !s_fallback && (tile + 1) * (int64_t)kScanTile >= n) *total = (int32_t)(prefix + agg);
     }
   }
   __syncthreads();
+  if (s_fallback) {
+    // The wait gave up: the tile's exclusive prefix straight from the inputs
+    // of every earlier tile (bounded work, no waiting), published as the
+    // look-back would have published it.  The scan's result is unchanged;
+    // the status bit reports that a wait ran out.
+    const int64_t lim = tile * (int64_t)kScanTile;
+    unsigned long long acc = 0;
+    for (int64_t i = tid; i < lim; i += kScanThreads) acc += in(i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) s_part[wid] = acc;
+    __syncthreads();
+    if (tid == 0) {
+      unsigned long long prefix = 0;
+      for (int w = 0; w < kScanThreads / 32; ++w) prefix += s_part[w];
+      st_relaxed(&status[tile], kFlagIncl | (prefix + s_agg));
+      if (total && (tile + 1) * (int64_t)kScanTile >= n) *total = (int32_t)(prefix + s_agg);
+      s_prefix = prefix;
+    }
+    __syncthreads();
+  }
   uint32_t run = (uint32_t)s_prefix + s_warp[wid] + (incl - sum);
 #pragma unroll
   for (int j = 0; j < kScanItems; ++j) {
@@ -281,8 +319,9 @@ void scan(Ctx& c, In in, Out out, int64_t n, int slot, int32_t* total) {
   int64_t per_slot = c.scan_status_size / 8;
   if (tiles > per_slot) throw ArgError("scan larger than its status slot");
   unsigned long long* st = c.scan_status + slot * per_slot;
+  const long long limit = c.scan_wait_polls == 0 ? kSpinLimit : (long long)c.scan_wait_polls;
   k_scan<In, Out><<<(unsigned)tiles, kScanThreads, 0, c.stream>>>(in, out, n, st, &c.dsc->scan_tiles[slot],
-                                                                  total, &c.dsc->status);
+                                                                  total, &c.dsc->status, limit);
   VLB_LAUNCHED(c);
 }
 

@@ -13,6 +13,10 @@ namespace vlb {
 
 constexpr int kWarp = 32;
 constexpr int kNumStages = 12;
+// Events 10 and 11 of a profiled step bracket the gather kernel alone; its
+// time is stage 10 ("forces_kernel").
+constexpr int kEvGatherBegin = 10;
+constexpr int kEvGatherEnd = 11;
 constexpr int kChunk = 128;       // default particles per work item of the gather and CIC
 constexpr int kMinChunk = 32;     // smallest chunk a tuning may set (sizes the item list)
 
@@ -63,7 +67,9 @@ struct DeviceScalars {
   double proj_pos[3], proj_prev[3], proj_vel[3], proj_force[3];
   double proj_charge, proj_mass, proj_sigma, proj_ball;
   int32_t proj_active;
+  int32_t proj_soft;                 // VLB_SOFTENING_DEVICE or VLB_SOFTENING_BALL
   int32_t film_due;                  // 1: this step appends a film frame (uploaded with the projectile)
+  int32_t pad_film;
   double e_el, e_jel;
   unsigned long long film_inside;    // particles within the film radius of the origin (a frame's count)
   int32_t film_next;                 // frames taken since vlb_film_reserve
@@ -162,6 +168,9 @@ struct Ctx {
   // launch shapes (vlb_set_tuning): particles per work item, persistent-grid
   // CTAs per SM of the gather, the coarse deposit, the push and the record move
   int chunk = kChunk, field_cps = 3, cic_cps = 4, push_cps = 8, move_cps = 8;
+  // polls of a look-back wait before it gives up: 0 the default, -1 none
+  // (every tile after the first takes the scan's fallback at once)
+  int scan_wait_polls = 0;
   bool field_tc = true;  // the gather's y sums on the tensor cores (chunk <= 128)
   unsigned* tc_sync = nullptr;  // grid-barrier counter of the tensor-core chains
   // the learned denoiser of the fine density (vlb_set_denoiser)

@@ -88,9 +88,12 @@ class GaussianSoftening:
 
 @dataclass
 class Projectile:
-    """Incident ion (src/projectile.jl:141-168).  The fused force path uses a
-    Gaussian of width scale(softening); out-of-stencil particles see the ball
-    of the same radius, as the reference's device path does."""
+    """Incident ion (src/projectile.jl:141-168).  With softening_mode
+    VLB_SOFTENING_DEVICE (the default) the fused force path uses a Gaussian of
+    width scale(softening) and out-of-stencil particles see the ball of the
+    same radius, as the reference's device path does; with VLB_SOFTENING_BALL
+    every particle sees the ball, as its CPU path does
+    (src/projectile.jl:203-232)."""
     mass: float
     charge: float
     softening: object
@@ -98,6 +101,7 @@ class Projectile:
     position: np.ndarray
     previous: np.ndarray
     velocity: np.ndarray
+    softening_mode: int = L.VLB_SOFTENING_DEVICE
 
     @staticmethod
     def make(*, mass, charge, energy, impact=0.0, x0, dt, softening) -> "Projectile":
@@ -122,6 +126,7 @@ class Projectile:
         d.sigma = self.softening.scale
         d.ball_radius = self.softening.scale
         d.active = 1
+        d.softening = self.softening_mode
         return d
 
     def from_desc(self, d: L.ProjectileDesc):
@@ -553,13 +558,19 @@ class Simulation:
     def __init__(self, p: SimulationParameters, profile: RadialProfile, *, projectile: Projectile | None = None,
                  seed: int = -1, consistent_startup: bool = False, device: int = 0,
                  fixed_point: bool = False, use_graph: bool = True, capture_radius: float = 8.0,
-                 precision: int = L.VLB_POISSON_FP32):
+                 precision: int = L.VLB_POISSON_FP32, softening_mode: int | None = None):
+        """softening_mode: VLB_SOFTENING_DEVICE (the reference's device path)
+        or VLB_SOFTENING_BALL (its CPU path); None keeps the projectile's."""
         self.params = p
         self.meshes = build_meshes(p.nfine, p.ninner, p.nouter, p.rcluster, p.rbox)
         self.smoothing = gaussian_smoothing(self.meshes.fine.axis)
         self.jellium = Jellium.of(p.nions)
         self.weight = p.nelectrons / p.nparticles
         self.projectile = projectile
+        if projectile is not None and softening_mode is not None:
+            if softening_mode not in (L.VLB_SOFTENING_DEVICE, L.VLB_SOFTENING_BALL):
+                raise ValueError("softening_mode must be VLB_SOFTENING_DEVICE or VLB_SOFTENING_BALL")
+            projectile.softening_mode = softening_mode
         self.fixed_point = fixed_point
         self.precision = precision
         self.use_graph = use_graph
@@ -595,14 +606,21 @@ class Simulation:
 
     def prime_leapfrog(self, positions, momenta, consistent: bool = False):
         """Two-stage priming (src/simulation.jl:233-277), with the Fortran's
-        dt/M coefficient unless `consistent`."""
+        dt/M coefficient unless `consistent`.  The forces at q(-dt/2) carry the
+        projectile's reaction on the device path (its forces! fuses the
+        projectile, src/simulation.jl:521) and not on the CPU path (there the
+        reaction comes with advance_projectile!, skipped while priming,
+        src/simulation.jl:343, 454-460)."""
         M, dt = self.mass, self.params.dt
         half = positions - (dt / (2 * M)) * momenta
         k, d = pack_positions(half, self.x0, self.h)
         pk, pd = pack_positions(positions, self.x0, self.h)
         acc = self.accelerator
         acc.upload(k, d, pk, pd)
-        acc.fused_step(self.projectile, self._params(advance=False, push=False, capture=0.0))
+        pr = self.projectile
+        if pr is not None and pr.softening_mode == L.VLB_SOFTENING_BALL:
+            pr = None
+        acc.fused_step(pr, self._params(advance=False, push=False, capture=0.0))
         k, d, pk, pd = acc.download()
         f = acc.force().astype(np.float64).T
         q0 = unpack_positions(pk, pd, self.x0, self.h)

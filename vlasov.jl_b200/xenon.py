@@ -26,7 +26,7 @@ import time
 def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point: bool = False,
         uniform: bool = False, nsteps: int | None = None, device: int = 0, seed: int = -1, quiet: bool = False,
         precision: str = "fp32", energy_every: int = 0, isolated: bool = False, film_stride: int = 0,
-        film_out: str | None = None):
+        film_out: str | None = None, softening: str = "device"):
     """Runs the crossing; returns a dict with the capture curve (q(<8) and
     outcount after every step), the final charge and the timing, and with
     energy_every > 0 the energy budget of every energy_every-th step
@@ -34,7 +34,10 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
     cluster alone, no projectile (the budget's conservation test).
     film_stride > 0: the movie's frames (scripts/xenon.jl:370-410) at step 1
     and every film_stride-th step, taken on the device and written to
-    film_out (.npz: frames, times_fs, proj_x, proj_y, q_capture, q_net)."""
+    film_out (.npz: frames, times_fs, proj_x, proj_y, q_capture, q_net).
+    softening: "device" (the reference's device path: a Gaussian of width 5
+    for stencil particles, the ball for the rest) or "ball" (its CPU path:
+    the ball of radius 5 for every particle)."""
     import numpy as np
     from . import simulation as S
 
@@ -47,8 +50,9 @@ def run(npart: int = 8_000_000, nfine: int = 64, *, every: int = 50, fixed_point
     from . import _lib as L
     prec = {"fp32": L.VLB_POISSON_FP32, "3xtf32": L.VLB_POISSON_3XTF32, "bf16x3": L.VLB_POISSON_BF16X3}[precision]
     proj = None if isolated else S.xenon_projectile(v=v, x0=x0, dt=dt)
+    soft = {"device": L.VLB_SOFTENING_DEVICE, "ball": L.VLB_SOFTENING_BALL}[softening]
     sim = S.Simulation(p, prof, projectile=proj, seed=seed, fixed_point=fixed_point, device=device,
-                       precision=prec)
+                       precision=prec, softening_mode=soft)
     built = time.time() - t0
     if not quiet:
         print(f"Na196 + Xe25+, 500 keV, b = 45 a0 | {npart:.1e} particles, grid {2 * nfine + 2}^3")
@@ -120,12 +124,14 @@ def main(argv=None):
     ap.add_argument("--film", type=int, default=0,
                     help="take the movie's frames at step 1 and every N steps on the device (the script's N is 4)")
     ap.add_argument("--film-out", default="film.npz", help="where --film writes its frames")
+    ap.add_argument("--softening", default="device", choices=["device", "ball"],
+                    help="the reference's device path (Gaussian in the stencil) or its CPU path (the ball everywhere)")
     a = ap.parse_args(argv)
     if a.nfine % 2:
         ap.error("--nfine must be even")
     r = run(a.particules, a.nfine, fixed_point=a.fixed_point, uniform=a.uniform, nsteps=a.steps,
             precision=a.precision, energy_every=a.energy_every, isolated=a.isolated, film_stride=a.film,
-            film_out=a.film_out if a.film else None)
+            film_out=a.film_out if a.film else None, softening=a.softening)
     if a.json:
         with open(a.json, "w") as f:
             json.dump(r, f)
