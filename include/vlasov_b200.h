@@ -202,6 +202,16 @@ VLB_API int vlb_upload_particles(vlb_ctx* ctx, const int32_t* knode, const float
 VLB_API int vlb_download_particles(vlb_ctx* ctx, int32_t* knode, float* delta,
                            int32_t* pknode, float* pdelta);
 
+/* The same for the slots [first, first + count) of the cloud, host SoA arrays
+ * of 3*count: the chunked transfers of a cloud built or read a slice at a
+ * time (the construction of src/simulation.jl:171-216 and its priming,
+ * src/simulation.jl:233-277, without a whole host copy of the cloud).
+ * Slots out of [0, npart) return VLB_ERR_ARG. */
+VLB_API int vlb_upload_particles_range(vlb_ctx* ctx, int64_t first, int64_t count, const int32_t* knode,
+                               const float* delta, const int32_t* pknode, const float* pdelta);
+VLB_API int vlb_download_particles_range(vlb_ctx* ctx, int64_t first, int64_t count, int32_t* knode,
+                                 float* delta, int32_t* pknode, float* pdelta);
+
 /* _pack!(acc, ::PackedPositions) -> _sort_and_list! (src/accelerator.jl:360-387,
  * 466-503): stable counting sort of the cloud by cell (the particles are
  * moved), occupied-cell list, bounds, out-of-stencil list.  Returns the
@@ -442,6 +452,8 @@ VLB_API int vlb_set_grid(vlb_ctx* ctx, int32_t which, const float* host);
 
 /* The force buffer acc.force, SoA 3*npart, in slot order. */
 VLB_API int vlb_get_forces(vlb_ctx* ctx, float* host);
+/* The forces of slots [first, first + count): host SoA [3*count]. */
+VLB_API int vlb_get_forces_range(vlb_ctx* ctx, int64_t first, int64_t count, float* host);
 VLB_API int vlb_set_forces(vlb_ctx* ctx, const float* host);
 
 /* enclosed_charge(cloud, proj, radius) (src/projectile.jl:243-247) on the
@@ -492,6 +504,18 @@ VLB_API int vlb_sample_thomas_fermi(const double* quantiles, int32_t nq, const d
                             int32_t nrho, double rmax, int64_t npart, double weight,
                             int32_t seed, int32_t consistent, double* positions,
                             double* momenta);
+
+/* The same draw as a stream (the construction of src/initial.jl:94-113 a
+ * chunk at a time): vlb_sampler_draw(s, n, ...) returns the next n particles
+ * of the Ran2(seed) cloud, so consecutive draws give the one-shot cloud bit
+ * for bit.  positions = momenta = NULL skips n particles (their uniforms are
+ * still consumed), as a rank that keeps only its slice of the cloud does.
+ * The sampler keeps copies of the profile tables. */
+typedef struct vlb_sampler vlb_sampler;
+VLB_API int vlb_sampler_create(const double* quantiles, int32_t nq, const double* density, int32_t nrho,
+                       double rmax, double weight, int32_t seed, int32_t consistent, vlb_sampler** out);
+VLB_API int vlb_sampler_draw(vlb_sampler* sampler, int64_t n, double* positions, double* momenta);
+VLB_API int vlb_sampler_destroy(vlb_sampler* sampler);
 
 /* next!(Ran2(seed)) n times (src/random.jl:80-90). */
 VLB_API int vlb_ran2(int32_t seed, int32_t consistent, int64_t n, float* out);

@@ -11,7 +11,8 @@ from .tables import (SplineAxis, SplineMesh, NestedMeshes, GaussianSmoothing, Lo
 from .simulation import (SimulationParameters, Jellium, BallSoftening, GaussianSoftening, Projectile,
                          RadialProfile, read_radial_profile, thomas_fermi_profile, uniform_sphere_profile,
                          sample_thomas_fermi, ran2, pack_positions, unpack_positions, DeviceAccelerator,
-                         Simulation, StepDiagnostics, EnergyBudget, Film, xenon_projectile)
+                         Simulation, StepDiagnostics, EnergyBudget, Film, xenon_projectile, ThomasFermiStream,
+                         STREAM_CHUNK, stream_half_step_cloud, prime_back_chunked)
 from . import _lib
 from . import xenon
 from . import sharded

@@ -56,7 +56,9 @@ EXPORTS = (
     "vlb_get_grid", "vlb_set_grid", "vlb_get_forces", "vlb_set_forces",
     "vlb_enclosed_charge", "vlb_profile", "vlb_stage_count", "vlb_stage_name", "vlb_stage_times",
     "vlb_launch_count", "vlb_fp32_peak", "vlb_stream", "vlb_sample_thomas_fermi", "vlb_ran2", "vlb_pack_positions",
-    "vlb_unpack_positions", "vlb_total_charge_noalloc",
+    "vlb_unpack_positions", "vlb_total_charge_noalloc", "vlb_upload_particles_range",
+    "vlb_download_particles_range", "vlb_get_forces_range", "vlb_sampler_create", "vlb_sampler_draw",
+    "vlb_sampler_destroy",
 )
 
 P_D = C.POINTER(C.c_double)
@@ -207,6 +209,13 @@ def lib():
             "vlb_pack_positions": (C.c_int, [C.c_int64, P_D, C.c_double, C.c_double, P_I, P_F]),
             "vlb_unpack_positions": (C.c_int, [C.c_int64, P_I, P_F, C.c_double, C.c_double, P_D]),
             "vlb_total_charge_noalloc": (C.c_int, [vp, vp, C.c_int32, vp, vp]),
+            "vlb_upload_particles_range": (C.c_int, [vp, C.c_int64, C.c_int64, P_I, P_F, P_I, P_F]),
+            "vlb_download_particles_range": (C.c_int, [vp, C.c_int64, C.c_int64, P_I, P_F, P_I, P_F]),
+            "vlb_get_forces_range": (C.c_int, [vp, C.c_int64, C.c_int64, P_F]),
+            "vlb_sampler_create": (C.c_int, [P_D, C.c_int32, P_D, C.c_int32, C.c_double, C.c_double, C.c_int32,
+                                             C.c_int32, C.POINTER(vp)]),
+            "vlb_sampler_draw": (C.c_int, [vp, C.c_int64, P_D, P_D]),
+            "vlb_sampler_destroy": (C.c_int, [vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

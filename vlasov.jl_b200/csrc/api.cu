@@ -537,6 +537,73 @@ int vlb_download_particles(vlb_ctx* ctx, int32_t* knode, float* delta, int32_t* 
   });
 }
 
+// Slots [first, first + count) of the cloud, from or to host SoA arrays of
+// 3*count (all x, then all y, then all z): the chunked form of upload!/
+// download!, so that a cloud can be built or read a slice at a time.
+int vlb_upload_particles_range(vlb_ctx* ctx, int64_t first, int64_t count, const int32_t* knode, const float* delta,
+                               const int32_t* pknode, const float* pdelta) {
+  CTX_OR_FAIL;
+  if (!knode || !delta || !pknode || !pdelta) return fail(VLB_ERR_ARG, "null particle array");
+  if (first < 0 || count < 0 || first > c.N || count > c.N - first)
+    return fail(VLB_ERR_ARG, "vlb_upload_particles_range: slots out of the cloud");
+  return guarded([&]() -> int {
+    Particles& P = c.part[c.cur];
+    const size_t n = (size_t)count, bytes = n * 4;
+    if (n) {
+      for (int a = 0; a < 3; ++a) {
+        const size_t o = a * (size_t)c.Npad + (size_t)first;
+        VLB_CUDA(cudaMemcpyAsync(P.k + o, knode + a * n, bytes, cudaMemcpyHostToDevice, c.stream));
+        VLB_CUDA(cudaMemcpyAsync(P.d + o, delta + a * n, bytes, cudaMemcpyHostToDevice, c.stream));
+        VLB_CUDA(cudaMemcpyAsync(P.pk + o, pknode + a * n, bytes, cudaMemcpyHostToDevice, c.stream));
+        VLB_CUDA(cudaMemcpyAsync(P.pd + o, pdelta + a * n, bytes, cudaMemcpyHostToDevice, c.stream));
+      }
+    }
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    c.sorted = false;
+    c.items_valid = false;
+    c.keys_ready = false;
+    return VLB_OK;
+  });
+}
+
+int vlb_download_particles_range(vlb_ctx* ctx, int64_t first, int64_t count, int32_t* knode, float* delta,
+                                 int32_t* pknode, float* pdelta) {
+  CTX_OR_FAIL;
+  if (first < 0 || count < 0 || first > c.N || count > c.N - first)
+    return fail(VLB_ERR_ARG, "vlb_download_particles_range: slots out of the cloud");
+  return guarded([&]() -> int {
+    Particles& P = c.part[c.cur];
+    const size_t n = (size_t)count, bytes = n * 4;
+    if (n) {
+      for (int a = 0; a < 3; ++a) {
+        const size_t o = a * (size_t)c.Npad + (size_t)first;
+        if (knode) VLB_CUDA(cudaMemcpyAsync(knode + a * n, P.k + o, bytes, cudaMemcpyDeviceToHost, c.stream));
+        if (delta) VLB_CUDA(cudaMemcpyAsync(delta + a * n, P.d + o, bytes, cudaMemcpyDeviceToHost, c.stream));
+        if (pknode) VLB_CUDA(cudaMemcpyAsync(pknode + a * n, P.pk + o, bytes, cudaMemcpyDeviceToHost, c.stream));
+        if (pdelta) VLB_CUDA(cudaMemcpyAsync(pdelta + a * n, P.pd + o, bytes, cudaMemcpyDeviceToHost, c.stream));
+      }
+    }
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
+int vlb_get_forces_range(vlb_ctx* ctx, int64_t first, int64_t count, float* host) {
+  CTX_OR_FAIL;
+  if (!host) return fail(VLB_ERR_ARG, "null host buffer");
+  if (first < 0 || count < 0 || first > c.N || count > c.N - first)
+    return fail(VLB_ERR_ARG, "vlb_get_forces_range: slots out of the cloud");
+  return guarded([&]() -> int {
+    const size_t n = (size_t)count;
+    if (n)
+      for (int a = 0; a < 3; ++a)
+        VLB_CUDA(cudaMemcpyAsync(host + a * n, c.force + a * (size_t)c.Npad + (size_t)first, n * 4,
+                                 cudaMemcpyDeviceToHost, c.stream));
+    VLB_CUDA(cudaStreamSynchronize(c.stream));
+    return VLB_OK;
+  });
+}
+
 int vlb_sort(vlb_ctx* ctx, int32_t* noccupied, int32_t* outcount) {
   CTX_OR_FAIL;
   return guarded([&]() -> int {

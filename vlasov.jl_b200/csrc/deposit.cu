@@ -13,10 +13,10 @@
 // (src/deposition.jl:213-245).
 //
 // Coarse grid (src/kernels.jl:1207-1273, src/devicemesh.jl:93-106):
-// trilinear cloud-in-cell on the stretched collocation points, each thread
-// walking a block of consecutive sorted particles into a private window of
-// shared memory that is added to the grid once.  The cell lookup is the
-// reference's Float32 LocateTable walk.
+// trilinear cloud-in-cell on the stretched collocation points, one CTA per
+// occupied fine cell, each thread adding its particles into a private window
+// column of shared memory that is summed and added to the grid once per cell.
+// The cell lookup is the reference's Float32 LocateTable walk.
 
 #include "vlb_internal.cuh"
 
@@ -292,178 +292,168 @@ __global__ void k_coarse_from_fixed(float* __restrict__ rho, const unsigned long
     rho[t] = (float)((double)(long long)fixed[t] * kFixedInv);
 }
 
-// One warp per work item of the cell sort (a run of at most `chunk` particles
-// of one fine cell).  Each lane adds its particles' eight trilinear
-// contributions into a 4^3 register window anchored at the coarse point left
-// of the fine cell's lower edge: the fine cell is one knot spacing wide, and
-// the collocation gaps of the coarse grid are wide enough that its particles'
-// left points lie within three of the anchor.  A particle whose left point
-// does not (a cell clamped at the edge of the fine grid) adds its corners with
-// global atomics.  The window is summed over the warp and added to the grid
-// once per item.  Contributions carry charge / (wx wy wz)
-// (src/devicemesh.jl:104); the walk is the reference's
-// (src/kernels.jl:1083-1273) with the scatter grouped by cell.  With `fixed`
-// the additions go to an int64 grid in fixed point (scale 2^40): each item's
-// window sums are fixed by the sort, so the grid does not depend on the
-// order in which items run.
+// One CTA per occupied fine cell (cells taken from a dynamic counter).  The
+// cell is one knot spacing wide and the coarse collocation gaps are at least
+// 2.19 a0 against the fine h = 2.44 a0, so its particles' left coarse points
+// lie within two of the anchor, the point left of the cell's lower edge: a
+// 4^3 window of coarse points holds all their corners.  Each thread adds the
+// eight trilinear corners of its particles (slots tid, tid + 256, ..., two
+// particles' loads in flight at a time) into its own column of a 4^3 x 256
+// window in shared memory (no atomics, no conflicts: word e * 256 + tid).
+// At the cell's end each warp sums eight window entries over the 256
+// columns in a fixed order and adds them to the grid once.  Cells of at most
+// kCicSmall particles skip the window: their corners go to the grid with
+// atomics directly.  So do the corners of a particle whose left point falls
+// outside the window (cells clamped at the edge of the fine grid).
+// Contributions carry charge / (wx wy wz) (src/devicemesh.jl:104); the walk
+// is the reference's (src/kernels.jl:1083-1273) with the scatter grouped by
+// cell.  With `fixed` the additions go to an int64 grid in fixed point
+// (scale 2^40): each cell's window sums are fixed by the sort, and the
+// direct corners are integers, so the grid does not depend on the order in
+// which cells run.
+constexpr int kCicSmall = 32;
+
+struct CicWin {
+  int anc[3];
+  CicAxis A[3];
+};
+
+__device__ __forceinline__ void cic_cell_window(CicWin& W, int kx, int ky, int kz, const float* gt,
+                                                const float* igap, int ng, float lx0, float linvw,
+                                                const int32_t* cells, int ncells, float x0f, float hf) {
+  const int kc[3] = {kx, ky, kz};
+  const float halfh = 0.5f * hf;
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    float wdummy;
+    const float edge = fsub(fadd(x0f, fmul((float)(kc[ax] - 1), hf)), halfh);
+    const int c = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, edge, wdummy);
+    W.anc[ax] = c > 0 ? c - 1 : -1000;
+    cic_axis(W.A[ax], W.anc[ax], ng, gt);
+  }
+}
+
+// The corners of one particle: into the thread's window column `win` (entry
+// e at win[e * kCicThreads]) when they fit, else to the grid.  win ==
+// nullptr: always to the grid.
+__device__ __forceinline__ void cic_particle(const CicWin& W, int k0, int k1, int k2, float d0, float d1, float d2,
+                                             float x0f, float hf, float charge, const float* gt, const float* igap,
+                                             const float* idl, int ng, float lx0, float linvw, const int32_t* cells,
+                                             int ncells, float* win, float* rho, unsigned long long* fixed) {
+  const size_t n = ng, nn = n * n;
+  const float px = fadd(fadd(x0f, fmul((float)(k0 - 1), hf)), d0);
+  const float py = fadd(fadd(x0f, fmul((float)(k1 - 1), hf)), d1);
+  const float pz = fadd(fadd(x0f, fmul((float)(k2 - 1), hf)), d2);
+  float ax, ay, az, ix0, ix1, iy0, iy1, iz0, iz1;
+  const int ix = cic_locate(W.A[0], W.anc[0], px, ax, ix0, ix1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
+  const int iy = cic_locate(W.A[1], W.anc[1], py, ay, iy0, iy1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
+  const int iz = cic_locate(W.A[2], W.anc[2], pz, az, iz0, iz1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
+  if (!(ix > 0 && iy > 0 && iz > 0)) return;
+  const int i0 = ix - 1, j0 = iy - 1, m0 = iz - 1;  // 0-based left points
+  const float wx0 = ax * ix0, wx1 = (1.f - ax) * ix1;
+  const float wy0 = ay * iy0, wy1 = (1.f - ay) * iy1;
+  const float wz0 = charge * az * iz0, wz1 = charge * (1.f - az) * iz1;
+  const int lx = i0 - W.anc[0], ly = j0 - W.anc[1], lz = m0 - W.anc[2];
+  if (win && (unsigned)lx <= kCicW - 2 && (unsigned)ly <= kCicW - 2 && (unsigned)lz <= kCicW - 2) {
+    const int e = lx + kCicW * (ly + kCicW * lz);
+    float* c = win + (size_t)e * kCicThreads;
+    constexpr int SY = kCicW * kCicThreads, SZ = kCicW * kCicW * kCicThreads;
+    const float a00 = wx0 * wy0, a10 = wx1 * wy0, a01 = wx0 * wy1, a11 = wx1 * wy1;
+    c[0] += a00 * wz0;
+    c[kCicThreads] += a10 * wz0;
+    c[SY] += a01 * wz0;
+    c[SY + kCicThreads] += a11 * wz0;
+    c[SZ] += a00 * wz1;
+    c[SZ + kCicThreads] += a10 * wz1;
+    c[SZ + SY] += a01 * wz1;
+    c[SZ + SY + kCicThreads] += a11 * wz1;
+  } else {
+    const size_t b = (size_t)i0 + n * j0 + nn * m0;
+    cic_add(rho, fixed, b, wx0 * wy0 * wz0);
+    cic_add(rho, fixed, b + nn, wx0 * wy0 * wz1);
+    cic_add(rho, fixed, b + n, wx0 * wy1 * wz0);
+    cic_add(rho, fixed, b + n + nn, wx0 * wy1 * wz1);
+    cic_add(rho, fixed, b + 1, wx1 * wy0 * wz0);
+    cic_add(rho, fixed, b + 1 + nn, wx1 * wy0 * wz1);
+    cic_add(rho, fixed, b + 1 + n, wx1 * wy1 * wz0);
+    cic_add(rho, fixed, b + 1 + n + nn, wx1 * wy1 * wz1);
+  }
+}
+
 __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
-    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
-    const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int nk,
+    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds, DeviceScalars* dsc, int nk,
     int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ gt_g, int ng,
     float lx0, float linvw, const int32_t* __restrict__ cells_g, int ncells, const float* __restrict__ dl_g,
-    float x0f, float hf, float charge, float* rho, unsigned long long* fixed, int chunk) {
+    float x0f, float hf, float charge, float* rho, unsigned long long* fixed) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float* gt = reinterpret_cast<float*>(smem);                   // [ng]
+  float* win = reinterpret_cast<float*>(smem);                  // [kCicW3][kCicThreads]
+  float* gt = win + kCicW3 * kCicThreads;                       // [ng]
   float* igap = gt + ng;                                        // [ng] 1 / (gt[c] - gt[c-1])
   float* idl = igap + ng;                                       // [ng] 1 / dual length
   int32_t* cells = reinterpret_cast<int32_t*>(idl + ng);        // [ncells]
-  for (int e = threadIdx.x; e < ng; e += kCicThreads) {
+  __shared__ int s_g;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < ng; e += kCicThreads) {
     gt[e] = gt_g[e];
     igap[e] = e > 0 ? 1.f / (gt_g[e] - gt_g[e - 1]) : 0.f;
     idl[e] = 1.f / dl_g[e];
   }
-  for (int e = threadIdx.x; e < ncells; e += kCicThreads) cells[e] = cells_g[e];
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const int nitems = dsc->nitems;
+  for (int e = tid; e < ncells; e += kCicThreads) cells[e] = cells_g[e];
+  const int nocc = dsc->noccupied;
   const size_t n = ng, nn = n * n;
-  const float halfh = 0.5f * hf;
+  float* col = win + tid;
   for (;;) {
-    int item = 0;
-    if (lane == 0) item = (int)atomicAdd(&dsc->work_cic, 1ull);
-    item = __shfl_sync(0xffffffffu, item, 0);
-    if (item >= nitems) break;
-    const int g = item_cell[item];
-    const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
-    const int s1 = min(s0 + chunk, bounds[g + 1]);
+    __syncthreads();  // the window and s_g are free
+    if (tid == 0) s_g = (int)atomicAdd(&dsc->work_cic, 1ull);
+    __syncthreads();
+    const int g = s_g;
+    if (g >= nocc) break;
+    const int s0 = bounds[g], s1 = bounds[g + 1];
     int kx, ky, kz;
     cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
-    int anc[3];
-    {
-      const int kc[3] = {kx, ky, kz};
-#pragma unroll
-      for (int ax = 0; ax < 3; ++ax) {
-        float wdummy;
-        const float edge = fsub(fadd(x0f, fmul((float)(kc[ax] - 1), hf)), halfh);
-        const int c = locate_cell(gt, igap, ng, lx0, linvw, cells, ncells, edge, wdummy);
-        anc[ax] = c > 0 ? c - 1 : -1000;
+    CicWin W;
+    cic_cell_window(W, kx, ky, kz, gt, igap, ng, lx0, linvw, cells, ncells, x0f, hf);
+    if (s1 - s0 <= kCicSmall) {
+      const int s = s0 + tid;
+      if (s < s1)
+        cic_particle(W, k[s], k[Npad + s], k[2 * Npad + s], d[s], d[Npad + s], d[2 * Npad + s], x0f, hf, charge,
+                     gt, igap, idl, ng, lx0, linvw, cells, ncells, nullptr, rho, fixed);
+      continue;
+    }
+#pragma unroll 8
+    for (int e = 0; e < kCicW3; ++e) col[(size_t)e * kCicThreads] = 0.f;
+    // two particles per iteration, their twelve loads issued together
+    for (int s = s0 + tid; s < s1; s += 2 * kCicThreads) {
+      const int t = s + kCicThreads;
+      const bool two = t < s1;
+      const int a0 = k[s], a1 = k[Npad + s], a2 = k[2 * Npad + s];
+      const float b0 = d[s], b1 = d[Npad + s], b2 = d[2 * Npad + s];
+      int c0 = 0, c1 = 0, c2 = 0;
+      float e0 = 0.f, e1 = 0.f, e2 = 0.f;
+      if (two) {
+        c0 = k[t]; c1 = k[Npad + t]; c2 = k[2 * Npad + t];
+        e0 = d[t]; e1 = d[Npad + t]; e2 = d[2 * Npad + t];
       }
+      cic_particle(W, a0, a1, a2, b0, b1, b2, x0f, hf, charge, gt, igap, idl, ng, lx0, linvw, cells, ncells, col,
+                   rho, fixed);
+      if (two)
+        cic_particle(W, c0, c1, c2, e0, e1, e2, x0f, hf, charge, gt, igap, idl, ng, lx0, linvw, cells, ncells, col,
+                     rho, fixed);
     }
-    CicAxis AX, AY, AZ;
-    cic_axis(AX, anc[0], ng, gt);
-    cic_axis(AY, anc[1], ng, gt);
-    cic_axis(AZ, anc[2], ng, gt);
-    float acc[kCicW3];
+    __syncthreads();
+    // warp w sums entries 8w .. 8w+7 over the 256 columns: lane order, then
+    // a fixed butterfly; one addition to the grid per nonzero entry
 #pragma unroll
-    for (int e = 0; e < kCicW3; ++e) acc[e] = 0.f;
-    // the next particle's loads are in flight while this one is added
-    int nk3[3] = {0, 0, 0};
-    float nd3[3] = {0.f, 0.f, 0.f};
-    if (s0 + lane < s1) {
+    for (int q = 0; q < kCicW3 / 8; ++q) {
+      const int e = warp * (kCicW3 / 8) + q;
+      const float* row = win + (size_t)e * kCicThreads;
+      float v = 0.f;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        nk3[a] = k[a * Npad + s0 + lane];
-        nd3[a] = d[a * Npad + s0 + lane];
-      }
-    }
-    for (int s = s0 + lane; s < s1; s += 32) {
-      const int ck[3] = {nk3[0], nk3[1], nk3[2]};
-      const float cd[3] = {nd3[0], nd3[1], nd3[2]};
-      if (s + 32 < s1) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          nk3[a] = k[a * Npad + s + 32];
-          nd3[a] = d[a * Npad + s + 32];
-        }
-      }
-      const float px = fadd(fadd(x0f, fmul((float)(ck[0] - 1), hf)), cd[0]);
-      const float py = fadd(fadd(x0f, fmul((float)(ck[1] - 1), hf)), cd[1]);
-      const float pz = fadd(fadd(x0f, fmul((float)(ck[2] - 1), hf)), cd[2]);
-      float ax, ay, az, ix0, ix1, iy0, iy1, iz0, iz1;
-      const int ix = cic_locate(AX, anc[0], px, ax, ix0, ix1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
-      const int iy = cic_locate(AY, anc[1], py, ay, iy0, iy1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
-      const int iz = cic_locate(AZ, anc[2], pz, az, iz0, iz1, gt, igap, idl, ng, lx0, linvw, cells, ncells);
-      if (!(ix > 0 && iy > 0 && iz > 0)) continue;
-      const int i0 = ix - 1, j0 = iy - 1, k0 = iz - 1;  // 0-based left points
-      const float wx0 = ax * ix0, wx1 = (1.f - ax) * ix1;
-      const float wy0 = ay * iy0, wy1 = (1.f - ay) * iy1;
-      const float wz0 = charge * az * iz0, wz1 = charge * (1.f - az) * iz1;
-      const int lx = i0 - anc[0], ly = j0 - anc[1], lz = k0 - anc[2];
-      if ((unsigned)lx <= kCicW - 2 && (unsigned)ly <= kCicW - 2 && (unsigned)lz <= kCicW - 2) {
-        float fx[kCicW], fy[kCicW], fz[kCicW];
-        window_axis(lx, wx0, wx1, fx);
-        window_axis(ly, wy0, wy1, fy);
-        window_axis(lz, wz0, wz1, fz);
-#pragma unroll
-        for (int ey = 0; ey < kCicW; ++ey)
-#pragma unroll
-          for (int ex = 0; ex < kCicW; ++ex) {
-            const float fxy = fx[ex] * fy[ey];
-#pragma unroll
-            for (int ez = 0; ez < kCicW; ++ez) acc[ex + kCicW * (ey + kCicW * ez)] += fxy * fz[ez];
-          }
-      } else {
-        const size_t b = (size_t)i0 + n * j0 + nn * k0;
-        cic_add(rho, fixed, b, wx0 * wy0 * wz0);
-        cic_add(rho, fixed, b + nn, wx0 * wy0 * wz1);
-        cic_add(rho, fixed, b + n, wx0 * wy1 * wz0);
-        cic_add(rho, fixed, b + n + nn, wx0 * wy1 * wz1);
-        cic_add(rho, fixed, b + 1, wx1 * wy0 * wz0);
-        cic_add(rho, fixed, b + 1 + nn, wx1 * wy0 * wz1);
-        cic_add(rho, fixed, b + 1 + n, wx1 * wy1 * wz0);
-        cic_add(rho, fixed, b + 1 + n + nn, wx1 * wy1 * wz1);
-      }
-    }
-    // recursive halving over the warp: after the five steps lane l holds the
-    // totals of entries l and 32 + l
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-      const bool up = lane & 16;
-      const float send = up ? acc[i] : acc[i + 32];
-      const float keep = up ? acc[i + 32] : acc[i];
-      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-    // acc[i], i < 32, is entry i + 32 * (lane has bit 4); pair the halves
-    // of the remaining 32 over bits 3..0, then move the kept pair together
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const bool up = lane & 8;
-      const float send = up ? acc[i] : acc[i + 16];
-      const float keep = up ? acc[i + 16] : acc[i];
-      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const bool up = lane & 4;
-      const float send = up ? acc[i] : acc[i + 8];
-      const float keep = up ? acc[i + 8] : acc[i];
-      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const bool up = lane & 2;
-      const float send = up ? acc[i] : acc[i + 4];
-      const float keep = up ? acc[i + 4] : acc[i];
-      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const bool up = lane & 1;
-      const float send = up ? acc[i] : acc[i + 2];
-      const float keep = up ? acc[i + 2] : acc[i];
-      acc[i] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
-    }
-    // lane l now holds, in acc[0] and acc[1], entries e0 = 32 b4 + 16 b3 +
-    // 8 b2 + 4 b1 + 2 b0 and e0 + 1, b the bits of l
-    const int e0 = 32 * ((lane >> 4) & 1) + 16 * ((lane >> 3) & 1) + 8 * ((lane >> 2) & 1) + 4 * ((lane >> 1) & 1) +
-                   2 * (lane & 1);
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const float v = acc[r];
-      if (v != 0.f) {
-        const int e = e0 + r;
+      for (int j = 0; j < kCicThreads / 32; ++j) v += row[lane + 32 * j];
+      v = warp_sumf(v);
+      if (lane == 0 && v != 0.f) {
         const int ex = e % kCicW, ey = (e / kCicW) % kCicW, ez = e / (kCicW * kCicW);
-        cic_add(rho, fixed, (size_t)(anc[0] + ex) + n * (anc[1] + ey) + nn * (anc[2] + ez), v);
+        cic_add(rho, fixed, (size_t)(W.anc[0] + ex) + n * (W.anc[1] + ey) + nn * (W.anc[2] + ez), v);
       }
     }
   }
@@ -538,7 +528,8 @@ void launch_deposit_fine(Ctx& c, double charge, int mode) {
 }
 
 size_t cic_smem(const Ctx& c) {
-  return 3 * (size_t)c.coarse.n * sizeof(float) + (size_t)c.coarse.loc_ncell * sizeof(int32_t);
+  return (size_t)kCicW3 * kCicThreads * sizeof(float) + 3 * (size_t)c.coarse.n * sizeof(float) +
+         (size_t)c.coarse.loc_ncell * sizeof(int32_t);
 }
 
 // The raw coarse deposit: into rho_coarse (float32) or, in fixed point,
@@ -554,9 +545,8 @@ void launch_deposit_coarse(Ctx& c, double charge, int mode) {
     VLB_CUDA(cudaMemsetAsync(C.rho, 0, tot * sizeof(float), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_cic, 0, sizeof(unsigned long long), c.stream));
   k_deposit_cic<<<c.num_sms * c.cic_cps, kCicThreads, cic_smem(c), c.stream>>>(
-      c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.fine.nk, c.Npad, P.k, P.d, C.colloc, C.n,
-      C.loc_x0, C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho,
-      fixed ? c.rho_fixed_c : nullptr, c.chunk);
+      c.occupied, c.bounds, c.dsc, c.fine.nk, c.Npad, P.k, P.d, C.colloc, C.n, C.loc_x0, C.loc_invw, C.loc_cells,
+      C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho, fixed ? c.rho_fixed_c : nullptr);
   VLB_LAUNCHED(c);
 }
 

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <vector>
 
 #include "../../include/vlasov_b200.h"
 
@@ -89,22 +90,78 @@ int vlb_ran2(int32_t seed, int32_t consistent, int64_t n, float* out) {
   return VLB_OK;
 }
 
+}  // extern "C"
+
+// The seeded Thomas-Fermi draw as a stream: the generator and the profile
+// persist between draws, so a cloud drawn in consecutive chunks is the
+// one-shot cloud (src/initial.jl:94-113, six uniforms per particle).
+struct vlb_sampler {
+  Ran2 rng;
+  std::vector<double> q, rho;
+  double rmax, weight;
+  vlb_sampler(int32_t seed, bool consistent) : rng(seed, consistent), rmax(0), weight(0) {}
+};
+
+namespace {
+
+void draw(vlb_sampler& S, int64_t n, double* positions, double* momenta) {
+  const double fermi = std::cbrt(3 * (M_PI * M_PI));  // FERMI_COEFFICIENT
+  const int nq = (int)S.q.size(), nrho = (int)S.rho.size();
+  for (int64_t i = 0; i < n; ++i) {
+    double x[6];
+    for (int a = 0; a < 6; ++a) x[a] = (double)S.rng.next();
+    if (!positions) continue;  // a skipped particle still consumes its six uniforms
+    const double r = interp_regular(S.q.data(), x[0], nq);
+    on_sphere(r, x[1], x[2], positions + 3 * i);
+    const double rho = interp_regular(S.rho.data(), r / S.rmax, nrho);
+    const double p = std::cbrt(x[3]) * fermi * std::cbrt(rho);
+    on_sphere(p * S.weight, x[4], x[5], momenta + 3 * i);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int vlb_sampler_create(const double* quantiles, int32_t nq, const double* density, int32_t nrho, double rmax,
+                       double weight, int32_t seed, int32_t consistent, vlb_sampler** out) {
+  if (!out) return VLB_ERR_ARG;
+  *out = nullptr;
+  if (!quantiles || !density || nq < 2 || nrho < 2 || !(rmax > 0)) return VLB_ERR_ARG;
+  try {
+    vlb_sampler* S = new vlb_sampler(seed, consistent != 0);
+    S->q.assign(quantiles, quantiles + nq);
+    S->rho.assign(density, density + nrho);
+    S->rmax = rmax;
+    S->weight = weight;
+    *out = S;
+  } catch (...) {
+    return VLB_ERR_NOMEM;
+  }
+  return VLB_OK;
+}
+
+int vlb_sampler_draw(vlb_sampler* sampler, int64_t n, double* positions, double* momenta) {
+  if (!sampler || n < 0 || (!positions) != (!momenta)) return VLB_ERR_ARG;
+  draw(*sampler, n, positions, momenta);
+  return VLB_OK;
+}
+
+int vlb_sampler_destroy(vlb_sampler* sampler) {
+  if (!sampler) return VLB_ERR_ARG;
+  delete sampler;
+  return VLB_OK;
+}
+
 int vlb_sample_thomas_fermi(const double* quantiles, int32_t nq, const double* density, int32_t nrho, double rmax,
                             int64_t npart, double weight, int32_t seed, int32_t consistent, double* positions,
                             double* momenta) {
   if (!quantiles || !density || !positions || !momenta || nq < 2 || nrho < 2 || npart < 0 || !(rmax > 0))
     return VLB_ERR_ARG;
-  Ran2 rng(seed, consistent != 0);
-  const double fermi = std::cbrt(3 * (M_PI * M_PI));  // FERMI_COEFFICIENT
-  for (int64_t i = 0; i < npart; ++i) {
-    double x[6];
-    for (int a = 0; a < 6; ++a) x[a] = (double)rng.next();
-    const double r = interp_regular(quantiles, x[0], nq);
-    on_sphere(r, x[1], x[2], positions + 3 * i);
-    const double rho = interp_regular(density, r / rmax, nrho);
-    const double p = std::cbrt(x[3]) * fermi * std::cbrt(rho);
-    on_sphere(p * weight, x[4], x[5], momenta + 3 * i);
-  }
+  vlb_sampler* S = nullptr;
+  if (int rc = vlb_sampler_create(quantiles, nq, density, nrho, rmax, weight, seed, consistent, &S)) return rc;
+  draw(*S, npart, positions, momenta);
+  delete S;
   return VLB_OK;
 }
 

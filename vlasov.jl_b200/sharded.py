@@ -214,14 +214,19 @@ class ShardedSimulation:
     """Simulation (src/simulation.jl:171-216, 472-531) of one rank's slice of
     the cloud, on this rank's GPU.
 
-    sampling="slice": every rank draws the whole cloud from Ran2(seed) and
+    sampling="slice": every rank draws the Ran2(seed) cloud in order and
     keeps its slice -- the single-GPU cloud exactly, at the cost of drawing
-    it N times.  sampling="per-rank": rank r draws its own slice from
-    Ran2(seed - r) -- the same distribution, drawn once."""
+    the particles before the slice on every rank.  sampling="per-rank": rank
+    r draws its own slice from Ran2(seed - r) -- the same distribution, drawn
+    once.  Either way the draw is streamed (stream_chunk particles at a time,
+    packed and uploaded chunk by chunk, the priming's second half chunked as
+    well), so that a rank's host holds a few chunks and never its slice;
+    stream_chunk = 0 draws the slice whole."""
 
     def __init__(self, p: S.SimulationParameters, profile: S.RadialProfile, *, comm, device: int = 0,
                  projectile: S.Projectile | None = None, seed: int = -1, fixed_point: bool = True,
-                 precision: int = L.VLB_POISSON_FP32, sampling: str = "per-rank", capture_radius: float = 8.0):
+                 precision: int = L.VLB_POISSON_FP32, sampling: str = "per-rank", capture_radius: float = 8.0,
+                 stream_chunk: int = S.STREAM_CHUNK):
         self.params, self.comm, self.device = p, comm, device
         self.meshes = S.build_meshes(p.nfine, p.ninner, p.nouter, p.rcluster, p.rbox)
         self.smoothing = S.gaussian_smoothing(self.meshes.fine.axis)
@@ -232,18 +237,28 @@ class ShardedSimulation:
         self.fixed_point, self.precision, self.capture_radius = fixed_point, precision, capture_radius
         a, b = shard_range(self.npart_global, comm.rank, comm.size)
         self.slice = (a, b)
-        if sampling == "slice":
-            pos, mom = S.sample_thomas_fermi(profile, self.npart_global, self.weight, seed=seed)
-            pos, mom = pos[a:b].copy(), mom[a:b].copy()
-        elif sampling == "per-rank":
-            pos, mom = S.sample_thomas_fermi(profile, b - a, self.weight, seed=seed - comm.rank)
-        else:
+        if sampling not in ("slice", "per-rank"):
             raise ValueError(f"unknown sampling {sampling!r}")
         self.accelerator = S.DeviceAccelerator(self.meshes, self.smoothing, b - a, self.weight, device)
         self.x0, self.h = self.accelerator.x0, self.accelerator.h
         self.stepper = ShardedStepper(LibraryShard(self.accelerator, self._deposit_mode(), device), comm,
                                       self.npart_global)
-        self.prime_leapfrog(pos, mom)
+        if stream_chunk > 0:
+            stream = S.ThomasFermiStream(profile, self.weight, seed=seed if sampling == "slice" else seed - comm.rank)
+            lo, hi = (a, b) if sampling == "slice" else (0, b - a)
+            try:
+                S.stream_half_step_cloud(self.accelerator, stream, lo, hi, self.mass, p.dt, stream_chunk)
+            finally:
+                stream.close()
+            self._prime_forces()
+            S.prime_back_chunked(self.accelerator, self.mass, p.dt, False, stream_chunk)
+        else:
+            if sampling == "slice":
+                pos, mom = S.sample_thomas_fermi(profile, self.npart_global, self.weight, seed=seed)
+                pos, mom = pos[a:b].copy(), mom[a:b].copy()
+            else:
+                pos, mom = S.sample_thomas_fermi(profile, b - a, self.weight, seed=seed - comm.rank)
+            self.prime_leapfrog(pos, mom)
 
     @property
     def mass(self):
@@ -276,7 +291,7 @@ class ShardedSimulation:
         pk, pd = S.pack_positions(positions, self.x0, self.h)
         acc = self.accelerator
         acc.upload(k, d, pk, pd)
-        self.stepper.step(self.projectile, self._params(advance=False, push=False, capture=0.0))
+        self._prime_forces()
         k, d, pk, pd = acc.download()
         f = acc.force().astype(np.float64).T
         q0 = S.unpack_positions(pk, pd, self.x0, self.h)
@@ -285,6 +300,15 @@ class ShardedSimulation:
         k, d = S.pack_positions(q0, self.x0, self.h)
         pk, pd = S.pack_positions(back, self.x0, self.h)
         acc.upload(k, d, pk, pd)
+
+    def _prime_forces(self):
+        """The forces of the whole cloud at the half step back (a forces-only
+        sharded step): with the projectile's reaction on the device path,
+        without it on the CPU path (see Simulation._prime_forces)."""
+        pr = self.projectile
+        if pr is not None and pr.softening_mode == L.VLB_SOFTENING_BALL:
+            pr = None
+        self.stepper.step(pr, self._params(advance=False, push=False, capture=0.0))
 
     def step(self, energy: bool = False) -> ShardedDiagnostics:
         """With energy, the diagnostics carry the budget's two sums over the

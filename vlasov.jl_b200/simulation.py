@@ -190,6 +190,81 @@ def sample_thomas_fermi(profile: RadialProfile, npart: int, weight: float, seed:
     return pos, mom
 
 
+class ThomasFermiStream:
+    """The seeded Thomas-Fermi cloud (src/initial.jl:94-113) drawn a chunk at
+    a time: consecutive draws give the particles of sample_thomas_fermi's
+    one-shot cloud in order, bit for bit (vlb_sampler)."""
+
+    def __init__(self, profile: RadialProfile, weight: float, seed: int = -1, consistent: bool = False):
+        self._q = np.ascontiguousarray(profile.quantiles, dtype=np.float64)
+        self._r = np.ascontiguousarray(profile.density, dtype=np.float64)
+        h = C.c_void_p()
+        L.check(L.lib().vlb_sampler_create(L.pd(self._q), len(self._q), L.pd(self._r), len(self._r),
+                                           float(profile.rmax), float(weight), int(seed), int(consistent),
+                                           C.byref(h)))
+        self._h = h
+
+    def draw(self, n: int):
+        """(positions, momenta) float64 (n, 3) of the next n particles."""
+        pos, mom = np.empty((n, 3)), np.empty((n, 3))
+        L.check(L.lib().vlb_sampler_draw(self._h, int(n), L.pd(pos), L.pd(mom)))
+        return pos, mom
+
+    def skip(self, n: int):
+        L.check(L.lib().vlb_sampler_draw(self._h, int(n), None, None))
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            L.lib().vlb_sampler_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+STREAM_CHUNK = 1 << 20  # particles per chunk of a streamed construction (about 150 MB of host arrays)
+
+
+def stream_half_step_cloud(acc: "DeviceAccelerator", stream: ThomasFermiStream, lo: int, hi: int, M: float,
+                           dt: float, chunk: int = STREAM_CHUNK):
+    """The first half of prime_leapfrog! (src/simulation.jl:233-277) for the
+    particles [lo, hi) of a cloud drawn from `stream` (the particles before lo
+    are drawn and dropped): each chunk's current position q0 and its half
+    step back q0 - dt/(2M) p, packed into the slots [0, hi - lo) of `acc`
+    chunk by chunk, so that no whole host copy of the cloud exists."""
+    if lo:
+        for a in range(0, lo, chunk):
+            stream.skip(min(chunk, lo - a))
+    for a in range(lo, hi, chunk):
+        n = min(chunk, hi - a)
+        pos, mom = stream.draw(n)
+        k, d = pack_positions(pos - (dt / (2 * M)) * mom, acc.x0, acc.h)
+        pk, pd = pack_positions(pos, acc.x0, acc.h)
+        del pos, mom
+        acc.upload_range(a - lo, k, d, pk, pd)
+
+
+def prime_back_chunked(acc: "DeviceAccelerator", M: float, dt: float, consistent: bool = False,
+                       chunk: int = STREAM_CHUNK):
+    """The second half of prime_leapfrog!, after the forces at the half step:
+    per chunk of slots, q(-dt) = -q0 + 2 q(-dt/2) + c F with the Fortran's
+    c = dt/M (dt^2/4M when `consistent`), then (q0, q(-dt)) as the record."""
+    coef = dt * dt / (4 * M) if consistent else dt / M
+    for a in range(0, acc.npart, chunk):
+        n = min(chunk, acc.npart - a)
+        k, d, pk, pd = acc.download_range(a, n)
+        f = acc.force_range(a, n).astype(np.float64).T
+        q0 = unpack_positions(pk, pd, acc.x0, acc.h)
+        hp = unpack_positions(k, d, acc.x0, acc.h)
+        back = -q0 + 2 * hp + coef * f
+        k, d = pack_positions(q0, acc.x0, acc.h)
+        pk, pd = pack_positions(back, acc.x0, acc.h)
+        acc.upload_range(a, k, d, pk, pd)
+
+
 def ran2(seed: int, n: int, consistent: bool = False) -> np.ndarray:
     out = np.empty(n, dtype=np.float32)
     L.check(L.lib().vlb_ran2(seed, int(consistent), n, L.pf(out)))
@@ -291,6 +366,31 @@ class DeviceAccelerator:
         return self._h
 
     # --- cloud transfer (upload!/download!, src/accelerator.jl:48-68)
+    def upload_range(self, first: int, k, d, pk, pd):
+        """Slots [first, first + count) from (3, count) arrays."""
+        arrs = [np.ascontiguousarray(a, dtype=t) for a, t in
+                ((k, np.int32), (d, np.float32), (pk, np.int32), (pd, np.float32))]
+        count = arrs[0].shape[1]
+        for a in arrs:
+            if a.shape != (3, count):
+                raise ValueError("particle arrays must share one (3, count) shape")
+        L.check(L.lib().vlb_upload_particles_range(self._h, int(first), int(count), L.pi(arrs[0]), L.pf(arrs[1]),
+                                                   L.pi(arrs[2]), L.pf(arrs[3])))
+
+    def download_range(self, first: int, count: int):
+        k = np.empty((3, count), np.int32)
+        d = np.empty((3, count), np.float32)
+        pk = np.empty((3, count), np.int32)
+        pd = np.empty((3, count), np.float32)
+        L.check(L.lib().vlb_download_particles_range(self._h, int(first), int(count), L.pi(k), L.pf(d), L.pi(pk),
+                                                     L.pf(pd)))
+        return k, d, pk, pd
+
+    def force_range(self, first: int, count: int) -> np.ndarray:
+        f = np.empty((3, count), np.float32)
+        L.check(L.lib().vlb_get_forces_range(self._h, int(first), int(count), L.pf(f)))
+        return f
+
     def upload(self, k, d, pk, pd):
         arrs = [np.ascontiguousarray(a, dtype=t) for a, t in
                 ((k, np.int32), (d, np.float32), (pk, np.int32), (pd, np.float32))]
@@ -558,9 +658,13 @@ class Simulation:
     def __init__(self, p: SimulationParameters, profile: RadialProfile, *, projectile: Projectile | None = None,
                  seed: int = -1, consistent_startup: bool = False, device: int = 0,
                  fixed_point: bool = False, use_graph: bool = True, capture_radius: float = 8.0,
-                 precision: int = L.VLB_POISSON_FP32, softening_mode: int | None = None):
+                 precision: int = L.VLB_POISSON_FP32, softening_mode: int | None = None,
+                 stream_chunk: int = STREAM_CHUNK):
         """softening_mode: VLB_SOFTENING_DEVICE (the reference's device path)
-        or VLB_SOFTENING_BALL (its CPU path); None keeps the projectile's."""
+        or VLB_SOFTENING_BALL (its CPU path); None keeps the projectile's.
+        stream_chunk > 0: the cloud is drawn, packed, uploaded and primed
+        stream_chunk particles at a time (the same cloud as a one-shot draw,
+        with a bounded host peak); 0: drawn whole on the host."""
         self.params = p
         self.meshes = build_meshes(p.nfine, p.ninner, p.nouter, p.rcluster, p.rbox)
         self.smoothing = gaussian_smoothing(self.meshes.fine.axis)
@@ -576,11 +680,20 @@ class Simulation:
         self.use_graph = use_graph
         self.capture_radius = capture_radius
         self.denoise = False       # set by denoiser.attach()
-        positions, momenta = sample_thomas_fermi(profile, p.nparticles, self.weight, seed=seed)
         self.accelerator = DeviceAccelerator(self.meshes, self.smoothing, p.nparticles, self.weight, device)
         self.x0, self.h = self.accelerator.x0, self.accelerator.h
         self.steps_done = 0
-        self.prime_leapfrog(positions, momenta, consistent=consistent_startup)
+        if stream_chunk > 0:
+            stream = ThomasFermiStream(profile, self.weight, seed=seed)
+            try:
+                stream_half_step_cloud(self.accelerator, stream, 0, p.nparticles, self.mass, p.dt, stream_chunk)
+            finally:
+                stream.close()
+            self._prime_forces()
+            prime_back_chunked(self.accelerator, self.mass, p.dt, consistent_startup, stream_chunk)
+        else:
+            positions, momenta = sample_thomas_fermi(profile, p.nparticles, self.weight, seed=seed)
+            self.prime_leapfrog(positions, momenta, consistent=consistent_startup)
 
     @property
     def mass(self):
@@ -617,10 +730,7 @@ class Simulation:
         pk, pd = pack_positions(positions, self.x0, self.h)
         acc = self.accelerator
         acc.upload(k, d, pk, pd)
-        pr = self.projectile
-        if pr is not None and pr.softening_mode == L.VLB_SOFTENING_BALL:
-            pr = None
-        acc.fused_step(pr, self._params(advance=False, push=False, capture=0.0))
+        self._prime_forces()
         k, d, pk, pd = acc.download()
         f = acc.force().astype(np.float64).T
         q0 = unpack_positions(pk, pd, self.x0, self.h)
@@ -630,6 +740,14 @@ class Simulation:
         k, d = pack_positions(q0, self.x0, self.h)
         pk, pd = pack_positions(back, self.x0, self.h)
         acc.upload(k, d, pk, pd)
+
+    def _prime_forces(self):
+        """The forces at the half step back, on the uploaded (q(-dt/2), q0)
+        records: a forces-only step, the projectile not advanced."""
+        pr = self.projectile
+        if pr is not None and pr.softening_mode == L.VLB_SOFTENING_BALL:
+            pr = None
+        self.accelerator.fused_step(pr, self._params(advance=False, push=False, capture=0.0))
 
     def step(self, energy: bool = False, film: bool = False) -> StepDiagnostics:
         """step!(sim; energy) on the device.  With energy, the diagnostics
