@@ -164,7 +164,10 @@ typedef struct vlb_step_result {
   int32_t noccupied;           /* occupied fine cells */
   int32_t status;              /* device-side error flags (VLB_STATUS_*), 0 when clean */
   int32_t denoised;            /* 1: the step used the denoiser's density, 0: the deposit's */
-  int32_t pad_;
+  int32_t sort_path;           /* the step's sort: 1 the single-pass placement of a cloud still in
+                                  its last sort's order (every particle within one cell of its old
+                                  one), 2 that placement given up for the radix passes (a particle
+                                  moved further), 0 the radix passes alone (no earlier order) */
   double hartree;              /* energy steps: 1/2 sum w phi_H at the step's positions (src/simulation.jl:511) */
   double interaction;          /* energy steps: sum w phi at the advanced positions (src/simulation.jl:393) */
 } vlb_step_result;

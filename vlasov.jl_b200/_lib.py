@@ -102,7 +102,7 @@ class StepResult(C.Structure):
                 ("projectile_force", C.c_double * 3), ("e_electrons", C.c_double), ("e_jellium", C.c_double),
                 ("enclosed_charge", C.c_double), ("total_charge", C.c_double), ("nout", C.c_int32),
                 ("outcount", C.c_int32), ("noccupied", C.c_int32), ("status", C.c_int32),
-                ("denoised", C.c_int32), ("pad_", C.c_int32), ("hartree", C.c_double),
+                ("denoised", C.c_int32), ("sort_path", C.c_int32), ("hartree", C.c_double),
                 ("interaction", C.c_double)]
 
 

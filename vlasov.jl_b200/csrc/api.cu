@@ -167,7 +167,9 @@ void destroy_ctx(Ctx* c) {
   }
   dfree(c->force);
   dfree(c->keys); dfree(c->keys_alt); dfree(c->skeys); dfree(c->perm); dfree(c->vals_alt);
-  dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off); dfree(c->occupied); dfree(c->bounds);
+  dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off);
+  for (int p = 0; p < 2; ++p) { dfree(c->occ_buf[p]); dfree(c->bnd_buf[p]); dfree(c->cidx_buf[p]); }
+  dfree(c->dir_cnt); dfree(c->dir_base);
   dfree(c->outlist); dfree(c->chunk_start); dfree(c->item_cell); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
   dfree(c->rho_fixed_c); dfree(c->red_items); dfree(c->red_tail); dfree(c->red_blocks); dfree(c->diag_part);
   dfree(c->e_items); dfree(c->e_blocks);
@@ -250,6 +252,12 @@ int status_code(Ctx& c) {
 
 void stage_mark(Ctx& c, int i) {
   if (c.profile) VLB_CUDA(cudaEventRecord(c.ev[i], c.stream));
+}
+
+// occupied / bounds name the sort products that describe part[cur]
+void sync_sort_products(Ctx& c) {
+  c.occupied = c.occ_buf[c.cur];
+  c.bounds = c.bnd_buf[c.cur];
 }
 
 void reset_step_scalars(Ctx& c) {
@@ -344,6 +352,7 @@ void capture_graphs(Ctx& c, const vlb_step_params& p) {
       cudaStreamEndCapture(c.stream, &graph);
       if (graph) cudaGraphDestroy(graph);
       c.cur = saved;
+      sync_sort_products(c);
       throw;
     }
     VLB_CUDA(cudaStreamEndCapture(c.stream, &graph));
@@ -351,6 +360,7 @@ void capture_graphs(Ctx& c, const vlb_step_params& p) {
     VLB_CUDA(cudaGraphDestroy(graph));
   }
   c.cur = saved;
+  sync_sort_products(c);
   c.graph_params = p;
   c.graph_valid = true;
 }
@@ -444,8 +454,19 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->radix_table = dalloc<uint32_t>(c->radix_table_size);
     c->counts = dalloc<int32_t>(c->ncell);
     c->cell_off = dalloc<int32_t>(c->ncell);
-    c->occupied = dalloc<int32_t>(c->ncell);
-    c->bounds = dalloc<int32_t>(c->ncell + 1);
+    for (int p = 0; p < 2; ++p) {
+      c->occ_buf[p] = dalloc<int32_t>(c->ncell);
+      c->bnd_buf[p] = dalloc<int32_t>(c->ncell + 1);
+      c->cidx_buf[p] = dalloc<int32_t>(c->ncell);
+      VLB_CUDA(cudaMemset(c->occ_buf[p], 0, (size_t)c->ncell * 4));
+      VLB_CUDA(cudaMemset(c->bnd_buf[p], 0, ((size_t)c->ncell + 1) * 4));
+      VLB_CUDA(cudaMemset(c->cidx_buf[p], 0, (size_t)c->ncell * 4));
+    }
+    c->occupied = c->occ_buf[0];
+    c->bounds = c->bnd_buf[0];
+    const size_t maxocc = (size_t)std::min<int64_t>(c->ncell, N);
+    c->dir_cnt = dalloc<int32_t>(maxocc * 27);
+    c->dir_base = dalloc<int32_t>(maxocc * 27);
     c->outlist = dalloc<int32_t>(N);
     c->chunk_start = dalloc<int32_t>(c->ncell);
     c->item_cell = dalloc<int32_t>(N / kMinChunk + c->ncell + 1);
@@ -517,6 +538,7 @@ int vlb_upload_particles(vlb_ctx* ctx, const int32_t* knode, const float* delta,
     c.sorted = false;
     c.items_valid = false;
     c.keys_ready = false;
+    c.order_valid = false;
     return VLB_OK;
   });
 }
@@ -562,6 +584,7 @@ int vlb_upload_particles_range(vlb_ctx* ctx, int64_t first, int64_t count, const
     c.sorted = false;
     c.items_valid = false;
     c.keys_ready = false;
+    c.order_valid = false;
     return VLB_OK;
   });
 }
@@ -814,6 +837,7 @@ void collect_step(Ctx& c, vlb_projectile* proj, const vlb_step_params* params, v
     result->noccupied = h.noccupied;
     result->status = h.status;
     result->denoised = h.denoised;
+    result->sort_path = c.last_sort_near ? (h.sort_far ? 2 : 1) : 0;
     result->hartree = params->energy ? 0.5 * h.energy[0] : 0.0;
     result->interaction = params->energy ? h.energy[1] : 0.0;
   }
@@ -835,6 +859,7 @@ int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, 
       VLB_CUDA(cudaGraphLaunch(c.gexec[g], c.stream));
       c.launches += c.graph_launches;
       c.cur ^= 1;
+      sync_sort_products(c);
     } else {
       const long long before = c.launches;
       enqueue_step(c, *params);
@@ -1077,7 +1102,10 @@ void capture_batch(vlb_batch& b, const vlb_step_params& p) {
     } catch (...) {
       cudaStreamEndCapture(b.origin, &graph);
       if (graph) cudaGraphDestroy(graph);
-      for (size_t i = 0; i < b.ctx.size(); ++i) b.ctx[i]->cur = saved[i];
+      for (size_t i = 0; i < b.ctx.size(); ++i) {
+        b.ctx[i]->cur = saved[i];
+        sync_sort_products(*b.ctx[i]);
+      }
       throw;
     }
     VLB_CUDA(cudaStreamEndCapture(b.origin, &graph));
@@ -1087,6 +1115,7 @@ void capture_batch(vlb_batch& b, const vlb_step_params& p) {
   }
   for (size_t i = 0; i < b.ctx.size(); ++i) {
     b.ctx[i]->cur = saved[i];
+    sync_sort_products(*b.ctx[i]);
     b.ctx[i]->keys_ready = true;
   }
   b.epoch0.resize(b.ctx.size());
@@ -1187,6 +1216,7 @@ int vlb_batch_step(vlb_batch* b, vlb_projectile* projs, const vlb_step_params* p
       VLB_CUDA(cudaGraphLaunch(b->gexec[g], b->origin));
       for (Ctx* c : b->ctx) {
         c->cur ^= 1;
+        sync_sort_products(*c);
         c->keys_ready = true;
         c->launches += c->graph_launches;
       }

@@ -91,16 +91,20 @@ struct ScanOutArray { uint32_t* a; __device__ void operator()(int64_t i, uint32_
 struct ScanInOccupied { const int32_t* c; __device__ uint32_t operator()(int64_t i) const { return c[i] > 0 ? 1u : 0u; } };
 struct ScanOutOccupied {
   int32_t* occupied;
+  int32_t* index;  // dense cell -> occupied index (meaningful for occupied cells only)
   __device__ void operator()(int64_t i, uint32_t p, uint32_t v) const {
-    if (v) occupied[p] = (int32_t)i;
+    if (v) {
+      occupied[p] = (int32_t)i;
+      index[i] = (int32_t)p;
+    }
   }
 };
 
-// One CTA over the occupied cells g < nocc (in increasing cell order), each
-// thread a contiguous run of them: exclusive prefixes of the particle count
-// (bounds), of the number of work items (ceil(count / chunk)) and of the
-// particles of cells whose 10^3 stencil leaves the fine grid (out_start, -1
-// for the others); totals into bounds[nocc], nitems and outcount.
+// One CTA over the occupied cells g < nocc (in increasing cell order):
+// exclusive prefixes of the particle count (bounds), of the number of work
+// items (ceil(count / chunk)) and of the particles of cells whose 10^3
+// stencil leaves the fine grid (out_start, -1 for the others); totals into
+// bounds[nocc], nitems and outcount.
 constexpr int kListThreads = 1024;
 
 __device__ __forceinline__ void block_scan3(uint32_t& a, uint32_t& b, uint32_t& c, uint32_t* tot) {
@@ -146,39 +150,58 @@ __global__ void __launch_bounds__(kListThreads) k_cell_lists(const int32_t* __re
                                                              const int32_t* __restrict__ occupied, DeviceScalars* dsc,
                                                              int nk, int n, int32_t* __restrict__ bounds,
                                                              int32_t* __restrict__ chunk_start,
-                                                             int32_t* __restrict__ out_start, int chunk) {
+                                                             int32_t* __restrict__ out_start, int chunk,
+                                                             int parity) {
+  // chunks of kListThreads * 4 occupied cells, four consecutive cells per
+  // thread: their cell codes, then their counts, as independent loads; a
+  // block scan of the thread sums and the running totals of earlier chunks
+  constexpr int kPer = 4;
   const int nocc = dsc->noccupied;
-  const int per = (nocc + kListThreads - 1) / kListThreads;
-  const int g0 = min((int)threadIdx.x * per, nocc), g1 = min(g0 + per, nocc);
-  uint32_t sc = 0, sch = 0, so = 0;
-  for (int g = g0; g < g1; ++g) {
-    const int cell = occupied[g];
-    const uint32_t c = (uint32_t)counts[cell];
-    int kx, ky, kz;
-    cell_knots((uint32_t)cell, nk, kx, ky, kz);
-    sc += c;
-    sch += (c + chunk - 1) / chunk;
-    if (!field_fits(kx, ky, kz, n)) so += c;
-  }
-  uint32_t tot[3];
-  block_scan3(sc, sch, so, tot);
-  for (int g = g0; g < g1; ++g) {
-    const int cell = occupied[g];
-    const uint32_t c = (uint32_t)counts[cell];
-    int kx, ky, kz;
-    cell_knots((uint32_t)cell, nk, kx, ky, kz);
-    const bool fits = field_fits(kx, ky, kz, n);
-    bounds[g] = (int32_t)sc;
-    chunk_start[g] = (int32_t)sch;
-    out_start[g] = fits ? -1 : (int32_t)so;
-    sc += c;
-    sch += (c + chunk - 1) / chunk;
-    if (!fits) so += c;
+  uint32_t carry[3] = {0u, 0u, 0u};
+  for (int base = 0; base < nocc; base += kListThreads * kPer) {
+    const int g0 = base + (int)threadIdx.x * kPer;
+    int cell[kPer];
+    uint32_t cnt[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) cell[j] = g0 + j < nocc ? occupied[g0 + j] : -1;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) cnt[j] = cell[j] >= 0 ? (uint32_t)counts[cell[j]] : 0u;
+    bool fits[kPer];
+    uint32_t sc = 0, sch = 0, so = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      int kx = 1, ky = 1, kz = 1;
+      if (cell[j] >= 0) cell_knots((uint32_t)cell[j], nk, kx, ky, kz);
+      fits[j] = cell[j] < 0 || field_fits(kx, ky, kz, n);
+      sc += cnt[j];
+      sch += (cnt[j] + chunk - 1) / chunk;
+      if (!fits[j]) so += cnt[j];
+    }
+    uint32_t tot[3];
+    block_scan3(sc, sch, so, tot);
+    sc += carry[0];
+    sch += carry[1];
+    so += carry[2];
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+      const int g = g0 + j;
+      if (g >= nocc) break;
+      bounds[g] = (int32_t)sc;
+      chunk_start[g] = (int32_t)sch;
+      out_start[g] = fits[j] ? -1 : (int32_t)so;
+      sc += cnt[j];
+      sch += (cnt[j] + chunk - 1) / chunk;
+      if (!fits[j]) so += cnt[j];
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) carry[q] += tot[q];
+    __syncthreads();  // block_scan3's shared sums are reused by the next chunk
   }
   if (threadIdx.x == 0) {
-    bounds[nocc] = (int32_t)tot[0];
-    dsc->nitems = (int32_t)tot[1];
-    dsc->outcount = (int32_t)tot[2];
+    bounds[nocc] = (int32_t)carry[0];
+    dsc->nitems = (int32_t)carry[1];
+    dsc->outcount = (int32_t)carry[2];
+    dsc->nocc_par[parity] = nocc;
   }
 }
 
@@ -205,7 +228,8 @@ __global__ void __launch_bounds__(256) k_expand_lists(const int32_t* __restrict_
 template <class In, class Out>
 __global__ void __launch_bounds__(kScanThreads) k_scan(In in, Out out, int64_t n, unsigned long long* status,
                                                        unsigned long long* ticket, int32_t* total,
-                                                       int32_t* err, long long spin_limit) {
+                                                       int32_t* err, long long spin_limit, const int32_t* gate) {
+  if (gate && *gate == 0) return;  // a gated scan of the radix path that the step did not take
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ unsigned long long s_prefix;
   __shared__ unsigned long long s_part[kScanThreads / 32];
@@ -313,7 +337,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(In in, Out out, int64_t n
 }
 
 template <class In, class Out>
-void scan(Ctx& c, In in, Out out, int64_t n, int slot, int32_t* total) {
+void scan(Ctx& c, In in, Out out, int64_t n, int slot, int32_t* total, const int32_t* gate = nullptr) {
   if (n <= 0) return;
   int64_t tiles = (n + kScanTile - 1) / kScanTile;
   int64_t per_slot = c.scan_status_size / 8;
@@ -321,14 +345,16 @@ void scan(Ctx& c, In in, Out out, int64_t n, int slot, int32_t* total) {
   unsigned long long* st = c.scan_status + slot * per_slot;
   const long long limit = c.scan_wait_polls == 0 ? kSpinLimit : (long long)c.scan_wait_polls;
   k_scan<In, Out><<<(unsigned)tiles, kScanThreads, 0, c.stream>>>(in, out, n, st, &c.dsc->scan_tiles[slot],
-                                                                  total, &c.dsc->status, limit);
+                                                                  total, &c.dsc->status, limit, gate);
   VLB_LAUNCHED(c);
 }
 
 // ------------------------------------------------------------- radix sort
 __global__ void __launch_bounds__(kRadixThreads) k_radix_upsweep(const uint32_t* __restrict__ keys, int64_t N,
                                                                  int shift, uint32_t mask,
-                                                                 uint32_t* __restrict__ table, int64_t ntiles) {
+                                                                 uint32_t* __restrict__ table, int64_t ntiles,
+                                                                 const int32_t* gate) {
+  if (gate && *gate == 0) return;
   __shared__ uint32_t hist[1 << kMaxDigitBits];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   for (int b = tid; b <= (int)mask; b += kRadixThreads) hist[b] = 0;
@@ -363,7 +389,8 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_upsweep(const uint32_t*
 __global__ void __launch_bounds__(kRadixThreads) k_radix_downsweep(
     const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, uint32_t* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, int64_t N, int shift, uint32_t mask, const uint32_t* __restrict__ table,
-    int64_t ntiles) {
+    int64_t ntiles, const int32_t* gate) {
+  if (gate && *gate == 0) return;
   __shared__ uint32_t whist[kRadixWarps][1 << kMaxDigitBits];
   __shared__ uint32_t sbase[1 << kMaxDigitBits];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -423,6 +450,159 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_downsweep(
     uint32_t pos = sbase[d] + whist[w][d] + local[r];
     if (keys_out) keys_out[pos] = key[r];
     vals_out[pos] = val[r];
+  }
+}
+
+// ------------------------------------------------ the nearly sorted path
+// After a step the cloud is still in the order of its last sort: slots are
+// grouped by old cell (in increasing cell order), and the push has written
+// every particle's new cell key.  A particle that moves at most one cell per
+// axis has a key difference D = new - old equal to one of 27 offsets
+// dx + nk dy + nk^2 dz (dx, dy, dz in {-1, 0, 1}; direction d = (dx + 1) +
+// 3 (dy + 1) + 9 (dz + 1)).  The stable order by new key then follows from
+// counts alone: the particles of new cell c come from the old cells
+// c - off(d), in increasing old-cell order (decreasing d), each group in slot
+// order.  So
+//   A  counts, per old cell and direction, its particles;
+//   B  gives each (old cell, direction) group its first slot in the new
+//      order: one warp per new cell sums the groups that precede it;
+//   C  ranks each particle within its group by slot: perm[base + rank] = s.
+// A particle whose D is none of the 27 offsets sets sort_far, and the step
+// takes the radix passes instead (gated on that flag).  Each new cell's
+// groups must add up to its count from the push's histogram, else B sets
+// the flag as well: the path never guesses.
+
+__device__ __forceinline__ int direction_of(int64_t D, int nk) {
+  const int64_t nk2 = (int64_t)nk * nk;
+  const int64_t t = D + 1 + nk + nk2;
+  if (t < 0 || t > 2 + 2 * (int64_t)nk + 2 * nk2) return -1;
+  const int dz = (int)(t / nk2);
+  const int64_t r = t - dz * nk2;
+  const int dy = (int)(r / nk);
+  const int dx = (int)(r - dy * nk);
+  if (dx > 2 || dy > 2 || dz > 2) return -1;
+  return dx + 3 * dy + 9 * dz;
+}
+
+__device__ __forceinline__ int64_t direction_offset(int d, int nk) {
+  const int dx = d % 3 - 1, dy = (d / 3) % 3 - 1, dz = d / 9 - 1;
+  return dx + (int64_t)nk * (dy + (int64_t)nk * dz);
+}
+
+constexpr int kDirs = 27;
+constexpr int kNearThreads = 256;
+
+// A: one warp per old occupied cell; per-warp counters in shared memory.
+__global__ void __launch_bounds__(kNearThreads) k_near_count(const int32_t* __restrict__ occ_old,
+                                                            const int32_t* __restrict__ bnd_old,
+                                                            DeviceScalars* dsc, int par_old,
+                                                            const uint32_t* __restrict__ keys, int nk,
+                                                            int32_t* __restrict__ dir_cnt) {
+  __shared__ int32_t cnt[kNearThreads / 32][kDirs];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nocc = dsc->nocc_par[par_old];
+  const int warps = gridDim.x * (kNearThreads / 32);
+  bool far = false;
+  for (int g = blockIdx.x * (kNearThreads / 32) + w; g < nocc; g += warps) {
+    if (lane < kDirs) cnt[w][lane] = 0;
+    __syncwarp();
+    const int64_t o = occ_old[g];
+    const int s0 = bnd_old[g], s1 = bnd_old[g + 1];
+    for (int base = s0; base < s1; base += 32) {
+      const int s = base + lane;
+      const bool valid = s < s1;
+      const unsigned m = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const int d = direction_of((int64_t)keys[s] - o, nk);
+        far |= d < 0;
+        const int dd = d < 0 ? kDirs : d;
+        const unsigned peers = __match_any_sync(m, dd);
+        if (d >= 0 && lane == __ffs(peers) - 1) cnt[w][d] += __popc(peers);
+      }
+      __syncwarp();
+    }
+    if (lane < kDirs) dir_cnt[(size_t)g * kDirs + lane] = cnt[w][lane];
+    __syncwarp();
+  }
+  if (__any_sync(0xffffffffu, far) && lane == 0) atomicOr(&dsc->sort_far, 1);
+}
+
+// B: one warp per new occupied cell c.  Lane l < 27 holds the group of
+// direction d = 26 - l (its old cell c - off(d) increases with l); an
+// exclusive scan over the lanes gives each group's first slot.
+__global__ void __launch_bounds__(kNearThreads) k_near_bases(const int32_t* __restrict__ occ_new,
+                                                            const int32_t* __restrict__ bnd_new,
+                                                            const int32_t* __restrict__ occ_old,
+                                                            const int32_t* __restrict__ cidx_old,
+                                                            DeviceScalars* dsc, int par_old, int ncell, int nk,
+                                                            const int32_t* __restrict__ dir_cnt,
+                                                            int32_t* __restrict__ dir_base) {
+  if (dsc->sort_far) return;
+  const int lane = threadIdx.x & 31;
+  const int nocc_new = dsc->noccupied, nocc_old = dsc->nocc_par[par_old];
+  const int warps = gridDim.x * (kNearThreads / 32);
+  bool bad = false;
+  for (int g = blockIdx.x * (kNearThreads / 32) + (threadIdx.x >> 5); g < nocc_new; g += warps) {
+    const int64_t c = occ_new[g];
+    int len = 0, gs = -1;
+    const int d = kDirs - 1 - lane;
+    if (lane < kDirs) {
+      const int64_t src = c - direction_offset(d, nk);
+      if (src >= 0 && src < ncell) {
+        const int go = cidx_old[src];
+        if (go >= 0 && go < nocc_old && occ_old[go] == (int32_t)src) {
+          gs = go;
+          len = dir_cnt[(size_t)go * kDirs + d];
+        }
+      }
+    }
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int start = bnd_new[g];
+    if (len > 0) dir_base[(size_t)gs * kDirs + d] = start + incl - len;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    bad |= total != bnd_new[g + 1] - start;
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&dsc->sort_far, 2);
+}
+
+// C: one warp per old occupied cell, slots in order, a running rank per
+// direction: perm[base + rank] = slot.
+__global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __restrict__ occ_old,
+                                                            const int32_t* __restrict__ bnd_old,
+                                                            const DeviceScalars* dsc, int par_old,
+                                                            const uint32_t* __restrict__ keys, int nk,
+                                                            const int32_t* __restrict__ dir_base,
+                                                            uint32_t* __restrict__ perm) {
+  if (dsc->sort_far) return;
+  __shared__ int32_t run[kNearThreads / 32][kDirs];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nocc = dsc->nocc_par[par_old];
+  const int warps = gridDim.x * (kNearThreads / 32);
+  for (int g = blockIdx.x * (kNearThreads / 32) + w; g < nocc; g += warps) {
+    if (lane < kDirs) run[w][lane] = dir_base[(size_t)g * kDirs + lane];
+    __syncwarp();
+    const int64_t o = occ_old[g];
+    const int s0 = bnd_old[g], s1 = bnd_old[g + 1];
+    for (int base = s0; base < s1; base += 32) {
+      const int s = base + lane;
+      const bool valid = s < s1;
+      const unsigned m = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const int d = direction_of((int64_t)keys[s] - o, nk);  // >= 0: A found no far particle
+        const unsigned peers = __match_any_sync(m, d);
+        const int leader = __ffs(peers) - 1;
+        const int r0 = run[w][d];
+        perm[r0 + __popc(peers & lanemask_lt())] = (uint32_t)s;
+        __syncwarp(m);
+        if (lane == leader) run[w][d] = r0 + __popc(peers);
+      }
+      __syncwarp();
+    }
   }
 }
 
@@ -489,6 +669,12 @@ void launch_sort(Ctx& c) {
   const int nk = c.fine.nk, n = c.fine.n;
   Particles& P = c.part[c.cur];
   Particles& Q = c.part[c.cur ^ 1];
+  // the products of the last sort describe part[cur]'s order (parity po);
+  // this sort writes parity pn, which describes part[cur ^ 1]
+  const int po = c.cur, pn = c.cur ^ 1;
+  const bool near = c.keys_ready && c.order_valid;
+  c.occupied = c.occ_buf[pn];
+  c.bounds = c.bnd_buf[pn];
   VLB_CUDA(cudaMemsetAsync(c.scan_status, 0, c.scan_status_size * sizeof(unsigned long long), c.stream));
   VLB_CUDA(cudaMemsetAsync(c.dsc->scan_tiles, 0, sizeof(c.dsc->scan_tiles), c.stream));
   if (!c.keys_ready) {
@@ -498,9 +684,9 @@ void launch_sort(Ctx& c) {
   }
   // the occupied cells, then their bounds, work items and out-of-stencil
   // slots (cell_off holds the out-of-stencil start of each occupied cell)
-  scan(c, ScanInOccupied{c.counts}, ScanOutOccupied{c.occupied}, c.ncell, 1, &c.dsc->noccupied);
+  scan(c, ScanInOccupied{c.counts}, ScanOutOccupied{c.occupied, c.cidx_buf[pn]}, c.ncell, 1, &c.dsc->noccupied);
   k_cell_lists<<<1, kListThreads, 0, c.stream>>>(c.counts, c.occupied, c.dsc, nk, n, c.bounds, c.chunk_start,
-                                                 c.cell_off, c.chunk);
+                                                 c.cell_off, c.chunk, pn);
   VLB_LAUNCHED(c);
   k_expand_lists<<<c.num_sms * 4, 256, 0, c.stream>>>(c.bounds, c.chunk_start, c.cell_off, c.dsc, c.item_cell,
                                                       c.outlist, c.chunk);
@@ -508,6 +694,20 @@ void launch_sort(Ctx& c) {
   // the histogram is spent: zero it for the push that may refill it
   VLB_CUDA(cudaMemsetAsync(c.counts, 0, sizeof(int32_t) * c.ncell, c.stream));
   c.keys_ready = false;
+  const int32_t* gate = nullptr;
+  if (near) {
+    const int grid = c.num_sms * 8;
+    k_near_count<<<grid, kNearThreads, 0, c.stream>>>(c.occ_buf[po], c.bnd_buf[po], c.dsc, po, c.keys, nk,
+                                                      c.dir_cnt);
+    VLB_LAUNCHED(c);
+    k_near_bases<<<grid, kNearThreads, 0, c.stream>>>(c.occupied, c.bounds, c.occ_buf[po], c.cidx_buf[po], c.dsc,
+                                                      po, c.ncell, nk, c.dir_cnt, c.dir_base);
+    VLB_LAUNCHED(c);
+    k_near_place<<<grid, kNearThreads, 0, c.stream>>>(c.occ_buf[po], c.bnd_buf[po], c.dsc, po, c.keys, nk,
+                                                      c.dir_base, c.perm);
+    VLB_LAUNCHED(c);
+    gate = &c.dsc->sort_far;  // the radix passes below run only if that path gave up
+  }
   // radix passes over the key bits
   int bits = 1;
   while ((1ll << bits) < (long long)c.ncell) ++bits;
@@ -523,11 +723,13 @@ void launch_sort(Ctx& c) {
     bool last = p == passes - 1;
     uint32_t* kout = last ? c.skeys : (p % 2 == 0 ? c.keys_alt : c.keys);
     uint32_t* vout = ((passes - 1 - p) % 2 == 0) ? c.perm : c.vals_alt;
-    k_radix_upsweep<<<(unsigned)ntiles, kRadixThreads, 0, c.stream>>>(kin, N, shift, mask, c.radix_table, ntiles);
+    k_radix_upsweep<<<(unsigned)ntiles, kRadixThreads, 0, c.stream>>>(kin, N, shift, mask, c.radix_table, ntiles,
+                                                                      gate);
     VLB_LAUNCHED(c);
-    scan(c, ScanInArray{c.radix_table}, ScanOutArray{c.radix_table}, (int64_t)(mask + 1) * ntiles, 2 + p, nullptr);
+    scan(c, ScanInArray{c.radix_table}, ScanOutArray{c.radix_table}, (int64_t)(mask + 1) * ntiles, 2 + p, nullptr,
+         gate);
     k_radix_downsweep<<<(unsigned)ntiles, kRadixThreads, 0, c.stream>>>(kin, vin, kout, vout, N, shift, mask,
-                                                                        c.radix_table, ntiles);
+                                                                        c.radix_table, ntiles, gate);
     VLB_LAUNCHED(c);
     kin = kout;
     vin = vout;
@@ -539,6 +741,8 @@ void launch_sort(Ctx& c) {
   c.cur ^= 1;
   c.sorted = true;
   c.items_valid = true;
+  c.order_valid = true;
+  c.last_sort_near = near;
 }
 
 }  // namespace vlb

@@ -60,8 +60,8 @@ struct DeviceScalars {
   int32_t pad_dn;
   unsigned long long work_energy;    // work counter of the energy kernel
   double energy[2];                  // sum w phi: [0] on the Hartree coefficients, [1] on the total
+  int32_t sort_far;                  // the nearly sorted path of the sort gave up (1: a far mover, 2: a count)
   int32_t reset_end;
-  int32_t pad0;
   // --- persistent ---
   double multipole[10];              // q, centre xyz, quadrupole (xx yy zz xy xz yz)
   double proj_pos[3], proj_prev[3], proj_vel[3], proj_force[3];
@@ -74,6 +74,7 @@ struct DeviceScalars {
   unsigned long long film_inside;    // particles within the film radius of the origin (a frame's count)
   int32_t film_next;                 // frames taken since vlb_film_reserve
   int32_t film_pad;
+  int32_t nocc_par[2];               // occupied cells of the sort products of each parity
 };
 
 struct Level {
@@ -142,8 +143,18 @@ struct Ctx {
   int64_t radix_table_size = 0;
   int32_t* counts = nullptr;     // [ncell]
   int32_t* cell_off = nullptr;   // [ncell]
-  int32_t* occupied = nullptr;   // [ncell]
-  int32_t* bounds = nullptr;     // [ncell+1]
+  // The sort's products by parity: buffers p describe part[p]'s slot order
+  // after the sort that filled part[p].  occupied and bounds point at the
+  // current parity's.
+  int32_t* occ_buf[2] = {nullptr, nullptr};   // [ncell] occupied cells, increasing
+  int32_t* bnd_buf[2] = {nullptr, nullptr};   // [ncell+1]
+  int32_t* cidx_buf[2] = {nullptr, nullptr};  // [ncell] cell -> its index in occ_buf (occupied cells only)
+  int32_t* occupied = nullptr;
+  int32_t* bounds = nullptr;
+  int32_t* dir_cnt = nullptr;    // [min(ncell, N)][27] nearly sorted path: particles per (old cell, direction)
+  int32_t* dir_base = nullptr;   // [min(ncell, N)][27] their first slot in the new order
+  bool order_valid = false;      // part[cur] is in the order its sort products describe
+  bool last_sort_near = false;   // the last sort tried the nearly sorted path
   int32_t* outlist = nullptr;    // [N]
   int32_t* chunk_start = nullptr;  // [ncell] first chunk of occupied cell g
   int32_t* item_cell = nullptr;    // [N / kChunk + ncell] occupied cell of each chunk

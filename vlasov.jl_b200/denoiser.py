@@ -26,6 +26,7 @@ it is, deposit_smoothed! at src/accelerator.jl:531).
     python -c 'import __graft_entry__ as g; g.load().denoiser.main()' train --out weights.npz
     python -c 'import __graft_entry__ as g; g.load().denoiser.main()' evaluate --weights weights.npz
     python -c 'import __graft_entry__ as g; g.load().denoiser.main()' profile
+    python -c 'import __graft_entry__ as g; g.load().denoiser.main()' floor --json floor.json
 """
 from __future__ import annotations
 
@@ -303,7 +304,7 @@ def _collect_pairs(impacts, nsteps, every, low, high, device, log):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("command", choices=["train", "evaluate", "profile"])
+    ap.add_argument("command", choices=["train", "evaluate", "profile", "floor"])
     ap.add_argument("--steps", type=int, default=704, help="steps of each data run")
     ap.add_argument("--every", type=int, default=4)
     ap.add_argument("--low", type=int, default=LOW)
@@ -340,6 +341,9 @@ def main(argv=None):
                                            "batch": a.batch, "lr": a.lr})
     elif a.command == "profile":
         out.update(profile(a.weights, impact=a.impact, npart=a.low, device=a.device, log=log))
+    elif a.command == "floor":
+        out.update(counting_floor(a.weights, impact=a.impact, nsteps=a.steps, low=a.low, high=a.high,
+                                  device=a.device, log=log))
     else:
         out.update(evaluate(a.weights, impact=a.impact, nsteps=a.steps, every=a.every, low=a.low, high=a.high,
                             device=a.device, log=log))
@@ -444,6 +448,61 @@ def evaluate(weights_path=None, *, impact: float = 45.0, nsteps: int = 704, ever
     log(f"capture curve vs {high:.0e}: max |dq| {res['plain_low']['max_dq_vs_high']:.4f} plain, "
         f"{res['denoised_low']['max_dq_vs_high']:.4f} denoised; time ratio {res['time_ratio_denoised_vs_high']:.3f}")
     return res
+
+
+def counting_floor(weights_path=None, *, impact: float = 45.0, nsteps: int = 704, low: int = LOW,
+                   high: int = HIGH, high_seeds=(-22, -23), low_seeds=(-21, -24, -25), device: int = 0,
+                   log=print):
+    """Where the capture-curve bar stands against the curve's own counting
+    noise.  q(<8 a0) is a count of pseudo-particles (enclosed_charge,
+    src/projectile.jl:243-247), so two runs of the same collision with
+    different seeds differ even at `high` particles.  Runs: plain at `high`
+    with each of high_seeds; plain and denoised at `low` with each of
+    low_seeds.  Reports max and rms |dq| over the steps between the two
+    `high` runs, and of every `low` run (plain, denoised) against the first
+    `high` run, with the counting noise sqrt(q w) of one curve."""
+    w, scale, _ = load_weights(weights_path)
+    curves = {}
+
+    def run(name, npart, seed, den):
+        sim = make_run(npart, impact, seed, device=device)
+        if den:
+            attach(sim, w, scale)
+        q = np.zeros(nsteps)
+        t0 = time.perf_counter()
+        for s in range(nsteps):
+            d = sim.step()
+            if d.status:
+                raise RuntimeError(f"{name}: device status {d.status} at step {s + 1}")
+            q[s] = d.enclosed_charge
+        wall = time.perf_counter() - t0
+        sim.accelerator.close()
+        curves[name] = q
+        log(f"{name}: {nsteps} steps in {wall:.1f} s, final q(<8) {q[-1]:.4f}")
+
+    for sd in high_seeds:
+        run(f"plain {high:.0e} seed {sd}", high, sd, False)
+    for sd in low_seeds:
+        run(f"plain {low:.0e} seed {sd}", low, sd, False)
+        run(f"denoised {low:.0e} seed {sd}", low, sd, True)
+    ref_name = f"plain {high:.0e} seed {high_seeds[0]}"
+    ref = curves[ref_name]
+    rows = []
+    for name, q in curves.items():
+        if name == ref_name:
+            continue
+        dq = np.abs(q - ref)
+        rows.append({"run": name, "vs": ref_name, "max_dq": float(dq.max()),
+                     "rms_dq": float(np.sqrt(np.mean(dq ** 2))), "final_dq": float(dq[-1])})
+        log(f"{name} vs {ref_name}: max |dq| {dq.max():.4f}, rms {np.sqrt(np.mean(dq ** 2)):.4f}, "
+            f"final {dq[-1]:.4f}")
+    qmean = float(np.mean(ref[nsteps // 2:]))
+    noise = {"q_mean_second_half": qmean, "sigma_count_high": math.sqrt(qmean * 196.0 / high),
+             "sigma_count_low": math.sqrt(qmean * 196.0 / low)}
+    log(f"counting noise of one curve at q = {qmean:.3f}: {noise['sigma_count_high']:.4f} e at {high:.0e}, "
+        f"{noise['sigma_count_low']:.4f} e at {low:.0e}")
+    return {"impact": impact, "nsteps": nsteps, "rows": rows, "noise": noise,
+            "q8": {k: v.tolist() for k, v in curves.items()}}
 
 
 if __name__ == "__main__":

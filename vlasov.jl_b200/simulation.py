@@ -613,6 +613,7 @@ class StepDiagnostics:
     denoised: int = 0            # 1: the step's fine density came from the learned denoiser
     hartree: float = 0.0         # energy steps: 1/2 sum w phi_H at the step's positions
     interaction: float = 0.0     # energy steps: sum w phi at the advanced positions
+    sort_path: int = 0           # 1: single-pass placement, 2: placement given up for radix, 0: radix alone
 
 
 @dataclass
@@ -760,7 +761,7 @@ class Simulation:
         self.steps_done += 1
         return StepDiagnostics(r.kinetic, r.escaped, tuple(r.angular), r.enclosed_charge, r.nout, r.outcount,
                                r.noccupied, tuple(r.projectile_force), r.total_charge, r.status, r.denoised,
-                               r.hartree, r.interaction)
+                               r.hartree, r.interaction, r.sort_path)
 
     def film(self, capacity: int, radius: float = 35.0):
         """Reserves `capacity` frames of the reference's movie

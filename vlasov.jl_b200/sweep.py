@@ -102,7 +102,7 @@ class Batch:
             r = res[i]
             out.append(S.StepDiagnostics(r.kinetic, r.escaped, tuple(r.angular), r.enclosed_charge, r.nout,
                                          r.outcount, r.noccupied, tuple(r.projectile_force), r.total_charge,
-                                         r.status, r.denoised, r.hartree, r.interaction))
+                                         r.status, r.denoised, r.hartree, r.interaction, r.sort_path))
         return out
 
     def close(self):
