@@ -473,6 +473,7 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_downsweep(
 // the flag as well: the path never guesses.
 
 __device__ __forceinline__ int direction_of(int64_t D, int nk) {
+  if (D == 0) return 13;  // most particles stay in their cell
   const int64_t nk2 = (int64_t)nk * nk;
   const int64_t t = D + 1 + nk + nk2;
   if (t < 0 || t > 2 + 2 * (int64_t)nk + 2 * nk2) return -1;
