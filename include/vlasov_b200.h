@@ -464,7 +464,9 @@ VLB_API int vlb_set_forces(vlb_ctx* ctx, const float* host);
 VLB_API int vlb_enclosed_charge(vlb_ctx* ctx, const double position[3], double radius, double* q);
 
 /* Accumulated device time per stage since the last reset (ms), measured
- * with CUDA events when profiling is on; names via vlb_stage_name. */
+ * with CUDA events when profiling is on; names via vlb_stage_name.  Stages
+ * 0..8 tile the step (sort .. capture); stage 10, "forces_kernel", is the
+ * gather kernel alone, inside stage 5; stage 9 is unused. */
 VLB_API int vlb_profile(vlb_ctx* ctx, int32_t enable);
 VLB_API int vlb_stage_count(void);
 VLB_API const char* vlb_stage_name(int32_t i);

@@ -9,7 +9,8 @@ that moved further makes the step take the radix passes (sort_path = 2).
 Both must give cellsort!'s permutation, occupied list, bounds and
 out-of-stencil list bit for bit: here on the 58^3 grid with a close
 projectile, after a step with a twenty-fold dt that sends particles several
-cells, and at the headline size (8e6 particles, 130^3)."""
+cells (and the steps after it, whose cloud keeps those velocities), and at
+the headline size (8e6 particles, 130^3)."""
 import numpy as np
 import pytest
 
@@ -54,9 +55,11 @@ def test_step_sorts_take_the_single_pass_placement(orc, cuda_device, use_graph):
         assert d.status == 0
         sim.params.dt = 0.5
         assert _forces_only_sort_matches_cellsort(orc, sim) == 2
-        # and the next ordinary steps go back to the single pass
-        assert [sim.step().sort_path for _ in range(3)][1:] == [1, 1]
-        assert _forces_only_sort_matches_cellsort(orc, sim) == 1
+        # the cloud keeps that step's velocities: the next steps still send
+        # particles several cells, and each sort is exact whichever path it takes
+        for _ in range(2):
+            assert sim.step().sort_path in (1, 2)
+        assert _forces_only_sort_matches_cellsort(orc, sim) in (1, 2)
     finally:
         sim.accelerator.close()
 

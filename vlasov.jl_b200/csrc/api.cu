@@ -22,7 +22,7 @@ thread_local std::string g_err;
 
 const char* kStageNames[kNumStages] = {"sort",          "deposit_fine", "deposit_coarse", "poisson",
                                         "coefficients",  "forces",       "projectile",     "push",
-                                        "capture",       "transfer",     "forces_kernel",  "reserved11"};
+                                        "capture",       "unused9",      "forces_kernel",  "reserved11"};
 
 int fail(int code, const std::string& msg) {
   g_err = msg;
@@ -162,10 +162,12 @@ void setup_level(Level& D, const vlb_level_desc& L, bool coarse) {
   const size_t tot = (size_t)n * n * n;
   D.rho = dalloc<float>(tot);
   D.phi = dalloc<float>(tot);
-  D.csol = dalloc<float>(tot);
+  // csol is padded by 16 floats: the gather's bulk copies of stencil rows
+  // start on 16-byte boundaries and read up to 15 floats past a row's end
+  D.csol = dalloc<float>(tot + 16);
   VLB_CUDA(cudaMemset(D.rho, 0, tot * sizeof(float)));
   VLB_CUDA(cudaMemset(D.phi, 0, tot * sizeof(float)));
-  VLB_CUDA(cudaMemset(D.csol, 0, tot * sizeof(float)));
+  VLB_CUDA(cudaMemset(D.csol, 0, (tot + 16) * sizeof(float)));
   D.csol_hartree = dalloc<float>(tot);
   VLB_CUDA(cudaMemset(D.csol_hartree, 0, tot * sizeof(float)));
 }
@@ -197,7 +199,9 @@ void destroy_ctx(Ctx* c) {
   dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off);
   for (int p = 0; p < 2; ++p) { dfree(c->occ_buf[p]); dfree(c->bnd_buf[p]); dfree(c->cidx_buf[p]); }
   dfree(c->dir_cnt); dfree(c->dir_base);
-  dfree(c->outlist); dfree(c->chunk_start); dfree(c->item_cell); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
+  dfree(c->outlist);
+  for (int p = 0; p < 2; ++p) { dfree(c->cstart_buf[p]); dfree(c->item_buf[p]); }
+  dfree(c->item_dir); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
   dfree(c->rho_fixed_c); dfree(c->red_items); dfree(c->red_tail); dfree(c->red_blocks); dfree(c->diag_part);
   dfree(c->e_items); dfree(c->e_blocks);
   for (auto& w : c->work) dfree(w);
@@ -285,6 +289,8 @@ void stage_mark(Ctx& c, int i) {
 void sync_sort_products(Ctx& c) {
   c.occupied = c.occ_buf[c.cur];
   c.bounds = c.bnd_buf[c.cur];
+  c.item_cell = c.item_buf[c.cur];
+  c.chunk_start = c.cstart_buf[c.cur];
 }
 
 void reset_step_scalars(Ctx& c) {
@@ -497,8 +503,13 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->dir_cnt = dalloc<int32_t>(maxocc * 27);
     c->dir_base = dalloc<int32_t>(maxocc * 27);
     c->outlist = dalloc<int32_t>(N);
-    c->chunk_start = dalloc<int32_t>(c->ncell);
-    c->item_cell = dalloc<int32_t>(N / kMinChunk + c->ncell + 1);
+    for (int p = 0; p < 2; ++p) {
+      c->cstart_buf[p] = dalloc<int32_t>(c->ncell);
+      c->item_buf[p] = dalloc<int32_t>(N / kMinChunk + c->ncell + 1);
+    }
+    c->chunk_start = c->cstart_buf[0];
+    c->item_cell = c->item_buf[0];
+    c->item_dir = dalloc<int32_t>(((size_t)N / kMinChunk + c->ncell + 1) * 27);
     const int64_t scan_tiles = std::max<int64_t>({(N + 4095) / 4096, (c->ncell + 4095) / 4096,
                                                   (c->radix_table_size + 4095) / 4096}) + 1;
     c->scan_status_size = 8 * scan_tiles;
@@ -1412,7 +1423,7 @@ int vlb_profile(vlb_ctx* ctx, int32_t enable) {
   return VLB_OK;
 }
 
-int vlb_stage_count(void) { return 9; }
+int vlb_stage_count(void) { return kEvGatherBegin + 1; }
 
 const char* vlb_stage_name(int32_t i) { return (i >= 0 && i < kNumStages) ? kStageNames[i] : ""; }
 

@@ -13,10 +13,11 @@
 // (src/deposition.jl:213-245).
 //
 // Coarse grid (src/kernels.jl:1207-1273, src/devicemesh.jl:93-106):
-// trilinear cloud-in-cell on the stretched collocation points, one CTA per
-// occupied fine cell, each thread adding its particles into a private window
-// column of shared memory that is summed and added to the grid once per cell.
-// The cell lookup is the reference's Float32 LocateTable walk.
+// trilinear cloud-in-cell on the stretched collocation points, a warp on a
+// run of the sort's work items, each lane adding its particles into its
+// column of the warp's window in shared memory, which is summed and added to
+// the grid once per cell of the run.  The cell lookup is the reference's
+// Float32 LocateTable walk.
 
 #include "vlb_internal.cuh"
 
@@ -292,26 +293,29 @@ __global__ void k_coarse_from_fixed(float* __restrict__ rho, const unsigned long
     rho[t] = (float)((double)(long long)fixed[t] * kFixedInv);
 }
 
-// One CTA per occupied fine cell (cells taken from a dynamic counter).  The
-// cell is one knot spacing wide and the coarse collocation gaps are at least
-// 2.19 a0 against the fine h = 2.44 a0, so its particles' left coarse points
-// lie within two of the anchor, the point left of the cell's lower edge: a
-// 4^3 window of coarse points holds all their corners.  Each thread adds the
-// eight trilinear corners of its particles (slots tid, tid + 256, ..., two
-// particles' loads in flight at a time) into its own column of a 4^3 x 256
-// window in shared memory (no atomics, no conflicts: word e * 256 + tid).
-// At the cell's end each warp sums eight window entries over the 256
-// columns in a fixed order and adds them to the grid once.  Cells of at most
-// kCicSmall particles skip the window: their corners go to the grid with
-// atomics directly.  So do the corners of a particle whose left point falls
-// outside the window (cells clamped at the edge of the fine grid).
-// Contributions carry charge / (wx wy wz) (src/devicemesh.jl:104); the walk
-// is the reference's (src/kernels.jl:1083-1273) with the scatter grouped by
-// cell.  With `fixed` the additions go to an int64 grid in fixed point
-// (scale 2^40): each cell's window sums are fixed by the sort, and the
-// direct corners are integers, so the grid does not depend on the order in
-// which cells run.
-constexpr int kCicSmall = 32;
+// One warp at a time on a run of kCicClaim consecutive work items of the
+// cell sort (each at most `chunk` particles of one fine cell; a run usually
+// lies in one or two cells), claimed from a dynamic counter.  The fine cell
+// is one knot spacing wide and the coarse collocation gaps are at least
+// 2.19 a0 against the fine h = 2.44 a0, so a cell's particles' left coarse
+// points lie within two of the anchor, the point left of the cell's lower
+// edge: a 4^3 window of coarse points holds all their corners.  Each lane
+// adds its particles' eight trilinear corners into its own column of the
+// warp's 64-entry window in shared memory (rows padded to 33 words: no bank
+// conflicts for the lanes' updates nor for the sums over lanes).  When the
+// cell changes, and at the end of the run, the warp flushes the window: lane
+// l sums entries l and l + 32 over the 32 columns in a fixed order and adds
+// them to the grid.  Particles whose left point falls outside the window
+// (cells clamped at the edge of the fine grid) add their corners with
+// atomics directly.  Contributions carry charge / (wx wy wz)
+// (src/devicemesh.jl:104); the walk is the reference's
+// (src/kernels.jl:1083-1273) with the scatter grouped by cell.  With `fixed`
+// the additions go to an int64 grid in fixed point (scale 2^40): the runs
+// are fixed by the sort and each window's sums are taken in a fixed order,
+// so the grid does not depend on which warp takes which run.
+constexpr int kCicClaim = 8;
+constexpr int kCicRow = 33;  // padded window row: entry e, lane l at e * 33 + l
+constexpr int kCicWarps = kCicThreads / 32;
 
 struct CicWin {
   int anc[3];
@@ -333,13 +337,12 @@ __device__ __forceinline__ void cic_cell_window(CicWin& W, int kx, int ky, int k
   }
 }
 
-// The corners of one particle: into the thread's window column `win` (entry
-// e at win[e * kCicThreads]) when they fit, else to the grid.  win ==
-// nullptr: always to the grid.
+// The corners of one particle: into the lane's window column `col` (entry e
+// at col[e * kCicRow]) when they fit, else to the grid.
 __device__ __forceinline__ void cic_particle(const CicWin& W, int k0, int k1, int k2, float d0, float d1, float d2,
                                              float x0f, float hf, float charge, const float* gt, const float* igap,
                                              const float* idl, int ng, float lx0, float linvw, const int32_t* cells,
-                                             int ncells, float* win, float* rho, unsigned long long* fixed) {
+                                             int ncells, float* col, float* rho, unsigned long long* fixed) {
   const size_t n = ng, nn = n * n;
   const float px = fadd(fadd(x0f, fmul((float)(k0 - 1), hf)), d0);
   const float py = fadd(fadd(x0f, fmul((float)(k1 - 1), hf)), d1);
@@ -354,19 +357,18 @@ __device__ __forceinline__ void cic_particle(const CicWin& W, int k0, int k1, in
   const float wy0 = ay * iy0, wy1 = (1.f - ay) * iy1;
   const float wz0 = charge * az * iz0, wz1 = charge * (1.f - az) * iz1;
   const int lx = i0 - W.anc[0], ly = j0 - W.anc[1], lz = m0 - W.anc[2];
-  if (win && (unsigned)lx <= kCicW - 2 && (unsigned)ly <= kCicW - 2 && (unsigned)lz <= kCicW - 2) {
-    const int e = lx + kCicW * (ly + kCicW * lz);
-    float* c = win + (size_t)e * kCicThreads;
-    constexpr int SY = kCicW * kCicThreads, SZ = kCicW * kCicW * kCicThreads;
+  if ((unsigned)lx <= kCicW - 2 && (unsigned)ly <= kCicW - 2 && (unsigned)lz <= kCicW - 2) {
+    float* c = col + (size_t)(lx + kCicW * (ly + kCicW * lz)) * kCicRow;
+    constexpr int X = kCicRow, Y = kCicW * kCicRow, Z = kCicW * kCicW * kCicRow;
     const float a00 = wx0 * wy0, a10 = wx1 * wy0, a01 = wx0 * wy1, a11 = wx1 * wy1;
     c[0] += a00 * wz0;
-    c[kCicThreads] += a10 * wz0;
-    c[SY] += a01 * wz0;
-    c[SY + kCicThreads] += a11 * wz0;
-    c[SZ] += a00 * wz1;
-    c[SZ + kCicThreads] += a10 * wz1;
-    c[SZ + SY] += a01 * wz1;
-    c[SZ + SY + kCicThreads] += a11 * wz1;
+    c[X] += a10 * wz0;
+    c[Y] += a01 * wz0;
+    c[Y + X] += a11 * wz0;
+    c[Z] += a00 * wz1;
+    c[Z + X] += a10 * wz1;
+    c[Z + Y] += a01 * wz1;
+    c[Z + Y + X] += a11 * wz1;
   } else {
     const size_t b = (size_t)i0 + n * j0 + nn * m0;
     cic_add(rho, fixed, b, wx0 * wy0 * wz0);
@@ -380,18 +382,40 @@ __device__ __forceinline__ void cic_particle(const CicWin& W, int k0, int k1, in
   }
 }
 
-__global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
-    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds, DeviceScalars* dsc, int nk,
+// The warp's window to the grid, then zeroed: lane l takes entries l and l + 32.
+__device__ __forceinline__ void cic_flush(float* win, int lane, const CicWin& W, size_t n, float* rho,
+                                          unsigned long long* fixed) {
+  __syncwarp();
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int e = lane + 32 * h;
+    float* row = win + (size_t)e * kCicRow;
+    float v = 0.f;
+#pragma unroll 8
+    for (int j = 0; j < 32; ++j) {  // lane l reads word 33 l + j: bank (l + j) mod 32, no conflict
+      v += row[j];
+      row[j] = 0.f;
+    }
+    if (v != 0.f) {
+      const int ex = e % kCicW, ey = (e / kCicW) % kCicW, ez = e / (kCicW * kCicW);
+      cic_add(rho, fixed, (size_t)(W.anc[0] + ex) + n * (W.anc[1] + ey) + n * n * (W.anc[2] + ez), v);
+    }
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kCicThreads, 3) k_deposit_cic(
+    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
+    const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int nk,
     int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ gt_g, int ng,
     float lx0, float linvw, const int32_t* __restrict__ cells_g, int ncells, const float* __restrict__ dl_g,
-    float x0f, float hf, float charge, float* rho, unsigned long long* fixed) {
+    float x0f, float hf, float charge, float* rho, unsigned long long* fixed, int chunk) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float* win = reinterpret_cast<float*>(smem);                  // [kCicW3][kCicThreads]
-  float* gt = win + kCicW3 * kCicThreads;                       // [ng]
+  float* wins = reinterpret_cast<float*>(smem);                 // [kCicWarps][kCicW3][kCicRow]
+  float* gt = wins + kCicWarps * kCicW3 * kCicRow;              // [ng]
   float* igap = gt + ng;                                        // [ng] 1 / (gt[c] - gt[c-1])
   float* idl = igap + ng;                                       // [ng] 1 / dual length
   int32_t* cells = reinterpret_cast<int32_t*>(idl + ng);        // [ncells]
-  __shared__ int s_g;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int e = tid; e < ng; e += kCicThreads) {
     gt[e] = gt_g[e];
@@ -399,63 +423,56 @@ __global__ void __launch_bounds__(kCicThreads, 2) k_deposit_cic(
     idl[e] = 1.f / dl_g[e];
   }
   for (int e = tid; e < ncells; e += kCicThreads) cells[e] = cells_g[e];
-  const int nocc = dsc->noccupied;
-  const size_t n = ng, nn = n * n;
-  float* col = win + tid;
+  float* win = wins + (size_t)warp * kCicW3 * kCicRow;
+  for (int e = lane; e < kCicW3 * kCicRow; e += 32) win[e] = 0.f;
+  __syncthreads();
+  const int nitems = dsc->nitems;
+  const size_t n = ng;
+  float* col = win + lane;
   for (;;) {
-    __syncthreads();  // the window and s_g are free
-    if (tid == 0) s_g = (int)atomicAdd(&dsc->work_cic, 1ull);
-    __syncthreads();
-    const int g = s_g;
-    if (g >= nocc) break;
-    const int s0 = bounds[g], s1 = bounds[g + 1];
-    int kx, ky, kz;
-    cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
+    int i0 = 0;
+    if (lane == 0) i0 = (int)atomicAdd(&dsc->work_cic, (unsigned long long)kCicClaim);
+    i0 = __shfl_sync(0xffffffffu, i0, 0);
+    if (i0 >= nitems) break;
+    const int i1 = min(i0 + kCicClaim, nitems);
+    int gcur = -1;
     CicWin W;
-    cic_cell_window(W, kx, ky, kz, gt, igap, ng, lx0, linvw, cells, ncells, x0f, hf);
-    if (s1 - s0 <= kCicSmall) {
-      const int s = s0 + tid;
-      if (s < s1)
-        cic_particle(W, k[s], k[Npad + s], k[2 * Npad + s], d[s], d[Npad + s], d[2 * Npad + s], x0f, hf, charge,
-                     gt, igap, idl, ng, lx0, linvw, cells, ncells, nullptr, rho, fixed);
-      continue;
-    }
-#pragma unroll 8
-    for (int e = 0; e < kCicW3; ++e) col[(size_t)e * kCicThreads] = 0.f;
-    // two particles per iteration, their twelve loads issued together
-    for (int s = s0 + tid; s < s1; s += 2 * kCicThreads) {
-      const int t = s + kCicThreads;
-      const bool two = t < s1;
-      const int a0 = k[s], a1 = k[Npad + s], a2 = k[2 * Npad + s];
-      const float b0 = d[s], b1 = d[Npad + s], b2 = d[2 * Npad + s];
-      int c0 = 0, c1 = 0, c2 = 0;
-      float e0 = 0.f, e1 = 0.f, e2 = 0.f;
-      if (two) {
-        c0 = k[t]; c1 = k[Npad + t]; c2 = k[2 * Npad + t];
-        e0 = d[t]; e1 = d[Npad + t]; e2 = d[2 * Npad + t];
+    for (int item = i0; item < i1; ++item) {
+      const int g = item_cell[item];
+      if (g != gcur) {
+        if (gcur >= 0) cic_flush(win, lane, W, n, rho, fixed);
+        int kx, ky, kz;
+        cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
+        cic_cell_window(W, kx, ky, kz, gt, igap, ng, lx0, linvw, cells, ncells, x0f, hf);
+        gcur = g;
       }
-      cic_particle(W, a0, a1, a2, b0, b1, b2, x0f, hf, charge, gt, igap, idl, ng, lx0, linvw, cells, ncells, col,
-                   rho, fixed);
-      if (two)
-        cic_particle(W, c0, c1, c2, e0, e1, e2, x0f, hf, charge, gt, igap, idl, ng, lx0, linvw, cells, ncells, col,
-                     rho, fixed);
-    }
-    __syncthreads();
-    // warp w sums entries 8w .. 8w+7 over the 256 columns: lane order, then
-    // a fixed butterfly; one addition to the grid per nonzero entry
+      const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
+      const int s1 = min(s0 + chunk, bounds[g + 1]);
+      // the next particle's loads are in flight while this one is added
+      int nk3[3] = {0, 0, 0};
+      float nd3[3] = {0.f, 0.f, 0.f};
+      if (s0 + lane < s1) {
 #pragma unroll
-    for (int q = 0; q < kCicW3 / 8; ++q) {
-      const int e = warp * (kCicW3 / 8) + q;
-      const float* row = win + (size_t)e * kCicThreads;
-      float v = 0.f;
+        for (int a = 0; a < 3; ++a) {
+          nk3[a] = k[a * Npad + s0 + lane];
+          nd3[a] = d[a * Npad + s0 + lane];
+        }
+      }
+      for (int s = s0 + lane; s < s1; s += 32) {
+        const int ck[3] = {nk3[0], nk3[1], nk3[2]};
+        const float cd[3] = {nd3[0], nd3[1], nd3[2]};
+        if (s + 32 < s1) {
 #pragma unroll
-      for (int j = 0; j < kCicThreads / 32; ++j) v += row[lane + 32 * j];
-      v = warp_sumf(v);
-      if (lane == 0 && v != 0.f) {
-        const int ex = e % kCicW, ey = (e / kCicW) % kCicW, ez = e / (kCicW * kCicW);
-        cic_add(rho, fixed, (size_t)(W.anc[0] + ex) + n * (W.anc[1] + ey) + nn * (W.anc[2] + ez), v);
+          for (int a = 0; a < 3; ++a) {
+            nk3[a] = k[a * Npad + s + 32];
+            nd3[a] = d[a * Npad + s + 32];
+          }
+        }
+        cic_particle(W, ck[0], ck[1], ck[2], cd[0], cd[1], cd[2], x0f, hf, charge, gt, igap, idl, ng, lx0, linvw,
+                     cells, ncells, col, rho, fixed);
       }
     }
+    if (gcur >= 0) cic_flush(win, lane, W, n, rho, fixed);
   }
 }
 
@@ -528,7 +545,7 @@ void launch_deposit_fine(Ctx& c, double charge, int mode) {
 }
 
 size_t cic_smem(const Ctx& c) {
-  return (size_t)kCicW3 * kCicThreads * sizeof(float) + 3 * (size_t)c.coarse.n * sizeof(float) +
+  return (size_t)kCicWarps * kCicW3 * kCicRow * sizeof(float) + 3 * (size_t)c.coarse.n * sizeof(float) +
          (size_t)c.coarse.loc_ncell * sizeof(int32_t);
 }
 
@@ -545,8 +562,9 @@ void launch_deposit_coarse(Ctx& c, double charge, int mode) {
     VLB_CUDA(cudaMemsetAsync(C.rho, 0, tot * sizeof(float), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_cic, 0, sizeof(unsigned long long), c.stream));
   k_deposit_cic<<<c.num_sms * c.cic_cps, kCicThreads, cic_smem(c), c.stream>>>(
-      c.occupied, c.bounds, c.dsc, c.fine.nk, c.Npad, P.k, P.d, C.colloc, C.n, C.loc_x0, C.loc_invw, C.loc_cells,
-      C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho, fixed ? c.rho_fixed_c : nullptr);
+      c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.fine.nk, c.Npad, P.k, P.d, C.colloc, C.n,
+      C.loc_x0, C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho,
+      fixed ? c.rho_fixed_c : nullptr, c.chunk);
   VLB_LAUNCHED(c);
 }
 

@@ -355,8 +355,10 @@ constexpr int kFtRows = 128;                       // the MMA's M: particles per
 constexpr int kFtN = 112;                          // the MMA's N: 100 stencil columns, padded
 constexpr unsigned kFtA = 128u * 128u;             // one A operand: 128 rows x 32 TF32
 constexpr unsigned kFtB = (unsigned)kFtN * 128u;   // the B operand: 112 rows x 32 TF32
-constexpr unsigned kFtBars = 4u * kFtA + 2u * kFtB;
-constexpr unsigned kFtSmem = kFtBars + 32u;        // + two mbarriers and the tensor-memory slot
+constexpr unsigned kFtStage = 4u * kFtA + 2u * kFtB;  // the raw stencil tile: 100 rows of 16 floats
+constexpr unsigned kFtStageBytes = 100u * 64u;
+constexpr unsigned kFtBars = kFtStage + kFtStageBytes;
+constexpr unsigned kFtSmem = kFtBars + 32u;        // + three mbarriers and the tensor-memory slot
 constexpr unsigned kFtCols = 256;
 constexpr unsigned kFtColG = 128;                  // first column of Yg
 
@@ -433,14 +435,39 @@ __device__ __forceinline__ void ft_copy_a(unsigned char* A, int r, const float* 
                  : "memory");
 }
 
-// Row t < 100 (t = 10 kk + ii) of a cell's stencil: c[kk][0..9][ii].
-__device__ __forceinline__ void ft_load_b(const FtItem& it, int t, const float* __restrict__ csol, int n,
+// The cell's 10^3 stencil of csol staged by the TMA unit: row r = 10 kk + jj
+// (z plane kk, y row jj) is one 64-byte bulk copy of the 16 floats from the
+// row's first x index rounded down to a 16-byte boundary (csol is padded by
+// 16 floats past its end, so that the last rows' copies stay inside it);
+// the 100 copies complete on the stencil's mbarrier (6,400 bytes).  Thread
+// t < 100 issues row t; thread 0 arms the barrier.
+__device__ __forceinline__ size_t ft_row_index(const FtItem& it, int r, int n) {
+  const int kk = r / 10, jj = r - 10 * kk;
+  return (size_t)(2 * it.kx - 6) + (size_t)n * ((size_t)(2 * it.ky - 6 + jj) + (size_t)n * (size_t)(2 * it.kz - 6 + kk));
+}
+
+__device__ __forceinline__ void ft_stage_b(const FtItem& it, int t, const float* __restrict__ csol, int n,
+                                           unsigned char* raw, unsigned bar) {
+  if (t == 0) mbar_expect_tx(bar, kFtStageBytes);
+  if (t < 100) {
+    const size_t a0 = ft_row_index(it, t, n) & ~(size_t)3;
+    bulk_g2s(smem_u32(raw + 64u * t), csol + a0, 64u, bar);
+  }
+}
+
+// Row t < 100 (t = 10 kk + ii) of a cell's stencil from the staged tile:
+// c[jj] = csol at (ii, jj, kk) of the stencil = raw row (kk, jj) at its
+// alignment offset plus ii.
+__device__ __forceinline__ void ft_read_b(const FtItem& it, int t, int n, const unsigned char* raw,
                                           float (&c)[10]) {
   const int kk = t / 10, ii = t - 10 * kk;
-  const float* src = csol + (size_t)(2 * it.kx - 6 + ii) +
-                     (size_t)n * ((size_t)(2 * it.ky - 6) + (size_t)n * (size_t)(2 * it.kz - 6 + kk));
+  const float* rf = reinterpret_cast<const float*>(raw);
 #pragma unroll
-  for (int jj = 0; jj < 10; ++jj) c[jj] = __ldg(src + (size_t)n * jj);
+  for (int jj = 0; jj < 10; ++jj) {
+    const int r = 10 * kk + jj;
+    const int off = (int)(ft_row_index(it, r, n) & 3);
+    c[jj] = rf[16 * r + off + ii];
+  }
 }
 
 // That row of the B operand: [hi | hi | lo | 0 0].  Rows 100..111 are never
@@ -515,7 +542,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   extern __shared__ __align__(1024) unsigned char ftsm[];
   __shared__ double red[2][4][4];
   uint64_t* bars = reinterpret_cast<uint64_t*>(ftsm + kFtBars);
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(ftsm + kFtBars + 16);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(ftsm + kFtBars + 24);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nitems = dsc->nitems;
   const ProjF P = load_proj(dsc, w);
@@ -527,9 +554,12 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
+  unsigned char* raw = ftsm + kFtStage;
+  const unsigned sbar = smem_u32(&bars[2]);
   if (tid == 0) {
     mbar_init(smem_u32(&bars[0]), 1);
     mbar_init(smem_u32(&bars[1]), 1);
+    mbar_init(sbar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_before();
@@ -618,23 +648,32 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   bool ok = true;                  // the same in every thread after each barrier
   unsigned pending = 0;            // bit b: a commit on bars[b] not yet seen complete
 
+  unsigned sphase = 0;             // parity of the next completion of the stencil barrier
+  bool staging = false;            // stencil copies issued and not yet seen complete
   FtPart pc;
   load_part(cur, dc, pc);
   if (cur.has) {
-    if (tid < 100) {
-      float c[10];
-      ft_load_b(cur, tid, csol, n, c);
-      ft_store_b(ftsm + 4u * kFtA, tid, c);
+    ft_stage_b(cur, tid, csol, n, raw, sbar);
+    staging = true;
+    copy_a(0, pc);
+    ok = __all_sync(0xffffffffu, mbar_wait(sbar, sphase));
+    if (ok) {
+      staging = false;
+      sphase ^= 1u;
+      if (tid < 100) {
+        float c[10];
+        ft_read_b(cur, tid, n, raw, c);
+        ft_store_b(ftsm + 4u * kFtA, tid, c);
+      }
     }
     staged0 = cur.code;
-    copy_a(0, pc);
   }
   asm volatile("cp.async.wait_all;" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   fence_before();
-  __syncthreads();
-  if (tid == 0 && cur.has) issue(0);
-  if (cur.has) pending |= 1u;
+  ok = __syncthreads_and(ok) != 0;
+  if (tid == 0 && cur.has && ok) issue(0);
+  if (cur.has && ok) pending |= 1u;
 
   int b = 0;
   for (int t = 0; cur.item >= 0; ++t) {
@@ -651,9 +690,11 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     // of item t-1, completed in the previous iteration), in flight during
     // item t's finish
     copy_a(nb, pn);
-    const bool restage = nxt.has && (nb ? staged1 : staged0) != nxt.code;
-    float cb[10];
-    if (restage && tid < 100) ft_load_b(nxt, tid, csol, n, cb);
+    const bool restage = nxt.has && ok && (nb ? staged1 : staged0) != nxt.code;
+    if (restage) {
+      ft_stage_b(nxt, tid, csol, n, raw, sbar);  // the tile is free: read before the last barrier
+      staging = true;
+    }
 
     // ---- item t
     bool got = false;
@@ -705,7 +746,17 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     // MMAs of item t-1, completed in the previous iteration), then wait for
     // its A rows
     if (restage) {
-      if (tid < 100) ft_store_b(ftsm + 4u * kFtA + (unsigned)nb * kFtB, tid, cb);
+      const bool sok = __all_sync(0xffffffffu, mbar_wait(sbar, sphase));
+      ok = ok && sok;
+      if (sok) {
+        staging = false;
+        sphase ^= 1u;
+        if (tid < 100) {
+          float cb[10];
+          ft_read_b(nxt, tid, n, raw, cb);
+          ft_store_b(ftsm + 4u * kFtA + (unsigned)nb * kFtB, tid, cb);
+        }
+      }
       if (nb)
         staged1 = nxt.code;
       else
@@ -735,6 +786,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   // wait that gave up, at most one commit per barrier is outstanding)
   for (int bb = 0; bb < 2; ++bb)
     if (pending & (1u << bb)) mbar_wait(smem_u32(&bars[bb]), (phase >> bb) & 1u);
+  if (staging) mbar_wait(sbar, sphase);  // no stencil copy may still be writing the tile
   fence_before();
   __syncthreads();
   if (warp == 0) {

@@ -202,6 +202,7 @@ __global__ void __launch_bounds__(kListThreads) k_cell_lists(const int32_t* __re
     dsc->nitems = (int32_t)carry[1];
     dsc->outcount = (int32_t)carry[2];
     dsc->nocc_par[parity] = nocc;
+    dsc->nitems_par[parity] = (int32_t)carry[1];
   }
 }
 
@@ -463,10 +464,13 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_downsweep(
 // counts alone: the particles of new cell c come from the old cells
 // c - off(d), in increasing old-cell order (decreasing d), each group in slot
 // order.  So
-//   A  counts, per old cell and direction, its particles;
+//   A  counts, per old work item and direction, its particles;
+//   A2 turns them into each item's prefix within its cell, and the cell's
+//      totals per direction;
 //   B  gives each (old cell, direction) group its first slot in the new
 //      order: one warp per new cell sums the groups that precede it;
-//   C  ranks each particle within its group by slot: perm[base + rank] = s.
+//   C  ranks each particle within its group by slot: perm[base + prefix +
+//      rank] = s.
 // A particle whose D is none of the 27 offsets sets sort_far, and the step
 // takes the radix passes instead (gated on that flag).  Each new cell's
 // groups must add up to its count from the push's histogram, else B sets
@@ -493,22 +497,30 @@ __device__ __forceinline__ int64_t direction_offset(int d, int nk) {
 constexpr int kDirs = 27;
 constexpr int kNearThreads = 256;
 
-// A: one warp per old occupied cell; per-warp counters in shared memory.
-__global__ void __launch_bounds__(kNearThreads) k_near_count(const int32_t* __restrict__ occ_old,
+// The work items of the last sort (runs of at most chunk_old particles of
+// one old cell, in slot order) spread the work evenly: A and C take one warp
+// per item, A2 one warp per old cell over its few items.
+
+// A: per item, the particles of each direction -> item_dir[item][27].
+__global__ void __launch_bounds__(kNearThreads) k_near_count(const int32_t* __restrict__ item_old,
+                                                            const int32_t* __restrict__ cstart_old,
+                                                            const int32_t* __restrict__ occ_old,
                                                             const int32_t* __restrict__ bnd_old,
-                                                            DeviceScalars* dsc, int par_old,
+                                                            DeviceScalars* dsc, int par_old, int chunk_old,
                                                             const uint32_t* __restrict__ keys, int nk,
-                                                            int32_t* __restrict__ dir_cnt) {
+                                                            int32_t* __restrict__ item_dir) {
   __shared__ int32_t cnt[kNearThreads / 32][kDirs];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int nocc = dsc->nocc_par[par_old];
+  const int nitems = dsc->nitems_par[par_old];
   const int warps = gridDim.x * (kNearThreads / 32);
   bool far = false;
-  for (int g = blockIdx.x * (kNearThreads / 32) + w; g < nocc; g += warps) {
+  for (int item = blockIdx.x * (kNearThreads / 32) + w; item < nitems; item += warps) {
     if (lane < kDirs) cnt[w][lane] = 0;
     __syncwarp();
+    const int g = item_old[item];
     const int64_t o = occ_old[g];
-    const int s0 = bnd_old[g], s1 = bnd_old[g + 1];
+    const int s0 = bnd_old[g] + (item - cstart_old[g]) * chunk_old;
+    const int s1 = min(s0 + chunk_old, bnd_old[g + 1]);
     for (int base = s0; base < s1; base += 32) {
       const int s = base + lane;
       const bool valid = s < s1;
@@ -516,16 +528,49 @@ __global__ void __launch_bounds__(kNearThreads) k_near_count(const int32_t* __re
       if (valid) {
         const int d = direction_of((int64_t)keys[s] - o, nk);
         far |= d < 0;
-        const int dd = d < 0 ? kDirs : d;
-        const unsigned peers = __match_any_sync(m, dd);
+        const unsigned peers = __match_any_sync(m, d < 0 ? kDirs : d);
         if (d >= 0 && lane == __ffs(peers) - 1) cnt[w][d] += __popc(peers);
       }
       __syncwarp();
     }
-    if (lane < kDirs) dir_cnt[(size_t)g * kDirs + lane] = cnt[w][lane];
+    if (lane < kDirs) item_dir[(size_t)item * kDirs + lane] = cnt[w][lane];
     __syncwarp();
   }
   if (__any_sync(0xffffffffu, far) && lane == 0) atomicOr(&dsc->sort_far, 1);
+}
+
+// A2: per old cell (one warp, lane d a direction), the exclusive prefix of
+// its items' counts in item order, in place, and the cell's totals.
+__global__ void __launch_bounds__(kNearThreads) k_near_prefix(const int32_t* __restrict__ cstart_old,
+                                                             const DeviceScalars* dsc, int par_old,
+                                                             int32_t* __restrict__ item_dir,
+                                                             int32_t* __restrict__ dir_cnt) {
+  if (dsc->sort_far) return;
+  const int lane = threadIdx.x & 31;
+  const int nocc = dsc->nocc_par[par_old], nitems = dsc->nitems_par[par_old];
+  const int warps = gridDim.x * (kNearThreads / 32);
+  for (int g = blockIdx.x * (kNearThreads / 32) + (threadIdx.x >> 5); g < nocc; g += warps) {
+    const int i0 = cstart_old[g], i1 = g + 1 < nocc ? cstart_old[g + 1] : nitems;
+    if (lane >= kDirs) continue;
+    int run = 0;
+    int i = i0;
+    for (; i + 4 <= i1; i += 4) {  // four independent loads in flight
+      int v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = item_dir[(size_t)(i + u) * kDirs + lane];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        item_dir[(size_t)(i + u) * kDirs + lane] = run;
+        run += v[u];
+      }
+    }
+    for (; i < i1; ++i) {
+      const int v = item_dir[(size_t)i * kDirs + lane];
+      item_dir[(size_t)i * kDirs + lane] = run;
+      run += v;
+    }
+    dir_cnt[(size_t)g * kDirs + lane] = run;
+  }
 }
 
 // B: one warp per new occupied cell c.  Lane l < 27 holds the group of
@@ -571,24 +616,30 @@ __global__ void __launch_bounds__(kNearThreads) k_near_bases(const int32_t* __re
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&dsc->sort_far, 2);
 }
 
-// C: one warp per old occupied cell, slots in order, a running rank per
-// direction: perm[base + rank] = slot.
-__global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __restrict__ occ_old,
+// C: one warp per item, slots in order, a running rank per direction from
+// the group's first slot, the item's prefix within its cell: perm[rank] = s.
+__global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __restrict__ item_old,
+                                                            const int32_t* __restrict__ cstart_old,
+                                                            const int32_t* __restrict__ occ_old,
                                                             const int32_t* __restrict__ bnd_old,
-                                                            const DeviceScalars* dsc, int par_old,
+                                                            const DeviceScalars* dsc, int par_old, int chunk_old,
                                                             const uint32_t* __restrict__ keys, int nk,
+                                                            const int32_t* __restrict__ item_dir,
                                                             const int32_t* __restrict__ dir_base,
                                                             uint32_t* __restrict__ perm) {
   if (dsc->sort_far) return;
   __shared__ int32_t run[kNearThreads / 32][kDirs];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int nocc = dsc->nocc_par[par_old];
+  const int nitems = dsc->nitems_par[par_old];
   const int warps = gridDim.x * (kNearThreads / 32);
-  for (int g = blockIdx.x * (kNearThreads / 32) + w; g < nocc; g += warps) {
-    if (lane < kDirs) run[w][lane] = dir_base[(size_t)g * kDirs + lane];
+  for (int item = blockIdx.x * (kNearThreads / 32) + w; item < nitems; item += warps) {
+    const int g = item_old[item];
+    if (lane < kDirs)
+      run[w][lane] = dir_base[(size_t)g * kDirs + lane] + item_dir[(size_t)item * kDirs + lane];
     __syncwarp();
     const int64_t o = occ_old[g];
-    const int s0 = bnd_old[g], s1 = bnd_old[g + 1];
+    const int s0 = bnd_old[g] + (item - cstart_old[g]) * chunk_old;
+    const int s1 = min(s0 + chunk_old, bnd_old[g + 1]);
     for (int base = s0; base < s1; base += 32) {
       const int s = base + lane;
       const bool valid = s < s1;
@@ -604,6 +655,7 @@ __global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __re
       }
       __syncwarp();
     }
+    __syncwarp();
   }
 }
 
@@ -676,6 +728,9 @@ void launch_sort(Ctx& c) {
   const bool near = c.keys_ready && c.order_valid;
   c.occupied = c.occ_buf[pn];
   c.bounds = c.bnd_buf[pn];
+  c.item_cell = c.item_buf[pn];
+  c.chunk_start = c.cstart_buf[pn];
+  c.chunk_par[pn] = c.chunk;
   VLB_CUDA(cudaMemsetAsync(c.scan_status, 0, c.scan_status_size * sizeof(unsigned long long), c.stream));
   VLB_CUDA(cudaMemsetAsync(c.dsc->scan_tiles, 0, sizeof(c.dsc->scan_tiles), c.stream));
   if (!c.keys_ready) {
@@ -698,13 +753,17 @@ void launch_sort(Ctx& c) {
   const int32_t* gate = nullptr;
   if (near) {
     const int grid = c.num_sms * 8;
-    k_near_count<<<grid, kNearThreads, 0, c.stream>>>(c.occ_buf[po], c.bnd_buf[po], c.dsc, po, c.keys, nk,
-                                                      c.dir_cnt);
+    const int chunk_old = c.chunk_par[po];
+    k_near_count<<<grid, kNearThreads, 0, c.stream>>>(c.item_buf[po], c.cstart_buf[po], c.occ_buf[po],
+                                                      c.bnd_buf[po], c.dsc, po, chunk_old, c.keys, nk, c.item_dir);
+    VLB_LAUNCHED(c);
+    k_near_prefix<<<grid, kNearThreads, 0, c.stream>>>(c.cstart_buf[po], c.dsc, po, c.item_dir, c.dir_cnt);
     VLB_LAUNCHED(c);
     k_near_bases<<<grid, kNearThreads, 0, c.stream>>>(c.occupied, c.bounds, c.occ_buf[po], c.cidx_buf[po], c.dsc,
                                                       po, c.ncell, nk, c.dir_cnt, c.dir_base);
     VLB_LAUNCHED(c);
-    k_near_place<<<grid, kNearThreads, 0, c.stream>>>(c.occ_buf[po], c.bnd_buf[po], c.dsc, po, c.keys, nk,
+    k_near_place<<<grid, kNearThreads, 0, c.stream>>>(c.item_buf[po], c.cstart_buf[po], c.occ_buf[po],
+                                                      c.bnd_buf[po], c.dsc, po, chunk_old, c.keys, nk, c.item_dir,
                                                       c.dir_base, c.perm);
     VLB_LAUNCHED(c);
     gate = &c.dsc->sort_far;  // the radix passes below run only if that path gave up

@@ -75,6 +75,7 @@ struct DeviceScalars {
   int32_t film_next;                 // frames taken since vlb_film_reserve
   int32_t film_pad;
   int32_t nocc_par[2];               // occupied cells of the sort products of each parity
+  int32_t nitems_par[2];             // and their work items
 };
 
 struct Level {
@@ -160,8 +161,12 @@ struct Ctx {
   bool order_valid = false;      // part[cur] is in the order its sort products describe
   bool last_sort_near = false;   // the last sort tried the nearly sorted path
   int32_t* outlist = nullptr;    // [N]
-  int32_t* chunk_start = nullptr;  // [ncell] first chunk of occupied cell g
-  int32_t* item_cell = nullptr;    // [N / kChunk + ncell] occupied cell of each chunk
+  int32_t* chunk_start = nullptr;  // [ncell] first chunk of occupied cell g (current parity's)
+  int32_t* item_cell = nullptr;    // [N / kMinChunk + ncell] occupied cell of each chunk (current parity's)
+  int32_t* cstart_buf[2] = {nullptr, nullptr};
+  int32_t* item_buf[2] = {nullptr, nullptr};
+  int chunk_par[2] = {kChunk, kChunk};  // the chunk each parity's work items were cut with
+  int32_t* item_dir = nullptr;     // [N / kMinChunk + ncell][27] nearly sorted path: per item and direction
   unsigned long long* scan_status = nullptr;  // look-back tile states
   int64_t scan_status_size = 0;
   // deposit

@@ -589,7 +589,7 @@ class DeviceAccelerator:
         n = L.lib().vlb_stage_count()
         ms = np.zeros(12)
         L.check(L.lib().vlb_stage_times(self._h, L.pd(ms), 12))
-        return {L.lib().vlb_stage_name(i).decode(): ms[i] for i in range(n)}
+        return {L.lib().vlb_stage_name(i).decode(): ms[i] for i in range(n) if i != 9}
 
     def stream_handle(self) -> int:
         s = C.c_void_p()
