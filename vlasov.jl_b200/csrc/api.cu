@@ -76,33 +76,6 @@ float* upload_f(const double* src, size_t n) {
   return upload(v.data(), n);
 }
 
-// Rounding to TF32 with ties away from zero, on the bits: the device's
-// tf32_rna (tc_util.cuh), so that both sides split a value identically.
-float tf32_rna_host(float x) {
-  uint32_t u;
-  std::memcpy(&u, &x, 4);
-  u = (u + 0x1000u) & 0xFFFFE000u;
-  std::memcpy(&x, &u, 4);
-  return x;
-}
-
-// The gather's A-operand rows of a smoothing table ([ncol][10] values):
-// per column [hi(10) | lo(10) | hi(10) | 0 0], hi = tf32(v) and lo =
-// tf32(v - hi) of the float32 value v, the K-folded 3xTF32 operand row.
-float* upload_tf32_split_rows(const double* tab, int ncol) {
-  std::vector<float> rows((size_t)ncol * 32, 0.f);
-  for (int col = 0; col < ncol; ++col)
-    for (int j = 0; j < 10; ++j) {
-      const float v = (float)tab[(size_t)col * 10 + j];
-      const float hi = tf32_rna_host(v);
-      const float lo = tf32_rna_host(v - hi);
-      rows[(size_t)col * 32 + j] = hi;
-      rows[(size_t)col * 32 + 10 + j] = lo;
-      rows[(size_t)col * 32 + 20 + j] = hi;
-    }
-  return upload(rows.data(), rows.size());
-}
-
 // A^T zero-padded to `pad` columns: out[i][r] = A[r][i]
 float* upload_transposed(const double* A, int n, int pad) {
   std::vector<float> v((size_t)n * pad, 0.f);
@@ -190,7 +163,7 @@ void destroy_ctx(Ctx* c) {
   }
   free_level(c->fine);
   free_level(c->coarse);
-  dfree(c->overlap); dfree(c->gradient); dfree(c->nodes); dfree(c->ov_split); dfree(c->gr_split);
+  dfree(c->overlap); dfree(c->gradient); dfree(c->nodes);
   for (int b = 0; b < 2; ++b) {
     dfree(c->part[b].k); dfree(c->part[b].d); dfree(c->part[b].pk); dfree(c->part[b].pd);
   }
@@ -462,8 +435,6 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->overlap = upload_f(S.overlap, (size_t)c->ncol * 10);
     c->gradient = upload_f(S.gradient, (size_t)c->ncol * 10);
     c->nodes = upload_f(S.nodes, (size_t)c->ncol * 8);
-    c->ov_split = upload_tf32_split_rows(S.overlap, c->ncol);
-    c->gr_split = upload_tf32_split_rows(S.gradient, c->ncol);
     const size_t P = 3 * (size_t)c->Npad;
     for (int b = 0; b < 2; ++b) {
       c->part[b].k = dalloc<int32_t>(P);

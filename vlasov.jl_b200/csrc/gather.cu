@@ -378,14 +378,13 @@ struct FtItem {
   bool has;         // the stencil fits: MMAs and forces
 };
 
-// One particle of an item: delta, slot, its y table column (the A rows are
-// copied from the split tables) and the four x and z table columns as
+// One particle of an item: delta, slot, and the six table columns as
 // neighbour pairs (ten values each).
 struct FtPart {
   float dx, dy, dz;
-  int s, cy;
+  int s;
   bool valid;
-  float2 ox[5], gx[5], oz[5], gz[5];
+  float2 oy[5], gy[5], ox[5], gx[5], oz[5], gz[5];
 };
 
 // An item's cell data as loaded (used an iteration later, so that no
@@ -425,14 +424,25 @@ __device__ __forceinline__ void ft_load_pairs(const float* __restrict__ tab, int
   for (int a = 0; a < 5; ++a) v[a] = __ldg(p + a);
 }
 
-// Row r of an A operand: the particle's split table row (32 TF32 values,
-// [hi | lo | hi | 0 0] of its ten y weights, made once per context) copied
-// from global memory by eight 16-byte asynchronous copies, one per K group.
-__device__ __forceinline__ void ft_copy_a(unsigned char* A, int r, const float* __restrict__ row) {
+// Row r of an A operand from the ten values v: [hi | lo | hi | 0 0].
+__device__ __forceinline__ void ft_store_a(unsigned char* A, int r, const float2 (&v2)[5]) {
+  float hi[10], lo[10];
 #pragma unroll
-  for (int kg = 0; kg < 8; ++kg)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_u32(A + ft_off(r, kg))), "l"(row + 4 * kg)
-                 : "memory");
+  for (int j = 0; j < 5; ++j) {
+    hi[2 * j] = tf32_rna(v2[j].x);
+    hi[2 * j + 1] = tf32_rna(v2[j].y);
+    lo[2 * j] = tf32_rna(__fsub_rn(v2[j].x, hi[2 * j]));
+    lo[2 * j + 1] = tf32_rna(__fsub_rn(v2[j].y, hi[2 * j + 1]));
+  }
+  auto at = [&](int kg) { return reinterpret_cast<float4*>(A + ft_off(r, kg)); };
+  *at(0) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+  *at(1) = make_float4(hi[4], hi[5], hi[6], hi[7]);
+  *at(2) = make_float4(hi[8], hi[9], lo[0], lo[1]);
+  *at(3) = make_float4(lo[2], lo[3], lo[4], lo[5]);
+  *at(4) = make_float4(lo[6], lo[7], lo[8], lo[9]);
+  *at(5) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+  *at(6) = make_float4(hi[4], hi[5], hi[6], hi[7]);
+  *at(7) = make_float4(hi[8], hi[9], 0.f, 0.f);
 }
 
 // The cell's 10^3 stencil of csol staged by the TMA unit: row r = 10 kk + jj
@@ -536,9 +546,8 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
     const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int64_t Npad,
     const float* __restrict__ d, const float* __restrict__ csol, int n, int nk, const float* __restrict__ ov,
-    const float* __restrict__ gr, const float* __restrict__ ovs, const float* __restrict__ grs, int nbdt, int ncol,
-    float spacing, float x0, float h, double w, float* __restrict__ force, int chunk,
-    double* __restrict__ red_items) {
+    const float* __restrict__ gr, int nbdt, int ncol, float spacing, float x0, float h, double w,
+    float* __restrict__ force, int chunk, double* __restrict__ red_items) {
   extern __shared__ __align__(1024) unsigned char ftsm[];
   __shared__ double red[2][4][4];
   uint64_t* bars = reinterpret_cast<uint64_t*>(ftsm + kFtBars);
@@ -596,23 +605,24 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     p.dy = dd[1];
     p.dz = dd[2];
     const int cx = table_column(p.dx, spacing, nbdt, ncol);
-    p.cy = table_column(p.dy, spacing, nbdt, ncol);
+    const int cy = table_column(p.dy, spacing, nbdt, ncol);
     const int cz = table_column(p.dz, spacing, nbdt, ncol);
+    ft_load_pairs(ov, cy, p.oy);
+    ft_load_pairs(gr, cy, p.gy);
     ft_load_pairs(ov, cx, p.ox);
     ft_load_pairs(gr, cx, p.gx);
     ft_load_pairs(ov, cz, p.oz);
     ft_load_pairs(gr, cz, p.gz);
   };
 
-  // the A rows of particle p into buffer buf: its y column's split rows of
-  // the overlap (Yo) and gradient (Yg) tables, asynchronously
-  auto copy_a = [&](int buf, const FtPart& p) {
+  // the A rows of particle p into buffer buf: its y tables split into
+  // head and tail (Yo from the overlap table, Yg from the gradient table)
+  auto store_a = [&](int buf, const FtPart& p) {
     if (p.valid) {
       unsigned char* Ao = ftsm + (unsigned)(2 * buf) * kFtA;
-      ft_copy_a(Ao, tid, ovs + (size_t)(p.cy - 1) * 32);
-      ft_copy_a(Ao + kFtA, tid, grs + (size_t)(p.cy - 1) * 32);
+      ft_store_a(Ao, tid, p.oy);
+      ft_store_a(Ao + kFtA, tid, p.gy);
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
   };
 
   auto issue = [&](int buf) {
@@ -655,7 +665,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   if (cur.has) {
     ft_stage_b(cur, tid, csol, n, raw, sbar);
     staging = true;
-    copy_a(0, pc);
+    store_a(0, pc);
     ok = __all_sync(0xffffffffu, mbar_wait(sbar, sphase));
     if (ok) {
       staging = false;
@@ -668,7 +678,6 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     }
     staged0 = cur.code;
   }
-  asm volatile("cp.async.wait_all;" ::: "memory");
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   fence_before();
   ok = __syncthreads_and(ok) != 0;
@@ -686,10 +695,6 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     g3 = cell_of(item_at(t + 4));
     FtPart pn;
     load_part(nxt, dn, pn);
-    // item t+1's A rows into the other buffers (their last reader, the MMAs
-    // of item t-1, completed in the previous iteration), in flight during
-    // item t's finish
-    copy_a(nb, pn);
     const bool restage = nxt.has && ok && (nb ? staged1 : staged0) != nxt.code;
     if (restage) {
       ft_stage_b(nxt, tid, csol, n, raw, sbar);  // the tile is free: read before the last barrier
@@ -742,9 +747,9 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
       red[b][warp][3] = ae;
     }
 
-    // ---- item t+1's stencil into the other B buffer (its last reader, the
-    // MMAs of item t-1, completed in the previous iteration), then wait for
-    // its A rows
+    // ---- item t+1's operands into the other buffers (their last reader,
+    // the MMAs of item t-1, completed in the previous iteration): the
+    // stencil, when it changed, and the particles' A rows
     if (restage) {
       const bool sok = __all_sync(0xffffffffu, mbar_wait(sbar, sphase));
       ok = ok && sok;
@@ -762,7 +767,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
       else
         staged0 = nxt.code;
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    store_a(nb, pn);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     fence_before();
     ok = __syncthreads_and(ok) != 0;  // after a wait that gave up, no more MMAs
@@ -1096,8 +1101,7 @@ void launch_forces(Ctx& c) {
   if (c.field_tc && c.chunk <= kFtRows) {
     k_field_tc<<<2 * c.num_sms, kFtThreads, kFtSmem, c.stream>>>(
         c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.d, F.csol, F.n, F.nk, c.overlap,
-        c.gradient, c.ov_split, c.gr_split, c.nbdt, c.ncol, c.spacing_f, c.x0f, c.hf, c.weight, c.force, c.chunk,
-        c.red_items);
+        c.gradient, c.nbdt, c.ncol, c.spacing_f, c.x0f, c.hf, c.weight, c.force, c.chunk, c.red_items);
   } else {
     VLB_CUDA(cudaMemsetAsync(&c.dsc->work_gather, 0, sizeof(unsigned long long), c.stream));
     k_field<<<c.num_sms * c.field_cps, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.chunk_start, c.item_cell,

@@ -476,17 +476,22 @@ __global__ void __launch_bounds__(kRadixThreads) k_radix_downsweep(
 // groups must add up to its count from the push's histogram, else B sets
 // the flag as well: the path never guesses.
 
+// Direction of a key difference D, or -1 for none of the 27 offsets.  With
+// t = D + 1 + nk + nk^2 = dx' + nk dy' + nk^2 dz' (each primed digit in 0..2
+// for a neighbour), the digits come from comparisons: dz' is 2, 1 or 0 as t
+// reaches 2 nk^2, nk^2 or not, dy' likewise on the remainder, and the last
+// remainder dx' must be at most 2 (any other D leaves a larger one).
 __device__ __forceinline__ int direction_of(int64_t D, int nk) {
   if (D == 0) return 13;  // most particles stay in their cell
   const int64_t nk2 = (int64_t)nk * nk;
-  const int64_t t = D + 1 + nk + nk2;
-  if (t < 0 || t > 2 + 2 * (int64_t)nk + 2 * nk2) return -1;
-  const int dz = (int)(t / nk2);
-  const int64_t r = t - dz * nk2;
-  const int dy = (int)(r / nk);
-  const int dx = (int)(r - dy * nk);
-  if (dx > 2 || dy > 2 || dz > 2) return -1;
-  return dx + 3 * dy + 9 * dz;
+  int64_t t = D + 1 + nk + nk2;
+  if (t < 0) return -1;
+  const int dz = t >= 2 * nk2 ? 2 : (t >= nk2 ? 1 : 0);
+  t -= dz * nk2;
+  const int dy = t >= 2 * (int64_t)nk ? 2 : (t >= nk ? 1 : 0);
+  t -= (int64_t)dy * nk;
+  if (t > 2) return -1;
+  return (int)t + 3 * dy + 9 * dz;
 }
 
 __device__ __forceinline__ int64_t direction_offset(int d, int nk) {
@@ -553,21 +558,15 @@ __global__ void __launch_bounds__(kNearThreads) k_near_prefix(const int32_t* __r
     const int i0 = cstart_old[g], i1 = g + 1 < nocc ? cstart_old[g + 1] : nitems;
     if (lane >= kDirs) continue;
     int run = 0;
-    int i = i0;
-    for (; i + 4 <= i1; i += 4) {  // four independent loads in flight
-      int v[4];
+    for (int i = i0; i < i1; i += 16) {  // up to sixteen independent loads in flight
+      int v[16];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = item_dir[(size_t)(i + u) * kDirs + lane];
+      for (int u = 0; u < 16; ++u) v[u] = i + u < i1 ? item_dir[(size_t)(i + u) * kDirs + lane] : 0;
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        item_dir[(size_t)(i + u) * kDirs + lane] = run;
+      for (int u = 0; u < 16; ++u) {
+        if (i + u < i1) item_dir[(size_t)(i + u) * kDirs + lane] = run;
         run += v[u];
       }
-    }
-    for (; i < i1; ++i) {
-      const int v = item_dir[(size_t)i * kDirs + lane];
-      item_dir[(size_t)i * kDirs + lane] = run;
-      run += v;
     }
     dir_cnt[(size_t)g * kDirs + lane] = run;
   }

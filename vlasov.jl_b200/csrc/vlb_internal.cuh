@@ -129,10 +129,6 @@ struct Ctx {
   float* overlap = nullptr;   // [ncol][10]
   float* gradient = nullptr;  // [ncol][10]
   float* nodes = nullptr;     // [ncol][8]
-  // the gather's A-operand rows per table column: [hi | lo | hi | 0 0] of
-  // the ten values, hi = TF32 rounding (ties away), lo = that of value - hi
-  float* ov_split = nullptr;  // [ncol][32]
-  float* gr_split = nullptr;  // [ncol][32]
   // particle state, double buffered for the sort
   Particles part[2];
   int cur = 0;
