@@ -47,6 +47,7 @@ def test_smallest_crossing_captures_about_one_electron(cuda_device):
 
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "capture_host_1e5.npz"
+ENSEMBLE = Path(__file__).resolve().parent / "golden" / "capture_host_1e5_ensemble.npz"
 
 
 def test_cpu_path_mode_follows_the_reference_cpu_run(cuda_device):
@@ -55,32 +56,54 @@ def test_cpu_path_mode_follows_the_reference_cpu_run(cuda_device):
     reaction while priming), against that path's own float64 run
     (tests/golden/capture_host_1e5.npz, tests/golden/make_capture_host.py).
 
-    The crossing is chaotic once the ion has passed the cluster's centre: the
-    CPU path against itself, started from the same cloud rounded to the packed
-    float32 form, stays within one particle (0.002 e) to step 400 and then
-    spreads to 0.051 e.  q(<8) is a count, one pseudo-particle carrying
-    0.00196 e here: the GPU step computes in float32 with the device path's
-    discrete choices, which moves the few particles lying within rounding
-    distance of the 8 a0 sphere.  So the bar is three pseudo-particles
-    (0.0059 e) at every step to 400, and beyond it no more than twice the
-    CPU path's spread against itself (maximum and rms); the out-of-stencil
-    counts within 1 % at steps 350 and 700.  A step's out-of-stencil count is taken by its sort, on the
-    positions the previous step left; the fixture counts after each step, so
-    step s of the GPU run is compared with entry s - 1 of the fixture."""
+    q(<8) is a count, one pseudo-particle carrying 0.00196 e here.  To step
+    400 the GPU stays within three pseudo-particles (0.0059 e); the CPU path
+    itself with its state rounded to the packed float32 form after every
+    step, as a device holds it, departs by two (0.0039 e).
+
+    The crossing is chaotic once the ion has passed the cluster's centre.
+    Eight CPU-path runs perturbed by float32 rounding (the packed start, the
+    per-step rounding, seeded one-ulp moves of the start cloud:
+    tests/golden/make_capture_ensemble.py) depart from the base run by at
+    most 0.071 e after step 400 (rms at most 0.021 e) and end between 0.974
+    and 1.027 e.  The GPU step adds float32 arithmetic to every force, and
+    in this mode still decides which particles take the fine field by the
+    device path's stencil fit, not the CPU path's margin test, which matters
+    once the cloud reaches the fine grid's edge (the out count rises from
+    step 550) and the ion leaves the fine grid (x = 50, step 600).  So after
+    step 400 it is held to 1.75 times the ensemble's largest departure
+    (maximum and rms), and its final charge to the ensemble's range of final
+    charges, give or take 0.01 e.
+
+    A step's out-of-stencil count is taken by its sort, on the positions the
+    previous step left; the fixture counts after each step, so step s of the
+    GPU run is compared with entry s - 1 of the fixture.  The count is the
+    expanding cloud's front leaving the fine grid: from step 600 it rises by
+    up to 50 particles a step (1.5 % of the count), so it is held to the time
+    the front arrives: within the fixture's counts two steps either side,
+    give or take 1 %, at steps 350 and 700."""
     g = np.load(GOLDEN)
+    e = np.load(ENSEMBLE)
     r = vb.xenon.run(100_000, 28, device=cuda_device, quiet=True, softening="ball")
     q, out = np.asarray(r["q8"]), np.asarray(r["outcount"])
-    qh, qp = g["q8"], g["q8_packed"]
+    qh = g["q8"]
+    members = np.vstack([g["q8_packed"][None, :], e["q8"]])
+    dm = np.abs(members - qh[None, :])
+    env_max = dm[:, 400:].max()
+    env_rms = np.sqrt(np.mean(dm[:, 400:] ** 2, axis=1)).max()
     d = np.abs(q - qh)
-    self_spread = np.abs(qh - qp)
+    rms = np.sqrt(np.mean(d[400:] ** 2))
+    finals = np.concatenate([[qh[-1]], members[:, -1]])
     print(f"\n[config 1, ball softening] q(<8) at 350 / 700: GPU {q[349]:.4f} / {q[-1]:.4f}, "
           f"CPU path {qh[349]:.4f} / {qh[-1]:.4f}; max |dq| to step 400 {d[:400].max():.4f}, after "
-          f"{d[400:].max():.4f} (CPU path vs itself {self_spread[400:].max():.4f}); rms after "
-          f"{np.sqrt(np.mean(d[400:] ** 2)):.4f} (self {np.sqrt(np.mean(self_spread[400:] ** 2)):.4f}); "
+          f"{d[400:].max():.4f} (ensemble {env_max:.4f}); rms after {rms:.4f} (ensemble {env_rms:.4f}); "
+          f"finals {finals.min():.4f}..{finals.max():.4f}; "
           f"out {out[349]} / {out[-1]} vs {g['outcount'][348]} / {g['outcount'][698]}")
     assert d[:400].max() <= 3 * float(g["weight"]) + 1e-12
-    assert d[400:].max() <= 2 * self_spread[400:].max()
-    assert np.sqrt(np.mean(d[400:] ** 2)) <= 2 * np.sqrt(np.mean(self_spread[400:] ** 2))
+    assert d[400:].max() <= 1.75 * env_max
+    assert rms <= 1.75 * env_rms
+    assert finals.min() - 0.01 <= q[-1] <= finals.max() + 0.01
     for s in (349, 699):
-        assert abs(out[s] - g["outcount"][s - 1]) <= 0.01 * g["outcount"][s - 1]
+        near = g["outcount"][max(s - 3, 0):min(s + 2, len(g["outcount"]))]
+        assert 0.99 * near.min() <= out[s] <= 1.01 * near.max(), (s, out[s], near)
     assert np.allclose(r["x_ion"], g["x_ion"], rtol=0, atol=1e-3)

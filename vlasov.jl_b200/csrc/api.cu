@@ -135,12 +135,10 @@ void setup_level(Level& D, const vlb_level_desc& L, bool coarse) {
   const size_t tot = (size_t)n * n * n;
   D.rho = dalloc<float>(tot);
   D.phi = dalloc<float>(tot);
-  // csol is padded by 16 floats: the gather's bulk copies of stencil rows
-  // start on 16-byte boundaries and read up to 15 floats past a row's end
-  D.csol = dalloc<float>(tot + 16);
+  D.csol = dalloc<float>(tot);
   VLB_CUDA(cudaMemset(D.rho, 0, tot * sizeof(float)));
   VLB_CUDA(cudaMemset(D.phi, 0, tot * sizeof(float)));
-  VLB_CUDA(cudaMemset(D.csol, 0, (tot + 16) * sizeof(float)));
+  VLB_CUDA(cudaMemset(D.csol, 0, tot * sizeof(float)));
   D.csol_hartree = dalloc<float>(tot);
   VLB_CUDA(cudaMemset(D.csol_hartree, 0, tot * sizeof(float)));
 }
@@ -163,11 +161,12 @@ void destroy_ctx(Ctx* c) {
   }
   free_level(c->fine);
   free_level(c->coarse);
-  dfree(c->overlap); dfree(c->gradient); dfree(c->nodes);
+  dfree(c->overlap); dfree(c->gradient); dfree(c->ovgr); dfree(c->nodes);
   for (int b = 0; b < 2; ++b) {
     dfree(c->part[b].k); dfree(c->part[b].d); dfree(c->part[b].pk); dfree(c->part[b].pd);
   }
   dfree(c->force);
+  dfree(c->csol_rows);
   dfree(c->keys); dfree(c->keys_alt); dfree(c->skeys); dfree(c->perm); dfree(c->vals_alt);
   dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off);
   for (int p = 0; p < 2; ++p) { dfree(c->occ_buf[p]); dfree(c->bnd_buf[p]); dfree(c->cidx_buf[p]); }
@@ -344,6 +343,8 @@ bool same_params(const vlb_step_params& a, const vlb_step_params& b) {
 // the cloud from part[cur] to part[cur^1], so graph g starts from cur == g.
 void capture_graphs(Ctx& c, const vlb_step_params& p) {
   const int saved = c.cur;
+  // the step's result reports the sort that ran eagerly, not the captured one
+  const bool ran_near = c.last_sort_near;
   for (int g = 0; g < 2; ++g) {
     if (c.gexec[g]) {
       VLB_CUDA(cudaGraphExecDestroy(c.gexec[g]));
@@ -358,6 +359,7 @@ void capture_graphs(Ctx& c, const vlb_step_params& p) {
       cudaStreamEndCapture(c.stream, &graph);
       if (graph) cudaGraphDestroy(graph);
       c.cur = saved;
+      c.last_sort_near = ran_near;
       sync_sort_products(c);
       throw;
     }
@@ -366,6 +368,8 @@ void capture_graphs(Ctx& c, const vlb_step_params& p) {
     VLB_CUDA(cudaGraphDestroy(graph));
   }
   c.cur = saved;
+  c.graph_sort_near = c.last_sort_near;
+  c.last_sort_near = ran_near;
   sync_sort_products(c);
   c.graph_params = p;
   c.graph_valid = true;
@@ -434,6 +438,17 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->ncol = S.nbdt + 1;
     c->overlap = upload_f(S.overlap, (size_t)c->ncol * 10);
     c->gradient = upload_f(S.gradient, (size_t)c->ncol * 10);
+    {
+      const std::vector<float> ov = to_float(S.overlap, (size_t)c->ncol * 10);
+      const std::vector<float> gr = to_float(S.gradient, (size_t)c->ncol * 10);
+      std::vector<float> both((size_t)c->ncol * 20);
+      for (size_t col = 0; col < (size_t)c->ncol; ++col)
+        for (int e = 0; e < 10; ++e) {
+          both[col * 20 + e] = ov[col * 10 + e];
+          both[col * 20 + 10 + e] = gr[col * 10 + e];
+        }
+      c->ovgr = upload(both.data(), both.size());
+    }
     c->nodes = upload_f(S.nodes, (size_t)c->ncol * 8);
     const size_t P = 3 * (size_t)c->Npad;
     for (int b = 0; b < 2; ++b) {
@@ -870,6 +885,7 @@ int vlb_step(vlb_ctx* ctx, vlb_projectile* proj, const vlb_step_params* params, 
       VLB_CUDA(cudaGraphLaunch(c.gexec[g], c.stream));
       c.launches += c.graph_launches;
       c.cur ^= 1;
+      c.last_sort_near = c.graph_sort_near;
       sync_sort_products(c);
     } else {
       const long long before = c.launches;
@@ -1099,7 +1115,11 @@ void destroy_batch_graphs(vlb_batch& b) {
 void capture_batch(vlb_batch& b, const vlb_step_params& p) {
   destroy_batch_graphs(b);
   std::vector<int> saved(b.ctx.size());
-  for (size_t i = 0; i < b.ctx.size(); ++i) saved[i] = b.ctx[i]->cur;
+  std::vector<char> ran_near(b.ctx.size());  // the results report the sorts that ran eagerly
+  for (size_t i = 0; i < b.ctx.size(); ++i) {
+    saved[i] = b.ctx[i]->cur;
+    ran_near[i] = b.ctx[i]->last_sort_near;
+  }
   b.cur0 = saved;
   for (int g = 0; g < 2; ++g) {
     for (size_t i = 0; i < b.ctx.size(); ++i) {
@@ -1115,6 +1135,7 @@ void capture_batch(vlb_batch& b, const vlb_step_params& p) {
       if (graph) cudaGraphDestroy(graph);
       for (size_t i = 0; i < b.ctx.size(); ++i) {
         b.ctx[i]->cur = saved[i];
+        b.ctx[i]->last_sort_near = ran_near[i];
         sync_sort_products(*b.ctx[i]);
       }
       throw;
@@ -1126,6 +1147,8 @@ void capture_batch(vlb_batch& b, const vlb_step_params& p) {
   }
   for (size_t i = 0; i < b.ctx.size(); ++i) {
     b.ctx[i]->cur = saved[i];
+    b.ctx[i]->graph_sort_near = b.ctx[i]->last_sort_near;
+    b.ctx[i]->last_sort_near = ran_near[i];
     sync_sort_products(*b.ctx[i]);
     b.ctx[i]->keys_ready = true;
   }
@@ -1227,6 +1250,7 @@ int vlb_batch_step(vlb_batch* b, vlb_projectile* projs, const vlb_step_params* p
       VLB_CUDA(cudaGraphLaunch(b->gexec[g], b->origin));
       for (Ctx* c : b->ctx) {
         c->cur ^= 1;
+        c->last_sort_near = c->graph_sort_near;
         sync_sort_products(*c);
         c->keys_ready = true;
         c->launches += c->graph_launches;

@@ -341,12 +341,13 @@ __global__ void __launch_bounds__(kGThreads) k_field(
 //
 // Pipeline, one iteration per item t: the loads go out first (delta of item
 // t+2, cell data of t+3 (used at the end of the iteration), item_cell of
-// t+4, the six tables of item t+1 and,
-// when its cell differs from the buffer's, its stencil); then the threads
-// wait for item t's MMAs (issued at the end of the previous iteration),
-// read D, finish item t with the tables loaded one iteration earlier, and
-// only then split item t+1's y tables and stencil into the other
-// shared-memory buffers and hand them to the MMA.  Items go round-robin to
+// t+4, the six tables of item t+1 as three 80-byte rows of the interleaved
+// overlap/gradient table and, when its cell differs from the staged one,
+// its stencil as one TMA tile copy); then the threads wait for item t's
+// MMAs (issued at the end of the previous iteration), read D, finish item t
+// with the tables loaded one iteration earlier, and only then split item
+// t+1's y tables and stencil into the operand buffers (single: their last
+// reader has completed) and hand them to the MMA.  Items go round-robin to
 // the CTAs (item = blockIdx.x + t gridDim.x).  The reaction sums of an item:
 // each warp's float butterfly, then the four warps in order, in float64.
 // Every wait is bounded.
@@ -355,8 +356,12 @@ constexpr int kFtRows = 128;                       // the MMA's M: particles per
 constexpr int kFtN = 112;                          // the MMA's N: 100 stencil columns, padded
 constexpr unsigned kFtA = 128u * 128u;             // one A operand: 128 rows x 32 TF32
 constexpr unsigned kFtB = (unsigned)kFtN * 128u;   // the B operand: 112 rows x 32 TF32
-constexpr unsigned kFtStage = 4u * kFtA + 2u * kFtB;  // the raw stencil tile: 100 rows of 16 floats
-constexpr unsigned kFtStageBytes = 100u * 64u;
+// One A operand per sum (Yo, Yg) and one B: item t+1's rows are written only
+// after item t's MMAs completed, so single buffers suffice and leave the SM's
+// L1 room for the interleaved tables.
+constexpr unsigned kFtStage = 2u * kFtA + kFtB;  // the raw stencil tile (1024-byte aligned)
+constexpr int kFtBoxX = 20;                        // floats per staged x row: 80 bytes, 16-byte multiple
+constexpr unsigned kFtStageBytes = 10u * 10u * kFtBoxX * 4u;
 constexpr unsigned kFtBars = kFtStage + kFtStageBytes;
 constexpr unsigned kFtSmem = kFtBars + 32u;        // + three mbarriers and the tensor-memory slot
 constexpr unsigned kFtCols = 256;
@@ -418,10 +423,22 @@ __device__ __forceinline__ FtItem ft_derive(const FtRaw& r, int chunk, int n, in
   return it;
 }
 
-__device__ __forceinline__ void ft_load_pairs(const float* __restrict__ tab, int col, float2 (&v)[5]) {
-  const float2* p = reinterpret_cast<const float2*>(tab + (size_t)(col - 1) * 10);
-#pragma unroll
-  for (int a = 0; a < 5; ++a) v[a] = __ldg(p + a);
+// A column's overlap and gradient rows as neighbour pairs, from the
+// interleaved table (80-byte rows: five 16-byte loads).
+__device__ __forceinline__ void ft_load_cols(const float4* __restrict__ ovgr, int col, float2 (&o)[5],
+                                             float2 (&g)[5]) {
+  const float4* p = ovgr + (size_t)(col - 1) * 5;
+  const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), e = __ldg(p + 3), f = __ldg(p + 4);
+  o[0] = make_float2(a.x, a.y);
+  o[1] = make_float2(a.z, a.w);
+  o[2] = make_float2(b.x, b.y);
+  o[3] = make_float2(b.z, b.w);
+  o[4] = make_float2(c.x, c.y);
+  g[0] = make_float2(c.z, c.w);
+  g[1] = make_float2(e.x, e.y);
+  g[2] = make_float2(e.z, e.w);
+  g[3] = make_float2(f.x, f.y);
+  g[4] = make_float2(f.z, f.w);
 }
 
 // Row r of an A operand from the ten values v: [hi | lo | hi | 0 0].
@@ -445,39 +462,30 @@ __device__ __forceinline__ void ft_store_a(unsigned char* A, int r, const float2
   *at(7) = make_float4(hi[8], hi[9], 0.f, 0.f);
 }
 
-// The cell's 10^3 stencil of csol staged by the TMA unit: row r = 10 kk + jj
-// (z plane kk, y row jj) is one 64-byte bulk copy of the 16 floats from the
-// row's first x index rounded down to a 16-byte boundary (csol is padded by
-// 16 floats past its end, so that the last rows' copies stay inside it);
-// the 100 copies complete on the stencil's mbarrier (6,400 bytes).  Thread
-// t < 100 issues row t; thread 0 arms the barrier.
-__device__ __forceinline__ size_t ft_row_index(const FtItem& it, int r, int n) {
-  const int kk = r / 10, jj = r - 10 * kk;
-  return (size_t)(2 * it.kx - 6) + (size_t)n * ((size_t)(2 * it.ky - 6 + jj) + (size_t)n * (size_t)(2 * it.kz - 6 + kk));
-}
-
-__device__ __forceinline__ void ft_stage_b(const FtItem& it, int t, const float* __restrict__ csol, int n,
-                                           unsigned char* raw, unsigned bar) {
-  if (t == 0) mbar_expect_tx(bar, kFtStageBytes);
-  if (t < 100) {
-    const size_t a0 = ft_row_index(it, t, n) & ~(size_t)3;
-    bulk_g2s(smem_u32(raw + 64u * t), csol + a0, 64u, bar);
+// The cell's 10^3 stencil of the fine coefficients staged by the TMA unit:
+// one box of 20 x 10 x 10 floats of the row-padded copy (pitch a multiple of
+// four floats), x from the stencil's first index rounded down to a multiple
+// of four (16 bytes: the box's x coordinate must be), y and z from the
+// stencil's first rows, into a dense [z][y][x] tile, completing on the
+// stencil's mbarrier (8,000 bytes).  Thread 0 arms the barrier and issues it.
+// The 20-float rows put the tile's z planes 200 words apart, eight banks, so
+// a warp's reads of one y row conflict at most two ways.
+__device__ __forceinline__ void ft_stage_b(const FtItem& it, int t, const CUtensorMap* map, unsigned char* raw,
+                                           unsigned bar) {
+  if (t == 0) {
+    mbar_expect_tx(bar, kFtStageBytes);
+    tma_load_3d(smem_u32(raw), map, (2 * it.kx - 6) & ~3, 2 * it.ky - 6, 2 * it.kz - 6, bar);
   }
 }
 
 // Row t < 100 (t = 10 kk + ii) of a cell's stencil from the staged tile:
-// c[jj] = csol at (ii, jj, kk) of the stencil = raw row (kk, jj) at its
-// alignment offset plus ii.
-__device__ __forceinline__ void ft_read_b(const FtItem& it, int t, int n, const unsigned char* raw,
-                                          float (&c)[10]) {
+// c[jj] = coefficient (ii, jj, kk) of the stencil, at x offset
+// ((2 kx - 6) & 3) + ii of the tile's row (kk, jj).
+__device__ __forceinline__ void ft_read_b(const FtItem& it, int t, const unsigned char* raw, float (&c)[10]) {
   const int kk = t / 10, ii = t - 10 * kk;
-  const float* rf = reinterpret_cast<const float*>(raw);
+  const float* rf = reinterpret_cast<const float*>(raw) + kFtBoxX * 10 * kk + ((2 * it.kx - 6) & 3) + ii;
 #pragma unroll
-  for (int jj = 0; jj < 10; ++jj) {
-    const int r = 10 * kk + jj;
-    const int off = (int)(ft_row_index(it, r, n) & 3);
-    c[jj] = rf[16 * r + off + ii];
-  }
+  for (int jj = 0; jj < 10; ++jj) c[jj] = rf[kFtBoxX * jj];
 }
 
 // That row of the B operand: [hi | hi | lo | 0 0].  Rows 100..111 are never
@@ -545,8 +553,8 @@ __device__ __forceinline__ void ft_finish(unsigned lane_base, const FtPart& p, f
 __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
     const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int64_t Npad,
-    const float* __restrict__ d, const float* __restrict__ csol, int n, int nk, const float* __restrict__ ov,
-    const float* __restrict__ gr, int nbdt, int ncol, float spacing, float x0, float h, double w,
+    const float* __restrict__ d, const __grid_constant__ CUtensorMap csol_map, int n, int nk,
+    const float4* __restrict__ ovgr, int nbdt, int ncol, float spacing, float x0, float h, double w,
     float* __restrict__ force, int chunk, double* __restrict__ red_items) {
   extern __shared__ __align__(1024) unsigned char ftsm[];
   __shared__ double red[2][4][4];
@@ -607,28 +615,24 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     const int cx = table_column(p.dx, spacing, nbdt, ncol);
     const int cy = table_column(p.dy, spacing, nbdt, ncol);
     const int cz = table_column(p.dz, spacing, nbdt, ncol);
-    ft_load_pairs(ov, cy, p.oy);
-    ft_load_pairs(gr, cy, p.gy);
-    ft_load_pairs(ov, cx, p.ox);
-    ft_load_pairs(gr, cx, p.gx);
-    ft_load_pairs(ov, cz, p.oz);
-    ft_load_pairs(gr, cz, p.gz);
+    ft_load_cols(ovgr, cy, p.oy, p.gy);
+    ft_load_cols(ovgr, cx, p.ox, p.gx);
+    ft_load_cols(ovgr, cz, p.oz, p.gz);
   };
 
-  // the A rows of particle p into buffer buf: its y tables split into
-  // head and tail (Yo from the overlap table, Yg from the gradient table)
-  auto store_a = [&](int buf, const FtPart& p) {
+  // the A rows of particle p: its y tables split into head and tail (Yo
+  // from the overlap table, Yg from the gradient table)
+  auto store_a = [&](const FtPart& p) {
     if (p.valid) {
-      unsigned char* Ao = ftsm + (unsigned)(2 * buf) * kFtA;
-      ft_store_a(Ao, tid, p.oy);
-      ft_store_a(Ao + kFtA, tid, p.gy);
+      ft_store_a(ftsm, tid, p.oy);
+      ft_store_a(ftsm + kFtA, tid, p.gy);
     }
   };
 
   auto issue = [&](int buf) {
     fence_after();
-    const unsigned ao = sbase + (unsigned)(2 * buf) * kFtA, ag = ao + kFtA;
-    const unsigned bb = sbase + 4u * kFtA + (unsigned)buf * kFtB;
+    const unsigned ao = sbase, ag = ao + kFtA;
+    const unsigned bb = sbase + 2u * kFtA;
     // the K steps holding the small terms first
 #pragma unroll
     for (int q = 3; q >= 0; --q) {
@@ -653,7 +657,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   float dc[3] = {0.f, 0.f, 0.f}, dn[3] = {0.f, 0.f, 0.f};
   load_delta(cur, dc);
   load_delta(nxt, dn);
-  int staged0 = -1, staged1 = -1;  // cell code in each B buffer
+  int staged = -1;                 // cell code of the stencil in B
   unsigned phase = 0;              // bit b: parity of the next completion of bars[b]
   bool ok = true;                  // the same in every thread after each barrier
   unsigned pending = 0;            // bit b: a commit on bars[b] not yet seen complete
@@ -663,20 +667,20 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   FtPart pc;
   load_part(cur, dc, pc);
   if (cur.has) {
-    ft_stage_b(cur, tid, csol, n, raw, sbar);
+    ft_stage_b(cur, tid, &csol_map, raw, sbar);
     staging = true;
-    store_a(0, pc);
+    store_a(pc);
     ok = __all_sync(0xffffffffu, mbar_wait(sbar, sphase));
     if (ok) {
       staging = false;
       sphase ^= 1u;
       if (tid < 100) {
         float c[10];
-        ft_read_b(cur, tid, n, raw, c);
-        ft_store_b(ftsm + 4u * kFtA, tid, c);
+        ft_read_b(cur, tid, raw, c);
+        ft_store_b(ftsm + 2u * kFtA, tid, c);
       }
     }
-    staged0 = cur.code;
+    staged = cur.code;
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   fence_before();
@@ -695,9 +699,9 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     g3 = cell_of(item_at(t + 4));
     FtPart pn;
     load_part(nxt, dn, pn);
-    const bool restage = nxt.has && ok && (nb ? staged1 : staged0) != nxt.code;
+    const bool restage = nxt.has && ok && staged != nxt.code;
     if (restage) {
-      ft_stage_b(nxt, tid, csol, n, raw, sbar);  // the tile is free: read before the last barrier
+      ft_stage_b(nxt, tid, &csol_map, raw, sbar);  // the tile is free: read before the last barrier
       staging = true;
     }
 
@@ -747,27 +751,24 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
       red[b][warp][3] = ae;
     }
 
-    // ---- item t+1's operands into the other buffers (their last reader,
-    // the MMAs of item t-1, completed in the previous iteration): the
-    // stencil, when it changed, and the particles' A rows
+    // ---- item t+1's operands (their last reader, the MMAs of item t, has
+    // completed: this warp saw it, or the item had none, or no MMA is issued
+    // any more): the stencil, when it changed, and the particles' A rows
     if (restage) {
       const bool sok = __all_sync(0xffffffffu, mbar_wait(sbar, sphase));
-      ok = ok && sok;
       if (sok) {
         staging = false;
         sphase ^= 1u;
-        if (tid < 100) {
+        if (ok && tid < 100) {
           float cb[10];
-          ft_read_b(nxt, tid, n, raw, cb);
-          ft_store_b(ftsm + 4u * kFtA + (unsigned)nb * kFtB, tid, cb);
+          ft_read_b(nxt, tid, raw, cb);
+          ft_store_b(ftsm + 2u * kFtA, tid, cb);
         }
       }
-      if (nb)
-        staged1 = nxt.code;
-      else
-        staged0 = nxt.code;
+      ok = ok && sok;
+      staged = nxt.code;
     }
-    store_a(nb, pn);
+    if (ok) store_a(pn);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     fence_before();
     ok = __syncthreads_and(ok) != 0;  // after a wait that gave up, no more MMAs
@@ -797,6 +798,27 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   if (warp == 0) {
     fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kFtCols) : "memory");
+  }
+}
+
+// The fine coefficients into rows of `pitch` floats (n even or odd; pitch a
+// multiple of four, the padding zero): float2 pairs when n is even, so that
+// both sides' rows start on 8-byte boundaries.
+__global__ void k_pad_rows(const float* __restrict__ src, int n, float* __restrict__ dst, int pitch, int rows) {
+  const int per = pitch / 2;
+  const int64_t tot = (int64_t)rows * per;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = t / per;
+    const int x = 2 * (int)(t - r * per);
+    const float* s = src + r * n;
+    float2 v = make_float2(0.f, 0.f);
+    if ((n & 1) == 0) {
+      if (x < n) v = *reinterpret_cast<const float2*>(s + x);
+    } else {
+      if (x < n) v.x = s[x];
+      if (x + 1 < n) v.y = s[x + 1];
+    }
+    *reinterpret_cast<float2*>(dst + r * pitch + x) = v;
   }
 }
 
@@ -1088,9 +1110,35 @@ __global__ void __launch_bounds__(256) k_energy_total(const double* __restrict__
 
 }  // namespace
 
+// The row-padded copy of the fine coefficients and the tensor map over it:
+// dims (pitch, n, n) floats, x fastest; strides pitch * 4 and pitch * n * 4
+// bytes (multiples of 16); box 20 x 10 x 10; no swizzle, zero fill.
 void field_setup(Ctx& c) {
-  (void)c;
   VLB_CUDA(cudaFuncSetAttribute(k_field_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFtSmem));
+  // two CTAs of 55 KB need the 132 KB shared-memory split (58 % of 228 KB);
+  // the remaining 124 KB of the SM's L1 holds the 80 KB interleaved tables
+  VLB_CUDA(cudaFuncSetAttribute(k_field_tc, cudaFuncAttributePreferredSharedMemoryCarveout, 58));
+  const int n = c.fine.n;
+  c.csol_pitch = (n + 3) & ~3;
+  const size_t rows = (size_t)c.csol_pitch * n * n;
+  VLB_CUDA(cudaMalloc(&c.csol_rows, rows * sizeof(float)));
+  VLB_CUDA(cudaMemset(c.csol_rows, 0, rows * sizeof(float)));
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q{};
+  VLB_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q));
+  if (!fn || q != cudaDriverEntryPointSuccess) throw CudaError(cudaErrorNotSupported, __FILE__, __LINE__);
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+  const cuuint64_t dims[3] = {(cuuint64_t)c.csol_pitch, (cuuint64_t)n, (cuuint64_t)n};
+  const cuuint64_t strides[2] = {(cuuint64_t)c.csol_pitch * 4, (cuuint64_t)c.csol_pitch * n * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)kFtBoxX, 10, 10};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = reinterpret_cast<Encode>(fn)(&c.csol_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, c.csol_rows, dims,
+                                                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw CudaError(cudaErrorInvalidValue, __FILE__, __LINE__);
 }
 
 void launch_forces(Ctx& c) {
@@ -1099,9 +1147,14 @@ void launch_forces(Ctx& c) {
   Particles& P = c.part[c.cur];
   if (c.profile) VLB_CUDA(cudaEventRecord(c.ev[kEvGatherBegin], c.stream));
   if (c.field_tc && c.chunk <= kFtRows) {
+    const int rows = F.n * F.n, per = c.csol_pitch / 2;
+    k_pad_rows<<<grid_for(c, (int64_t)rows * per, 256, 8), 256, 0, c.stream>>>(F.csol, F.n, c.csol_rows,
+                                                                               c.csol_pitch, rows);
+    VLB_LAUNCHED(c);
     k_field_tc<<<2 * c.num_sms, kFtThreads, kFtSmem, c.stream>>>(
-        c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.d, F.csol, F.n, F.nk, c.overlap,
-        c.gradient, c.nbdt, c.ncol, c.spacing_f, c.x0f, c.hf, c.weight, c.force, c.chunk, c.red_items);
+        c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.d, c.csol_map, F.n, F.nk,
+        reinterpret_cast<const float4*>(c.ovgr), c.nbdt, c.ncol, c.spacing_f, c.x0f, c.hf, c.weight, c.force,
+        c.chunk, c.red_items);
   } else {
     VLB_CUDA(cudaMemsetAsync(&c.dsc->work_gather, 0, sizeof(unsigned long long), c.stream));
     k_field<<<c.num_sms * c.field_cps, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.chunk_start, c.item_cell,

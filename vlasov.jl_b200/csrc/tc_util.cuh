@@ -43,6 +43,18 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
                : "memory");
 }
 
+// One box of a 3-D tiled tensor map (`map`: the address of a __grid_constant__
+// CUtensorMap parameter) at coordinates (x, y, z), x fastest, into shared
+// memory at dst, completing on bar.  x times the element size must be a
+// multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const void* map, int x, int y, int z, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(dst),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 

@@ -2,6 +2,7 @@
 // block, and the launch wrappers each kernel file exports.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is reached through the runtime)
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
@@ -128,6 +129,7 @@ struct Ctx {
   int nbdt = 0, ncol = 0;
   float* overlap = nullptr;   // [ncol][10]
   float* gradient = nullptr;  // [ncol][10]
+  float* ovgr = nullptr;      // [ncol][20]: each column's overlap row, then its gradient row (80-byte rows)
   float* nodes = nullptr;     // [ncol][8]
   // particle state, double buffered for the sort
   Particles part[2];
@@ -156,6 +158,7 @@ struct Ctx {
   int32_t* dir_base = nullptr;   // [min(ncell, N)][27] their first slot in the new order
   bool order_valid = false;      // part[cur] is in the order its sort products describe
   bool last_sort_near = false;   // the last sort tried the nearly sorted path
+  bool graph_sort_near = false;  // the captured step graphs' sorts try it
   int32_t* outlist = nullptr;    // [N]
   int32_t* chunk_start = nullptr;  // [ncell] first chunk of occupied cell g (current parity's)
   int32_t* item_cell = nullptr;    // [N / kMinChunk + ncell] occupied cell of each chunk (current parity's)
@@ -188,6 +191,13 @@ struct Ctx {
   // (every tile after the first takes the scan's fallback at once)
   int scan_wait_polls = 0;
   bool field_tc = true;  // the gather's y sums on the tensor cores (chunk <= 128)
+  // The fine spline coefficients with rows padded to a multiple of four
+  // floats (a pitch of 16-byte multiples), refreshed before each tensor-core
+  // gather, and the 3-D tiled tensor map over it from which the gather's
+  // stencil tiles are copied by the TMA unit.
+  float* csol_rows = nullptr;
+  int csol_pitch = 0;
+  CUtensorMap csol_map{};
   unsigned* tc_sync = nullptr;  // grid-barrier counter of the tensor-core chains
   // the learned denoiser of the fine density (vlb_set_denoiser)
   Denoiser* dn = nullptr;
