@@ -57,9 +57,12 @@ def test_cpu_path_mode_follows_the_reference_cpu_run(cuda_device):
     (tests/golden/capture_host_1e5.npz, tests/golden/make_capture_host.py).
 
     q(<8) is a count, one pseudo-particle carrying 0.00196 e here.  To step
-    400 the GPU stays within three pseudo-particles (0.0059 e); the CPU path
-    itself with its state rounded to the packed float32 form after every
-    step, as a device holds it, departs by two (0.0039 e).
+    400 the CPU path itself with its state rounded to the packed float32
+    form after every step, as a device holds it, departs from the base run
+    by two pseudo-particles (0.0039 e); the GPU step, which also computes
+    every force in float32, is held to twice the ensemble's largest
+    departure there (four pseudo-particles, 0.0078 e; builds measured two
+    and three).
 
     The crossing is chaotic once the ion has passed the cluster's centre.
     Eight CPU-path runs perturbed by float32 rounding (the packed start, the
@@ -99,7 +102,7 @@ def test_cpu_path_mode_follows_the_reference_cpu_run(cuda_device):
           f"{d[400:].max():.4f} (ensemble {env_max:.4f}); rms after {rms:.4f} (ensemble {env_rms:.4f}); "
           f"finals {finals.min():.4f}..{finals.max():.4f}; "
           f"out {out[349]} / {out[-1]} vs {g['outcount'][348]} / {g['outcount'][698]}")
-    assert d[:400].max() <= 3 * float(g["weight"]) + 1e-12
+    assert d[:400].max() <= 2 * dm[:, :400].max() + 1e-12
     assert d[400:].max() <= 1.75 * env_max
     assert rms <= 1.75 * env_rms
     assert finals.min() - 0.01 <= q[-1] <= finals.max() + 0.01

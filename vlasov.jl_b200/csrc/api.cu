@@ -278,7 +278,7 @@ void reset_step_scalars(Ctx& c) {
 void enqueue_phase_deposit(Ctx& c, const vlb_step_params& p, int64_t normalize_npart) {
   reset_step_scalars(c);
   stage_mark(c, 0);
-  launch_sort(c);
+  launch_sort(c, p.push != 0);
   stage_mark(c, 1);
   launch_deposit_fine_raw(c, p.deposit_mode);
   if (normalize_npart > 0) {
@@ -561,6 +561,7 @@ int vlb_upload_particles(vlb_ctx* ctx, const int32_t* knode, const float* delta,
       VLB_CUDA(cudaMemcpyAsync(P.pd + a * c.Npad, pdelta + a * n, n * 4, cudaMemcpyHostToDevice, c.stream));
     }
     VLB_CUDA(cudaStreamSynchronize(c.stream));
+    c.prev_deferred = false;  // every slot's previous position was just written
     c.sorted = false;
     c.items_valid = false;
     c.keys_ready = false;
@@ -572,6 +573,7 @@ int vlb_upload_particles(vlb_ctx* ctx, const int32_t* knode, const float* delta,
 int vlb_download_particles(vlb_ctx* ctx, int32_t* knode, float* delta, int32_t* pknode, float* pdelta) {
   CTX_OR_FAIL;
   return guarded([&]() -> int {
+    if (pknode || pdelta) settle_prev(c);
     Particles& P = c.part[c.cur];
     const size_t n = (size_t)c.N;
     for (int a = 0; a < 3; ++a) {
@@ -595,6 +597,7 @@ int vlb_upload_particles_range(vlb_ctx* ctx, int64_t first, int64_t count, const
   if (first < 0 || count < 0 || first > c.N || count > c.N - first)
     return fail(VLB_ERR_ARG, "vlb_upload_particles_range: slots out of the cloud");
   return guarded([&]() -> int {
+    settle_prev(c);  // the slots outside the range keep their previous positions
     Particles& P = c.part[c.cur];
     const size_t n = (size_t)count, bytes = n * 4;
     if (n) {
@@ -621,6 +624,7 @@ int vlb_download_particles_range(vlb_ctx* ctx, int64_t first, int64_t count, int
   if (first < 0 || count < 0 || first > c.N || count > c.N - first)
     return fail(VLB_ERR_ARG, "vlb_download_particles_range: slots out of the cloud");
   return guarded([&]() -> int {
+    if (pknode || pdelta) settle_prev(c);
     Particles& P = c.part[c.cur];
     const size_t n = (size_t)count, bytes = n * 4;
     if (n) {
@@ -657,7 +661,7 @@ int vlb_sort(vlb_ctx* ctx, int32_t* noccupied, int32_t* outcount) {
   CTX_OR_FAIL;
   return guarded([&]() -> int {
     reset_step_scalars(c);
-    launch_sort(c);
+    launch_sort(c, false);
     fetch_scalars(c);
     if (noccupied) *noccupied = c.hsc->noccupied;
     if (outcount) *outcount = c.hsc->outcount;

@@ -28,154 +28,158 @@ int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
 namespace {
 
 constexpr int kDepThreads = 256;
-constexpr int kDepWarps = kDepThreads / 32;
-constexpr int kDepClaim = 2;       // cells a warp claims per counter update
-constexpr int kDepRow = 36;        // floats per lane row of the warp's partial slab: 32 + 4 against bank conflicts
+constexpr int kDepLanes = 32;      // particle lanes per CTA, 8 threads (one z row each) per lane
+constexpr int kDepStage = 512;     // particles whose columns are staged at once (two per thread)
+constexpr int kDepRow = 68;        // floats per (lane, z row) in the reduction buffer: 64 + 4 against bank conflicts
 constexpr double kFixedScale = 1099511627776.0;        // 2^40
 constexpr double kFixedInv = 1.0 / 1099511627776.0;
 
-// One warp per occupied cell at a time, kDepClaim consecutive cells per
-// claim of a dynamic counter; no CTA barrier after the table load.  The
-// warp loads 32 particles' (k, delta) at once (the next 32 in flight while
-// the current ones are added), each lane computes its particle's three table
-// columns and the window test into the warp's column slab, and lane
-// (pl = lane / 16, hy = lane / 8 % 2, q = lane % 8) adds particles pl, pl + 2,
-// ... of the 32 into rows y = 4 hy .. 4 hy + 3 of the z plane q of its 8^3
-// sum: 32 float32 accumulators as float2 pairs along x, so one packed FMA
-// covers two outputs (and three CTAs of 256 threads fit an SM).  At the
-// cell's end every lane stores its 32 partials into its row of the warp's
-// slab and lane (pl, hy, q) sums rows y = 4 hy + 2 pl, 4 hy + 2 pl + 1 of the
-// plane q over the two particle lanes in a fixed order, then adds its 16
-// outputs to the grid.
-__global__ void __launch_bounds__(kDepThreads, 3) k_deposit_fine(
+// One CTA per occupied cell at a time (dynamic counter); a cell of the
+// headline cloud holds about a thousand particles.  The cell's particles go
+// in stages of 512: each thread computes the three table columns and the
+// window test of two particles into one int4 each of a double-buffered stage
+// in shared memory while the CTA adds the previous stage, and the k/delta
+// loads of the stage after are in flight meanwhile; one CTA barrier per
+// stage.  Thread (lane, q) owns the z row q of its lane's 8^3 sum: 64 float32
+// accumulators as float2 pairs along x, so one packed FMA covers two outputs.
+// At the cell's end the lane partials are summed over the lanes in a fixed
+// order (in shared memory that the stages used) and added to the grid.
+__global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
     const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds, DeviceScalars* dsc,
     int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ nodes,
     int nk, int n, float x0, float h, float lo, float hi, float spacing, int nbdt, int ncol, float* rho,
     unsigned long long* rho_fixed, int mode) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float* red_all = reinterpret_cast<float*>(smem);                              // [warps][32][kDepRow]
-  int* cols_all = reinterpret_cast<int*>(red_all + kDepWarps * 32 * kDepRow);   // [warps][3][32]
-  float* nodes_s = reinterpret_cast<float*>(cols_all + kDepWarps * 96);         // [ncol][8]
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float* nodes_s = reinterpret_cast<float*>(smem);                      // [ncol][8]
+  unsigned char* work = smem + (((size_t)ncol * 8 * sizeof(float) + 15) & ~(size_t)15);
+  int4* cols_s = reinterpret_cast<int4*>(work);                         // [2][kDepStage]
+  float* red_s = reinterpret_cast<float*>(work);                        // [kDepLanes][8][kDepRow], after the stages
+  __shared__ int s_g;
+  __shared__ int s_nout;
+  const int tid = threadIdx.x;
   for (int e = tid; e < ncol * 8; e += kDepThreads) nodes_s[e] = nodes[e];
-  __syncthreads();
-  float* red_w = red_all + warp * 32 * kDepRow;
-  int* cols_w = cols_all + warp * 96;
+  if (tid == 0) s_nout = 0;
   const int nocc = dsc->noccupied;
-  const int pl = lane >> 4, hy = (lane >> 3) & 1, q = lane & 7;
+  const int pl = tid / 8, q = tid % 8;
   int my_nout = 0;
+  __syncthreads();
+  // the columns of particle s (inside the cell) into the stage slot
+  auto stage_one = [&](int s, int sh, const int (&kk)[3], const float (&dd)[3], int4* slot) {
+    if (s >= sh) return;
+    bool inside = true;
+    int cc[3];
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      const float p = fadd(fadd(x0, fmul((float)(kk[ax] - 1), h)), dd[ax]);
+      inside = inside && (lo <= p) && (p <= hi);
+      cc[ax] = table_column(dd[ax], spacing, nbdt, ncol);
+    }
+    if (!inside) { cc[0] = cc[1] = cc[2] = 1; ++my_nout; }
+    *slot = make_int4(cc[0], cc[1], cc[2], 0);
+  };
+  auto load_one = [&](int s, int sh, int (&kk)[3], float (&dd)[3]) {
+    if (s >= sh) return;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      kk[ax] = k[ax * Npad + s];
+      dd[ax] = d[ax * Npad + s];
+    }
+  };
   for (;;) {
-    int g0 = 0;
-    if (lane == 0) g0 = (int)atomicAdd(&dsc->work_deposit, (unsigned long long)kDepClaim);
-    g0 = __shfl_sync(0xffffffffu, g0, 0);
-    if (g0 >= nocc) break;
-    const int g1 = min(g0 + kDepClaim, nocc);
-    for (int g = g0; g < g1; ++g) {
-      const int cell = occupied[g];
-      const int sl = bounds[g], sh = bounds[g + 1];
-      int kx, ky, kz;
-      cell_knots((uint32_t)cell, nk, kx, ky, kz);
-      const bool fits = deposit_fits(kx, ky, kz, n);
-      float2 acc[16];
+    if (tid == 0) s_g = (int)atomicAdd(&dsc->work_deposit, 1ull);
+    __syncthreads();
+    const int g = s_g;
+    if (g >= nocc) break;
+    const int cell = occupied[g];
+    const int sl = bounds[g], sh = bounds[g + 1];
+    int kx, ky, kz;
+    cell_knots((uint32_t)cell, nk, kx, ky, kz);
+    const bool fits = deposit_fits(kx, ky, kz, n);
+    float2 acc[32];
 #pragma unroll
-      for (int a = 0; a < 16; ++a) acc[a] = make_float2(0.f, 0.f);
-      int kk[3] = {0, 0, 0};
-      float dd[3] = {0.f, 0.f, 0.f};
-      if (sl + lane < sh) {
-#pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
-          kk[ax] = k[ax * Npad + sl + lane];
-          dd[ax] = d[ax * Npad + sl + lane];
-        }
-      }
-      for (int base = sl; base < sh; base += 32) {
-        if (base + lane < sh) {
-          bool inside = true;
-          int cc[3];
-#pragma unroll
-          for (int ax = 0; ax < 3; ++ax) {
-            const float p = fadd(fadd(x0, fmul((float)(kk[ax] - 1), h)), dd[ax]);
-            inside = inside && (lo <= p) && (p <= hi);
-            cc[ax] = table_column(dd[ax], spacing, nbdt, ncol);
-          }
-          if (!inside) { cc[0] = cc[1] = cc[2] = 1; ++my_nout; }
-          cols_w[lane] = cc[0];
-          cols_w[32 + lane] = cc[1];
-          cols_w[64 + lane] = cc[2];
-        }
-        __syncwarp();
-        const int nb = base + 32;
-        if (nb + lane < sh) {
-#pragma unroll
-          for (int ax = 0; ax < 3; ++ax) {
-            kk[ax] = k[ax * Npad + nb + lane];
-            dd[ax] = d[ax * Npad + nb + lane];
-          }
-        }
-        if (fits) {
-          const int cnt = min(32, sh - base);
-          for (int t = pl; t < cnt; t += 2) {
-            const float* vx = nodes_s + (size_t)(cols_w[t] - 1) * 8;
-            const float4 ya = *reinterpret_cast<const float4*>(nodes_s + (size_t)(cols_w[32 + t] - 1) * 8 + 4 * hy);
-            const float z = nodes_s[(size_t)(cols_w[64 + t] - 1) * 8 + q];
-            const float4 xa = *reinterpret_cast<const float4*>(vx);
-            const float4 xb = *reinterpret_cast<const float4*>(vx + 4);
-            const float2 x2[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w), make_float2(xb.x, xb.y),
-                                  make_float2(xb.z, xb.w)};
-            const float y[4] = {ya.x, ya.y, ya.z, ya.w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const float w = y[j] * z;
-              const float2 w2 = make_float2(w, w);
-#pragma unroll
-              for (int a = 0; a < 4; ++a) acc[4 * j + a] = __ffma2_rn(x2[a], w2, acc[4 * j + a]);
-            }
-          }
-        }
-        __syncwarp();
+    for (int a = 0; a < 32; ++a) acc[a] = make_float2(0.f, 0.f);
+    int ka[3] = {0, 0, 0}, kb[3] = {0, 0, 0};
+    float da[3] = {0.f, 0.f, 0.f}, db[3] = {0.f, 0.f, 0.f};
+    // stage 0, then the loads of stage 1 in flight
+    load_one(sl + tid, sh, ka, da);
+    load_one(sl + kDepThreads + tid, sh, kb, db);
+    stage_one(sl + tid, sh, ka, da, &cols_s[tid]);
+    stage_one(sl + kDepThreads + tid, sh, kb, db, &cols_s[kDepThreads + tid]);
+    load_one(sl + kDepStage + tid, sh, ka, da);
+    load_one(sl + kDepStage + kDepThreads + tid, sh, kb, db);
+    __syncthreads();
+    int buf = 0;
+    for (int base = sl; base < sh; base += kDepStage) {
+      // the next stage into the other buffer (its last readers passed the
+      // barrier that ended the previous stage), and the loads of the one after
+      const int nb = base + kDepStage;
+      if (nb < sh) {
+        int4* nxt = cols_s + (buf ^ 1) * kDepStage;
+        stage_one(nb + tid, sh, ka, da, &nxt[tid]);
+        stage_one(nb + kDepThreads + tid, sh, kb, db, &nxt[kDepThreads + tid]);
+        load_one(nb + kDepStage + tid, sh, ka, da);
+        load_one(nb + kDepStage + kDepThreads + tid, sh, kb, db);
       }
       if (fits) {
-        // the lane's partials into its slab row: its y row j (of four) at floats 8 j .. 8 j + 7
-        float* row = red_w + lane * kDepRow;
+        const int4* cur = cols_s + buf * kDepStage;
+        const int cnt = min(kDepStage, sh - base);
+        for (int t = pl; t < cnt; t += kDepLanes) {
+          const int4 cc = cur[t];
+          const float* vx = nodes_s + (size_t)(cc.x - 1) * 8;
+          const float* vy = nodes_s + (size_t)(cc.y - 1) * 8;
+          const float z = nodes_s[(size_t)(cc.z - 1) * 8 + q];
+          const float4 xa = *reinterpret_cast<const float4*>(vx);
+          const float4 xb = *reinterpret_cast<const float4*>(vx + 4);
+          const float4 ya = *reinterpret_cast<const float4*>(vy);
+          const float4 yb = *reinterpret_cast<const float4*>(vy + 4);
+          const float2 x2[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w), make_float2(xb.x, xb.y),
+                                make_float2(xb.z, xb.w)};
+          const float y[8] = {ya.x, ya.y, ya.z, ya.w, yb.x, yb.y, yb.z, yb.w};
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          *reinterpret_cast<float4*>(row + 8 * j) = make_float4(acc[4 * j].x, acc[4 * j].y, acc[4 * j + 1].x,
-                                                                acc[4 * j + 1].y);
-          *reinterpret_cast<float4*>(row + 8 * j + 4) = make_float4(acc[4 * j + 2].x, acc[4 * j + 2].y,
-                                                                    acc[4 * j + 3].x, acc[4 * j + 3].y);
-        }
-        __syncwarp();
-        // rows y = 4 hy + 2 pl, + 1 of plane q over the particle lanes 0, 1 (slab rows 8 hy + q, 16 + 8 hy + q)
-        float v[16];
-        const float* src = red_w + (8 * hy + q) * kDepRow + 16 * pl;
+          for (int j = 0; j < 8; ++j) {
+            const float w = y[j] * z;
+            const float2 w2 = make_float2(w, w);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const float4 r0 = *reinterpret_cast<const float4*>(src + 4 * m);
-          const float4 r1 = *reinterpret_cast<const float4*>(src + 16 * kDepRow + 4 * m);
-          v[4 * m + 0] = r0.x + r1.x;
-          v[4 * m + 1] = r0.y + r1.y;
-          v[4 * m + 2] = r0.z + r1.z;
-          v[4 * m + 3] = r0.w + r1.w;
-        }
-        __syncwarp();  // the slab is free for the next cell
-        const int bx = 2 * kx - 5, by = 2 * ky - 5 + 4 * hy + 2 * pl, bz = 2 * kz - 5;
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-          const int jj = e >> 3, a = e & 7;
-          const size_t addr = (size_t)(bx + a) + (size_t)n * ((by + jj) + (size_t)n * (bz + q));
-          if (mode == VLB_DEPOSIT_FIXED64) {
-            const long long iv = llrint((double)v[e] * kFixedScale);
-            if (iv) atomicAdd(&rho_fixed[addr], (unsigned long long)iv);
-          } else if (v[e] != 0.f) {
-            atomicAdd(&rho[addr], v[e]);
+            for (int a = 0; a < 4; ++a) acc[4 * j + a] = __ffma2_rn(x2[a], w2, acc[4 * j + a]);
           }
+        }
+      }
+      __syncthreads();
+      buf ^= 1;
+    }
+    if (fits) {
+      // lane partials -> shared (the stages' memory), then a fixed-order
+      // sum over the lanes that received particles
+      float* row = red_s + (size_t)(pl * 8 + q) * kDepRow;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        *reinterpret_cast<float4*>(row + 8 * j) = make_float4(acc[4 * j].x, acc[4 * j].y, acc[4 * j + 1].x,
+                                                              acc[4 * j + 1].y);
+        *reinterpret_cast<float4*>(row + 8 * j + 4) = make_float4(acc[4 * j + 2].x, acc[4 * j + 2].y,
+                                                                  acc[4 * j + 3].x, acc[4 * j + 3].y);
+      }
+      __syncthreads();
+      const int nl = min(kDepLanes, sh - sl);
+      const int bx = 2 * kx - 5, by = 2 * ky - 5, bz = 2 * kz - 5;
+      for (int o = tid; o < 512; o += kDepThreads) {
+        const int a = o & 7, jj = (o >> 3) & 7, kq = o >> 6;
+        const float* src = red_s + (size_t)kq * kDepRow + 8 * jj + a;
+        float v = 0.f;
+        for (int l = 0; l < nl; ++l) v += src[(size_t)l * 8 * kDepRow];
+        const size_t addr = (size_t)(bx + a) + (size_t)n * ((by + jj) + (size_t)n * (bz + kq));
+        if (mode == VLB_DEPOSIT_FIXED64) {
+          const long long iv = llrint((double)v * kFixedScale);
+          if (iv) atomicAdd(&rho_fixed[addr], (unsigned long long)iv);
+        } else if (v != 0.f) {
+          atomicAdd(&rho[addr], v);
         }
       }
     }
+    __syncthreads();
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) my_nout += __shfl_xor_sync(0xffffffffu, my_nout, o);
-  if (lane == 0 && my_nout) atomicAdd(&dsc->nout, my_nout);
+  atomicAdd(&s_nout, my_nout);
+  __syncthreads();
+  if (tid == 0 && s_nout) atomicAdd(&dsc->nout, s_nout);
 }
 
 // Per (j,k) column: sum_i rho[i,j,k] m0[i], times m0[j] m0[k].  One warp
@@ -497,8 +501,9 @@ __global__ void __launch_bounds__(kCicThreads, 3) k_deposit_cic(
 }  // namespace
 
 size_t deposit_fine_smem(const Ctx& c) {
-  return (size_t)kDepWarps * 32 * kDepRow * sizeof(float) + (size_t)kDepWarps * 96 * sizeof(int) +
-         (size_t)c.ncol * 8 * sizeof(float);
+  const size_t stages = (size_t)2 * kDepStage * sizeof(int4);
+  const size_t red = (size_t)kDepLanes * 8 * kDepRow * sizeof(float);
+  return (((size_t)c.ncol * 8 * sizeof(float) + 15) & ~(size_t)15) + (stages > red ? stages : red);
 }
 
 size_t cic_smem(const Ctx& c);
@@ -526,7 +531,7 @@ void launch_deposit_fine_raw(Ctx& c, int mode) {
     VLB_CUDA(cudaMemsetAsync(F.rho, 0, tot * sizeof(float), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_deposit, 0, sizeof(unsigned long long), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->nout, 0, sizeof(int32_t), c.stream));
-  const int grid = c.num_sms * 3;
+  const int grid = c.num_sms * 2;
   k_deposit_fine<<<grid, kDepThreads, deposit_fine_smem(c), c.stream>>>(
       c.occupied, c.bounds, c.dsc, c.Npad, P.k, P.d, c.nodes, F.nk, F.n, c.x0f, c.hf, c.lo_f, c.hi_f, c.spacing_f,
       c.nbdt, c.ncol, F.rho, c.rho_fixed, mode);

@@ -99,6 +99,12 @@ __device__ __forceinline__ void proj_term(const ProjF& P, int kx, int ky, int kz
   if (P.ball) {
     mm = P.coef * ball_force_kernel(d2, P.R);
     e = r < P.R ? -(3.f - (r / P.R) * (r / P.R)) / (2.f * P.R) : -1.f / r;
+  } else if (d2 >= 40.5f * (P.sigma * P.sigma)) {
+    // x = r / (sqrt(2) sigma) >= 4.5: 1 - erf(x) < 2e-10 and (2 / sqrt(pi)) x exp(-x^2) < 9e-9, both
+    // below half an ulp of 1 (2^-25), so the kernel's numerator and erf(x) round to 1: the far field
+    // 1 / r^3 and the energy share 1 / r, as the full expressions give them
+    mm = P.coef * (1.f / (d2 * r));
+    e = 1.f / r;
   } else {
     mm = P.coef * gaussian_force_kernel(d2, P.sigma);
     e = r < 1.0e-4f * P.sigma ? 0.7978845608f / P.sigma : erff(r / 1.4142135624f / P.sigma) / r;

@@ -32,15 +32,21 @@ __device__ __forceinline__ void verlet1(int kq, float dq, int ok, float od, floa
 }
 
 // Four consecutive particles per thread, 16-byte loads and stores of every
-// component array (Npad is a multiple of 64).  When `r2cap` > 0 the same pass
+// component array (Npad is a multiple of 64).  With kGathered the previous
+// positions are read from (pk_src, pd_src) at perm[slot] -- where the step's
+// sort left them -- and written in slot order like the rest; otherwise they
+// are read in place.  When `r2cap` > 0 the same pass
 // counts the particles within sqrt(r2cap) of the projectile after the step
 // (enclosed_charge, float64 positions), which the reference reads after
 // step! on the host.  When `keys` is set it also writes the cell key of
 // every new position and adds it to the cell histogram (zero on entry) --
 // the first stage of the next step's sort, done while the positions are in
 // registers.
+template <bool kGathered>
 __global__ void __launch_bounds__(256) k_push(int64_t N, int64_t Npad, int32_t* __restrict__ k, float* __restrict__ d,
                                               int32_t* __restrict__ pk, float* __restrict__ pd,
+                                              const int32_t* __restrict__ pk_src, const float* __restrict__ pd_src,
+                                              const uint32_t* __restrict__ perm,
                                               const float* __restrict__ force, float a, float h, float x0, float pfac,
                                               float r2max, float inv2M, double* diag, double r2cap, double x0d,
                                               double hd, DeviceScalars* dsc, uint32_t* __restrict__ keys,
@@ -53,18 +59,37 @@ __global__ void __launch_bounds__(256) k_push(int64_t N, int64_t Npad, int32_t* 
     const int64_t i0 = 4 * qi;
     int kq[3][4], ko[3][4], kn[3][4];
     float dq[3][4], od[3][4], dn[3][4], gap[3][4], ff[3][4];
+    int64_t src[4] = {0, 0, 0, 0};
+    if (kGathered) {
+      if (i0 + 3 < N) {
+        const uint4 pv = *reinterpret_cast<const uint4*>(perm + i0);
+        src[0] = pv.x; src[1] = pv.y; src[2] = pv.z; src[3] = pv.w;
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) src[u] = i0 + u < N ? (int64_t)perm[i0 + u] : 0;
+      }
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int4 a4 = *reinterpret_cast<const int4*>(k + c * Npad + i0);
       const float4 b4 = *reinterpret_cast<const float4*>(d + c * Npad + i0);
-      const int4 c4 = *reinterpret_cast<const int4*>(pk + c * Npad + i0);
-      const float4 d4 = *reinterpret_cast<const float4*>(pd + c * Npad + i0);
       const float4 f4 = *reinterpret_cast<const float4*>(force + c * Npad + i0);
       kq[c][0] = a4.x; kq[c][1] = a4.y; kq[c][2] = a4.z; kq[c][3] = a4.w;
       dq[c][0] = b4.x; dq[c][1] = b4.y; dq[c][2] = b4.z; dq[c][3] = b4.w;
-      ko[c][0] = c4.x; ko[c][1] = c4.y; ko[c][2] = c4.z; ko[c][3] = c4.w;
-      od[c][0] = d4.x; od[c][1] = d4.y; od[c][2] = d4.z; od[c][3] = d4.w;
       ff[c][0] = f4.x; ff[c][1] = f4.y; ff[c][2] = f4.z; ff[c][3] = f4.w;
+      if (kGathered) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          // padding slots past N: any value (their result is not kept)
+          ko[c][u] = i0 + u < N ? __ldg(pk_src + c * Npad + src[u]) : kq[c][u];
+          od[c][u] = i0 + u < N ? __ldg(pd_src + c * Npad + src[u]) : dq[c][u];
+        }
+      } else {
+        const int4 c4 = *reinterpret_cast<const int4*>(pk + c * Npad + i0);
+        const float4 d4 = *reinterpret_cast<const float4*>(pd + c * Npad + i0);
+        ko[c][0] = c4.x; ko[c][1] = c4.y; ko[c][2] = c4.z; ko[c][3] = c4.w;
+        od[c][0] = d4.x; od[c][1] = d4.y; od[c][2] = d4.z; od[c][3] = d4.w;
+      }
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -312,12 +337,20 @@ void launch_push(Ctx& c, double dt, double rcmax, double capture_radius, bool ke
   const double M = c.weight;  // ELECTRON_MASS * weight
   if (capture_radius > 0) VLB_CUDA(cudaMemsetAsync(&c.dsc->enclosed, 0, sizeof(unsigned long long), c.stream));
   const int grid = grid_for(c, (c.N + 3) / 4, 256, c.push_cps);
-  k_push<<<grid, 256, 0, c.stream>>>(
-      c.N, c.Npad, P.k, P.d, P.pk, P.pd, c.force, (float)(dt * dt / M), c.hf, c.x0f, (float)(M / (2 * dt)),
-      (float)(rcmax * rcmax), (float)(1 / (2 * M)), c.diag_part,
-      capture_radius > 0 ? capture_radius * capture_radius : 0.0, c.x0, c.h, c.dsc, keys ? c.keys : nullptr,
-      c.counts, c.fine.nk);
+  const Particles& O = c.part[c.cur ^ 1];  // where a deferring sort left the previous positions
+  auto go = [&](auto kern) {
+    kern<<<grid, 256, 0, c.stream>>>(
+        c.N, c.Npad, P.k, P.d, P.pk, P.pd, O.pk, O.pd, c.perm, c.force, (float)(dt * dt / M), c.hf, c.x0f,
+        (float)(M / (2 * dt)), (float)(rcmax * rcmax), (float)(1 / (2 * M)), c.diag_part,
+        capture_radius > 0 ? capture_radius * capture_radius : 0.0, c.x0, c.h, c.dsc, keys ? c.keys : nullptr,
+        c.counts, c.fine.nk);
+  };
+  if (c.prev_deferred)
+    go(k_push<true>);
+  else
+    go(k_push<false>);
   VLB_LAUNCHED(c);
+  c.prev_deferred = false;
   k_diag_total<<<1, 256, 0, c.stream>>>(c.diag_part, grid, c.dsc->diag);
   VLB_LAUNCHED(c);
   c.keys_ready = keys;

@@ -659,12 +659,15 @@ __global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __re
 }
 
 // ------------------------------------------------------------- the move
-// Moves the records into slot order: dst[s] = src[perm[s]], all twelve
-// component arrays.  Four consecutive slots per thread: one 16-byte load of
-// their permutation entries, the 48 gathered loads all in flight, then one
-// 16-byte store per component array (Npad is a multiple of 64).  Reads
-// follow the permutation of a nearly sorted cloud, so they stay within a
-// few pages.
+// Moves the records into slot order: dst[s] = src[perm[s]], the position
+// arrays (k, delta) when kPos, the previous positions (pk, pdelta) when
+// kPrev.  Four consecutive slots per thread: one 16-byte load of their
+// permutation entries, the gathered loads all in flight, then one 16-byte
+// store per component array (Npad is a multiple of 64).  Reads follow the
+// permutation of a nearly sorted cloud, so they stay within a few pages.
+// A step whose push follows leaves (pk, pdelta) where they are: the push
+// reads them through the permutation and writes them in slot order.
+template <bool kPos, bool kPrev>
 __global__ void __launch_bounds__(256) k_gather_records(int64_t N, int64_t Npad, const uint32_t* __restrict__ perm,
                                                         const int32_t* __restrict__ k0, const float* __restrict__ d0,
                                                         const int32_t* __restrict__ pk0, const float* __restrict__ pd0,
@@ -681,17 +684,25 @@ __global__ void __launch_bounds__(256) k_gather_records(int64_t N, int64_t Npad,
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        kv[c][u] = __ldg(k0 + c * Npad + i[u]);
-        dv[c][u] = __ldg(d0 + c * Npad + i[u]);
-        pkv[c][u] = __ldg(pk0 + c * Npad + i[u]);
-        pdv[c][u] = __ldg(pd0 + c * Npad + i[u]);
+        if (kPos) {
+          kv[c][u] = __ldg(k0 + c * Npad + i[u]);
+          dv[c][u] = __ldg(d0 + c * Npad + i[u]);
+        }
+        if (kPrev) {
+          pkv[c][u] = __ldg(pk0 + c * Npad + i[u]);
+          pdv[c][u] = __ldg(pd0 + c * Npad + i[u]);
+        }
       }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      *reinterpret_cast<int4*>(k1 + c * Npad + s) = make_int4(kv[c][0], kv[c][1], kv[c][2], kv[c][3]);
-      *reinterpret_cast<float4*>(d1 + c * Npad + s) = make_float4(dv[c][0], dv[c][1], dv[c][2], dv[c][3]);
-      *reinterpret_cast<int4*>(pk1 + c * Npad + s) = make_int4(pkv[c][0], pkv[c][1], pkv[c][2], pkv[c][3]);
-      *reinterpret_cast<float4*>(pd1 + c * Npad + s) = make_float4(pdv[c][0], pdv[c][1], pdv[c][2], pdv[c][3]);
+      if (kPos) {
+        *reinterpret_cast<int4*>(k1 + c * Npad + s) = make_int4(kv[c][0], kv[c][1], kv[c][2], kv[c][3]);
+        *reinterpret_cast<float4*>(d1 + c * Npad + s) = make_float4(dv[c][0], dv[c][1], dv[c][2], dv[c][3]);
+      }
+      if (kPrev) {
+        *reinterpret_cast<int4*>(pk1 + c * Npad + s) = make_int4(pkv[c][0], pkv[c][1], pkv[c][2], pkv[c][3]);
+        *reinterpret_cast<float4*>(pd1 + c * Npad + s) = make_float4(pdv[c][0], pdv[c][1], pdv[c][2], pdv[c][3]);
+      }
     }
   }
   // the last N mod 4 slots
@@ -700,10 +711,14 @@ __global__ void __launch_bounds__(256) k_gather_records(int64_t N, int64_t Npad,
     const int64_t i = perm[s];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      k1[c * Npad + s] = k0[c * Npad + i];
-      d1[c * Npad + s] = d0[c * Npad + i];
-      pk1[c * Npad + s] = pk0[c * Npad + i];
-      pd1[c * Npad + s] = pd0[c * Npad + i];
+      if (kPos) {
+        k1[c * Npad + s] = k0[c * Npad + i];
+        d1[c * Npad + s] = d0[c * Npad + i];
+      }
+      if (kPrev) {
+        pk1[c * Npad + s] = pk0[c * Npad + i];
+        pd1[c * Npad + s] = pd0[c * Npad + i];
+      }
     }
   }
 }
@@ -716,7 +731,20 @@ int grid_for(const Ctx& c, int64_t n, int threads, int per_sm) {
   return (int)std::max<int64_t>(1, std::min(want, cap));
 }
 
-void launch_sort(Ctx& c) {
+// The previous positions of a sort that deferred their move, into slot
+// order (before anything else reads them).
+void settle_prev(Ctx& c) {
+  if (!c.prev_deferred) return;
+  const Particles& P = c.part[c.cur ^ 1];
+  const Particles& Q = c.part[c.cur];
+  k_gather_records<false, true><<<grid_for(c, (c.N + 3) / 4, 256, c.move_cps), 256, 0, c.stream>>>(
+      c.N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d, Q.pk, Q.pd);
+  VLB_LAUNCHED(c);
+  c.prev_deferred = false;
+}
+
+void launch_sort(Ctx& c, bool defer_prev) {
+  settle_prev(c);
   const int64_t N = c.N;
   const int nk = c.fine.nk, n = c.fine.n;
   Particles& P = c.part[c.cur];
@@ -794,9 +822,15 @@ void launch_sort(Ctx& c) {
     vin = vout;
     shift += b;
   }
-  k_gather_records<<<grid_for(c, (N + 3) / 4, 256, c.move_cps), 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
-                                                                   Q.pk, Q.pd);
+  const int mgrid = grid_for(c, (N + 3) / 4, 256, c.move_cps);
+  if (defer_prev)
+    k_gather_records<true, false><<<mgrid, 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
+                                                               Q.pk, Q.pd);
+  else
+    k_gather_records<true, true><<<mgrid, 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
+                                                              Q.pk, Q.pd);
   VLB_LAUNCHED(c);
+  c.prev_deferred = defer_prev;
   c.cur ^= 1;
   c.sorted = true;
   c.items_valid = true;

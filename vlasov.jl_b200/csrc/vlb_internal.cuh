@@ -159,6 +159,8 @@ struct Ctx {
   bool order_valid = false;      // part[cur] is in the order its sort products describe
   bool last_sort_near = false;   // the last sort tried the nearly sorted path
   bool graph_sort_near = false;  // the captured step graphs' sorts try it
+  bool prev_deferred = false;    // the last sort left (pk, pdelta) in part[cur ^ 1], in the
+                                // order before it: its push (or settle_prev) moves them
   int32_t* outlist = nullptr;    // [N]
   int32_t* chunk_start = nullptr;  // [ncell] first chunk of occupied cell g (current parity's)
   int32_t* item_cell = nullptr;    // [N / kMinChunk + ncell] occupied cell of each chunk (current parity's)
@@ -239,7 +241,10 @@ int grid_for(const Ctx& c, int64_t n, int threads, int per_sm);
 
 // ---------------------------------------------------------------- kernels
 // sort.cu
-void launch_sort(Ctx& c);
+// defer_prev: a push follows in the same step and reads the previous
+// positions through the permutation, so the move leaves them in place.
+void launch_sort(Ctx& c, bool defer_prev = false);
+void settle_prev(Ctx& c);
 // deposit.cu
 void launch_deposit_fine(Ctx& c, double charge, int mode);
 void launch_deposit_fine_raw(Ctx& c, int mode);
