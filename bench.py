@@ -37,7 +37,9 @@ GATHER_BYTES_PER_PARTICLE = 24.0        # delta in, force out
 # DRAM bytes (read + write) of one gather launch per particle, from the ncu
 # captures of 4e6 particles (profiles/k_field_tc_4M.md, profiles/k_field_4M.md)
 GATHER_TRAFFIC_PER_PARTICLE = {"tcgen05": (49486336 + 6479616) / 4e6, "fp32": (49494784 + 7127296) / 4e6}
-PUSH_BYTES_PER_PARTICLE = 48 + 12 + 48 + 4  # read (k, d, pk, pd) + force; write the record + the next sort's cell key
+# read (k, d) in slot order, (pk, pd) where the step's sort left them (through perm: 4 B), the force;
+# write the record and the next sort's cell key
+PUSH_BYTES_PER_PARTICLE = 24 + 24 + 4 + 12 + 48 + 4
 
 
 def parse():
@@ -411,7 +413,8 @@ def main():
                                     "frac": GATHER_BYTES_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e9
                                     / pk_.get("hbm_gbs", 1),
                                     "note": "12 B of delta read + 12 B of force written a particle"}},
-        "roofline_hbm": {"kernel": "k_push (packed Verlet)", "bound": "hbm", "achieved": push_gbs,
+        "roofline_hbm": {"kernel": "k_push (packed Verlet, previous positions read through the sort's permutation)",
+                         "bound": "hbm", "achieved": push_gbs,
                          "peak": pk_.get("hbm_gbs"), "unit": "GB/s", "frac": push_gbs / pk_.get("hbm_gbs", 1),
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({how})"},
         "stages_ms": stages,

@@ -229,6 +229,12 @@ VLB_API int vlb_sort(vlb_ctx* ctx, int32_t* noccupied, int32_t* outcount);
 VLB_API int vlb_get_sort(vlb_ctx* ctx, int32_t* perm, int32_t* occupied, int32_t* bounds,
                  int32_t* outlist);
 
+/* The sizes vlb_get_sort writes for the last sort of the current cloud:
+ * noccupied (occupied; bounds holds noccupied + 1) and outcount (outlist).
+ * A caller that sorted through a step phase (vlb_step_deposit returns no
+ * counts) reads them here before allocating.  Either pointer may be NULL. */
+VLB_API int vlb_get_sort_sizes(vlb_ctx* ctx, int32_t* noccupied, int32_t* outcount);
+
 /* deposit_smoothed!(rho, acc, mesh, sm, positions; charge)
  * (src/accelerator.jl:531-565): table columns, sorted 8^3 deposit, charge
  * renormalisation.  Needs vlb_sort.  `mode` is VLB_DEPOSIT_*.  Returns nout

@@ -47,7 +47,7 @@ VLB_STATUS_MMA_TIMEOUT = 8
 # every symbol include/vlasov_b200.h declares
 EXPORTS = (
     "vlb_last_error", "vlb_version", "vlb_create", "vlb_destroy", "vlb_upload_particles",
-    "vlb_download_particles", "vlb_sort", "vlb_get_sort", "vlb_deposit_fine", "vlb_deposit_coarse",
+    "vlb_download_particles", "vlb_sort", "vlb_get_sort", "vlb_get_sort_sizes", "vlb_deposit_fine", "vlb_deposit_coarse",
     "vlb_poisson", "vlb_set_precision", "vlb_coefficients", "vlb_mean_field", "vlb_forces", "vlb_projectile_forces",
     "vlb_push", "vlb_step", "vlb_interaction_energy", "vlb_film_reserve", "vlb_film_frames", "vlb_film_download",
     "vlb_film_clear", "vlb_dn_weight_count", "vlb_set_denoiser", "vlb_clear_denoiser", "vlb_dn_create",
@@ -155,6 +155,7 @@ def lib():
             "vlb_download_particles": (C.c_int, [vp, P_I, P_F, P_I, P_F]),
             "vlb_sort": (C.c_int, [vp, P_I, P_I]),
             "vlb_get_sort": (C.c_int, [vp, P_I, P_I, P_I, P_I]),
+            "vlb_get_sort_sizes": (C.c_int, [vp, P_I, P_I]),
             "vlb_deposit_fine": (C.c_int, [vp, C.c_double, C.c_int32, P_I, P_D]),
             "vlb_deposit_coarse": (C.c_int, [vp, C.c_double]),
             "vlb_poisson": (C.c_int, [vp, C.c_int32]),

@@ -685,6 +685,17 @@ int vlb_get_sort(vlb_ctx* ctx, int32_t* perm, int32_t* occupied, int32_t* bounds
   });
 }
 
+int vlb_get_sort_sizes(vlb_ctx* ctx, int32_t* noccupied, int32_t* outcount) {
+  CTX_OR_FAIL;
+  if (!c.sorted) return fail(VLB_ERR_STATE, "no sort has run on the current cloud");
+  return guarded([&]() -> int {
+    fetch_scalars(c);
+    if (noccupied) *noccupied = c.hsc->noccupied;
+    if (outcount) *outcount = c.hsc->outcount;
+    return VLB_OK;
+  });
+}
+
 int vlb_deposit_fine(vlb_ctx* ctx, double charge, int32_t mode, int32_t* nout, double* total_charge) {
   CTX_OR_FAIL;
   if (mode != VLB_DEPOSIT_FLOAT32 && mode != VLB_DEPOSIT_FIXED64) return fail(VLB_ERR_ARG, "unknown deposit mode");

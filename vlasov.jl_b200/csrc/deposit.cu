@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
   unsigned char* work = smem + (((size_t)ncol * 8 * sizeof(float) + 15) & ~(size_t)15);
   int4* cols_s = reinterpret_cast<int4*>(work);                         // [2][kDepStage]
   float* red_s = reinterpret_cast<float*>(work);                        // [kDepLanes][8][kDepRow], after the stages
-  __shared__ int s_g;
+  __shared__ int s_g, s_q;
   __shared__ int s_nout;
   const int tid = threadIdx.x;
   for (int e = tid; e < ncol * 8; e += kDepThreads) nodes_s[e] = nodes[e];
@@ -85,29 +85,50 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
       dd[ax] = d[ax * Npad + s];
     }
   };
-  for (;;) {
-    if (tid == 0) s_g = (int)atomicAdd(&dsc->work_deposit, 1ull);
-    __syncthreads();
-    const int g = s_g;
-    if (g >= nocc) break;
+  // Cells go through a queue two deep: while cell g is added, the next cell
+  // gn is known (with its bounds) and the one after is being claimed, so the
+  // loads of gn's first stage go out during g's last stage.
+  if (tid == 0) {
+    s_g = (int)atomicAdd(&dsc->work_deposit, 1ull);
+    s_q = (int)atomicAdd(&dsc->work_deposit, 1ull);
+  }
+  __syncthreads();
+  int g = s_g, gn = s_q;
+  int sl = 0, sh = 0, sln = 0, shn = 0;
+  if (g < nocc) { sl = bounds[g]; sh = bounds[g + 1]; }
+  if (gn < nocc) { sln = bounds[gn]; shn = bounds[gn + 1]; }
+  int ka[3] = {0, 0, 0}, kb[3] = {0, 0, 0};
+  float da[3] = {0.f, 0.f, 0.f}, db[3] = {0.f, 0.f, 0.f};
+  if (g < nocc) {
+    load_one(sl + tid, sh, ka, da);
+    load_one(sl + kDepThreads + tid, sh, kb, db);
+  }
+  // the loads of a cell's first stage, or of the next stage of this cell
+  auto load_stage = [&](int base, int end) {
+    load_one(base + tid, end, ka, da);
+    load_one(base + kDepThreads + tid, end, kb, db);
+  };
+  while (g < nocc) {
+    __syncthreads();  // every thread holds gn: the queue slot is free
+    if (tid == 0) s_q = (int)atomicAdd(&dsc->work_deposit, 1ull);
     const int cell = occupied[g];
-    const int sl = bounds[g], sh = bounds[g + 1];
     int kx, ky, kz;
     cell_knots((uint32_t)cell, nk, kx, ky, kz);
     const bool fits = deposit_fits(kx, ky, kz, n);
     float2 acc[32];
 #pragma unroll
     for (int a = 0; a < 32; ++a) acc[a] = make_float2(0.f, 0.f);
-    int ka[3] = {0, 0, 0}, kb[3] = {0, 0, 0};
-    float da[3] = {0.f, 0.f, 0.f}, db[3] = {0.f, 0.f, 0.f};
-    // stage 0, then the loads of stage 1 in flight
-    load_one(sl + tid, sh, ka, da);
-    load_one(sl + kDepThreads + tid, sh, kb, db);
+    // stage 0 from the registers, then the loads of the next stage to come
     stage_one(sl + tid, sh, ka, da, &cols_s[tid]);
     stage_one(sl + kDepThreads + tid, sh, kb, db, &cols_s[kDepThreads + tid]);
-    load_one(sl + kDepStage + tid, sh, ka, da);
-    load_one(sl + kDepStage + kDepThreads + tid, sh, kb, db);
+    if (sl + kDepStage < sh)
+      load_stage(sl + kDepStage, sh);
+    else if (gn < nocc)
+      load_stage(sln, shn);
     __syncthreads();
+    const int gnn = s_q;
+    int slnn = 0, shnn = 0;
+    if (gnn < nocc) { slnn = bounds[gnn]; shnn = bounds[gnn + 1]; }
     int buf = 0;
     for (int base = sl; base < sh; base += kDepStage) {
       // the next stage into the other buffer (its last readers passed the
@@ -117,8 +138,10 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
         int4* nxt = cols_s + (buf ^ 1) * kDepStage;
         stage_one(nb + tid, sh, ka, da, &nxt[tid]);
         stage_one(nb + kDepThreads + tid, sh, kb, db, &nxt[kDepThreads + tid]);
-        load_one(nb + kDepStage + tid, sh, ka, da);
-        load_one(nb + kDepStage + kDepThreads + tid, sh, kb, db);
+        if (nb + kDepStage < sh)
+          load_stage(nb + kDepStage, sh);
+        else if (gn < nocc)
+          load_stage(sln, shn);
       }
       if (fits) {
         const int4* cur = cols_s + buf * kDepStage;
@@ -175,7 +198,8 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
         }
       }
     }
-    __syncthreads();
+    g = gn; sl = sln; sh = shn;
+    gn = gnn; sln = slnn; shn = shnn;
   }
   atomicAdd(&s_nout, my_nout);
   __syncthreads();

@@ -175,15 +175,16 @@ __device__ __forceinline__ float sphere_potential(float Q, float R, float r) {
 }
 
 // Right-hand side of the interior with the Dirichlet lifting
-// (src/poisson.jl:275-294), one thread per interior point, i fastest.
-// One block per (j, k) line of the interior, threads along i.
-__global__ void k_rhs(float* __restrict__ rhs, const float* __restrict__ rho, const float* __restrict__ P,
-                      const float* __restrict__ D, int n) {
+// (src/poisson.jl:275-294), one thread per interior point, i fastest: a
+// grid-stride loop over the n^3 interior points (n^3 < 2^31).
+__global__ void __launch_bounds__(256) k_rhs(float* __restrict__ rhs, const float* __restrict__ rho,
+                                             const float* __restrict__ P, const float* __restrict__ D, int n) {
   const int N = n + 2;
   const size_t sj = N, sk = (size_t)N * N;
-  const int j = blockIdx.y, k = blockIdx.z;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const size_t t = (size_t)i + (size_t)n * (j + (size_t)n * k);
+  const unsigned un = (unsigned)n, tot = un * un * un;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+    const unsigned jk = t / un, i = t - jk * un;
+    const unsigned k = jk / un, j = jk - k * un;
     const size_t row = sj * (j + 1) + sk * (k + 1);
     const size_t c = (size_t)(i + 1) + row;
     float v = fmul(-12.566370614359172f, rho[c]);
@@ -197,13 +198,15 @@ __global__ void k_rhs(float* __restrict__ rhs, const float* __restrict__ rho, co
   }
 }
 
-// phi + V_xc(rho) + V_jel(r) at the collocation points (phi may be null)
-__global__ void k_meanfield_src(float* __restrict__ out, const float* __restrict__ phi,
-                                const float* __restrict__ rho, const float* __restrict__ g, int n, float nions,
-                                float radius) {
-  const int j = blockIdx.y, k = blockIdx.z;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const size_t t = (size_t)i + (size_t)n * (j + (size_t)n * k);
+// phi + V_xc(rho) + V_jel(r) at the collocation points (phi may be null):
+// a grid-stride loop over the n^3 points, i fastest (n^3 < 2^31).
+__global__ void __launch_bounds__(256) k_meanfield_src(float* __restrict__ out, const float* __restrict__ phi,
+                                                       const float* __restrict__ rho, const float* __restrict__ g,
+                                                       int n, float nions, float radius) {
+  const unsigned un = (unsigned)n, tot = un * un * un;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += gridDim.x * blockDim.x) {
+    const unsigned jk = t / un, i = t - jk * un;
+    const unsigned k = jk / un, j = jk - k * un;
     const float r = sqrtf(g[i] * g[i] + g[j] * g[j] + g[k] * g[k]);
     const float extra = xc_potential(rho[t]) + sphere_potential(nions, radius, r);
     out[t] = phi ? phi[t] + extra : extra;
@@ -401,7 +404,7 @@ ProductArgs base_args(const Level& L, bool interior) {
 // solve_interior! with the faces already in phi (src/devicemesh.jl:133-146)
 void solve_interior(Ctx& c, Level& L) {
   const int ni = L.ni;
-  k_rhs<<<dim3(1, ni, ni), std::min(1024, (ni + 31) / 32 * 32), 0, c.stream>>>(c.work[2], L.rho, L.phi, L.lap, ni);
+  k_rhs<<<grid_for(c, (int64_t)ni * ni * ni, 256, 8), 256, 0, c.stream>>>(c.work[2], L.rho, L.phi, L.lap, ni);
   VLB_LAUNCHED(c);
   ProductArgs a = base_args(L, true);
   if (c.mode_precision != VLB_POISSON_FP32) {
@@ -463,8 +466,8 @@ void launch_coefficients(Ctx& c, Level& L, const float* src, float* dst) {
 // mean field of effective_potential! (src/devicemesh.jl:171-183) in one pass
 void launch_mean_field_coefficients(Ctx& c, Level& L, const float* phi, float* csol, double nions,
                                     double radius) {
-  k_meanfield_src<<<dim3(1, L.n, L.n), std::min(1024, (L.n + 31) / 32 * 32), 0, c.stream>>>(c.work[2], phi, L.rho, L.colloc, L.n,
-                                                                            (float)nions, (float)radius);
+  k_meanfield_src<<<grid_for(c, (int64_t)L.n * L.n * L.n, 256, 8), 256, 0, c.stream>>>(
+      c.work[2], phi, L.rho, L.colloc, L.n, (float)nions, (float)radius);
   VLB_LAUNCHED(c);
   coefficients(c, L, c.work[2], c.work[0], c.work[1], csol);
 }
@@ -472,8 +475,8 @@ void launch_mean_field_coefficients(Ctx& c, Level& L, const float* phi, float* c
 // csol += S^-1 [V_xc(rho) + V_jel(r)] (src/devicemesh.jl:171-183)
 void launch_mean_field_add(Ctx& c, Level& L, double nions, double radius) {
   const size_t tot = (size_t)L.n * L.n * L.n;
-  k_meanfield_src<<<dim3(1, L.n, L.n), std::min(1024, (L.n + 31) / 32 * 32), 0, c.stream>>>(c.work[2], nullptr, L.rho, L.colloc,
-                                                                            L.n, (float)nions, (float)radius);
+  k_meanfield_src<<<grid_for(c, (int64_t)L.n * L.n * L.n, 256, 8), 256, 0, c.stream>>>(
+      c.work[2], nullptr, L.rho, L.colloc, L.n, (float)nions, (float)radius);
   VLB_LAUNCHED(c);
   coefficients(c, L, c.work[2], c.work[0], c.work[1], c.work[2]);
   k_add<<<grid_for(c, (int64_t)tot, 256, 8), 256, 0, c.stream>>>(L.csol, c.work[2], tot);

@@ -417,7 +417,9 @@ class DeviceAccelerator:
 
     def sort_products(self):
         """perm, occupied cells, bounds and out-of-stencil slots of the last sort."""
-        nocc, outc = self._nocc, self._outc
+        n_occ, n_out = C.c_int32(), C.c_int32()
+        L.check(L.lib().vlb_get_sort_sizes(self._h, C.byref(n_occ), C.byref(n_out)))
+        nocc, outc = n_occ.value, n_out.value
         perm = np.empty(self.npart, np.int32)
         occ = np.empty(max(nocc, 1), np.int32)
         bnd = np.empty(nocc + 1, np.int32)
