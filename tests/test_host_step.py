@@ -154,3 +154,25 @@ def test_host_step_reproduces_the_golden_run_start(orc):
         assert abs(proj.position[0] - g["x_ion"][s]) < 1e-9
         assert st.noutf == g["margin_out"][s]
     assert g["q8"][199] > 0.05
+
+
+ENSEMBLE = Path(__file__).resolve().parent / "golden" / "capture_host_1e5_ensemble.npz"
+
+
+def test_capture_ensemble_members_agree_before_the_chaotic_phase():
+    """The ensemble of perturbed CPU-path runs (make_capture_ensemble.py) that
+    measures the crossing's own spread: eight members with the packed-start
+    run, each within two pseudo-particles of the base curve to step 400
+    (before the ion has crossed the cluster's centre) and ending near one
+    electron, as the reference's README reports for this crossing."""
+    g = np.load(GOLDEN)
+    e = np.load(ENSEMBLE)
+    assert e["q8"].shape == (7, 700)
+    assert list(e["names"]) == ["rounded", "ulp1", "ulp2", "ulp3", "ulp4", "ulp5", "rounded_ulp"]
+    w = float(g["weight"])
+    members = np.vstack([g["q8_packed"][None, :], e["q8"]])
+    d = np.abs(members - g["q8"][None, :])
+    assert d[:, :400].max() <= 2 * w + 1e-12
+    assert np.all(np.abs(members[:, -1] - 1.0) <= 0.1)
+    # the ulp moves and the per-step rounding change the run: the members differ after step 400
+    assert d[:, 400:].max(axis=1).min() > 10 * w
