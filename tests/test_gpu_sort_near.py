@@ -40,6 +40,21 @@ def _forces_only_sort_matches_cellsort(orc, sim):
     return r.sort_path
 
 
+def _step_sorted_as_cellsort(orc, sim):
+    """One step (a graph replay when the step's parameters are unchanged),
+    checked through the previous positions it leaves: the push writes them
+    in the order of the step's sort, so they are the cloud as the step found
+    it, permuted by cellsort!.  Returns the step's sort path."""
+    acc = sim.accelerator
+    k, d, _, _ = acc.download()
+    path = sim.step().sort_path
+    _, _, pk, pd = acc.download()
+    rperm, _, _, _ = orc.cellsort(k, sim.meshes.fine.axis.nknots)
+    assert np.array_equal(pk, k[:, rperm])
+    assert np.array_equal(pd.view(np.uint32), d[:, rperm].view(np.uint32))
+    return path
+
+
 @pytest.mark.parametrize("use_graph", [False, True], ids=["eager", "graph"])
 def test_step_sorts_take_the_single_pass_placement(orc, cuda_device, use_graph):
     p = vb.SimulationParameters.for_grid(28, rcluster=78.0, rbox=235.0, nparticles=60_000, dt=0.5)
@@ -60,7 +75,16 @@ def test_step_sorts_take_the_single_pass_placement(orc, cuda_device, use_graph):
         # step's velocities, so later steps may still send particles several
         # cells: each sort is exact whichever path it takes
         assert sim.step().sort_path == 0
-        assert sim.step().sort_path in (1, 2)
+        # the steps after it, replayed from a graph when use_graph: both the
+        # single-pass placement and its fallback (a captured step runs the radix
+        # passes in a conditional node) must give cellsort!'s order
+        seen = {_step_sorted_as_cellsort(orc, sim) for _ in range(4)}
+        assert seen <= {1, 2}
+        sim.params.dt = 10.0
+        assert _step_sorted_as_cellsort(orc, sim) in (0, 1, 2)
+        seen |= {_step_sorted_as_cellsort(orc, sim) for _ in range(3)}
+        assert 2 in seen, seen
+        sim.params.dt = 0.5
         assert _forces_only_sort_matches_cellsort(orc, sim) in (1, 2)
     finally:
         sim.accelerator.close()

@@ -173,7 +173,7 @@ void destroy_ctx(Ctx* c) {
   dfree(c->dir_cnt); dfree(c->dir_base);
   dfree(c->outlist);
   for (int p = 0; p < 2; ++p) { dfree(c->cstart_buf[p]); dfree(c->item_buf[p]); }
-  dfree(c->item_dir); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
+  dfree(c->item_dir); dfree(c->item_rec); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
   dfree(c->rho_fixed_c); dfree(c->red_items); dfree(c->red_tail); dfree(c->red_blocks); dfree(c->diag_part);
   dfree(c->e_items); dfree(c->e_blocks);
   for (auto& w : c->work) dfree(w);
@@ -345,6 +345,7 @@ void capture_graphs(Ctx& c, const vlb_step_params& p) {
   const int saved = c.cur;
   // the step's result reports the sort that ran eagerly, not the captured one
   const bool ran_near = c.last_sort_near;
+  const long long launches0 = c.launches;
   for (int g = 0; g < 2; ++g) {
     if (c.gexec[g]) {
       VLB_CUDA(cudaGraphExecDestroy(c.gexec[g]));
@@ -352,6 +353,7 @@ void capture_graphs(Ctx& c, const vlb_step_params& p) {
     }
     c.cur = g;
     cudaGraph_t graph = nullptr;
+    const long long l0 = c.launches;
     VLB_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
     try {
       enqueue_step(c, p);
@@ -366,7 +368,9 @@ void capture_graphs(Ctx& c, const vlb_step_params& p) {
     VLB_CUDA(cudaStreamEndCapture(c.stream, &graph));
     VLB_CUDA(cudaGraphInstantiate(&c.gexec[g], graph, 0));
     VLB_CUDA(cudaGraphDestroy(graph));
+    if (g == 0) c.graph_launches = c.launches - l0;
   }
+  c.launches = launches0;
   c.cur = saved;
   c.graph_sort_near = c.last_sort_near;
   c.last_sort_near = ran_near;
@@ -496,6 +500,7 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->chunk_start = c->cstart_buf[0];
     c->item_cell = c->item_buf[0];
     c->item_dir = dalloc<int32_t>(((size_t)N / kMinChunk + c->ncell + 1) * 27);
+    c->item_rec = dalloc<int4>((size_t)N / kMinChunk + c->ncell + 1);
     const int64_t scan_tiles = std::max<int64_t>({(N + 4095) / 4096, (c->ncell + 4095) / 4096,
                                                   (c->radix_table_size + 4095) / 4096}) + 1;
     c->scan_status_size = 8 * scan_tiles;
@@ -1142,6 +1147,8 @@ void capture_batch(vlb_batch& b, const vlb_step_params& p) {
       b.ctx[i]->keys_ready = true;  // the captured step follows a step whose push wrote them
     }
     cudaGraph_t graph = nullptr;
+    std::vector<long long> l0(b.ctx.size());
+    for (size_t i = 0; i < b.ctx.size(); ++i) l0[i] = b.ctx[i]->launches;
     VLB_CUDA(cudaStreamBeginCapture(b.origin, cudaStreamCaptureModeThreadLocal));
     try {
       enqueue_batch(b, p);
@@ -1159,6 +1166,8 @@ void capture_batch(vlb_batch& b, const vlb_step_params& p) {
     cudaError_t e = cudaGraphInstantiate(&b.gexec[g], graph, 0);
     cudaGraphDestroy(graph);
     VLB_CUDA(e);
+    if (g == 0)
+      for (size_t i = 0; i < b.ctx.size(); ++i) b.ctx[i]->graph_launches = b.ctx[i]->launches - l0[i];
   }
   for (size_t i = 0; i < b.ctx.size(); ++i) {
     b.ctx[i]->cur = saved[i];

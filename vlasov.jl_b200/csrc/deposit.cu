@@ -40,7 +40,8 @@ constexpr double kFixedInv = 1.0 / 1099511627776.0;
 // window test of two particles into one int4 each of a double-buffered stage
 // in shared memory while the CTA adds the previous stage, and the k/delta
 // loads of the stage after are in flight meanwhile; one CTA barrier per
-// stage.  Thread (lane, q) owns the z row q of its lane's 8^3 sum: 64 float32
+// stage (the columns stored as the offsets of their node rows).  Thread
+// (lane, q) owns the z row q of its lane's 8^3 sum: 64 float32
 // accumulators as float2 pairs along x, so one packed FMA covers two outputs.
 // At the cell's end the lane partials are summed over the lanes in a fixed
 // order (in shared memory that the stages used) and added to the grid.
@@ -75,7 +76,8 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
       cc[ax] = table_column(dd[ax], spacing, nbdt, ncol);
     }
     if (!inside) { cc[0] = cc[1] = cc[2] = 1; ++my_nout; }
-    *slot = make_int4(cc[0], cc[1], cc[2], 0);
+    // the node rows' offsets in the shared table (8 floats a column)
+    *slot = make_int4((cc[0] - 1) * 8, (cc[1] - 1) * 8, (cc[2] - 1) * 8, 0);
   };
   auto load_one = [&](int s, int sh, int (&kk)[3], float (&dd)[3]) {
     if (s >= sh) return;
@@ -148,9 +150,9 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
         const int cnt = min(kDepStage, sh - base);
         for (int t = pl; t < cnt; t += kDepLanes) {
           const int4 cc = cur[t];
-          const float* vx = nodes_s + (size_t)(cc.x - 1) * 8;
-          const float* vy = nodes_s + (size_t)(cc.y - 1) * 8;
-          const float z = nodes_s[(size_t)(cc.z - 1) * 8 + q];
+          const float* vx = nodes_s + cc.x;
+          const float* vy = nodes_s + cc.y;
+          const float z = nodes_s[cc.z + q];
           const float4 xa = *reinterpret_cast<const float4*>(vx);
           const float4 xb = *reinterpret_cast<const float4*>(vx + 4);
           const float4 ya = *reinterpret_cast<const float4*>(vy);

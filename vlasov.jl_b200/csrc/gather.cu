@@ -398,34 +398,33 @@ struct FtPart {
   float2 oy[5], gy[5], ox[5], gx[5], oz[5], gz[5];
 };
 
-// An item's cell data as loaded (used an iteration later, so that no
-// thread waits on the loads).
+// An item's record as loaded (used an iteration later, so that no thread
+// waits on the load): the sort writes one int4 per work item -- its cell
+// code, first slot, end slot and the cell's knots packed 10 bits each.
 struct FtRaw {
-  int item, code, b0, b1, cs;
+  int item;
+  int4 rec;
 };
 
-__device__ __forceinline__ FtRaw ft_load_item(int item, int g, int nitems, const int32_t* __restrict__ occupied,
-                                              const int32_t* __restrict__ bounds,
-                                              const int32_t* __restrict__ chunk_start) {
-  FtRaw r{-1, 0, 0, 0, 0};
+__device__ __forceinline__ FtRaw ft_load_item(int item, int nitems, const int4* __restrict__ items) {
+  FtRaw r{-1, make_int4(0, 0, 0, 0)};
   if (item >= nitems) return r;
   r.item = item;
-  r.code = occupied[g];
-  r.b0 = bounds[g];
-  r.b1 = bounds[g + 1];
-  r.cs = chunk_start[g];
+  r.rec = items[item];
   return r;
 }
 
-__device__ __forceinline__ FtItem ft_derive(const FtRaw& r, int chunk, int n, int nk) {
+__device__ __forceinline__ FtItem ft_derive(const FtRaw& r, int n) {
   FtItem it{-1, 0, 0, 0, 0, 0, 0, false};
   if (r.item < 0) return it;
   it.item = r.item;
-  it.code = r.code;
-  cell_knots((uint32_t)it.code, nk, it.kx, it.ky, it.kz);
+  it.code = r.rec.x;
+  it.kx = r.rec.w & 1023;
+  it.ky = (r.rec.w >> 10) & 1023;
+  it.kz = r.rec.w >> 20;
   it.has = field_fits(it.kx, it.ky, it.kz, n);
-  it.s0 = r.b0 + (r.item - r.cs) * chunk;
-  it.s1 = min(it.s0 + chunk, r.b1);
+  it.s0 = r.rec.y;
+  it.s1 = r.rec.z;
   return it;
 }
 
@@ -557,8 +556,7 @@ __device__ __forceinline__ void ft_finish(unsigned lane_base, const FtPart& p, f
 }
 
 __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
-    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
-    const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int64_t Npad,
+    const int4* __restrict__ items, DeviceScalars* dsc, int64_t Npad,
     const float* __restrict__ d, const __grid_constant__ CUtensorMap csol_map, int n, int nk,
     const float4* __restrict__ ovgr, int nbdt, int ncol, float spacing, float x0, float h, double w,
     float* __restrict__ force, int chunk, double* __restrict__ red_items) {
@@ -651,15 +649,13 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
 
   const int G = gridDim.x;
   auto item_at = [&](int t) { return (int)blockIdx.x + t * G; };
-  auto cell_of = [&](int item) { return item < nitems ? item_cell[item] : 0; };
-  auto load_item = [&](int item, int g) { return ft_load_item(item, g, nitems, occupied, bounds, chunk_start); };
-  auto resolve = [&](int item, int g) { return ft_derive(load_item(item, g), chunk, n, nk); };
+  auto load_item = [&](int item) { return ft_load_item(item, nitems, items); };
+  auto resolve = [&](int item) { return ft_derive(load_item(item), n); };
 
   // items t (cur), t+1 (nxt, delta in dn), t+2 (after); item_cell of t+3
-  FtItem cur = resolve(item_at(0), cell_of(item_at(0)));
-  FtItem nxt = resolve(item_at(1), cell_of(item_at(1)));
-  FtItem after = resolve(item_at(2), cell_of(item_at(2)));
-  int g3 = cell_of(item_at(3));
+  FtItem cur = resolve(item_at(0));
+  FtItem nxt = resolve(item_at(1));
+  FtItem after = resolve(item_at(2));
   float dc[3] = {0.f, 0.f, 0.f}, dn[3] = {0.f, 0.f, 0.f};
   load_delta(cur, dc);
   load_delta(nxt, dn);
@@ -701,8 +697,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     // tables of t+1 and, when needed, its stencil
     float d2[3] = {0.f, 0.f, 0.f};
     load_delta(after, d2);
-    const FtRaw raw3 = load_item(item_at(t + 3), g3);
-    g3 = cell_of(item_at(t + 4));
+    const FtRaw raw3 = load_item(item_at(t + 3));
     FtPart pn;
     load_part(nxt, dn, pn);
     const bool restage = nxt.has && ok && staged != nxt.code;
@@ -786,7 +781,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
       red_items[4 * (size_t)cur.item + tid] = ((red[b][0][tid] + red[b][1][tid]) + red[b][2][tid]) + red[b][3][tid];
     cur = nxt;
     nxt = after;
-    after = ft_derive(raw3, chunk, n, nk);
+    after = ft_derive(raw3, n);
     pc = pn;
 #pragma unroll
     for (int k = 0; k < 3; ++k) dn[k] = d2[k];
@@ -1158,7 +1153,7 @@ void launch_forces(Ctx& c) {
                                                                                c.csol_pitch, rows);
     VLB_LAUNCHED(c);
     k_field_tc<<<2 * c.num_sms, kFtThreads, kFtSmem, c.stream>>>(
-        c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.d, c.csol_map, F.n, F.nk,
+        c.item_rec, c.dsc, c.Npad, P.d, c.csol_map, F.n, F.nk,
         reinterpret_cast<const float4*>(c.ovgr), c.nbdt, c.ncol, c.spacing_f, c.x0f, c.hf, c.weight, c.force,
         c.chunk, c.red_items);
   } else {
