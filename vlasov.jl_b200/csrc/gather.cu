@@ -953,12 +953,47 @@ __global__ void __launch_bounds__(kGThreads) k_tail(const int32_t* __restrict__ 
 // the grid, reads its stencil from global memory.  Positions are rebuilt in
 // float64 as the host does; the 10^3 sum is FP32, the sums over particles
 // float64, one per work item, reduced in a fixed order.
-constexpr int kEW = 14;
+constexpr int kEW = 14;   // tile rows (y) and planes (z): the stencils of the cell and its neighbours
+constexpr int kEX = 16;   // tile row pitch (x): the cell's own stencil rows start 16-byte aligned
 constexpr int kEThreads = 128;
+constexpr int kEClaim = 8;     // work items a warp claims at once
 
 // sum_{ii,jj,kk} c[ii + sy jj + sz kk] ox[ii] oy[jj] oz[kk] (c 8-byte aligned,
 // sy and sz even): y first into five packed accumulators per plane, then x,
 // then z, as the gather contracts.
+// The same sum from rows that start on 16-byte boundaries (row pitch sy and
+// plane pitch sz multiples of four): two 16-byte and one 8-byte load a row.
+__device__ __forceinline__ float smoothed_sum_a16(const float* __restrict__ c, int sy, int sz, const float (&ox)[10],
+                                                  const float (&oy)[10], const float (&oz)[10]) {
+  float2 ox2[5];
+#pragma unroll
+  for (int a = 0; a < 5; ++a) ox2[a] = make_float2(ox[2 * a], ox[2 * a + 1]);
+  float phi = 0.f;
+#pragma unroll 2
+  for (int kk = 0; kk < 10; ++kk) {
+    float2 y2[5];
+#pragma unroll
+    for (int a = 0; a < 5; ++a) y2[a] = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int jj = 0; jj < 10; ++jj) {
+      const float* row = c + jj * sy + kk * sz;
+      const float4 c0 = *reinterpret_cast<const float4*>(row);
+      const float4 c1 = *reinterpret_cast<const float4*>(row + 4);
+      const float2 c2 = *reinterpret_cast<const float2*>(row + 8);
+      const float2 cp[5] = {make_float2(c0.x, c0.y), make_float2(c0.z, c0.w), make_float2(c1.x, c1.y),
+                            make_float2(c1.z, c1.w), c2};
+      const float2 w = make_float2(oy[jj], oy[jj]);
+#pragma unroll
+      for (int a = 0; a < 5; ++a) y2[a] = __ffma2_rn(cp[a], w, y2[a]);
+    }
+    float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int a = 0; a < 5; ++a) t = __ffma2_rn(ox2[a], y2[a], t);
+    phi = fmaf(oz[kk], t.x + t.y, phi);
+  }
+  return phi;
+}
+
 __device__ __forceinline__ float smoothed_sum(const float* __restrict__ c, int sy, int sz, const float (&ox)[10],
                                               const float (&oy)[10], const float (&oz)[10]) {
   float2 ox2[5];
@@ -992,90 +1027,99 @@ __global__ void __launch_bounds__(kEThreads) k_energy(
     const float* __restrict__ ov, int nbdt, int ncol, float spacing, double x0, double h, double lo, double hi,
     const float* __restrict__ csolc, const double* __restrict__ kc, int nkc, int nc, double w, int chunk,
     double* __restrict__ e_items) {
-  __shared__ float tiles[kEThreads / 32][kEW * kEW * kEW];
+  extern __shared__ __align__(16) float etiles[];  // [warps][kEW][kEW][kEX]
   const int lane = threadIdx.x & 31;
-  float* tile = tiles[threadIdx.x >> 5];
+  float* tile = etiles + (threadIdx.x >> 5) * (kEW * kEW * kEX);
   const int nitems = dsc->nitems;
   int cached = -1;
+  // runs of kEClaim consecutive work items per claim: a cell's items (about
+  // eight at the headline size) share one staging of its tile
   for (;;) {
-    int item = 0;
-    if (lane == 0) item = (int)atomicAdd(&dsc->work_energy, 1ull);
-    item = __shfl_sync(0xffffffffu, item, 0);
-    if (item >= nitems) break;
-    const int g = item_cell[item];
-    int kx, ky, kz;
-    cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
-    // 0-based corner of the 14^3 block: the cell's stencil corner 2k - 6, less two
-    const int cx0 = 2 * kx - 8, cy0 = 2 * ky - 8, cz0 = 2 * kz - 8;
-    if (g != cached) {
-      __syncwarp();
-      for (int e = lane; e < kEW * kEW * kEW; e += 32) {
-        const int i = cx0 + e % kEW, j = cy0 + (e / kEW) % kEW, kk = cz0 + e / (kEW * kEW);
-        tile[e] = (i >= 0 && j >= 0 && kk >= 0 && i < n && j < n && kk < n)
-                      ? csolf[(size_t)i + (size_t)n * (j + (size_t)n * kk)]
-                      : 0.f;
-      }
-      cached = g;
-      __syncwarp();
-    }
-    const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
-    const int s1 = min(s0 + chunk, bounds[g + 1]);
-    double e = 0.0;
-    for (int s = s0 + lane; s < s1; s += 32) {
-      const int kp[3] = {k[s], k[Npad + s], k[2 * Npad + s]};
-      const float dp[3] = {d[s], d[Npad + s], d[2 * Npad + s]};
-      double p[3];
-      bool inside = true;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        p[a] = x0 + (double)(kp[a] - 1) * h + (double)dp[a];
-        inside = inside && lo < p[a] && p[a] < hi;
-      }
-      double phi = 0.0;
-      if (inside) {
-        float ox[10], oy[10], oz[10];
-        {
-          const float* t0 = ov + (size_t)(table_column(dp[0], spacing, nbdt, ncol) - 1) * 10;
-          const float* t1 = ov + (size_t)(table_column(dp[1], spacing, nbdt, ncol) - 1) * 10;
-          const float* t2 = ov + (size_t)(table_column(dp[2], spacing, nbdt, ncol) - 1) * 10;
-#pragma unroll
-          for (int a = 0; a < 10; ++a) {
-            ox[a] = __ldg(t0 + a);
-            oy[a] = __ldg(t1 + a);
-            oz[a] = __ldg(t2 + a);
-          }
+    int i0 = 0;
+    if (lane == 0) i0 = (int)atomicAdd(&dsc->work_energy, (unsigned long long)kEClaim);
+    i0 = __shfl_sync(0xffffffffu, i0, 0);
+    if (i0 >= nitems) break;
+    const int i1 = min(i0 + kEClaim, nitems);
+    for (int item = i0; item < i1; ++item) {
+      const int g = item_cell[item];
+      int kx, ky, kz;
+      cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
+      // 0-based corner of the block: the cell's stencil corner 2k - 6, less
+      // four along x (the cell's own rows start 16-byte aligned) and two along
+      // y and z; a particle of a neighbouring cell has its stencil inside it
+      const int cx0 = 2 * kx - 10, cy0 = 2 * ky - 8, cz0 = 2 * kz - 8;
+      if (g != cached) {
+        __syncwarp();
+        for (int e = lane; e < kEW * kEW * kEX; e += 32) {
+          const int i = cx0 + e % kEX, j = cy0 + (e / kEX) % kEW, kk = cz0 + e / (kEX * kEW);
+          tile[e] = (i >= 0 && j >= 0 && kk >= 0 && i < n && j < n && kk < n)
+                        ? csolf[(size_t)i + (size_t)n * (j + (size_t)n * kk)]
+                        : 0.f;
         }
-        // stencil corner of the particle's own nearest knots, in the block
-        const int bx = 2 * kp[0] - 6 - cx0, by = 2 * kp[1] - 6 - cy0, bz = 2 * kp[2] - 6 - cz0;
-        if (bx >= 0 && by >= 0 && bz >= 0 && bx <= kEW - 10 && by <= kEW - 10 && bz <= kEW - 10)
-          phi = smoothed_sum(tile + bx + kEW * (by + kEW * bz), kEW, kEW * kEW, ox, oy, oz);
-        else
-          phi = smoothed_sum(csolf + (size_t)(2 * kp[0] - 6) + (size_t)n * ((2 * kp[1] - 6) + (size_t)n * (2 * kp[2] - 6)),
-                             n, n * n, ox, oy, oz);
-      } else {
-        const int ix = cell_index_d(kc, nkc, p[0]), iy = cell_index_d(kc, nkc, p[1]), iz = cell_index_d(kc, nkc, p[2]);
-        if (ix && iy && iz) {
-          double vx[4], vy[4], vz[4], dd;
-#pragma unroll
-          for (int a = 0; a < 4; ++a) {
-            basis_vd(kc, nkc, 2 * (ix - 1) + a + 1, p[0], vx[a], dd);
-            basis_vd(kc, nkc, 2 * (iy - 1) + a + 1, p[1], vy[a], dd);
-            basis_vd(kc, nkc, 2 * (iz - 1) + a + 1, p[2], vz[a], dd);
-          }
-          for (int ak = 0; ak < 4; ++ak)
-            for (int aj = 0; aj < 4; ++aj) {
-              const float* row =
-                  csolc + (size_t)2 * (ix - 1) + (size_t)nc * ((2 * (iy - 1) + aj) + (size_t)nc * (2 * (iz - 1) + ak));
-              const double wyz = vy[aj] * vz[ak];
-#pragma unroll
-              for (int ai = 0; ai < 4; ++ai) phi += (double)row[ai] * vx[ai] * wyz;
+        cached = g;
+        __syncwarp();
+      }
+      const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
+      const int s1 = min(s0 + chunk, bounds[g + 1]);
+      double e = 0.0;
+      for (int s = s0 + lane; s < s1; s += 32) {
+        const int kp[3] = {k[s], k[Npad + s], k[2 * Npad + s]};
+        const float dp[3] = {d[s], d[Npad + s], d[2 * Npad + s]};
+        double p[3];
+        bool inside = true;
+  #pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          p[a] = x0 + (double)(kp[a] - 1) * h + (double)dp[a];
+          inside = inside && lo < p[a] && p[a] < hi;
+        }
+        double phi = 0.0;
+        if (inside) {
+          float ox[10], oy[10], oz[10];
+          {
+            const float* t0 = ov + (size_t)(table_column(dp[0], spacing, nbdt, ncol) - 1) * 10;
+            const float* t1 = ov + (size_t)(table_column(dp[1], spacing, nbdt, ncol) - 1) * 10;
+            const float* t2 = ov + (size_t)(table_column(dp[2], spacing, nbdt, ncol) - 1) * 10;
+  #pragma unroll
+            for (int a = 0; a < 10; ++a) {
+              ox[a] = __ldg(t0 + a);
+              oy[a] = __ldg(t1 + a);
+              oz[a] = __ldg(t2 + a);
             }
+          }
+          // stencil corner of the particle's own nearest knots, in the block
+          const int bx = 2 * kp[0] - 6 - cx0, by = 2 * kp[1] - 6 - cy0, bz = 2 * kp[2] - 6 - cz0;
+          if (bx == 4 && by == 2 && bz == 2)  // still in the item's cell
+            phi = smoothed_sum_a16(tile + 4 + kEX * (2 + kEW * 2), kEX, kEX * kEW, ox, oy, oz);
+          else if (bx >= 0 && by >= 0 && bz >= 0 && bx <= kEX - 10 && by <= kEW - 10 && bz <= kEW - 10)
+            phi = smoothed_sum(tile + bx + kEX * (by + kEW * bz), kEX, kEX * kEW, ox, oy, oz);
+          else
+            phi = smoothed_sum(csolf + (size_t)(2 * kp[0] - 6) + (size_t)n * ((2 * kp[1] - 6) + (size_t)n * (2 * kp[2] - 6)),
+                               n, n * n, ox, oy, oz);
+        } else {
+          const int ix = cell_index_d(kc, nkc, p[0]), iy = cell_index_d(kc, nkc, p[1]), iz = cell_index_d(kc, nkc, p[2]);
+          if (ix && iy && iz) {
+            double vx[4], vy[4], vz[4], dd;
+  #pragma unroll
+            for (int a = 0; a < 4; ++a) {
+              basis_vd(kc, nkc, 2 * (ix - 1) + a + 1, p[0], vx[a], dd);
+              basis_vd(kc, nkc, 2 * (iy - 1) + a + 1, p[1], vy[a], dd);
+              basis_vd(kc, nkc, 2 * (iz - 1) + a + 1, p[2], vz[a], dd);
+            }
+            for (int ak = 0; ak < 4; ++ak)
+              for (int aj = 0; aj < 4; ++aj) {
+                const float* row =
+                    csolc + (size_t)2 * (ix - 1) + (size_t)nc * ((2 * (iy - 1) + aj) + (size_t)nc * (2 * (iz - 1) + ak));
+                const double wyz = vy[aj] * vz[ak];
+  #pragma unroll
+                for (int ai = 0; ai < 4; ++ai) phi += (double)row[ai] * vx[ai] * wyz;
+              }
+          }
         }
+        e += w * phi;
       }
-      e += w * phi;
+      e = warp_sum(e);
+      if (lane == 0) e_items[item] = e;
     }
-    e = warp_sum(e);
-    if (lane == 0) e_items[item] = e;
   }
 }
 
@@ -1114,8 +1158,11 @@ __global__ void __launch_bounds__(256) k_energy_total(const double* __restrict__
 // The row-padded copy of the fine coefficients and the tensor map over it:
 // dims (pitch, n, n) floats, x fastest; strides pitch * 4 and pitch * n * 4
 // bytes (multiples of 16); box 20 x 10 x 10; no swizzle, zero fill.
+size_t energy_smem() { return (size_t)(kEThreads / 32) * kEW * kEW * kEX * sizeof(float); }
+
 void field_setup(Ctx& c) {
   VLB_CUDA(cudaFuncSetAttribute(k_field_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFtSmem));
+  VLB_CUDA(cudaFuncSetAttribute(k_energy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)energy_smem()));
   // two CTAs of 55 KB need the 132 KB shared-memory split (58 % of 228 KB);
   // the remaining 124 KB of the SM's L1 holds the 80 KB interleaved tables
   VLB_CUDA(cudaFuncSetAttribute(k_field_tc, cudaFuncAttributePreferredSharedMemoryCarveout, 58));
@@ -1183,7 +1230,7 @@ void launch_energy(Ctx& c, const float* csolf, const float* csolc, double* out) 
   Level& C = c.coarse;
   Particles& P = c.part[c.cur];
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_energy, 0, sizeof(unsigned long long), c.stream));
-  k_energy<<<c.num_sms * 4, kEThreads, 0, c.stream>>>(
+  k_energy<<<c.num_sms * 4, kEThreads, energy_smem(), c.stream>>>(
       c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.k, P.d, csolf, F.n, F.nk, c.overlap, c.nbdt,
       c.ncol, c.spacing_f, c.x0, c.h, F.h_knots[2], F.h_knots[F.nk - 3], csolc, C.knots_d, C.nk, C.n, c.weight,
       c.chunk, c.e_items);
