@@ -961,6 +961,17 @@ constexpr int kEClaim = 8;     // work items a warp claims at once
 // sum_{ii,jj,kk} c[ii + sy jj + sz kk] ox[ii] oy[jj] oz[kk] (c 8-byte aligned,
 // sy and sz even): y first into five packed accumulators per plane, then x,
 // then z, as the gather contracts.
+// A column's overlap row from the interleaved table (its first ten floats of
+// the 80-byte row): two 16-byte loads and one 8-byte load.
+__device__ __forceinline__ void load_ov10(const float4* __restrict__ ovgr, int col, float (&v)[10]) {
+  const float4* p = ovgr + (size_t)(col - 1) * 5;
+  const float4 a = __ldg(p), b = __ldg(p + 1);
+  const float2 c = __ldg(reinterpret_cast<const float2*>(p + 2));
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  v[8] = c.x; v[9] = c.y;
+}
+
 // The same sum from rows that start on 16-byte boundaries (row pitch sy and
 // plane pitch sz multiples of four): two 16-byte and one 8-byte load a row.
 __device__ __forceinline__ float smoothed_sum_a16(const float* __restrict__ c, int sy, int sz, const float (&ox)[10],
@@ -1024,20 +1035,24 @@ __global__ void __launch_bounds__(kEThreads) k_energy(
     const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
     const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int64_t Npad,
     const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ csolf, int n, int nk,
-    const float* __restrict__ ov, int nbdt, int ncol, float spacing, double x0, double h, double lo, double hi,
+    const float4* __restrict__ ovgr, int nbdt, int ncol, float spacing, double x0, double h, double lo, double hi,
     const float* __restrict__ csolc, const double* __restrict__ kc, int nkc, int nc, double w, int chunk,
     double* __restrict__ e_items) {
-  extern __shared__ __align__(16) float etiles[];  // [warps][kEW][kEW][kEX]
-  const int lane = threadIdx.x & 31;
-  float* tile = etiles + (threadIdx.x >> 5) * (kEW * kEW * kEX);
+  extern __shared__ __align__(16) float etile[];  // [kEW][kEW][kEX]: the CTA's tile
+  __shared__ int s_item;
+  __shared__ double s_e[2][kEThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float* tile = etile;
   const int nitems = dsc->nitems;
   int cached = -1;
-  // runs of kEClaim consecutive work items per claim: a cell's items (about
-  // eight at the headline size) share one staging of its tile
+  // The CTA claims runs of kEClaim consecutive work items (a cell's items,
+  // about eight at the headline size, share one staging of its tile) and
+  // takes them one at a time, a particle a thread.
   for (;;) {
-    int i0 = 0;
-    if (lane == 0) i0 = (int)atomicAdd(&dsc->work_energy, (unsigned long long)kEClaim);
-    i0 = __shfl_sync(0xffffffffu, i0, 0);
+    if (tid == 0) s_item = (int)atomicAdd(&dsc->work_energy, (unsigned long long)kEClaim);
+    __syncthreads();
+    const int i0 = s_item;
+    __syncthreads();  // every thread has the run before the next claim
     if (i0 >= nitems) break;
     const int i1 = min(i0 + kEClaim, nitems);
     for (int item = i0; item < i1; ++item) {
@@ -1049,25 +1064,25 @@ __global__ void __launch_bounds__(kEThreads) k_energy(
       // y and z; a particle of a neighbouring cell has its stencil inside it
       const int cx0 = 2 * kx - 10, cy0 = 2 * ky - 8, cz0 = 2 * kz - 8;
       if (g != cached) {
-        __syncwarp();
-        for (int e = lane; e < kEW * kEW * kEX; e += 32) {
+        __syncthreads();  // the previous item's threads are done with the tile
+        for (int e = tid; e < kEW * kEW * kEX; e += kEThreads) {
           const int i = cx0 + e % kEX, j = cy0 + (e / kEX) % kEW, kk = cz0 + e / (kEX * kEW);
           tile[e] = (i >= 0 && j >= 0 && kk >= 0 && i < n && j < n && kk < n)
                         ? csolf[(size_t)i + (size_t)n * (j + (size_t)n * kk)]
                         : 0.f;
         }
         cached = g;
-        __syncwarp();
+        __syncthreads();
       }
       const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
       const int s1 = min(s0 + chunk, bounds[g + 1]);
       double e = 0.0;
-      for (int s = s0 + lane; s < s1; s += 32) {
+      for (int s = s0 + tid; s < s1; s += kEThreads) {
         const int kp[3] = {k[s], k[Npad + s], k[2 * Npad + s]};
         const float dp[3] = {d[s], d[Npad + s], d[2 * Npad + s]};
         double p[3];
         bool inside = true;
-  #pragma unroll
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
           p[a] = x0 + (double)(kp[a] - 1) * h + (double)dp[a];
           inside = inside && lo < p[a] && p[a] < hi;
@@ -1075,20 +1090,17 @@ __global__ void __launch_bounds__(kEThreads) k_energy(
         double phi = 0.0;
         if (inside) {
           float ox[10], oy[10], oz[10];
-          {
-            const float* t0 = ov + (size_t)(table_column(dp[0], spacing, nbdt, ncol) - 1) * 10;
-            const float* t1 = ov + (size_t)(table_column(dp[1], spacing, nbdt, ncol) - 1) * 10;
-            const float* t2 = ov + (size_t)(table_column(dp[2], spacing, nbdt, ncol) - 1) * 10;
-  #pragma unroll
-            for (int a = 0; a < 10; ++a) {
-              ox[a] = __ldg(t0 + a);
-              oy[a] = __ldg(t1 + a);
-              oz[a] = __ldg(t2 + a);
-            }
-          }
+          load_ov10(ovgr, table_column(dp[0], spacing, nbdt, ncol), ox);
+          load_ov10(ovgr, table_column(dp[1], spacing, nbdt, ncol), oy);
+          load_ov10(ovgr, table_column(dp[2], spacing, nbdt, ncol), oz);
           // stencil corner of the particle's own nearest knots, in the block
           const int bx = 2 * kp[0] - 6 - cx0, by = 2 * kp[1] - 6 - cy0, bz = 2 * kp[2] - 6 - cz0;
-          if (bx == 4 && by == 2 && bz == 2)  // still in the item's cell
+          // a particle still in the item's cell: rows 16-byte aligned, the
+          // same rows as its warp's other such particles (broadcast loads); one
+          // in a neighbouring cell: 8-byte loads at its offset (a second copy of
+          // the tile shifted by two floats, so that those rows align too, was
+          // measured slower: their lanes' scattered rows conflict in the banks)
+          if (bx == 4 && by == 2 && bz == 2)
             phi = smoothed_sum_a16(tile + 4 + kEX * (2 + kEW * 2), kEX, kEX * kEW, ox, oy, oz);
           else if (bx >= 0 && by >= 0 && bz >= 0 && bx <= kEX - 10 && by <= kEW - 10 && bz <= kEW - 10)
             phi = smoothed_sum(tile + bx + kEX * (by + kEW * bz), kEX, kEX * kEW, ox, oy, oz);
@@ -1099,7 +1111,7 @@ __global__ void __launch_bounds__(kEThreads) k_energy(
           const int ix = cell_index_d(kc, nkc, p[0]), iy = cell_index_d(kc, nkc, p[1]), iz = cell_index_d(kc, nkc, p[2]);
           if (ix && iy && iz) {
             double vx[4], vy[4], vz[4], dd;
-  #pragma unroll
+#pragma unroll
             for (int a = 0; a < 4; ++a) {
               basis_vd(kc, nkc, 2 * (ix - 1) + a + 1, p[0], vx[a], dd);
               basis_vd(kc, nkc, 2 * (iy - 1) + a + 1, p[1], vy[a], dd);
@@ -1110,15 +1122,24 @@ __global__ void __launch_bounds__(kEThreads) k_energy(
                 const float* row =
                     csolc + (size_t)2 * (ix - 1) + (size_t)nc * ((2 * (iy - 1) + aj) + (size_t)nc * (2 * (iz - 1) + ak));
                 const double wyz = vy[aj] * vz[ak];
-  #pragma unroll
+#pragma unroll
                 for (int ai = 0; ai < 4; ++ai) phi += (double)row[ai] * vx[ai] * wyz;
               }
           }
         }
         e += w * phi;
       }
+      // the item's sum: each warp's butterfly, then the warps in order (the
+      // partials alternate between two slots, so one barrier a item suffices)
       e = warp_sum(e);
-      if (lane == 0) e_items[item] = e;
+      if (lane == 0) s_e[item & 1][warp] = e;
+      __syncthreads();
+      if (tid == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < kEThreads / 32; ++q) t += s_e[item & 1][q];
+        e_items[item] = t;
+      }
     }
   }
 }
@@ -1158,7 +1179,7 @@ __global__ void __launch_bounds__(256) k_energy_total(const double* __restrict__
 // The row-padded copy of the fine coefficients and the tensor map over it:
 // dims (pitch, n, n) floats, x fastest; strides pitch * 4 and pitch * n * 4
 // bytes (multiples of 16); box 20 x 10 x 10; no swizzle, zero fill.
-size_t energy_smem() { return (size_t)(kEThreads / 32) * kEW * kEW * kEX * sizeof(float); }
+size_t energy_smem() { return (size_t)kEW * kEW * kEX * sizeof(float); }
 
 void field_setup(Ctx& c) {
   VLB_CUDA(cudaFuncSetAttribute(k_field_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFtSmem));
@@ -1230,8 +1251,9 @@ void launch_energy(Ctx& c, const float* csolf, const float* csolc, double* out) 
   Level& C = c.coarse;
   Particles& P = c.part[c.cur];
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_energy, 0, sizeof(unsigned long long), c.stream));
-  k_energy<<<c.num_sms * 4, kEThreads, energy_smem(), c.stream>>>(
-      c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.k, P.d, csolf, F.n, F.nk, c.overlap, c.nbdt,
+  k_energy<<<c.num_sms * 6, kEThreads, energy_smem(), c.stream>>>(
+      c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.Npad, P.k, P.d, csolf, F.n, F.nk,
+      reinterpret_cast<const float4*>(c.ovgr), c.nbdt,
       c.ncol, c.spacing_f, c.x0, c.h, F.h_knots[2], F.h_knots[F.nk - 3], csolc, C.knots_d, C.nk, C.n, c.weight,
       c.chunk, c.e_items);
   VLB_LAUNCHED(c);
