@@ -354,13 +354,17 @@ __global__ void k_coarse_from_fixed(float* __restrict__ rho, const unsigned long
 // the 32 columns, column (l + j) mod 32 at step j (distinct banks across the
 // lanes), and adds them to the grid.  Particles whose left point falls outside the window
 // (cells clamped at the edge of the fine grid) add their corners with
-// atomics directly.  Contributions carry charge / (wx wy wz)
+// atomics directly.  The run's particles are contiguous in slot order; the
+// warp walks them an iteration (32 particles of one item) at a time, reading
+// each item's slots from the sort's item records, with the loads of the next
+// kCicAhead iterations in flight.  Contributions carry charge / (wx wy wz)
 // (src/devicemesh.jl:104); the walk is the reference's
 // (src/kernels.jl:1083-1273) with the scatter grouped by cell.  With `fixed`
 // the additions go to an int64 grid in fixed point (scale 2^40): the runs
 // are fixed by the sort and each window's sums are taken in a fixed order,
 // so the grid does not depend on which warp takes which run.
 constexpr int kCicClaim = 8;
+constexpr int kCicAhead = 2;  // iterations whose loads are in flight ahead of the additions
 constexpr int kCicRow = 32;  // window row: entry e, lane l at e * 32 + l
 constexpr int kCicWarps = kCicThreads / 32;
 
@@ -452,12 +456,17 @@ __device__ __forceinline__ void cic_flush(float* win, int lane, const CicWin& W,
   __syncwarp();
 }
 
+// The k and delta of one lane's particle of an iteration.
+struct CicLoad {
+  int k[3];
+  float d[3];
+};
+
 __global__ void __launch_bounds__(kCicThreads, 3) k_deposit_cic(
-    const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds,
-    const int32_t* __restrict__ chunk_start, const int32_t* __restrict__ item_cell, DeviceScalars* dsc, int nk,
-    int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ gt_g, int ng,
-    float lx0, float linvw, const int32_t* __restrict__ cells_g, int ncells, const float* __restrict__ dl_g,
-    float x0f, float hf, float charge, float* rho, unsigned long long* fixed, int chunk) {
+    const int4* __restrict__ item_rec, DeviceScalars* dsc, int64_t Npad, const int32_t* __restrict__ k,
+    const float* __restrict__ d, const float* __restrict__ gt_g, int ng, float lx0, float linvw,
+    const int32_t* __restrict__ cells_g, int ncells, const float* __restrict__ dl_g, float x0f, float hf,
+    float charge, float* rho, unsigned long long* fixed) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* wins = reinterpret_cast<float*>(smem);                 // [kCicWarps][kCicW3][kCicRow]
   float* gt = wins + kCicWarps * kCicW3 * kCicRow;              // [ng]
@@ -486,44 +495,54 @@ __global__ void __launch_bounds__(kCicThreads, 3) k_deposit_cic(
     i0 = __shfl_sync(0xffffffffu, i0, 0);
     if (i0 >= nitems) break;
     const int i1 = min(i0 + kCicClaim, nitems);
-    int gcur = -1;
-    CicWin W;
-    for (int item = i0; item < i1; ++item) {
-      const int g = item_cell[item];
-      if (g != gcur) {
-        if (gcur >= 0) cic_flush(win, lane, W, n, rho, fixed);
-        int kx, ky, kz;
-        cell_knots((uint32_t)occupied[g], nk, kx, ky, kz);
-        cic_cell_window(W, kx, ky, kz, gt, igap, ng, lx0, linvw, cells, ncells, x0f, hf);
-        gcur = g;
-      }
-      const int s0 = bounds[g] + (item - chunk_start[g]) * chunk;
-      const int s1 = min(s0 + chunk, bounds[g + 1]);
-      // the next particle's loads are in flight while this one is added
-      int nk3[3] = {0, 0, 0};
-      float nd3[3] = {0.f, 0.f, 0.f};
-      if (s0 + lane < s1) {
+    // The run is a sequence of iterations (an item's particles s0 + 32 j + lane);
+    // the loads run kCicAhead iterations ahead of the additions, across the
+    // run's item boundaries, so that each warp keeps several rounds of k and
+    // delta in flight.
+    int4 rc = item_rec[i0];
+    int citem = i0, cs = rc.y;
+    int pitem = i0, ps = rc.y, pe = rc.z;
+    CicLoad q[kCicAhead];
+    auto fetch = [&](CicLoad& L) {
+      if (pitem < i1 && ps + lane < pe) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          nk3[a] = k[a * Npad + s0 + lane];
-          nd3[a] = d[a * Npad + s0 + lane];
+          L.k[a] = k[a * Npad + ps + lane];
+          L.d[a] = d[a * Npad + ps + lane];
         }
       }
-      for (int s = s0 + lane; s < s1; s += 32) {
-        const int ck[3] = {nk3[0], nk3[1], nk3[2]};
-        const float cd[3] = {nd3[0], nd3[1], nd3[2]};
-        if (s + 32 < s1) {
+      ps += 32;
+      if (ps >= pe && ++pitem < i1) {
+        const int4 r = item_rec[pitem];
+        ps = r.y;
+        pe = r.z;
+      }
+    };
 #pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            nk3[a] = k[a * Npad + s + 32];
-            nd3[a] = d[a * Npad + s + 32];
-          }
-        }
-        cic_particle(W, ck[0], ck[1], ck[2], cd[0], cd[1], cd[2], x0f, hf, charge, gt, igap, idl, ng, lx0, linvw,
-                     cells, ncells, col, rho, fixed);
+    for (int t = 0; t < kCicAhead; ++t) fetch(q[t]);
+    int gcode = -1;
+    CicWin W;
+    while (citem < i1) {
+      if (rc.x != gcode) {
+        if (gcode >= 0) cic_flush(win, lane, W, n, rho, fixed);
+        cic_cell_window(W, rc.w & 1023, (rc.w >> 10) & 1023, rc.w >> 20, gt, igap, ng, lx0, linvw, cells, ncells,
+                        x0f, hf);
+        gcode = rc.x;
+      }
+      const CicLoad cur = q[0];
+#pragma unroll
+      for (int t = 0; t + 1 < kCicAhead; ++t) q[t] = q[t + 1];
+      fetch(q[kCicAhead - 1]);
+      if (cs + lane < rc.z)
+        cic_particle(W, cur.k[0], cur.k[1], cur.k[2], cur.d[0], cur.d[1], cur.d[2], x0f, hf, charge, gt, igap, idl,
+                     ng, lx0, linvw, cells, ncells, col, rho, fixed);
+      cs += 32;
+      if (cs >= rc.z && ++citem < i1) {
+        rc = item_rec[citem];
+        cs = rc.y;
       }
     }
-    if (gcur >= 0) cic_flush(win, lane, W, n, rho, fixed);
+    if (gcode >= 0) cic_flush(win, lane, W, n, rho, fixed);
   }
 }
 
@@ -617,9 +636,8 @@ void launch_deposit_coarse(Ctx& c, double charge, int mode) {
     VLB_CUDA(cudaMemsetAsync(C.rho, 0, tot * sizeof(float), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_cic, 0, sizeof(unsigned long long), c.stream));
   k_deposit_cic<<<c.num_sms * c.cic_cps, kCicThreads, cic_smem(c), c.stream>>>(
-      c.occupied, c.bounds, c.chunk_start, c.item_cell, c.dsc, c.fine.nk, c.Npad, P.k, P.d, C.colloc, C.n,
-      C.loc_x0, C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen, c.x0f, c.hf, (float)charge, C.rho,
-      fixed ? c.rho_fixed_c : nullptr, c.chunk);
+      c.item_rec, c.dsc, c.Npad, P.k, P.d, C.colloc, C.n, C.loc_x0, C.loc_invw, C.loc_cells, C.loc_ncell, C.dlen,
+      c.x0f, c.hf, (float)charge, C.rho, fixed ? c.rho_fixed_c : nullptr);
   VLB_LAUNCHED(c);
 }
 
