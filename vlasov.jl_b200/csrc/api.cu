@@ -167,7 +167,7 @@ void destroy_ctx(Ctx* c) {
   }
   dfree(c->force);
   dfree(c->csol_rows);
-  dfree(c->keys); dfree(c->keys_alt); dfree(c->skeys); dfree(c->perm); dfree(c->vals_alt);
+  dfree(c->keys); dfree(c->keys_alt); dfree(c->skeys); dfree(c->perm); dfree(c->cols); dfree(c->vals_alt);
   dfree(c->radix_table); dfree(c->counts); dfree(c->cell_off);
   for (int p = 0; p < 2; ++p) { dfree(c->occ_buf[p]); dfree(c->bnd_buf[p]); dfree(c->cidx_buf[p]); }
   dfree(c->dir_cnt); dfree(c->dir_base);
@@ -473,6 +473,8 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     c->keys_alt = dalloc<uint32_t>(N);
     c->skeys = dalloc<uint32_t>(N);
     c->perm = dalloc<uint32_t>(N);
+    c->cols = dalloc<uint32_t>(N);
+    c->cols_packed = c->ncol <= 1024;
     c->vals_alt = dalloc<uint32_t>(N);
     const int64_t ntiles = (N + 4095) / 4096;
     c->radix_table_size = 1024 * ntiles;

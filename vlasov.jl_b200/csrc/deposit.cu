@@ -36,20 +36,23 @@ constexpr double kFixedInv = 1.0 / 1099511627776.0;
 
 // One CTA per occupied cell at a time (dynamic counter); a cell of the
 // headline cloud holds about a thousand particles.  The cell's particles go
-// in stages of 512: each thread computes the three table columns and the
-// window test of two particles into one int4 each of a double-buffered stage
-// in shared memory while the CTA adds the previous stage, and the k/delta
-// loads of the stage after are in flight meanwhile; one CTA barrier per
-// stage (the columns stored as the offsets of their node rows).  Thread
+// in stages of 512: each thread puts the three table columns and the window
+// test of two particles into one int4 each of a double-buffered stage in
+// shared memory while the CTA adds the previous stage, and the loads of the
+// stage after are in flight meanwhile; one CTA barrier per stage (the
+// columns stored as the offsets of their node rows).  With kPacked the
+// columns and the window flag come packed from the sort's record move (four
+// bytes a particle); otherwise the thread computes them from k and delta.  Thread
 // (lane, q) owns the z row q of its lane's 8^3 sum: 64 float32
 // accumulators as float2 pairs along x, so one packed FMA covers two outputs.
 // At the cell's end the lane partials are summed over the lanes in a fixed
 // order (in shared memory that the stages used) and added to the grid.
+template <bool kPacked>
 __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
     const int32_t* __restrict__ occupied, const int32_t* __restrict__ bounds, DeviceScalars* dsc,
-    int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const float* __restrict__ nodes,
-    int nk, int n, float x0, float h, float lo, float hi, float spacing, int nbdt, int ncol, float* rho,
-    unsigned long long* rho_fixed, int mode) {
+    int64_t Npad, const int32_t* __restrict__ k, const float* __restrict__ d, const uint32_t* __restrict__ cols,
+    const float* __restrict__ nodes, int nk, int n, float x0, float h, float lo, float hi, float spacing, int nbdt,
+    int ncol, float* rho, unsigned long long* rho_fixed, int mode) {
   extern __shared__ __align__(16) unsigned char smem[];
   float* nodes_s = reinterpret_cast<float*>(smem);                      // [ncol][8]
   unsigned char* work = smem + (((size_t)ncol * 8 * sizeof(float) + 15) & ~(size_t)15);
@@ -64,9 +67,20 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
   const int pl = tid / 8, q = tid % 8;
   int my_nout = 0;
   __syncthreads();
-  // the columns of particle s (inside the cell) into the stage slot
+  // the columns of particle s (inside the cell) into the stage slot: from
+  // the sort's packed columns (kPacked, in kk[0]) or from k and delta
   auto stage_one = [&](int s, int sh, const int (&kk)[3], const float (&dd)[3], int4* slot) {
     if (s >= sh) return;
+    if (kPacked) {
+      uint32_t pc = (uint32_t)kk[0];
+      if (pc & kColsOutside) {
+        pc = 0;  // column 1 on every axis
+        ++my_nout;
+      }
+      // the node rows' offsets in the shared table (8 floats a column)
+      *slot = make_int4((int)(pc & 1023u) * 8, (int)((pc >> 10) & 1023u) * 8, (int)((pc >> 20) & 1023u) * 8, 0);
+      return;
+    }
     bool inside = true;
     int cc[3];
 #pragma unroll
@@ -81,6 +95,10 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
   };
   auto load_one = [&](int s, int sh, int (&kk)[3], float (&dd)[3]) {
     if (s >= sh) return;
+    if (kPacked) {
+      kk[0] = (int)cols[s];
+      return;
+    }
 #pragma unroll
     for (int ax = 0; ax < 3; ++ax) {
       kk[ax] = k[ax * Npad + s];
@@ -610,11 +628,14 @@ size_t deposit_fine_smem(const Ctx& c) {
 size_t cic_smem(const Ctx& c);
 
 void deposit_setup(Ctx& c) {
-  VLB_CUDA(cudaFuncSetAttribute(k_deposit_fine, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  VLB_CUDA(cudaFuncSetAttribute(k_deposit_fine<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)deposit_fine_smem(c)));
+  VLB_CUDA(cudaFuncSetAttribute(k_deposit_fine<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)deposit_fine_smem(c)));
   VLB_CUDA(cudaFuncSetAttribute(k_deposit_cic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cic_smem(c)));
   // three CTAs of each per SM need the largest shared-memory split
-  VLB_CUDA(cudaFuncSetAttribute(k_deposit_fine, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  VLB_CUDA(cudaFuncSetAttribute(k_deposit_fine<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  VLB_CUDA(cudaFuncSetAttribute(k_deposit_fine<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   VLB_CUDA(cudaFuncSetAttribute(k_deposit_cic, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
 }
 
@@ -633,9 +654,14 @@ void launch_deposit_fine_raw(Ctx& c, int mode) {
   VLB_CUDA(cudaMemsetAsync(&c.dsc->work_deposit, 0, sizeof(unsigned long long), c.stream));
   VLB_CUDA(cudaMemsetAsync(&c.dsc->nout, 0, sizeof(int32_t), c.stream));
   const int grid = c.num_sms * 2;
-  k_deposit_fine<<<grid, kDepThreads, deposit_fine_smem(c), c.stream>>>(
-      c.occupied, c.bounds, c.dsc, c.Npad, P.k, P.d, c.nodes, F.nk, F.n, c.x0f, c.hf, c.lo_f, c.hi_f, c.spacing_f,
-      c.nbdt, c.ncol, F.rho, c.rho_fixed, mode);
+  if (c.cols_packed)
+    k_deposit_fine<true><<<grid, kDepThreads, deposit_fine_smem(c), c.stream>>>(
+        c.occupied, c.bounds, c.dsc, c.Npad, P.k, P.d, c.cols, c.nodes, F.nk, F.n, c.x0f, c.hf, c.lo_f, c.hi_f,
+        c.spacing_f, c.nbdt, c.ncol, F.rho, c.rho_fixed, mode);
+  else
+    k_deposit_fine<false><<<grid, kDepThreads, deposit_fine_smem(c), c.stream>>>(
+        c.occupied, c.bounds, c.dsc, c.Npad, P.k, P.d, c.cols, c.nodes, F.nk, F.n, c.x0f, c.hf, c.lo_f, c.hi_f,
+        c.spacing_f, c.nbdt, c.ncol, F.rho, c.rho_fixed, mode);
   VLB_LAUNCHED(c);
   k_publish_nout<<<1, 1, 0, c.stream>>>(c.dsc);
   VLB_LAUNCHED(c);

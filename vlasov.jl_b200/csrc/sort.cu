@@ -669,6 +669,14 @@ __global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __re
 }
 
 // ------------------------------------------------------------- the move
+// What the move needs to write each slot's packed deposit columns (cols null:
+// none).
+struct DepCols {
+  uint32_t* cols = nullptr;
+  float x0 = 0, h = 0, lo = 0, hi = 0, spacing = 0;
+  int nbdt = 0, ncol = 0;
+};
+
 // Moves the records into slot order: dst[s] = src[perm[s]], the position
 // arrays (k, delta) when kPos, the previous positions (pk, pdelta) when
 // kPrev.  Four consecutive slots per thread: one 16-byte load of their
@@ -676,13 +684,17 @@ __global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __re
 // store per component array (Npad is a multiple of 64).  Reads follow the
 // permutation of a nearly sorted cloud, so they stay within a few pages.
 // A step whose push follows leaves (pk, pdelta) where they are: the push
-// reads them through the permutation and writes them in slot order.
+// reads them through the permutation and writes them in slot order.  With
+// dc.cols set the move also writes each slot's packed deposit columns and
+// window flag (deposit_cols of the moved k and delta), so that the fine
+// deposit reads four bytes a particle instead of 24.
 template <bool kPos, bool kPrev>
 __global__ void __launch_bounds__(256) k_gather_records(int64_t N, int64_t Npad, const uint32_t* __restrict__ perm,
                                                         const int32_t* __restrict__ k0, const float* __restrict__ d0,
                                                         const int32_t* __restrict__ pk0, const float* __restrict__ pd0,
                                                         int32_t* __restrict__ k1, float* __restrict__ d1,
-                                                        int32_t* __restrict__ pk1, float* __restrict__ pd1) {
+                                                        int32_t* __restrict__ pk1, float* __restrict__ pd1,
+                                                        const DepCols dc = DepCols{}) {
   const int64_t nq = N / 4;
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t s = 4 * q;
@@ -703,6 +715,14 @@ __global__ void __launch_bounds__(256) k_gather_records(int64_t N, int64_t Npad,
           pdv[c][u] = __ldg(pd0 + c * Npad + i[u]);
         }
       }
+    if (kPos && dc.cols) {
+      uint32_t cv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        cv[u] = deposit_cols(kv[0][u], kv[1][u], kv[2][u], dv[0][u], dv[1][u], dv[2][u], dc.x0, dc.h, dc.lo, dc.hi,
+                             dc.spacing, dc.nbdt, dc.ncol);
+      *reinterpret_cast<uint4*>(dc.cols + s) = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+    }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       if (kPos) {
@@ -719,6 +739,9 @@ __global__ void __launch_bounds__(256) k_gather_records(int64_t N, int64_t Npad,
   for (int64_t s = 4 * nq + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < N;
        s += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = perm[s];
+    if (kPos && dc.cols)
+      dc.cols[s] = deposit_cols(k0[i], k0[Npad + i], k0[2 * Npad + i], d0[i], d0[Npad + i], d0[2 * Npad + i], dc.x0,
+                                dc.h, dc.lo, dc.hi, dc.spacing, dc.nbdt, dc.ncol);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       if (kPos) {
@@ -844,12 +867,23 @@ void launch_sort(Ctx& c, bool defer_prev) {
   // step more (1.959 against 1.900 ms at 8e6) than the gated launches do.
   radix_passes(c, c.stream, gate);
   const int mgrid = grid_for(c, (N + 3) / 4, 256, c.move_cps);
+  DepCols dc;
+  if (c.cols_packed) {
+    dc.cols = c.cols;
+    dc.x0 = c.x0f;
+    dc.h = c.hf;
+    dc.lo = c.lo_f;
+    dc.hi = c.hi_f;
+    dc.spacing = c.spacing_f;
+    dc.nbdt = c.nbdt;
+    dc.ncol = c.ncol;
+  }
   if (defer_prev)
     k_gather_records<true, false><<<mgrid, 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
-                                                               Q.pk, Q.pd);
+                                                               Q.pk, Q.pd, dc);
   else
     k_gather_records<true, true><<<mgrid, 256, 0, c.stream>>>(N, c.Npad, c.perm, P.k, P.d, P.pk, P.pd, Q.k, Q.d,
-                                                              Q.pk, Q.pd);
+                                                              Q.pk, Q.pd, dc);
   VLB_LAUNCHED(c);
   c.prev_deferred = defer_prev;
   c.cur ^= 1;

@@ -141,6 +141,11 @@ struct Ctx {
   uint32_t* keys_alt = nullptr;  // [N]
   uint32_t* skeys = nullptr;     // [N] sorted cell keys (slot order)
   uint32_t* perm = nullptr;      // [N]
+  // [N] each slot's fine-deposit table columns (10 bits each, minus one) and
+  // bit 30 set outside the deposit window, written by the sort's record move
+  // when ncol <= 1024 (cols_packed)
+  uint32_t* cols = nullptr;
+  bool cols_packed = false;
   uint32_t* vals_alt = nullptr;  // [N]
   uint32_t* radix_table = nullptr;
   int64_t radix_table_size = 0;
@@ -329,6 +334,26 @@ __device__ __forceinline__ int table_column(float d, float spacing, int nbdt, in
 }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+// The fine deposit's table columns and window test of one particle
+// (src/kernels.jl:754-779), packed: column - 1 in 10 bits per axis (ncol <=
+// 1024) and bit 30 set when the particle lies outside the window (the
+// deposit then takes column 1 on every axis, as the reference does).
+constexpr uint32_t kColsOutside = 1u << 30;
+__device__ __forceinline__ uint32_t deposit_cols(int k0, int k1, int k2, float d0, float d1, float d2, float x0,
+                                                 float h, float lo, float hi, float spacing, int nbdt, int ncol) {
+  const int kk[3] = {k0, k1, k2};
+  const float dd[3] = {d0, d1, d2};
+  bool inside = true;
+  uint32_t packed = 0;
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    const float p = fadd(fadd(x0, fmul((float)(kk[ax] - 1), h)), dd[ax]);
+    inside = inside && (lo <= p) && (p <= hi);
+    packed |= (uint32_t)(table_column(dd[ax], spacing, nbdt, ncol) - 1) << (10 * ax);
+  }
+  return inside ? packed : (packed | kColsOutside);
+}
 
 // 0-based cell of a clamped knot triple
 __device__ __forceinline__ uint32_t cell_key(int kx, int ky, int kz, int nk) {
