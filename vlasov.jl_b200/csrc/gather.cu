@@ -12,7 +12,8 @@
 // against the reference's order, which changes rounding only.  Two forms:
 // k_field_tc (the default) computes the sums over y of a whole item as
 // 3xTF32 GEMMs on the tensor cores and finishes each particle on the CUDA
-// cores; k_field computes everything with FP32 FMAs, one warp per item.  The projectile's Gaussian force
+// cores (its table columns read from the sort's packed columns when the
+// sort wrote them, the same table_column values the deposit uses); k_field computes everything with FP32 FMAs, one warp per item.  The projectile's Gaussian force
 // (src/projectile.jl:95-108) is evaluated per particle at the position
 // rebuilt from the *cell's* (clamped) knots, as the reference does, its
 // reaction subtracted, and the four reaction sums reduced per CTA in float64.
@@ -559,7 +560,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     const int4* __restrict__ items, DeviceScalars* dsc, int64_t Npad,
     const float* __restrict__ d, const __grid_constant__ CUtensorMap csol_map, int n, int nk,
     const float4* __restrict__ ovgr, int nbdt, int ncol, float spacing, float x0, float h, double w,
-    float* __restrict__ force, int chunk, double* __restrict__ red_items) {
+    float* __restrict__ force, int chunk, double* __restrict__ red_items, const uint32_t* __restrict__ cols) {
   extern __shared__ __align__(1024) unsigned char ftsm[];
   __shared__ double red[2][4][4];
   uint64_t* bars = reinterpret_cast<uint64_t*>(ftsm + kFtBars);
@@ -594,18 +595,21 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
                          | ((unsigned)(kFtN >> 3) << 17)     // N
                          | ((unsigned)(kFtRows >> 4) << 24); // M
 
-  auto load_delta = [&](const FtItem& it, float (&dd)[3]) {
+  // delta of the particle of item `it`, and in dd[3] the sort's packed
+  // table columns when they were written
+  auto load_delta = [&](const FtItem& it, float (&dd)[4]) {
     if (!it.has) return;
     const int s = it.s0 + tid;
     if (s < it.s1) {
       dd[0] = d[s];
       dd[1] = d[Npad + s];
       dd[2] = d[2 * Npad + s];
+      if (cols) dd[3] = __uint_as_float(cols[s]);
     }
   };
 
   // the loads of a particle of item `it` whose delta is dd: its six tables
-  auto load_part = [&](const FtItem& it, const float (&dd)[3], FtPart& p) {
+  auto load_part = [&](const FtItem& it, const float (&dd)[4], FtPart& p) {
     p.valid = false;
     p.s = 0;
     if (!it.has) return;
@@ -616,9 +620,17 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     p.dx = dd[0];
     p.dy = dd[1];
     p.dz = dd[2];
-    const int cx = table_column(p.dx, spacing, nbdt, ncol);
-    const int cy = table_column(p.dy, spacing, nbdt, ncol);
-    const int cz = table_column(p.dz, spacing, nbdt, ncol);
+    int cx, cy, cz;
+    if (cols) {
+      const uint32_t pc = __float_as_uint(dd[3]);
+      cx = (int)(pc & 1023u) + 1;
+      cy = (int)((pc >> 10) & 1023u) + 1;
+      cz = (int)((pc >> 20) & 1023u) + 1;
+    } else {
+      cx = table_column(p.dx, spacing, nbdt, ncol);
+      cy = table_column(p.dy, spacing, nbdt, ncol);
+      cz = table_column(p.dz, spacing, nbdt, ncol);
+    }
     ft_load_cols(ovgr, cy, p.oy, p.gy);
     ft_load_cols(ovgr, cx, p.ox, p.gx);
     ft_load_cols(ovgr, cz, p.oz, p.gz);
@@ -656,7 +668,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
   FtItem cur = resolve(item_at(0));
   FtItem nxt = resolve(item_at(1));
   FtItem after = resolve(item_at(2));
-  float dc[3] = {0.f, 0.f, 0.f}, dn[3] = {0.f, 0.f, 0.f};
+  float dc[4] = {0.f, 0.f, 0.f, 0.f}, dn[4] = {0.f, 0.f, 0.f, 0.f};
   load_delta(cur, dc);
   load_delta(nxt, dn);
   int staged = -1;                 // cell code of the stencil in B
@@ -695,7 +707,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     const int nb = b ^ 1;
     // ---- loads: delta of t+2, cell data of t+3, item_cell of t+4, the
     // tables of t+1 and, when needed, its stencil
-    float d2[3] = {0.f, 0.f, 0.f};
+    float d2[4] = {0.f, 0.f, 0.f, 0.f};
     load_delta(after, d2);
     const FtRaw raw3 = load_item(item_at(t + 3));
     FtPart pn;
@@ -784,7 +796,7 @@ __global__ void __launch_bounds__(kFtThreads, 2) k_field_tc(
     after = ft_derive(raw3, n);
     pc = pn;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) dn[k] = d2[k];
+    for (int k = 0; k < 4; ++k) dn[k] = d2[k];
     b = nb;
   }
 
@@ -1223,7 +1235,7 @@ void launch_forces(Ctx& c) {
     k_field_tc<<<2 * c.num_sms, kFtThreads, kFtSmem, c.stream>>>(
         c.item_rec, c.dsc, c.Npad, P.d, c.csol_map, F.n, F.nk,
         reinterpret_cast<const float4*>(c.ovgr), c.nbdt, c.ncol, c.spacing_f, c.x0f, c.hf, c.weight, c.force,
-        c.chunk, c.red_items);
+        c.chunk, c.red_items, c.cols_packed ? c.cols : nullptr);
   } else {
     VLB_CUDA(cudaMemsetAsync(&c.dsc->work_gather, 0, sizeof(unsigned long long), c.stream));
     k_field<<<c.num_sms * c.field_cps, kGThreads, 0, c.stream>>>(c.occupied, c.bounds, c.chunk_start, c.item_cell,
