@@ -29,18 +29,18 @@ namespace {
 
 constexpr int kDepThreads = 256;
 constexpr int kDepLanes = 32;      // particle lanes per CTA, 8 threads (one z row each) per lane
-constexpr int kDepStage = 512;     // particles whose columns are staged at once (two per thread)
+constexpr int kDepStageMax = 1024;  // particles whose columns are staged at once: 1024 packed, 512 computed
 constexpr int kDepRow = 68;        // floats per (lane, z row) in the reduction buffer: 64 + 4 against bank conflicts
 constexpr double kFixedScale = 1099511627776.0;        // 2^40
 constexpr double kFixedInv = 1.0 / 1099511627776.0;
 
 // One CTA per occupied cell at a time (dynamic counter); a cell of the
 // headline cloud holds about a thousand particles.  The cell's particles go
-// in stages of 512: each thread puts the three table columns and the window
-// test of two particles into one int4 each of a double-buffered stage in
-// shared memory while the CTA adds the previous stage, and the loads of the
-// stage after are in flight meanwhile; one CTA barrier per stage (the
-// columns stored as the offsets of their node rows).  With kPacked the
+// in stages of 1024 (512 when computed): each thread puts the three table
+// columns and the window test of four (two) particles into one int4 each of
+// a double-buffered stage in shared memory while the CTA adds the previous
+// stage, and the loads of the stage after are in flight meanwhile; one CTA
+// barrier per stage (the columns stored as the offsets of their node rows).  With kPacked the
 // columns and the window flag come packed from the sort's record move (four
 // bytes a particle); otherwise the thread computes them from k and delta.  Thread
 // (lane, q) owns the z row q of its lane's 8^3 sum: 64 float32
@@ -56,6 +56,8 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
   extern __shared__ __align__(16) unsigned char smem[];
   float* nodes_s = reinterpret_cast<float*>(smem);                      // [ncol][8]
   unsigned char* work = smem + (((size_t)ncol * 8 * sizeof(float) + 15) & ~(size_t)15);
+  constexpr int kPer = kPacked ? 4 : 2;  // particles a thread stages
+  constexpr int kDepStage = kPer * kDepThreads;
   int4* cols_s = reinterpret_cast<int4*>(work);                         // [2][kDepStage]
   float* red_s = reinterpret_cast<float*>(work);                        // [kDepLanes][8][kDepRow], after the stages
   __shared__ int s_g, s_q;
@@ -117,17 +119,26 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
   int sl = 0, sh = 0, sln = 0, shn = 0;
   if (g < nocc) { sl = bounds[g]; sh = bounds[g + 1]; }
   if (gn < nocc) { sln = bounds[gn]; shn = bounds[gn + 1]; }
-  int ka[3] = {0, 0, 0}, kb[3] = {0, 0, 0};
-  float da[3] = {0.f, 0.f, 0.f}, db[3] = {0.f, 0.f, 0.f};
-  if (g < nocc) {
-    load_one(sl + tid, sh, ka, da);
-    load_one(sl + kDepThreads + tid, sh, kb, db);
-  }
+  int kr[kPer][3];
+  float dr[kPer][3];
+#pragma unroll
+  for (int u = 0; u < kPer; ++u)
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+      kr[u][ax] = 0;
+      dr[u][ax] = 0.f;
+    }
   // the loads of a cell's first stage, or of the next stage of this cell
   auto load_stage = [&](int base, int end) {
-    load_one(base + tid, end, ka, da);
-    load_one(base + kDepThreads + tid, end, kb, db);
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) load_one(base + u * kDepThreads + tid, end, kr[u], dr[u]);
   };
+  // the loaded stage's columns into a stage buffer
+  auto put_stage = [&](int base, int end, int4* dst) {
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) stage_one(base + u * kDepThreads + tid, end, kr[u], dr[u], &dst[u * kDepThreads + tid]);
+  };
+  if (g < nocc) load_stage(sl, sh);
   while (g < nocc) {
     __syncthreads();  // every thread holds gn: the queue slot is free
     if (tid == 0) s_q = (int)atomicAdd(&dsc->work_deposit, 1ull);
@@ -139,8 +150,7 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
 #pragma unroll
     for (int a = 0; a < 32; ++a) acc[a] = make_float2(0.f, 0.f);
     // stage 0 from the registers, then the loads of the next stage to come
-    stage_one(sl + tid, sh, ka, da, &cols_s[tid]);
-    stage_one(sl + kDepThreads + tid, sh, kb, db, &cols_s[kDepThreads + tid]);
+    put_stage(sl, sh, cols_s);
     if (sl + kDepStage < sh)
       load_stage(sl + kDepStage, sh);
     else if (gn < nocc)
@@ -155,9 +165,7 @@ __global__ void __launch_bounds__(kDepThreads, 2) k_deposit_fine(
       // barrier that ended the previous stage), and the loads of the one after
       const int nb = base + kDepStage;
       if (nb < sh) {
-        int4* nxt = cols_s + (buf ^ 1) * kDepStage;
-        stage_one(nb + tid, sh, ka, da, &nxt[tid]);
-        stage_one(nb + kDepThreads + tid, sh, kb, db, &nxt[kDepThreads + tid]);
+        put_stage(nb, sh, cols_s + (buf ^ 1) * kDepStage);
         if (nb + kDepStage < sh)
           load_stage(nb + kDepStage, sh);
         else if (gn < nocc)
@@ -620,7 +628,7 @@ __global__ void __launch_bounds__(kCicThreads, 3) k_deposit_cic(
 }  // namespace
 
 size_t deposit_fine_smem(const Ctx& c) {
-  const size_t stages = (size_t)2 * kDepStage * sizeof(int4);
+  const size_t stages = (size_t)2 * kDepStageMax * sizeof(int4);
   const size_t red = (size_t)kDepLanes * 8 * kDepRow * sizeof(float);
   return (((size_t)c.ncol * 8 * sizeof(float) + 15) & ~(size_t)15) + (stages > red ? stages : red);
 }
