@@ -172,8 +172,8 @@ void destroy_ctx(Ctx* c) {
   for (int p = 0; p < 2; ++p) { dfree(c->occ_buf[p]); dfree(c->bnd_buf[p]); dfree(c->cidx_buf[p]); }
   dfree(c->dir_cnt); dfree(c->dir_base);
   dfree(c->outlist);
-  for (int p = 0; p < 2; ++p) { dfree(c->cstart_buf[p]); dfree(c->item_buf[p]); }
-  dfree(c->item_dir); dfree(c->item_rec); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
+  for (int p = 0; p < 2; ++p) { dfree(c->cstart_buf[p]); dfree(c->item_buf[p]); dfree(c->rec_buf[p]); }
+  dfree(c->item_dir); dfree(c->scan_status); dfree(c->rho_fixed); dfree(c->partials);
   dfree(c->rho_fixed_c); dfree(c->red_items); dfree(c->red_tail); dfree(c->red_blocks); dfree(c->diag_part);
   dfree(c->e_items); dfree(c->e_blocks);
   for (auto& w : c->work) dfree(w);
@@ -262,6 +262,7 @@ void sync_sort_products(Ctx& c) {
   c.occupied = c.occ_buf[c.cur];
   c.bounds = c.bnd_buf[c.cur];
   c.item_cell = c.item_buf[c.cur];
+  c.item_rec = c.rec_buf[c.cur];
   c.chunk_start = c.cstart_buf[c.cur];
 }
 
@@ -498,11 +499,12 @@ int vlb_create(const vlb_config* cfg, vlb_ctx** out) {
     for (int p = 0; p < 2; ++p) {
       c->cstart_buf[p] = dalloc<int32_t>(c->ncell);
       c->item_buf[p] = dalloc<int32_t>(N / kMinChunk + c->ncell + 1);
+      c->rec_buf[p] = dalloc<int4>((size_t)N / kMinChunk + c->ncell + 1);
     }
     c->chunk_start = c->cstart_buf[0];
     c->item_cell = c->item_buf[0];
     c->item_dir = dalloc<int32_t>(((size_t)N / kMinChunk + c->ncell + 1) * 27);
-    c->item_rec = dalloc<int4>((size_t)N / kMinChunk + c->ncell + 1);
+    c->item_rec = c->rec_buf[0];
     const int64_t scan_tiles = std::max<int64_t>({(N + 4095) / 4096, (c->ncell + 4095) / 4096,
                                                   (c->radix_table_size + 4095) / 4096}) + 1;
     c->scan_status_size = 8 * scan_tiles;

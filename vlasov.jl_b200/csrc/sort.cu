@@ -516,26 +516,26 @@ constexpr int kNearThreads = 256;
 // one old cell, in slot order) spread the work evenly: A and C take one warp
 // per item, A2 one warp per old cell over its few items.
 
-// A: per item, the particles of each direction -> item_dir[item][27].
-__global__ void __launch_bounds__(kNearThreads) k_near_count(const int32_t* __restrict__ item_old,
-                                                            const int32_t* __restrict__ cstart_old,
-                                                            const int32_t* __restrict__ occ_old,
-                                                            const int32_t* __restrict__ bnd_old,
-                                                            DeviceScalars* dsc, int par_old, int chunk_old,
-                                                            const uint32_t* __restrict__ keys, int nk,
+// A: per item, the particles of each direction -> item_dir[item][27].  The
+// item's old cell code and slots come from the last sort's item records (one
+// load, the next item's in flight meanwhile).
+__global__ void __launch_bounds__(kNearThreads) k_near_count(const int4* __restrict__ rec_old, DeviceScalars* dsc,
+                                                            int par_old, const uint32_t* __restrict__ keys, int nk,
                                                             int32_t* __restrict__ item_dir) {
   __shared__ int32_t cnt[kNearThreads / 32][kDirs];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nitems = dsc->nitems_par[par_old];
   const int warps = gridDim.x * (kNearThreads / 32);
   bool far = false;
-  for (int item = blockIdx.x * (kNearThreads / 32) + w; item < nitems; item += warps) {
+  int item = blockIdx.x * (kNearThreads / 32) + w;
+  int4 rec = item < nitems ? rec_old[item] : make_int4(0, 0, 0, 0);
+  for (; item < nitems; item += warps) {
+    const int next = item + warps;
+    const int4 rnext = next < nitems ? rec_old[next] : make_int4(0, 0, 0, 0);
     if (lane < kDirs) cnt[w][lane] = 0;
     __syncwarp();
-    const int g = item_old[item];
-    const int64_t o = occ_old[g];
-    const int s0 = bnd_old[g] + (item - cstart_old[g]) * chunk_old;
-    const int s1 = min(s0 + chunk_old, bnd_old[g + 1]);
+    const int64_t o = rec.x;
+    const int s0 = rec.y, s1 = rec.z;
     for (int base = s0; base < s1; base += 32) {
       const int s = base + lane;
       const bool valid = s < s1;
@@ -550,6 +550,7 @@ __global__ void __launch_bounds__(kNearThreads) k_near_count(const int32_t* __re
     }
     if (lane < kDirs) item_dir[(size_t)item * kDirs + lane] = cnt[w][lane];
     __syncwarp();
+    rec = rnext;
   }
   if (__any_sync(0xffffffffu, far) && lane == 0) atomicOr(&dsc->sort_far, 1);
 }
@@ -627,11 +628,11 @@ __global__ void __launch_bounds__(kNearThreads) k_near_bases(const int32_t* __re
 
 // C: one warp per item, slots in order, a running rank per direction from
 // the group's first slot, the item's prefix within its cell: perm[rank] = s.
+// The item's old cell code and slots come from the last sort's item records,
+// its old occupied index from the item's cell (two independent loads).
 __global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __restrict__ item_old,
-                                                            const int32_t* __restrict__ cstart_old,
-                                                            const int32_t* __restrict__ occ_old,
-                                                            const int32_t* __restrict__ bnd_old,
-                                                            const DeviceScalars* dsc, int par_old, int chunk_old,
+                                                            const int4* __restrict__ rec_old,
+                                                            const DeviceScalars* dsc, int par_old,
                                                             const uint32_t* __restrict__ keys, int nk,
                                                             const int32_t* __restrict__ item_dir,
                                                             const int32_t* __restrict__ dir_base,
@@ -643,12 +644,12 @@ __global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __re
   const int warps = gridDim.x * (kNearThreads / 32);
   for (int item = blockIdx.x * (kNearThreads / 32) + w; item < nitems; item += warps) {
     const int g = item_old[item];
+    const int4 rec = rec_old[item];
     if (lane < kDirs)
       run[w][lane] = dir_base[(size_t)g * kDirs + lane] + item_dir[(size_t)item * kDirs + lane];
     __syncwarp();
-    const int64_t o = occ_old[g];
-    const int s0 = bnd_old[g] + (item - cstart_old[g]) * chunk_old;
-    const int s1 = min(s0 + chunk_old, bnd_old[g + 1]);
+    const int64_t o = rec.x;
+    const int s0 = rec.y, s1 = rec.z;
     for (int base = s0; base < s1; base += 32) {
       const int s = base + lane;
       const bool valid = s < s1;
@@ -822,6 +823,7 @@ void launch_sort(Ctx& c, bool defer_prev) {
   c.occupied = c.occ_buf[pn];
   c.bounds = c.bnd_buf[pn];
   c.item_cell = c.item_buf[pn];
+  c.item_rec = c.rec_buf[pn];
   c.chunk_start = c.cstart_buf[pn];
   c.chunk_par[pn] = c.chunk;
   VLB_CUDA(cudaMemsetAsync(c.scan_status, 0, c.scan_status_size * sizeof(unsigned long long), c.stream));
@@ -846,18 +848,15 @@ void launch_sort(Ctx& c, bool defer_prev) {
   const int32_t* gate = nullptr;
   if (near) {
     const int grid = c.num_sms * 8;
-    const int chunk_old = c.chunk_par[po];
-    k_near_count<<<grid, kNearThreads, 0, c.stream>>>(c.item_buf[po], c.cstart_buf[po], c.occ_buf[po],
-                                                      c.bnd_buf[po], c.dsc, po, chunk_old, c.keys, nk, c.item_dir);
+    k_near_count<<<grid, kNearThreads, 0, c.stream>>>(c.rec_buf[po], c.dsc, po, c.keys, nk, c.item_dir);
     VLB_LAUNCHED(c);
     k_near_prefix<<<grid, kNearThreads, 0, c.stream>>>(c.cstart_buf[po], c.dsc, po, c.item_dir, c.dir_cnt);
     VLB_LAUNCHED(c);
     k_near_bases<<<grid, kNearThreads, 0, c.stream>>>(c.occupied, c.bounds, c.occ_buf[po], c.cidx_buf[po], c.dsc,
                                                       po, c.ncell, nk, c.dir_cnt, c.dir_base);
     VLB_LAUNCHED(c);
-    k_near_place<<<grid, kNearThreads, 0, c.stream>>>(c.item_buf[po], c.cstart_buf[po], c.occ_buf[po],
-                                                      c.bnd_buf[po], c.dsc, po, chunk_old, c.keys, nk, c.item_dir,
-                                                      c.dir_base, c.perm);
+    k_near_place<<<grid, kNearThreads, 0, c.stream>>>(c.item_buf[po], c.rec_buf[po], c.dsc, po, c.keys, nk,
+                                                      c.item_dir, c.dir_base, c.perm);
     VLB_LAUNCHED(c);
     gate = &c.dsc->sort_far;  // the radix passes below run only if that path gave up
   }

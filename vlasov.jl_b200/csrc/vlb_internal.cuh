@@ -170,6 +170,8 @@ struct Ctx {
   int32_t* chunk_start = nullptr;  // [ncell] first chunk of occupied cell g (current parity's)
   int32_t* item_cell = nullptr;    // [N / kMinChunk + ncell] occupied cell of each chunk (current parity's)
   int4* item_rec = nullptr;        // [N / kMinChunk + ncell] each chunk's cell code, slots and packed knots
+                                   // (current parity's)
+  int4* rec_buf[2] = {nullptr, nullptr};
   int32_t* cstart_buf[2] = {nullptr, nullptr};
   int32_t* item_buf[2] = {nullptr, nullptr};
   int chunk_par[2] = {kChunk, kChunk};  // the chunk each parity's work items were cut with
