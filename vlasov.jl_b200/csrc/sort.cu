@@ -511,6 +511,7 @@ __device__ __forceinline__ int64_t direction_offset(int d, int nk) {
 
 constexpr int kDirs = 27;
 constexpr int kNearThreads = 256;
+constexpr int kNearKeys = 4;  // 32-slot rounds whose keys a warp loads at once (a work item of 128)
 
 // The work items of the last sort (runs of at most chunk_old particles of
 // one old cell, in slot order) spread the work evenly: A and C take one warp
@@ -536,17 +537,27 @@ __global__ void __launch_bounds__(kNearThreads) k_near_count(const int4* __restr
     __syncwarp();
     const int64_t o = rec.x;
     const int s0 = rec.y, s1 = rec.z;
-    for (int base = s0; base < s1; base += 32) {
-      const int s = base + lane;
-      const bool valid = s < s1;
-      const unsigned m = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        const int d = direction_of((int64_t)keys[s] - o, nk);
-        far |= d < 0;
-        const unsigned peers = __match_any_sync(m, d < 0 ? kDirs : d);
-        if (d >= 0 && lane == __ffs(peers) - 1) cnt[w][d] += __popc(peers);
+    for (int base = s0; base < s1; base += 32 * kNearKeys) {
+      uint32_t kv[kNearKeys];  // the keys of up to 32 kNearKeys slots, all loads in flight
+#pragma unroll
+      for (int u = 0; u < kNearKeys; ++u) {
+        const int s = base + 32 * u + lane;
+        kv[u] = s < s1 ? keys[s] : 0u;
       }
-      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < kNearKeys; ++u) {
+        const int s = base + 32 * u + lane;
+        const bool valid = s < s1;
+        const unsigned m = __ballot_sync(0xffffffffu, valid);
+        if (m == 0) break;
+        if (valid) {
+          const int d = direction_of((int64_t)kv[u] - o, nk);
+          far |= d < 0;
+          const unsigned peers = __match_any_sync(m, d < 0 ? kDirs : d);
+          if (d >= 0 && lane == __ffs(peers) - 1) cnt[w][d] += __popc(peers);
+        }
+        __syncwarp();
+      }
     }
     if (lane < kDirs) item_dir[(size_t)item * kDirs + lane] = cnt[w][lane];
     __syncwarp();
@@ -650,20 +661,30 @@ __global__ void __launch_bounds__(kNearThreads) k_near_place(const int32_t* __re
     __syncwarp();
     const int64_t o = rec.x;
     const int s0 = rec.y, s1 = rec.z;
-    for (int base = s0; base < s1; base += 32) {
-      const int s = base + lane;
-      const bool valid = s < s1;
-      const unsigned m = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        const int d = direction_of((int64_t)keys[s] - o, nk);  // >= 0: A found no far particle
-        const unsigned peers = __match_any_sync(m, d);
-        const int leader = __ffs(peers) - 1;
-        const int r0 = run[w][d];
-        perm[r0 + __popc(peers & lanemask_lt())] = (uint32_t)s;
-        __syncwarp(m);
-        if (lane == leader) run[w][d] = r0 + __popc(peers);
+    for (int base = s0; base < s1; base += 32 * kNearKeys) {
+      uint32_t kv[kNearKeys];  // the keys of up to 32 kNearKeys slots, all loads in flight
+#pragma unroll
+      for (int u = 0; u < kNearKeys; ++u) {
+        const int s = base + 32 * u + lane;
+        kv[u] = s < s1 ? keys[s] : 0u;
       }
-      __syncwarp();
+#pragma unroll
+      for (int u = 0; u < kNearKeys; ++u) {  // slot order: the ranks follow it
+        const int s = base + 32 * u + lane;
+        const bool valid = s < s1;
+        const unsigned m = __ballot_sync(0xffffffffu, valid);
+        if (m == 0) break;
+        if (valid) {
+          const int d = direction_of((int64_t)kv[u] - o, nk);  // >= 0: A found no far particle
+          const unsigned peers = __match_any_sync(m, d);
+          const int leader = __ffs(peers) - 1;
+          const int r0 = run[w][d];
+          perm[r0 + __popc(peers & lanemask_lt())] = (uint32_t)s;
+          __syncwarp(m);
+          if (lane == leader) run[w][d] = r0 + __popc(peers);
+        }
+        __syncwarp();
+      }
     }
     __syncwarp();
   }
