@@ -414,8 +414,8 @@ typedef struct vlb_tuning {
   int32_t chunk;              /* 128 */
   int32_t field_ctas_per_sm;  /* 3: the smoothed gather */
   int32_t cic_ctas_per_sm;    /* 4: the coarse deposit */
-  int32_t push_ctas_per_sm;   /* 8: the Verlet push */
-  int32_t move_ctas_per_sm;   /* 8: the record move of the sort */
+  int32_t push_ctas_per_sm;   /* 2: the Verlet push */
+  int32_t move_ctas_per_sm;   /* 4: the record move of the sort */
   int32_t field_tensor_cores; /* 1: the gather's sums over y as 3xTF32 MMAs
                                  (tcgen05, two CTAs per SM, field_ctas_per_sm
                                  unused; needs chunk <= 128); 0: FP32 FMAs */

@@ -16,7 +16,7 @@ AT = vb.autotune
 class FakeAccelerator:
     """Stage times as a function of the launch shapes: the forces stage is
     fastest with the tensor-core gather and chunk 128, the coarse deposit
-    with 4 CTAs per SM, the push with 16; the others do not matter."""
+    with 4 CTAs per SM, the push with 2; the others do not matter."""
 
     def __init__(self):
         self.shapes = {"field_tensor_cores": 0, "chunk": 64, "field_ctas_per_sm": 3, "cic_ctas_per_sm": 2,
@@ -43,7 +43,7 @@ class FakeAccelerator:
             "sort": 0.43 + (0.01 if s["chunk"] == 256 else 0.0) + 0.001 * abs(s["move_ctas_per_sm"] - 8),
             "deposit_coarse": 0.19 + 0.02 * abs(s["cic_ctas_per_sm"] - 4) + 0.01 * (s["chunk"] != 128),
             "forces": (0.95 if s["field_tensor_cores"] else 1.04) + 0.05 * (s["chunk"] != 128),
-            "push": 0.17 + 0.001 * (16 - s["push_ctas_per_sm"]),
+            "push": 0.17 + 0.001 * s["push_ctas_per_sm"],
         }
         if self.profiling:
             for k, v in t.items():
@@ -80,7 +80,7 @@ def test_autotune_descends_each_coordinate_and_restores_the_run():
     assert best["field_tensor_cores"] == 1
     assert best["chunk"] == 128
     assert best["cic_ctas_per_sm"] == 4
-    assert best["push_ctas_per_sm"] == 16
+    assert best["push_ctas_per_sm"] == 2
     assert sim.accelerator.tuning() == best       # left set on the run
     assert sim.state == 41 and sim.use_graph       # the run as it was
     assert not sim.accelerator.profiling

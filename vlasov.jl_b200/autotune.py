@@ -26,8 +26,8 @@ SEARCH = {
     "chunk": ((64, 128, 256), ("deposit_coarse", "forces", "sort")),
     "field_ctas_per_sm": ((2, 3, 4), ("forces",)),
     "cic_ctas_per_sm": ((2, 4, 8), ("deposit_coarse",)),
-    "push_ctas_per_sm": ((4, 8, 16), ("push",)),
-    "move_ctas_per_sm": ((4, 8, 16), ("sort",)),
+    "push_ctas_per_sm": ((2, 4, 8), ("push",)),
+    "move_ctas_per_sm": ((2, 4, 8), ("sort",)),
 }
 
 

@@ -196,7 +196,7 @@ struct Ctx {
   int mode_precision = 0;     // VLB_POISSON_FP32, VLB_POISSON_3XTF32 or VLB_POISSON_BF16X3
   // launch shapes (vlb_set_tuning): particles per work item, persistent-grid
   // CTAs per SM of the gather, the coarse deposit, the push and the record move
-  int chunk = kChunk, field_cps = 3, cic_cps = 4, push_cps = 8, move_cps = 8;
+  int chunk = kChunk, field_cps = 3, cic_cps = 4, push_cps = 2, move_cps = 4;
   // polls of a look-back wait before it gives up: 0 the default, -1 none
   // (every tile after the first takes the scan's fallback at once)
   int scan_wait_polls = 0;
