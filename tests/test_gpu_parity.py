@@ -28,10 +28,10 @@ class Case:
     """A packed cloud on the xenon geometry: Thomas-Fermi positions, a tenth
     moved outside the fine grid (and a few outside both grids)."""
 
-    def __init__(self, orc, nfine=28, npart=40_000, seed=-1):
+    def __init__(self, orc, nfine=28, npart=40_000, seed=-1, nbdt=1000):
         self.p = vb.SimulationParameters.for_grid(nfine, rcluster=78.0, rbox=235.0, nparticles=npart, dt=0.5)
         self.meshes = vb.build_meshes(nfine, self.p.ninner, self.p.nouter, 78.0, 235.0)
-        self.sm = vb.gaussian_smoothing(self.meshes.fine.axis)
+        self.sm = vb.gaussian_smoothing(self.meshes.fine.axis, nbdt=nbdt)
         self.w = 196.0 / npart
         pos, mom = vb.sample_thomas_fermi(vb.thomas_fermi_profile(), npart, self.w, seed=seed)
         rng = np.random.default_rng(7)
