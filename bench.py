@@ -33,10 +33,11 @@ import numpy as np  # noqa: E402
 MEASURED = ROOT / "MEASURED_PEAKS.json"
 GATHER_FLOP_PER_PARTICLE = 4600.0       # 2000 FMA + 300 mul/FMA per 10^3 contraction
 GATHER_TC_FLOP_PER_PARTICLE = 12000.0   # 3 split products x (oy, gy) x 100 columns x 10 y x 2
-GATHER_BYTES_PER_PARTICLE = 24.0        # delta in, force out
+# delta in, force out; the tensor-core form also reads the sort's packed table columns (4 B)
+GATHER_BYTES_PER_PARTICLE = {"tcgen05": 28.0, "fp32": 24.0}
 # DRAM bytes (read + write) of one gather launch per particle, from the ncu
 # captures of 4e6 particles (profiles/k_field_tc_4M.md, profiles/k_field_4M.md)
-GATHER_TRAFFIC_PER_PARTICLE = {"tcgen05": (49486336 + 6479616) / 4e6, "fp32": (49494784 + 7127296) / 4e6}
+GATHER_TRAFFIC_PER_PARTICLE = {"tcgen05": (65935872 + 13056512) / 4e6, "fp32": (49494784 + 7127296) / 4e6}
 # read (k, d) in slot order, (pk, pd) where the step's sort left them (through perm: 4 B), the force;
 # write the record and the next sort's cell key
 PUSH_BYTES_PER_PARTICLE = 24 + 24 + 4 + 12 + 48 + 4
@@ -408,11 +409,13 @@ def main():
                              "the gather kernel's own event time (events around its launch in profiled eager steps)",
                      "kernel_ms": t_forces, "forces_stage_ms": stages.get("forces"),
                      "peak_source": "measured FP32 FMA kernel (vlb_fp32_peak), this GPU, this run",
-                     "hbm_beside": {"achieved": GATHER_BYTES_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e9,
+                     "hbm_beside": {"achieved": GATHER_BYTES_PER_PARTICLE[args.gather] * args.npart
+                                    / (t_forces * 1e-3) / 1e9,
                                     "peak": pk_.get("hbm_gbs"), "unit": "GB/s",
-                                    "frac": GATHER_BYTES_PER_PARTICLE * args.npart / (t_forces * 1e-3) / 1e9
-                                    / pk_.get("hbm_gbs", 1),
-                                    "note": "12 B of delta read + 12 B of force written a particle"}},
+                                    "frac": GATHER_BYTES_PER_PARTICLE[args.gather] * args.npart
+                                    / (t_forces * 1e-3) / 1e9 / pk_.get("hbm_gbs", 1),
+                                    "note": "12 B of delta read + 12 B of force written a particle"
+                                    + (" + 4 B of packed table columns read" if args.gather == "tcgen05" else "")}},
         "roofline_hbm": {"kernel": "k_push (packed Verlet, previous positions read through the sort's permutation)",
                          "bound": "hbm", "achieved": push_gbs,
                          "peak": pk_.get("hbm_gbs"), "unit": "GB/s", "frac": push_gbs / pk_.get("hbm_gbs", 1),
